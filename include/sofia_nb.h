@@ -1,0 +1,161 @@
+/*
+ * sofia_nb.h -- C ABI of the B200 (sm_100a) nonbonded hot path of Sofia.
+ *
+ * The reference exposes this path as argument-less Fortran subroutines over
+ * module state (Source/mod_neighbor.f90:8 neighbor_wrapper,
+ * Source/mod_force_nonbond.f90:105 lj_cut_coul_dsf_nonewton_NOMIC,
+ * Source/mod_force_dihed.f90:816 dihedral_opls_DSF,
+ * Source/mod_force_correction.f90:6,95,187 correct_12/13/14_bonds,
+ * Source/mod_cluster.f90:15 get_greatestCluster).  Each entry point below takes
+ * exactly the module arrays those subroutines read and write, with the
+ * reference's layout and 1-based indices, so a Fortran shim can pass its
+ * module arrays through ISO_C_BINDING unchanged (the precedent is the
+ * bind(c) PME interface at Source/mod_force.f90:14-23).
+ *
+ * Pointers may be host memory (copied to and from the GPU inside the call, like
+ * the reference's LEO `in`/`inout` transfers, Source/mod_force.f90:446-462) or
+ * device memory (used in place).  Calls are ordered on the context's CUDA
+ * stream and return after their results are visible to the caller.
+ *
+ * Return codes: SOFIA_OK, or an error with a message in sofia_last_error().
+ * No call aborts or traps.
+ */
+#ifndef SOFIA_NB_H
+#define SOFIA_NB_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOFIA_OK 0
+#define SOFIA_ENEEDGROW 1 /* output capacity too small; *needed_* holds the size to grow to */
+#define SOFIA_EINVAL 2    /* invalid argument */
+#define SOFIA_ECUDA 3     /* CUDA runtime error */
+#define SOFIA_ETIMEOUT 4  /* a bounded device wait gave up */
+#define SOFIA_ESTATE 5    /* device state check failed (non-finite values, SHAKE failure, ...) */
+
+/* type(ainfo) of Source/global.f90:82-85: {real*4 x,y,z; integer type}, 16 bytes. */
+typedef struct {
+    float x, y, z;
+    int32_t type;
+} sofia_ainfo;
+
+typedef struct {
+    int device; /* CUDA device ordinal */
+    int flags;  /* reserved, 0 */
+} sofia_nb_params;
+
+typedef struct sofia_nb_ctx sofia_nb_ctx;
+
+/* Context: one per host thread / replica (Source/mod_memory.f90:236-286 device setup). */
+int sofia_nb_create(const sofia_nb_params *params, sofia_nb_ctx **out);
+int sofia_nb_destroy(sofia_nb_ctx *ctx);
+const char *sofia_last_error(const sofia_nb_ctx *ctx);
+/* Blocks until all work of the context is done (offload_wait, Source/mod_force.f90:496). */
+int sofia_wait(sofia_nb_ctx *ctx);
+/* The context's cudaStream_t, for callers that order their own work with it. */
+void *sofia_stream(sofia_nb_ctx *ctx);
+
+/* DSF shift constants of init (Source/get_started.f90:112-116). */
+int sofia_dsf_constants(double alpha, float cut_coul, double *e_shift, double *f_shift);
+
+/* Cell grid of check_allocation (Source/mod_neighbor.f90:1446-1452). */
+int sofia_cell_grid(float box, float cut_coul, float rcut, float *rn, int32_t *ncellT,
+                    int32_t *ncellD);
+
+/*
+ * new_nlist + sort_posit_charge (Source/mod_neighbor.f90:923-1005): bins atoms
+ * (xyz2bin, :1381-1424) and returns the cell-sorted order.  Outputs (any may be
+ * NULL): tt[np] old->new 1-based, ttb[np] new->old 1-based, start/endposit[ncellT]
+ * 1-based per cell, atombin[np] cell of each sorted atom, position_sorted[np].
+ * Within a cell atoms follow the reference's linked-list order (descending
+ * input index).
+ */
+int sofia_cell_sort(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position, float box,
+                    float cut_coul, float rcut, int32_t *tt, int32_t *ttb, int32_t *start,
+                    int32_t *endposit, int32_t *atombin, sofia_ainfo *position_sorted);
+
+/*
+ * build_neighbor_nonewton_nomic (Source/mod_neighbor.f90:622-809), with the
+ * cell grid, stencil and binning of :1309-1526: full (non-Newton) list of every
+ * z /= i in the 27 cells around atom i with real*4 minimum-image dr2 < rv2 and
+ * z not in specbond(1:num3bond(i), i).
+ *   specbond[i*12 + l] : 1-based partners (Fortran specbond(12,np) column-major)
+ *   nlist[i*neigh_alloc + j] : 1-based neighbours in INPUT index order; may be
+ *       NULL, in which case the list stays resident in the context for
+ *       sofia_force_nonbond_dsf (the reference's `nocopy(nlist)`).
+ * Rows are ordered by stencil cell, then by ascending input index inside a cell;
+ * for input that is already cell sorted (sofia_cell_sort) this is exactly the
+ * reference's row order.  If a row exceeds neigh_alloc the call returns
+ * SOFIA_ENEEDGROW with *needed_alloc = roundup16(1.2*max) like the redo loop
+ * (:767-802); the caller grows and calls again.
+ */
+int sofia_neighbor_build(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
+                         const int32_t *specbond, const int32_t *num3bond, float box, double rv2,
+                         float cut_coul, float rcut, int32_t *nlist, int32_t *numneigh,
+                         int32_t neigh_alloc, int32_t *needed_alloc);
+
+/*
+ * lj_cut_coul_dsf_nonewton_NOMIC (Source/mod_force_nonbond.f90:105-196): LJ
+ * 12-6 + damped-shifted-force Coulomb over the full list, FP64 pair arithmetic
+ * on the real*4 arrays.  lj1..lj4 are [ntypes*ntypes] real*4 tables indexed
+ * (itype-1)*ntypes + jtype.  ff[i*3+c] receives the per-atom force (real*4),
+ * potential/e_coul the halved pair sums (:193-194), virial_diag3 (may be NULL)
+ * the halved sum of dx*dx*force per axis.  nlist == NULL uses the list left
+ * resident by the last sofia_neighbor_build.
+ */
+int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
+                            const float *q, const float *lj1, const float *lj2,
+                            const float *lj3, const float *lj4, int ntypes,
+                            const int32_t *nlist, const int32_t *numneigh, int32_t neigh_alloc,
+                            float box, float ibox, double rcut2, double cut_coulsq, double alpha,
+                            double e_shift, double f_shift, float coulpre, float *ff,
+                            double *potential, double *e_coul, double *virial_diag3);
+
+/*
+ * dihedral_opls_DSF (Source/mod_force_dihed.f90:816-1092): OPLS torsion with
+ * dihedcoeff[type][4] plus the 0.5-scaled DSF Coulomb and lj14 LJ of each
+ * dihedral's 1-4 pair (:1003-1048).  dihedlist[n*5 + k] = i1,i2,i3,i4,type
+ * (1-based); lj14 = [4][ntypes][ntypes] real*8.  Forces are ADDED to ffh;
+ * energies are ADDED to *e_dihedral, *e_coul_14, *pot_14.
+ */
+int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position, const float *q,
+                     int ntypes, const double *lj14, int ndihed, const int32_t *dihedlist,
+                     const double *dihedcoeff, float box, float ibox, double rcut2,
+                     double cut_coulsq, double alpha, double e_shift, double f_shift,
+                     float coulpre, float *ffh, double *e_dihedral, double *e_coul_14,
+                     double *pot_14);
+
+/*
+ * correct_12_bonds / correct_13_bonds / correct_14_bonds
+ * (Source/mod_force_correction.f90:6-93, 95-184, 187-278): for each row m of
+ * `list` (row stride `stride` ints, 1-based atom ids in columns col_a, col_b)
+ * add the Ewald real-space erfc term minus (1-fudge) of the bare Coulomb to ffc
+ * and the energy to *e_corr, the diagonal virial to virial3 (may be NULL).
+ */
+int sofia_correct_1x(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position, const float *q,
+                     int npairs, const int32_t *list, int stride, int col_a, int col_b,
+                     float box, float ibox, double cut_coulsq, double gewald, double fudge,
+                     float coulpre, float *ffc, double *e_corr, double *virial3);
+
+/*
+ * get_greatestCluster (Source/mod_cluster.f90:15-83) with
+ * build_ptta_wrap_cluster2 (Source/mod_build_ptta.f90:116-164), the molecule
+ * centre/cell list (Source/mod_neighbor_cluster.f90:15-709) and the flood fill
+ * and surface append (Source/mod_cluster.f90:163-247).  Returns the integer
+ * size in *size_out.  ptta_full[n_gly*atoms_per_gly*3] (real*8) and
+ * *greatest_belongsto are in/out exactly like the module variable and the
+ * caller's `greatest` argument.  mrcut/denscut in Angstrom, densmin integer.
+ * denstrack/belongsto (may be NULL) receive the per-molecule arrays.
+ */
+int sofia_greatest_cluster(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
+                           const int32_t *global_id, int n_gly, int atoms_per_gly, float box,
+                           double mrcut, double denscut, int densmin, double *ptta_full,
+                           int32_t *greatest_belongsto, int32_t *size_out, int32_t *denstrack,
+                           int32_t *belongsto);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

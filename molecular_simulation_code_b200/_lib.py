@@ -1,0 +1,81 @@
+"""Loads ``libsofia_nb.so`` and declares its C ABI (``include/sofia_nb.h``).
+
+There is no CPU fallback: if the shared library is missing or cannot be
+loaded, ``lib()`` raises, and every entry point of this package fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libsofia_nb.so")
+
+SOFIA_OK = 0
+SOFIA_ENEEDGROW = 1
+SOFIA_EINVAL = 2
+SOFIA_ECUDA = 3
+SOFIA_ETIMEOUT = 4
+SOFIA_ESTATE = 5
+
+
+class SofiaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"sofia error {code}: {msg}")
+        self.code = code
+
+
+class SofiaNbParams(C.Structure):
+    _fields_ = [("device", C.c_int), ("flags", C.c_int)]
+
+
+_P = C.c_void_p
+_I = C.c_int
+_F = C.c_float
+_D = C.c_double
+
+# name -> (restype, argtypes)
+SIGNATURES: dict[str, tuple] = {
+    "sofia_nb_create": (_I, [C.POINTER(SofiaNbParams), C.POINTER(_P)]),
+    "sofia_nb_destroy": (_I, [_P]),
+    "sofia_last_error": (C.c_char_p, [_P]),
+    "sofia_wait": (_I, [_P]),
+    "sofia_stream": (_P, [_P]),
+    "sofia_dsf_constants": (_I, [_D, _F, C.POINTER(_D), C.POINTER(_D)]),
+    "sofia_cell_grid": (_I, [_F, _F, _F, C.POINTER(_F), C.POINTER(C.c_int32),
+                             C.POINTER(C.c_int32)]),
+    "sofia_cell_sort": (_I, [_P, _I, _P, _F, _F, _F, _P, _P, _P, _P, _P, _P]),
+    "sofia_neighbor_build": (_I, [_P, _I, _P, _P, _P, _F, _D, _F, _F, _P, _P, C.c_int32,
+                                  C.POINTER(C.c_int32)]),
+    "sofia_force_nonbond_dsf": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, C.c_int32, _F,
+                                     _F, _D, _D, _D, _D, _D, _F, _P, C.POINTER(_D),
+                                     C.POINTER(_D), _P]),
+    "sofia_pair14_dsf": (_I, [_P, _I, _P, _P, _I, _P, _I, _P, _P, _F, _F, _D, _D, _D, _D, _D, _F,
+                              _P, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
+    "sofia_correct_1x": (_I, [_P, _I, _P, _P, _I, _P, _I, _I, _I, _F, _F, _D, _D, _D, _F, _P,
+                              C.POINTER(_D), _P]),
+    "sofia_greatest_cluster": (_I, [_P, _I, _P, _P, _I, _I, _F, _D, _D, _I, _P,
+                                    C.POINTER(C.c_int32), C.POINTER(C.c_int32), _P, _P]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded library; raises if it is missing (no silent fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise SofiaError(SOFIA_EINVAL, f"{LIB_PATH} is missing; run __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def declared_symbols() -> list[str]:
+    return list(SIGNATURES)
