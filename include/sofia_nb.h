@@ -117,12 +117,13 @@ int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *positi
  * dihedral_opls_DSF (Source/mod_force_dihed.f90:816-1092): OPLS torsion with
  * dihedcoeff[type][4] plus the 0.5-scaled DSF Coulomb and lj14 LJ of each
  * dihedral's 1-4 pair (:1003-1048).  dihedlist[n*5 + k] = i1,i2,i3,i4,type
- * (1-based); lj14 = [4][ntypes][ntypes] real*8.  Forces are ADDED to ffh;
- * energies are ADDED to *e_dihedral, *e_coul_14, *pot_14.
+ * (1-based, type <= ndihedtypes); dihedcoeff = [ndihedtypes][4] real*8;
+ * lj14 = [4][ntypes][ntypes] real*8.  Forces are ADDED to ffh; energies are
+ * ADDED to *e_dihedral, *e_coul_14, *pot_14.
  */
 int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position, const float *q,
                      int ntypes, const double *lj14, int ndihed, const int32_t *dihedlist,
-                     const double *dihedcoeff, float box, float ibox, double rcut2,
+                     const double *dihedcoeff, int ndihedtypes, float box, float ibox, double rcut2,
                      double cut_coulsq, double alpha, double e_shift, double f_shift,
                      float coulpre, float *ffh, double *e_dihedral, double *e_coul_14,
                      double *pot_14);

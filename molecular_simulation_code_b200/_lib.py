@@ -50,7 +50,7 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_force_nonbond_dsf": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, C.c_int32, _F,
                                      _F, _D, _D, _D, _D, _D, _F, _P, C.POINTER(_D),
                                      C.POINTER(_D), _P]),
-    "sofia_pair14_dsf": (_I, [_P, _I, _P, _P, _I, _P, _I, _P, _P, _F, _F, _D, _D, _D, _D, _D, _F,
+    "sofia_pair14_dsf": (_I, [_P, _I, _P, _P, _I, _P, _I, _P, _P, _I, _F, _F, _D, _D, _D, _D, _D, _F,
                               _P, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
     "sofia_correct_1x": (_I, [_P, _I, _P, _P, _I, _P, _I, _I, _I, _F, _F, _D, _D, _D, _F, _P,
                               C.POINTER(_D), _P]),

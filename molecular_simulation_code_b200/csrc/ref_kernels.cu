@@ -264,17 +264,20 @@ __global__ void __launch_bounds__(256) k_force_ref(
     const int itype = __float_as_int(pi.w);
     const double qtmp = (double)q[i];
     const int ioffset = (itype - 1) * ntypes;
-    const int num = numneigh[i];
+    const int num = min(numneigh[i], neigh_alloc);
     const int *row = nlist + (size_t)i * (size_t)neigh_alloc;
+    const bool itype_ok = (unsigned)(itype - 1) < (unsigned)ntypes;
     const double TWO_ALPHA_PI = (2.0 * k.alpha) * k.MY_PIS_INV;
     const double EPA = k.EWALD_P * k.alpha;
     const double AA = k.alpha * k.alpha;
     double ffx = 0.0, ffy = 0.0, ffz = 0.0, pot = 0.0, ec = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
     for (int j = lane; j < num; j += 32) {
         const int neigh = row[j] - 1;
+        if ((unsigned)neigh >= (unsigned)np) continue;
         const float4 pj = pos[neigh];
         double dx = x1 - (double)pj.x, dy = y1 - (double)pj.y, dz = z1 - (double)pj.z;
         const int jtype = __float_as_int(pj.w);
+        if (!itype_ok || (unsigned)(jtype - 1) >= (unsigned)ntypes) continue;
         // (b + sign(2^52,b)) - sign(2^52,dx) of :144-147 is rint(b) for |b| < 2^51
         const double bx = rint(dx * k.ibox), by = rint(dy * k.ibox), bz = rint(dz * k.ibox);
         dx = dx - k.box * bx;
@@ -357,15 +360,25 @@ __device__ __forceinline__ double minimg1(double d, float box, float ibox) {
 }
 
 // dihedral_opls_DSF, mod_force_dihed.f90:849-1068: torsion + 1-4 pair per dihedral.
-__global__ void k_dihedral_dsf(int ndihed, const float4 *__restrict__ pos,
+__global__ void k_dihedral_dsf(int ndihed, int np, const float4 *__restrict__ pos,
                                const float *__restrict__ q, int ntypes,
                                const double *__restrict__ lj14, const int *__restrict__ dl,
-                               const double *__restrict__ dc, DsfConst k, float box, float ibox,
-                               double *__restrict__ acc, double *__restrict__ pe) {
+                               const double *__restrict__ dc, int ndtypes, DsfConst k, float box,
+                               float ibox, double *__restrict__ acc, double *__restrict__ pe,
+                               int *__restrict__ status) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= ndihed) return;
     const int i1 = dl[n * 5] - 1, i2 = dl[n * 5 + 1] - 1, i3 = dl[n * 5 + 2] - 1,
               i4 = dl[n * 5 + 3] - 1, type = dl[n * 5 + 4];
+    pe[(size_t)n * 3 + 0] = 0.0;
+    pe[(size_t)n * 3 + 1] = 0.0;
+    pe[(size_t)n * 3 + 2] = 0.0;
+    if ((unsigned)i1 >= (unsigned)np || (unsigned)i2 >= (unsigned)np ||
+        (unsigned)i3 >= (unsigned)np || (unsigned)i4 >= (unsigned)np ||
+        (unsigned)(type - 1) >= (unsigned)ndtypes) {
+        atomicAdd(&status[sofia::ST_BADBIN], 1);
+        return;
+    }
     const float4 p1 = pos[i1], p2 = pos[i2], p3 = pos[i3], p4 = pos[i4];
     const double vb1x = minimg1((double)(p1.x - p2.x), box, ibox);
     const double vb1y = minimg1((double)(p1.y - p2.y), box, ibox);
@@ -451,7 +464,8 @@ __global__ void k_dihedral_dsf(int ndihed, const float4 *__restrict__ pos,
             (0.50 * prefactor) * ((erfcc / r + ((2.0 * k.alpha) / k.MY_PIS) * erfcd) + r * k.f_shift) * r;
         ec14 = (0.50 * prefactor) * ((erfcc - r * k.e_shift) - dr2 * k.f_shift);
         double forcelj = 0.0;
-        if (dr2 < k.rcut2) {
+        if (dr2 < k.rcut2 && (unsigned)(itype - 1) < (unsigned)ntypes &&
+            (unsigned)(jtype - 1) < (unsigned)ntypes) {
             const double dr6i = dr2i * dr2i * dr2i;
             const size_t o = (size_t)(itype - 1) * ntypes + (size_t)(jtype - 1);
             const size_t tn = (size_t)ntypes * ntypes;
@@ -484,14 +498,20 @@ __global__ void k_dihedral_dsf(int ndihed, const float4 *__restrict__ pos,
 }
 
 // correct_1x_bonds, mod_force_correction.f90:23-86 (and :111-178, :204-270).
-__global__ void k_correct_pairs(int npairs, const float4 *__restrict__ pos,
+__global__ void k_correct_pairs(int npairs, int np, const float4 *__restrict__ pos,
                                 const float *__restrict__ q, const int *__restrict__ list,
                                 int stride, int ca, int cb, DsfConst k, double gewald,
                                 double fudge, float coulpre, double *__restrict__ acc,
-                                double *__restrict__ pe) {
+                                double *__restrict__ pe, int *__restrict__ status) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= npairs) return;
     const int i1 = list[(size_t)m * stride + ca] - 1, i2 = list[(size_t)m * stride + cb] - 1;
+    double *o = pe + (size_t)m * 4;
+    if ((unsigned)i1 >= (unsigned)np || (unsigned)i2 >= (unsigned)np) {
+        o[0] = o[1] = o[2] = o[3] = 0.0;
+        atomicAdd(&status[sofia::ST_BADBIN], 1);
+        return;
+    }
     const float4 a = pos[i1], b = pos[i2];
     double dx = (double)(a.x - b.x), dy = (double)(a.y - b.y), dz = (double)(a.z - b.z);
     const double bx = rint(dx * k.ibox), by = rint(dy * k.ibox), bz = rint(dz * k.ibox);
@@ -518,7 +538,6 @@ __global__ void k_correct_pairs(int npairs, const float4 *__restrict__ pos,
     atomicAdd(&acc[i2 * 3 + 0], -dx * force);
     atomicAdd(&acc[i2 * 3 + 1], -dy * force);
     atomicAdd(&acc[i2 * 3 + 2], -dz * force);
-    double *o = pe + (size_t)m * 4;
     o[0] = e;
     o[1] = dx * dx * force;
     o[2] = dy * dy * force;
@@ -660,7 +679,6 @@ extern "C" int sofia_neighbor_build(sofia_nb_ctx *ctx, int np, const sofia_ainfo
     // the list lands in the caller's device buffer, or in the resident buffer
     int32_t *dlist;
     int32_t *dnum;
-    sofia::OutArg o_list, o_num;
     const size_t list_bytes = sizeof(int) * (size_t)np * (size_t)neigh_alloc;
     if (nlist && sofia::is_device_ptr(nlist)) {
         dlist = nlist;
@@ -702,8 +720,6 @@ extern "C" int sofia_neighbor_build(sofia_nb_ctx *ctx, int np, const sofia_ainfo
     if (numneigh && dnum != numneigh)
         SOFIA_CUDA(ctx, cudaMemcpyAsync(numneigh, dnum, sizeof(int) * (size_t)np,
                                         cudaMemcpyDeviceToHost, st));
-    (void)o_list;
-    (void)o_num;
     // keep the resident copy coherent when the caller's buffers were device memory
     if (dlist == nlist) {
         SOFIA_CUDA(ctx, ctx->res_nlist.ensure(list_bytes));
@@ -784,38 +800,26 @@ extern "C" int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ai
 
 extern "C" int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
                                 const float *q, int ntypes, const double *lj14, int ndihed,
-                                const int32_t *dihedlist, const double *dihedcoeff, float box,
-                                float ibox, double rcut2, double cut_coulsq, double alpha,
-                                double e_shift, double f_shift, float coulpre, float *ffh,
-                                double *e_dihedral, double *e_coul_14, double *pot_14) {
+                                const int32_t *dihedlist, const double *dihedcoeff,
+                                int ndihedtypes, float box, float ibox, double rcut2,
+                                double cut_coulsq, double alpha, double e_shift, double f_shift,
+                                float coulpre, float *ffh, double *e_dihedral, double *e_coul_14,
+                                double *pot_14) {
     if (!ctx) return SOFIA_EINVAL;
-    if (np <= 0 || !position || !q || !lj14 || ndihed < 0 || (ndihed > 0 && !dihedlist) ||
-        !dihedcoeff || !ffh)
+    if (np <= 0 || !position || !q || !lj14 || ntypes <= 0 || ndihed < 0 ||
+        (ndihed > 0 && !dihedlist) || !dihedcoeff || ndihedtypes <= 0 || !ffh)
         return sofia::fail(ctx, SOFIA_EINVAL, "bad args%s");
     if (ndihed == 0) return SOFIA_OK;
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     int rc;
     const void *dpos, *dq, *dlj, *ddl, *ddc;
-    int maxtype = 0;
-    (void)maxtype;
     if ((rc = sofia::stage_in(ctx, position, sizeof(float4) * (size_t)np, 0, &dpos))) return rc;
     if ((rc = sofia::stage_in(ctx, q, sizeof(float) * (size_t)np, 1, &dq))) return rc;
     if ((rc = sofia::stage_in(ctx, lj14, sizeof(double) * 4 * (size_t)ntypes * ntypes, 2, &dlj)))
         return rc;
     if ((rc = sofia::stage_in(ctx, dihedlist, sizeof(int) * 5 * (size_t)ndihed, 3, &ddl))) return rc;
-    // dihedral types are 1-based indices into dihedcoeff; the host side cannot
-    // know the table length, so the caller sizes it for every type used.
-    int ntd = 0;
-    {
-        // count types from a host copy of the list when it is host memory
-        if (!sofia::is_device_ptr(dihedlist))
-            for (int n = 0; n < ndihed; ++n) ntd = dihedlist[n * 5 + 4] > ntd ? dihedlist[n * 5 + 4] : ntd;
-        else
-            ntd = 64;
-    }
-    if ((rc = sofia::stage_in(ctx, dihedcoeff, sizeof(double) * 4 * (size_t)(ntd > 0 ? ntd : 1), 4,
-                              &ddc)))
+    if ((rc = sofia::stage_in(ctx, dihedcoeff, sizeof(double) * 4 * (size_t)ndihedtypes, 4, &ddc)))
         return rc;
     sofia::OutArg o_ff;
     if ((rc = sofia::stage_out(ctx, ffh, sizeof(float) * 3 * (size_t)np, 5, &o_ff, true))) return rc;
@@ -823,11 +827,12 @@ extern "C" int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
     SOFIA_CUDA(ctx, ctx->pe_atom.ensure(sizeof(double) * 3 * (size_t)ndihed));
     SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * 16));
     SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->acc64.p, 0, sizeof(double) * 3 * (size_t)np, st));
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
     DsfConst k = make_const(box, ibox, rcut2, cut_coulsq, alpha, e_shift, f_shift, coulpre);
     k_dihedral_dsf<<<sofia::grid_for(ndihed, 128), 128, 0, st>>>(
-        ndihed, (const float4 *)dpos, (const float *)dq, ntypes, (const double *)dlj,
-        (const int *)ddl, (const double *)ddc, k, box, ibox, ctx->acc64.as<double>(),
-        ctx->pe_atom.as<double>());
+        ndihed, np, (const float4 *)dpos, (const float *)dq, ntypes, (const double *)dlj,
+        (const int *)ddl, (const double *)ddc, ndihedtypes, k, box, ibox,
+        ctx->acc64.as<double>(), ctx->pe_atom.as<double>(), ctx->d_status);
     k_reduce_cols<<<1, 256, 0, st>>>(ndihed, 3, ctx->pe_atom.as<double>(),
                                      ctx->red_out.as<double>(), 1.0);
     k_add_to_float<<<sofia::grid_for(3L * np, 256), 256, 0, st>>>(3L * np, ctx->acc64.as<double>(),
@@ -836,7 +841,9 @@ extern "C" int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
     if ((rc = sofia::finish_out(ctx, o_ff))) return rc;
     SOFIA_CUDA(ctx, cudaMemcpyAsync(ctx->h_red, ctx->red_out.p, sizeof(double) * 3,
                                     cudaMemcpyDeviceToHost, st));
-    SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    if ((rc = check_status(ctx))) return rc;
+    if (ctx->h_status[sofia::ST_BADBIN])
+        return sofia::fail(ctx, SOFIA_EINVAL, "dihedral atom index or type out of range%s");
     if (e_dihedral) *e_dihedral += ctx->h_red[0];
     if (e_coul_14) *e_coul_14 += ctx->h_red[1];
     if (pot_14) *pot_14 += ctx->h_red[2];
@@ -868,9 +875,11 @@ extern "C" int sofia_correct_1x(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
     SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * 16));
     SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->acc64.p, 0, sizeof(double) * 3 * (size_t)np, st));
     DsfConst k = make_const(box, ibox, 0.0, cut_coulsq, 0.0, 0.0, 0.0, coulpre);
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
     k_correct_pairs<<<sofia::grid_for(npairs, 128), 128, 0, st>>>(
-        npairs, (const float4 *)dpos, (const float *)dq, (const int *)dlist, stride, col_a, col_b,
-        k, gewald, fudge, coulpre, ctx->acc64.as<double>(), ctx->pe_atom.as<double>());
+        npairs, np, (const float4 *)dpos, (const float *)dq, (const int *)dlist, stride, col_a,
+        col_b, k, gewald, fudge, coulpre, ctx->acc64.as<double>(), ctx->pe_atom.as<double>(),
+        ctx->d_status);
     k_reduce_cols<<<1, 256, 0, st>>>(npairs, 4, ctx->pe_atom.as<double>(),
                                      ctx->red_out.as<double>(), 1.0);
     k_add_to_float<<<sofia::grid_for(3L * np, 256), 256, 0, st>>>(3L * np, ctx->acc64.as<double>(),
@@ -879,7 +888,9 @@ extern "C" int sofia_correct_1x(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
     if ((rc = sofia::finish_out(ctx, o_ff))) return rc;
     SOFIA_CUDA(ctx, cudaMemcpyAsync(ctx->h_red, ctx->red_out.p, sizeof(double) * 4,
                                     cudaMemcpyDeviceToHost, st));
-    SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    if ((rc = check_status(ctx))) return rc;
+    if (ctx->h_status[sofia::ST_BADBIN])
+        return sofia::fail(ctx, SOFIA_EINVAL, "pair atom index out of range%s");
     if (e_corr) *e_corr += ctx->h_red[0];
     if (virial3) {
         virial3[0] += ctx->h_red[1];

@@ -197,7 +197,8 @@ def dihedral_opls_dsf(ctx: Context, position, q, ntypes: int, lj14, dihedlist, d
     dc = np.ascontiguousarray(dihedcoeff, np.float64)
     l14 = np.ascontiguousarray(lj14, np.float64)
     ctx.check(ctx._lib.sofia_pair14_dsf(ctx.handle, n, ptr(position), ptr(q), ntypes, ptr(l14),
-                                        int(dl.shape[0]), ptr(dl), ptr(dc), p.box, p.ibox,
+                                        int(dl.shape[0]), ptr(dl), ptr(dc), int(dc.shape[0]),
+                                        p.box, p.ibox,
                                         p.rcut2, p.cut_coulsq, float(p.alpha), p.e_shift,
                                         p.f_shift, p.coulpre, ptr(ffh), C.byref(ed),
                                         C.byref(ec), C.byref(p14)))
