@@ -156,6 +156,60 @@ int sofia_greatest_cluster(sofia_nb_ctx *ctx, int np, const sofia_ainfo *positio
                            int32_t *greatest_belongsto, int32_t *size_out, int32_t *denstrack,
                            int32_t *belongsto);
 
+/* ------------------------------------------------------------------------ */
+/*
+ * Production path (device-resident system).  Replaces the same call,
+ * lj_cut_coul_dsf_nonewton (Source/mod_force_nonbond.f90:105-196) with the list
+ * kept by neighbor_wrapper (Source/mod_neighbor.f90:8-86), but keeps the list,
+ * the static per-atom data and the positions resident on the GPU, the way the
+ * reference's MIC path keeps `nlist` resident (`nocopy`, Source/mod_force.f90:446-461).
+ * The list is a cluster-pair list over rlist = cut_coul + neighbor_pad and is
+ * rebuilt on the device whenever an atom has moved more than neighbor_pad/2.
+ *   precision SOFIA_PREC_MIXED: FP64 positions, FP64 displacement rounded to
+ *       FP32, FP32 pair arithmetic, 64-bit fixed-point force sums (2^-32 units).
+ *   precision SOFIA_PREC_FP64: the same kernel with FP64 pair arithmetic.
+ * Pair terms, cutoffs and energies are those of lj_cut_coul_dsf_nonewton
+ * (potential and e_coul are halved sums over the full list).
+ */
+#define SOFIA_PREC_MIXED 0
+#define SOFIA_PREC_FP64 1
+
+typedef struct {
+    int np;              /* atoms */
+    int ntypes;          /* atom types (<= 48) */
+    float box;           /* cubic box edge, Angstrom (real*4 box) */
+    double alpha;        /* DSF damping, 1/Angstrom */
+    float cut_coul;      /* Coulomb cutoff (== rcut) */
+    float rcut;          /* LJ cutoff */
+    float neighbor_pad;  /* list skin */
+    int precision;       /* SOFIA_PREC_MIXED or SOFIA_PREC_FP64 */
+    const int32_t *type; /* [np] 1-based */
+    const float *q;      /* [np] */
+    const float *lj1, *lj2, *lj3, *lj4; /* [ntypes*ntypes] real*4 */
+    const int32_t *specbond; /* [np*12] 1-based 1-2/1-3/1-4 partners */
+    const int32_t *num3bond; /* [np] */
+    const double *mass;      /* [ntypes] amu; may be NULL for force-only use */
+} sofia_system_desc;
+
+typedef struct sofia_system sofia_system;
+
+int sofia_system_create(sofia_nb_ctx *ctx, const sofia_system_desc *desc, sofia_system **out);
+int sofia_system_destroy(sofia_system *sys);
+/* Drop-in for lj_cut_coul_dsf_nonewton: reference AoS positions in (host or
+ * device), real*4 forces ff[np*3] out, energies (each may be NULL). */
+int sofia_force_nonbond_mixed(sofia_system *sys, const sofia_ainfo *position, float *ff,
+                              double *potential, double *e_coul, double *virial_diag3);
+/* Resident state: x, v as [np*3] doubles (host or device). */
+int sofia_system_set_state(sofia_system *sys, const double *x, const double *v);
+int sofia_system_get_state(sofia_system *sys, double *x, double *v, double *f);
+/* Forces on the resident positions with the given precision; rebuild != 0
+ * forces a list rebuild; energies[5] (may be NULL) = potential, e_coul, virial. */
+int sofia_system_compute_forces(sofia_system *sys, int precision, int rebuild,
+                                double *energies);
+/* stats[0..7]: list builds, clusters, list entries, row capacity, columns per
+ * side, cluster capacity, column reach, 0. */
+int sofia_system_stats(sofia_system *sys, int64_t *stats, int nstats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,6 +29,19 @@ class SofiaNbParams(C.Structure):
     _fields_ = [("device", C.c_int), ("flags", C.c_int)]
 
 
+SOFIA_PREC_MIXED = 0
+SOFIA_PREC_FP64 = 1
+
+
+class SofiaSystemDesc(C.Structure):
+    _fields_ = [("np", C.c_int), ("ntypes", C.c_int), ("box", C.c_float), ("alpha", C.c_double),
+                ("cut_coul", C.c_float), ("rcut", C.c_float), ("neighbor_pad", C.c_float),
+                ("precision", C.c_int), ("type", C.c_void_p), ("q", C.c_void_p),
+                ("lj1", C.c_void_p), ("lj2", C.c_void_p), ("lj3", C.c_void_p),
+                ("lj4", C.c_void_p), ("specbond", C.c_void_p), ("num3bond", C.c_void_p),
+                ("mass", C.c_void_p)]
+
+
 _P = C.c_void_p
 _I = C.c_int
 _F = C.c_float
@@ -56,6 +69,13 @@ SIGNATURES: dict[str, tuple] = {
                               C.POINTER(_D), _P]),
     "sofia_greatest_cluster": (_I, [_P, _I, _P, _P, _I, _I, _F, _D, _D, _I, _P,
                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32), _P, _P]),
+    "sofia_system_create": (_I, [_P, C.POINTER(SofiaSystemDesc), C.POINTER(_P)]),
+    "sofia_system_destroy": (_I, [_P]),
+    "sofia_force_nonbond_mixed": (_I, [_P, _P, _P, C.POINTER(_D), C.POINTER(_D), _P]),
+    "sofia_system_set_state": (_I, [_P, _P, _P]),
+    "sofia_system_get_state": (_I, [_P, _P, _P, _P]),
+    "sofia_system_compute_forces": (_I, [_P, _I, _I, _P]),
+    "sofia_system_stats": (_I, [_P, _P, _I]),
 }
 
 _lib = None

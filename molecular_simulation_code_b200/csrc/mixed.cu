@@ -1,0 +1,1068 @@
+// mixed.cu -- production nonbonded path: cluster-pair list + LJ/DSF kernel.
+//
+// The reference evaluates LJ + damped-shifted-force Coulomb over a full
+// per-atom Verlet list in FP64 (Source/mod_force_nonbond.f90:105-196).  Here
+// atoms are grouped into clusters of 8 (xy columns, sorted by z) and the list
+// holds, for every i-cluster, the j-clusters whose bounding boxes come within
+// rlist = rc + skin, each with a 64-bit mask of the interacting atom pairs
+// (padding, self pairs and 1-2/1-3/1-4 exclusions removed).  One warp works on
+// one i-cluster: lane = (i atom, j half) covers the 8x8 pair tile in two passes,
+// the i force stays in registers and no j force is ever written, so the kernel
+// needs no atomics.  Positions are FP64 in HBM; each pair displacement is
+// formed in FP64 and rounded to FP32 (mixed) or kept in FP64 (plain FP64
+// twin); per-lane sums are flushed to 64-bit fixed point (2^-32 kcal/mol/A)
+// and combined across lanes in integers, so forces are bit-reproducible and
+// independent of summation order across lanes.
+//
+// The list stays valid while no atom has moved more than skin/2 since the
+// build (checked every evaluation on the device; the reference triggers at the
+// full skin, Source/mod_neighbor.f90:895-913).
+#include <cmath>
+
+#include "system.cuh"
+
+namespace sofia {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int MAX_COL = 2048;  // atoms per xy column handled by the in-column sort
+constexpr int FLUSH = 4;       // j-clusters between FP32 -> fixed-point flushes
+
+__device__ __forceinline__ double wrap_shift(double x, double L) {
+    // shift s with x + s in [0, L)
+    return -L * floor(x / L);
+}
+
+__global__ void k_wrap_bin(int n, const double *__restrict__ x, const double *__restrict__ y,
+                           const double *__restrict__ z, double L, double s_col, int ncx,
+                           double *__restrict__ ix, double *__restrict__ iy,
+                           double *__restrict__ iz, double *__restrict__ rx,
+                           double *__restrict__ ry, double *__restrict__ rz,
+                           int *__restrict__ col_of, int *__restrict__ col_count,
+                           float *__restrict__ zkey) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double px = x[i], py = y[i], pz = z[i];
+    double sx = wrap_shift(px, L), sy = wrap_shift(py, L), sz = wrap_shift(pz, L);
+    double wx = px + sx, wy = py + sy, wz = pz + sz;
+    // guard the upper edge after rounding
+    if (wx >= L) { wx -= L; sx -= L; }
+    if (wy >= L) { wy -= L; sy -= L; }
+    if (wz >= L) { wz -= L; sz -= L; }
+    ix[i] = sx;
+    iy[i] = sy;
+    iz[i] = sz;
+    rx[i] = px;
+    ry[i] = py;
+    rz[i] = pz;
+    int cx = min((int)(wx / s_col), ncx - 1);
+    int cy = min((int)(wy / s_col), ncx - 1);
+    cx = max(cx, 0);
+    cy = max(cy, 0);
+    const int c = cx + cy * ncx;
+    col_of[i] = c;
+    zkey[i] = (float)wz;
+    atomicAdd(&col_count[c], 1);
+}
+
+__global__ void k_scan1(int n, const int *__restrict__ in, int *__restrict__ out, int round8) {
+    __shared__ int s[1024];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 1024) {
+        const int t = threadIdx.x;
+        int v = (base + t < n) ? in[base + t] : 0;
+        if (round8) v = (v + CL - 1) / CL;
+        s[t] = v;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            const int a = (t >= off) ? s[t - off] : 0;
+            __syncthreads();
+            s[t] += a;
+            __syncthreads();
+        }
+        if (base + t < n) out[base + t] = carry + s[t] - v;
+        __syncthreads();
+        if (t == 1023) carry += s[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = carry;
+}
+
+__global__ void k_col_scatter(int n, const int *__restrict__ col_of,
+                              const int *__restrict__ col_start, int *__restrict__ col_fill,
+                              int *__restrict__ col_atoms) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = col_of[i];
+    const int s = atomicAdd(&col_fill[c], 1);
+    col_atoms[col_start[c] + s] = i;
+}
+
+// Sort each column by (z, index); then lay the column out as clusters of 8.
+__global__ void k_col_sort_assign(int ncols, const int *__restrict__ col_start,
+                                  int *__restrict__ col_atoms, const float *__restrict__ zkey,
+                                  const int *__restrict__ cl_start, int *__restrict__ slot_orig,
+                                  int *__restrict__ cl_col, int *__restrict__ status) {
+    __shared__ unsigned long long s[MAX_COL];
+    const int c = blockIdx.x;
+    if (c >= ncols) return;
+    const int b = col_start[c], nc = col_start[c + 1] - b;
+    if (nc > MAX_COL) {
+        if (threadIdx.x == 0) atomicAdd(&status[ST_CELLOVER], 1);
+        return;
+    }
+    int m = 1;
+    while (m < nc) m <<= 1;
+    for (int t = threadIdx.x; t < m; t += blockDim.x) {
+        if (t < nc) {
+            const int i = col_atoms[b + t];
+            const unsigned zb = __float_as_uint(fmaxf(zkey[i], 0.0f));
+            s[t] = ((unsigned long long)zb << 32) | (unsigned)i;
+        } else {
+            s[t] = ~0ull;
+        }
+    }
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int t = threadIdx.x; t < m; t += blockDim.x) {
+                const int ix = t ^ j;
+                if (ix > t) {
+                    const bool up = ((t & k) == 0);
+                    const unsigned long long a = s[t], bb = s[ix];
+                    if ((a > bb) == up) {
+                        s[t] = bb;
+                        s[ix] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const int c0 = cl_start[c], ncl = cl_start[c + 1] - c0;
+    for (int t = threadIdx.x; t < ncl * CL; t += blockDim.x) {
+        slot_orig[c0 * CL + t] = (t < nc) ? (int)(s[t] & 0xffffffffu) : -1;
+        if ((t & (CL - 1)) == 0) cl_col[c0 + t / CL] = c;
+    }
+}
+
+// Gather the cluster-ordered records.  The position used is the build-time
+// wrapped image plus the minimum-image displacement since the build, so a
+// caller that wraps atoms back into the box between builds stays consistent.
+__global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
+                       const int *__restrict__ slot_orig, const double *__restrict__ x,
+                       const double *__restrict__ y, const double *__restrict__ z,
+                       const double *__restrict__ rx, const double *__restrict__ ry,
+                       const double *__restrict__ rz, const double *__restrict__ ix,
+                       const double *__restrict__ iy, const double *__restrict__ iz,
+                       const float *__restrict__ q, const int *__restrict__ type, double L,
+                       AtomRec *__restrict__ rec) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots || s >= ncl_dev[0] * CL) return;
+    const int o = slot_orig[s];
+    AtomRec r;
+    if (o >= 0) {
+        double dx = x[o] - rx[o], dy = y[o] - ry[o], dz = z[o] - rz[o];
+        dx -= L * rint(dx / L);
+        dy -= L * rint(dy / L);
+        dz -= L * rint(dz / L);
+        r.x = rx[o] + ix[o] + dx;
+        r.y = ry[o] + iy[o] + dy;
+        r.z = rz[o] + iz[o] + dz;
+        r.q = q[o];
+        r.type = type[o] - 1;
+    } else {
+        // padding: far away and distinct; every pair with it is masked out
+        r.x = 1.0e6 + 16.0 * s;
+        r.y = -1.0e6;
+        r.z = 1.0e6;
+        r.q = 0.0f;
+        r.type = 0;
+    }
+    rec[s] = r;
+}
+
+__global__ void k_bbox(int maxcl, const int *__restrict__ ncl_dev,
+                       const AtomRec *__restrict__ rec, const int *__restrict__ slot_orig,
+                       float4 *__restrict__ bb) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= maxcl || c >= ncl_dev[0]) return;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int k = 0; k < CL; ++k) {
+        if (slot_orig[c * CL + k] < 0) continue;
+        const AtomRec r = rec[c * CL + k];
+        lo[0] = fmin(lo[0], r.x);
+        lo[1] = fmin(lo[1], r.y);
+        lo[2] = fmin(lo[2], r.z);
+        hi[0] = fmax(hi[0], r.x);
+        hi[1] = fmax(hi[1], r.y);
+        hi[2] = fmax(hi[2], r.z);
+    }
+    bb[2 * c] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
+                            __double2float_rd(lo[2]), 0.0f);
+    bb[2 * c + 1] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
+                                __double2float_ru(hi[2]), 0.0f);
+}
+
+__device__ __forceinline__ float gap(float alo, float ahi, float blo, float bhi) {
+    return fmaxf(0.0f, fmaxf(blo - ahi, alo - bhi));
+}
+
+struct SearchArgs {
+    int maxcl, ncx, reach, jcap;
+    float L, s_col, rl2, rexcl2;
+    const int *ncl_dev, *cl_start, *cl_col, *slot_orig, *specbond, *num3bond;
+    const float4 *bb;
+    int *jlist, *jcount;
+    unsigned long long *jmask;
+    int *status;
+};
+
+// One warp per i-cluster: visit the xy columns within reach (periodic images
+// included), test every cluster's bounding box in three z images, compact the
+// accepted (cluster, image) pairs in visiting order and attach the pair mask.
+__global__ void __launch_bounds__(256) k_search(SearchArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (icl >= a.maxcl || icl >= a.ncl_dev[0]) return;
+    const float4 ilo = a.bb[2 * icl], ihi = a.bb[2 * icl + 1];
+    const int col = a.cl_col[icl];
+    const int cxi = col % a.ncx, cyi = col / a.ncx;
+    // i-cluster atoms: real-atom bits and orig ids (lanes 0..7 hold one each)
+    const int my_io = a.slot_orig[icl * CL + (lane & 7)];
+    const unsigned ireal = __ballot_sync(FULL, my_io >= 0) & 0xffu;
+    int count = 0;
+    int *row = a.jlist + (size_t)icl * a.jcap;
+    unsigned long long *mrow = a.jmask + (size_t)icl * a.jcap;
+    for (int dy = -a.reach; dy <= a.reach; ++dy) {
+        int cy = cyi + dy;
+        const int imy = (cy < 0) ? -1 : (cy >= a.ncx ? 1 : 0);
+        cy -= imy * a.ncx;
+        const float sy = imy * a.L;
+        const float gy = gap(ilo.y, ihi.y, cy * a.s_col + sy, (cy + 1) * a.s_col + sy);
+        if (gy * gy >= a.rl2) continue;
+        for (int dx = -a.reach; dx <= a.reach; ++dx) {
+            int cx = cxi + dx;
+            const int imx = (cx < 0) ? -1 : (cx >= a.ncx ? 1 : 0);
+            cx -= imx * a.ncx;
+            const float sx = imx * a.L;
+            const float gx = gap(ilo.x, ihi.x, cx * a.s_col + sx, (cx + 1) * a.s_col + sx);
+            if (gx * gx + gy * gy >= a.rl2) continue;
+            const int jc0 = a.cl_start[cx + cy * a.ncx], jc1 = a.cl_start[cx + cy * a.ncx + 1];
+            for (int imz = -1; imz <= 1; ++imz) {
+                const float sz = imz * a.L;
+                for (int base = jc0; base < jc1; base += 32) {
+                    const int jc = base + lane;
+                    bool acc = false, need_excl = false;
+                    unsigned long long mask = 0ull;
+                    if (jc < jc1) {
+                        const float4 jlo = a.bb[2 * jc], jhi = a.bb[2 * jc + 1];
+                        const float ex = gap(ilo.x, ihi.x, jlo.x + sx, jhi.x + sx);
+                        const float ey = gap(ilo.y, ihi.y, jlo.y + sy, jhi.y + sy);
+                        const float ez = gap(ilo.z, ihi.z, jlo.z + sz, jhi.z + sz);
+                        const float d2 = ex * ex + ey * ey + ez * ez;
+                        acc = d2 < a.rl2;
+                        if (acc) {
+                            need_excl = d2 < a.rexcl2;
+                            unsigned jreal = 0;
+#pragma unroll
+                            for (int k = 0; k < CL; ++k)
+                                jreal |= (a.slot_orig[jc * CL + k] >= 0 ? 1u : 0u) << k;
+#pragma unroll
+                            for (int ii = 0; ii < CL; ++ii)
+                                if ((ireal >> ii) & 1u) mask |= (unsigned long long)jreal << (ii * CL);
+                            if (jc == icl && imx == 0 && imy == 0 && imz == 0) {
+#pragma unroll
+                                for (int ii = 0; ii < CL; ++ii) mask &= ~(1ull << (ii * CL + ii));
+                            }
+                        }
+                    }
+                    const unsigned ballot = __ballot_sync(FULL, acc);
+                    // exclusions: the warp resolves each nearby accepted entry together
+                    unsigned todo = __ballot_sync(FULL, need_excl);
+                    while (todo) {
+                        const int src = __ffs(todo) - 1;
+                        todo &= todo - 1;
+                        const int jsrc = __shfl_sync(FULL, jc, src);
+                        unsigned bits[2];
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int b = lane + 32 * h;
+                            const int io = a.slot_orig[icl * CL + (b >> 3)];
+                            const int jo = a.slot_orig[jsrc * CL + (b & 7)];
+                            bool ex = false;
+                            if (io >= 0 && jo >= 0) {
+                                const int n3 = a.num3bond[io];
+                                for (int l = 0; l < n3 && l < 12; ++l)
+                                    ex |= (a.specbond[io * 12 + l] == jo + 1);
+                            }
+                            bits[h] = __ballot_sync(FULL, ex);
+                        }
+                        if (lane == src)
+                            mask &= ~((unsigned long long)bits[0] | ((unsigned long long)bits[1] << 32));
+                    }
+                    if (acc) {
+                        const int at = count + __popc(ballot & ((1u << lane) - 1u));
+                        if (at < a.jcap) {
+                            const int img = (imx + 1) + 3 * (imy + 1) + 9 * (imz + 1);
+                            row[at] = jc | (img << IMG_SHIFT);
+                            mrow[at] = mask;
+                        }
+                    }
+                    count += __popc(ballot);
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        a.jcount[icl] = min(count, a.jcap);
+        atomicMax(&a.status[ST_NCLUSTER], count);
+    }
+}
+
+// Displacement trigger: flag a rebuild when any atom moved more than skin/2
+// (minimum image) since the last build.
+__global__ void k_disp_check(int n, const double *__restrict__ x, const double *__restrict__ y,
+                             const double *__restrict__ z, const double *__restrict__ rx,
+                             const double *__restrict__ ry, const double *__restrict__ rz,
+                             double L, double lim2, int *__restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool far = false;
+    if (i < n) {
+        double dx = x[i] - rx[i], dy = y[i] - ry[i], dz = z[i] - rz[i];
+        dx -= L * rint(dx / L);
+        dy -= L * rint(dy / L);
+        dz -= L * rint(dz / L);
+        far = (dx * dx + dy * dy + dz * dz) > lim2 || !(dx == dx && dy == dy && dz == dz);
+    }
+    if (__any_sync(FULL, far) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+struct PairConst {
+    float rcut2, cut_coulsq, alpha2, pa, c2a, e_shift, f_shift, coulpre;
+    float A1, A2, A3, A4, A5;
+    double rcut2d, cut_coulsqd, alphad, e_shiftd, f_shiftd, coulpred, MY_PIS_INV;
+    double A1d, A2d, A3d, A4d, A5d, EWALD_Pd;
+    double L;
+    int ntypes;
+};
+
+template <typename T>
+struct PairMath;
+
+// FP32 pair: LJ 12-6 + DSF with the reference's polynomial erfc
+// (mod_force_nonbond.f90:152-175), using F*r = pref*(erfc + 2a/sqrt(pi) r e + f_shift r^2).
+template <>
+struct PairMath<float> {
+    template <bool EN>
+    __device__ __forceinline__ static float eval(float dx, float dy, float dz, float qiq,
+                                                 float4 lj, bool on, const PairConst &k,
+                                                 float &elj, float &ec) {
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float rinv = rsqrtf(r2);
+        const float r2inv = rinv * rinv;
+        const float r = r2 * rinv;
+        const float dr6i = r2inv * r2inv * r2inv;
+        const bool lj_on = on && r2 <= k.rcut2;
+        const bool c_on = on && r2 <= k.cut_coulsq;
+        const float flj = dr6i * fmaf(lj.x, dr6i, -lj.y);
+        const float pref = qiq * rinv;
+        const float ex = expf(-k.alpha2 * r2);
+        const float t = __fdividef(1.0f, fmaf(k.pa, r, 1.0f));
+        const float poly = fmaf(t, fmaf(t, fmaf(t, fmaf(t, k.A5, k.A4), k.A3), k.A2), k.A1);
+        const float erfcc = t * poly * ex;
+        const float fc = pref * fmaf(k.f_shift, r2, fmaf(k.c2a * ex, r, erfcc));
+        if (EN) {
+            // selects, not products: masked pairs may hold inf/NaN (r = 0)
+            elj = lj_on ? dr6i * fmaf(dr6i, lj.z, -lj.w) : 0.0f;
+            ec = c_on ? pref * (erfcc - fmaf(r, k.e_shift, r2 * k.f_shift)) : 0.0f;
+        }
+        const float fs = ((c_on ? fc : 0.0f) + (lj_on ? flj : 0.0f)) * r2inv;
+        return on ? fs : 0.0f;
+    }
+};
+
+template <>
+struct PairMath<double> {
+    template <bool EN>
+    __device__ __forceinline__ static double eval(double dx, double dy, double dz, double qiq,
+                                                  float4 lj, bool on, const PairConst &k,
+                                                  double &elj, double &ec) {
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double r = sqrt(r2);
+        const double rinv = 1.0 / r;
+        const double r2inv = 1.0 / r2;
+        const double dr6i = r2inv * r2inv * r2inv;
+        const bool lj_on = on && r2 <= k.rcut2d;
+        const bool c_on = on && r2 <= k.cut_coulsqd;
+        const double flj = dr6i * ((double)lj.x * dr6i - (double)lj.y);
+        const double pref = qiq * rinv;
+        const double ex = exp(-((k.alphad * k.alphad) * r) * r);
+        const double t = 1.0 / (1.0 + (k.EWALD_Pd * k.alphad) * r);
+        const double erfcc = t * (k.A1d + t * (k.A2d + t * (k.A3d + t * (k.A4d + t * k.A5d)))) * ex;
+        const double fc =
+            pref * (erfcc * rinv + ((2.0 * k.alphad) * k.MY_PIS_INV) * ex + r * k.f_shiftd) * r;
+        if (EN) {
+            elj = lj_on ? dr6i * (dr6i * (double)lj.z - (double)lj.w) : 0.0;
+            ec = c_on ? pref * ((erfcc - r * k.e_shiftd) - r2 * k.f_shiftd) : 0.0;
+        }
+        const double fs = ((c_on ? fc : 0.0) + (lj_on ? flj : 0.0)) * r2inv;
+        return on ? fs : 0.0;
+    }
+};
+
+__device__ __forceinline__ long long to_fix(double v) { return __double2ll_rn(v * FIX_SCALE); }
+
+// Pair kernel: one warp per i-cluster; lane = li (i atom, 0..7) + 8*lj (j quarter).
+template <typename T, bool EN>
+__global__ void __launch_bounds__(256) k_pair(
+    int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
+    const int *__restrict__ slot_orig, const int *__restrict__ jlist,
+    const unsigned long long *__restrict__ jmask, const int *__restrict__ jcount, int jcap,
+    const float4 *__restrict__ ljtab, PairConst k, long long *__restrict__ fx,
+    long long *__restrict__ fy, long long *__restrict__ fz, double *__restrict__ energy,
+    int *__restrict__ status) {
+    extern __shared__ float4 s_lj[];
+    for (int t = threadIdx.x; t < k.ntypes * k.ntypes; t += blockDim.x) s_lj[t] = ljtab[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int li = lane & 7, lj = lane >> 3;
+    const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (icl >= maxcl || icl >= ncl_dev[0]) return;
+    const AtomRec ri = rec[icl * CL + li];
+    const T qiq = (T)k.coulpre * (T)ri.q;
+    const int ti = ri.type * k.ntypes;
+    const int n = jcount[icl];
+    const int *row = jlist + (size_t)icl * jcap;
+    const unsigned long long *mrow = jmask + (size_t)icl * jcap;
+    T ax = 0, ay = 0, az = 0;
+    long long lx = 0, ly = 0, lz = 0;
+    double e_lj = 0.0, e_c = 0.0, vxx = 0.0, vyy = 0.0, vzz = 0.0;
+    const double L = k.L;
+    for (int e = 0; e < n; ++e) {
+        const int w = row[e];
+        const unsigned long long mask = mrow[e];
+        const int jc = w & ((1 << IMG_SHIFT) - 1);
+        const int img = w >> IMG_SHIFT;
+        const double sx = (double)(img % 3 - 1) * L;
+        const double sy = (double)((img / 3) % 3 - 1) * L;
+        const double sz = (double)(img / 9 - 1) * L;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int jj = lj + 4 * h;
+            const AtomRec rj = rec[jc * CL + jj];
+            const T dx = (T)(ri.x - (rj.x + sx));
+            const T dy = (T)(ri.y - (rj.y + sy));
+            const T dz = (T)(ri.z - (rj.z + sz));
+            const bool on = (mask >> (li * CL + jj)) & 1ull;
+            const float4 ljp = s_lj[ti + rj.type];
+            T elj = 0, ec = 0;
+            const T fs = PairMath<T>::template eval<EN>(dx, dy, dz, qiq * (T)rj.q, ljp, on, k,
+                                                        elj, ec);
+            ax += dx * fs;
+            ay += dy * fs;
+            az += dz * fs;
+            if (EN) {
+                e_lj += (double)elj;
+                e_c += (double)ec;
+                vxx += (double)(dx * dx * fs);
+                vyy += (double)(dy * dy * fs);
+                vzz += (double)(dz * dz * fs);
+            }
+        }
+        if ((e & (FLUSH - 1)) == FLUSH - 1) {
+            lx += to_fix((double)ax);
+            ly += to_fix((double)ay);
+            lz += to_fix((double)az);
+            ax = ay = az = 0;
+        }
+    }
+    lx += to_fix((double)ax);
+    ly += to_fix((double)ay);
+    lz += to_fix((double)az);
+#pragma unroll
+    for (int off = 8; off <= 16; off <<= 1) {
+        lx += __shfl_xor_sync(FULL, lx, off);
+        ly += __shfl_xor_sync(FULL, ly, off);
+        lz += __shfl_xor_sync(FULL, lz, off);
+    }
+    if (lj == 0) {
+        const int o = slot_orig[icl * CL + li];
+        if (o >= 0) {
+            fx[o] = lx;
+            fy[o] = ly;
+            fz[o] = lz;
+            const long long lim = 1ll << 62;
+            if (lx > lim || lx < -lim || ly > lim || ly < -lim || lz > lim || lz < -lim)
+                atomicAdd(&status[ST_FIXED_OVF], 1);
+        }
+    }
+    if (EN) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            e_lj += __shfl_xor_sync(FULL, e_lj, off);
+            e_c += __shfl_xor_sync(FULL, e_c, off);
+            vxx += __shfl_xor_sync(FULL, vxx, off);
+            vyy += __shfl_xor_sync(FULL, vyy, off);
+            vzz += __shfl_xor_sync(FULL, vzz, off);
+        }
+        if (lane == 0) {
+            double *o = energy + (size_t)icl * 5;
+            o[0] = e_lj;
+            o[1] = e_c;
+            o[2] = vxx;
+            o[3] = vyy;
+            o[4] = vzz;
+        }
+    }
+}
+
+__global__ void k_reduce_energy(int maxcl, const int *__restrict__ ncl_dev,
+                                const double *__restrict__ pe, double *__restrict__ out) {
+    __shared__ double s[256];
+    const int t = threadIdx.x;
+    const int n = min(maxcl, ncl_dev[0]);
+    const int chunk = (n + 255) / 256;
+    for (int c = 0; c < 5; ++c) {
+        double acc = 0.0;
+        const int b = t * chunk, e = min(n, b + chunk);
+        for (int i = b; i < e; ++i) acc += pe[(size_t)i * 5 + c];
+        s[t] = acc;
+        __syncthreads();
+        for (int off = 128; off > 0; off >>= 1) {
+            if (t < off) s[t] += s[t + off];
+            __syncthreads();
+        }
+        if (t == 0) out[c] = 0.5 * s[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_aos_to_soa(int n, const float4 *__restrict__ pos, double *__restrict__ x,
+                             double *__restrict__ y, double *__restrict__ z) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    x[i] = (double)p.x;
+    y[i] = (double)p.y;
+    z[i] = (double)p.z;
+}
+
+__global__ void k_fix_to_float(int n, const long long *__restrict__ fx,
+                               const long long *__restrict__ fy,
+                               const long long *__restrict__ fz, float *__restrict__ ff) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ff[3 * i + 0] = (float)((double)fx[i] * FIX_INV);
+    ff[3 * i + 1] = (float)((double)fy[i] * FIX_INV);
+    ff[3 * i + 2] = (float)((double)fz[i] * FIX_INV);
+}
+
+__global__ void k_fix_to_double(int n, const long long *__restrict__ fx,
+                                const long long *__restrict__ fy,
+                                const long long *__restrict__ fz, double *__restrict__ f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f[3 * i + 0] = (double)fx[i] * FIX_INV;
+    f[3 * i + 1] = (double)fy[i] * FIX_INV;
+    f[3 * i + 2] = (double)fz[i] * FIX_INV;
+}
+
+// Early-exit wrapper: the build kernels run only when the flag is set, so the
+// whole evaluation can be launched (or graph-captured) without a host round trip.
+__global__ void k_clear_if_flag(const int *__restrict__ flag, int *__restrict__ a, int n) {
+    if (!flag[0]) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+
+static int sys_alloc(Sys *s) {
+    sofia_nb_ctx *ctx = s->ctx;
+    const size_t n = (size_t)s->n;
+    for (int d = 0; d < 3; ++d) {
+        SOFIA_CUDA(ctx, s->x[d].ensure(sizeof(double) * n));
+        SOFIA_CUDA(ctx, s->v[d].ensure(sizeof(double) * n));
+        SOFIA_CUDA(ctx, s->f[d].ensure(sizeof(long long) * n));
+        SOFIA_CUDA(ctx, s->xref[d].ensure(sizeof(double) * n));
+        SOFIA_CUDA(ctx, s->img[d].ensure(sizeof(double) * n));
+    }
+    SOFIA_CUDA(ctx, s->col_count.ensure(sizeof(int) * (s->ncols + 1)));
+    SOFIA_CUDA(ctx, s->col_start.ensure(sizeof(int) * (s->ncols + 1)));
+    SOFIA_CUDA(ctx, s->col_fill.ensure(sizeof(int) * (s->ncols + 1)));
+    SOFIA_CUDA(ctx, s->cl_start.ensure(sizeof(int) * (s->ncols + 1)));
+    SOFIA_CUDA(ctx, s->col_atoms.ensure(sizeof(int) * n * 2));  // atoms + column of atom
+    SOFIA_CUDA(ctx, s->col_key.ensure(sizeof(float) * n));
+    const size_t maxcl = (size_t)s->max_clusters;
+    SOFIA_CUDA(ctx, s->slot_orig.ensure(sizeof(int) * maxcl * CL + sizeof(int) * maxcl));
+    SOFIA_CUDA(ctx, s->rec.ensure(sizeof(AtomRec) * maxcl * CL));
+    SOFIA_CUDA(ctx, s->bb.ensure(sizeof(float4) * 2 * maxcl));
+    SOFIA_CUDA(ctx, s->jcount.ensure(sizeof(int) * maxcl));
+    SOFIA_CUDA(ctx, s->nclusters.ensure(sizeof(int) * 4));
+    SOFIA_CUDA(ctx, s->energy.ensure(sizeof(double) * 5 * maxcl));
+    SOFIA_CUDA(ctx, s->red.ensure(sizeof(double) * 8));
+    SOFIA_CUDA(ctx, s->flag.ensure(sizeof(int) * 4));
+    SOFIA_CUDA(ctx, s->status_local.ensure(sizeof(int) * ST_NSLOTS));
+    return SOFIA_OK;
+}
+
+static int sys_alloc_list(Sys *s) {
+    const size_t maxcl = (size_t)s->max_clusters;
+    SOFIA_CUDA(s->ctx, s->jlist.ensure(sizeof(int) * maxcl * s->jcap));
+    SOFIA_CUDA(s->ctx, s->jmask.ensure(sizeof(unsigned long long) * maxcl * s->jcap));
+    return SOFIA_OK;
+}
+
+// Launch the list build (unconditionally).  Errors and overflows land in status_local.
+static int sys_build(Sys *s) {
+    sofia_nb_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = s->n;
+    int *col_of = s->col_atoms.as<int>() + n;
+    SOFIA_CUDA(ctx, cudaMemsetAsync(s->col_count.p, 0, sizeof(int) * (s->ncols + 1), st));
+    SOFIA_CUDA(ctx, cudaMemsetAsync(s->col_fill.p, 0, sizeof(int) * (s->ncols + 1), st));
+    k_wrap_bin<<<grid_for(n, 256), 256, 0, st>>>(
+        n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(), s->L, s->s_col,
+        s->ncx, s->img[0].as<double>(), s->img[1].as<double>(), s->img[2].as<double>(),
+        s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(), col_of,
+        s->col_count.as<int>(), s->col_key.as<float>());
+    k_scan1<<<1, 1024, 0, st>>>(s->ncols, s->col_count.as<int>(), s->col_start.as<int>(), 0);
+    k_scan1<<<1, 1024, 0, st>>>(s->ncols, s->col_count.as<int>(), s->cl_start.as<int>(), 1);
+    k_col_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, col_of, s->col_start.as<int>(),
+                                                    s->col_fill.as<int>(), s->col_atoms.as<int>());
+    int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
+    SOFIA_CUDA(ctx, cudaMemsetAsync(s->slot_orig.p, 0xff, sizeof(int) * (size_t)s->max_clusters * CL, st));
+    k_col_sort_assign<<<s->ncols, 256, 0, st>>>(s->ncols, s->col_start.as<int>(),
+                                                s->col_atoms.as<int>(), s->col_key.as<float>(),
+                                                s->cl_start.as<int>(), s->slot_orig.as<int>(),
+                                                cl_col, s->status_local.as<int>());
+    // number of clusters = cl_start[ncols]
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(s->nclusters.p, s->cl_start.as<int>() + s->ncols, sizeof(int),
+                                    cudaMemcpyDeviceToDevice, st));
+    const int nslots = s->max_clusters * CL;
+    k_pack<<<grid_for(nslots, 256), 256, 0, st>>>(
+        nslots, s->nclusters.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(),
+        s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
+        s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
+        s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
+        s->rec.as<AtomRec>());
+    k_bbox<<<grid_for(s->max_clusters, 128), 128, 0, st>>>(
+        s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->slot_orig.as<int>(),
+        s->bb.as<float4>());
+    SearchArgs a;
+    a.maxcl = s->max_clusters;
+    a.ncx = s->ncx;
+    a.reach = s->ncol_reach;
+    a.jcap = s->jcap;
+    a.L = (float)s->L;
+    a.s_col = (float)s->s_col;
+    const float rl = (float)s->rlist + 1e-3f;
+    a.rl2 = rl * rl;
+    a.rexcl2 = (float)(s->r_excl * s->r_excl);
+    a.ncl_dev = s->nclusters.as<int>();
+    a.cl_start = s->cl_start.as<int>();
+    a.cl_col = cl_col;
+    a.slot_orig = s->slot_orig.as<int>();
+    a.specbond = s->specbond.as<int>();
+    a.num3bond = s->num3bond.as<int>();
+    a.bb = s->bb.as<float4>();
+    a.jlist = s->jlist.as<int>();
+    a.jcount = s->jcount.as<int>();
+    a.jmask = s->jmask.as<unsigned long long>();
+    a.status = s->status_local.as<int>();
+    k_search<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(a);
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    s->n_builds++;
+    s->built = 1;
+    return SOFIA_OK;
+}
+
+static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
+    (void)lj_dummy;
+    PairConst k;
+    const double rcut2 = (double)(float)(s->rc * s->rc);
+    k.rcut2d = rcut2;
+    k.cut_coulsqd = rcut2;
+    k.rcut2 = (float)rcut2;
+    k.cut_coulsq = (float)rcut2;
+    k.alphad = s->alpha;
+    k.alpha2 = (float)(s->alpha * s->alpha);
+    const double EP = (double)0.3275911f;
+    k.EWALD_Pd = EP;
+    k.pa = (float)(EP * s->alpha);
+    const double mypis = (double)1.77245385090551602729f;
+    k.MY_PIS_INV = 1.0 / mypis;
+    k.c2a = (float)((2.0 * s->alpha) / mypis);
+    k.e_shiftd = s->e_shift;
+    k.f_shiftd = s->f_shift;
+    k.e_shift = (float)s->e_shift;
+    k.f_shift = (float)s->f_shift;
+    k.coulpre = s->coulpre;
+    k.coulpred = (double)s->coulpre;
+    k.A1d = (double)0.254829592f;
+    k.A2d = (double)-0.284496736f;
+    k.A3d = (double)1.421413741f;
+    k.A4d = (double)-1.453152027f;
+    k.A5d = (double)1.061405429f;
+    k.A1 = 0.254829592f;
+    k.A2 = -0.284496736f;
+    k.A3 = 1.421413741f;
+    k.A4 = -1.453152027f;
+    k.A5 = 1.061405429f;
+    k.L = s->L;
+    k.ntypes = s->ntypes;
+    return k;
+}
+
+// Launches: displacement check, conditional rebuild, pack, pair kernel.
+// `force_build` rebuilds regardless of the trigger.
+int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
+    sofia_nb_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = s->n;
+    bool build = force_build || !s->built;
+    if (!build) {
+        const double half = 0.5 * s->skin;
+        SOFIA_CUDA(ctx, cudaMemsetAsync(s->flag.p, 0, sizeof(int), st));
+        k_disp_check<<<grid_for(n, 256), 256, 0, st>>>(
+            n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
+            s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(), s->L,
+            half * half, s->flag.as<int>());
+        int h = 0;
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(&h, s->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+        build = h != 0;
+    }
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        if (build) {
+            SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * ST_NSLOTS, st));
+            int rc = sys_build(s);
+            if (rc) return rc;
+            int hs[ST_NSLOTS];
+            SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs),
+                                            cudaMemcpyDeviceToHost, st));
+            SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+            if (hs[ST_CELLOVER]) return fail(ctx, SOFIA_EINVAL, "an xy column holds more than 2048 atoms%s");
+            if (hs[ST_NCLUSTER] > s->jcap) {
+                // redo with a larger row capacity, like the reference's list regrow
+                s->jcap = (int)(hs[ST_NCLUSTER] * 1.2) + 16;
+                int r2 = sys_alloc_list(s);
+                if (r2) return r2;
+                continue;
+            }
+        } else {
+            const int nslots = s->max_clusters * CL;
+            k_pack<<<grid_for(nslots, 256), 256, 0, st>>>(
+                nslots, s->nclusters.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(),
+                s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
+                s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
+                s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(),
+                s->type.as<int>(), s->L, s->rec.as<AtomRec>());
+        }
+        break;
+    }
+    PairConst k = make_pair_const(s, nullptr);
+    const int blocks = grid_for((long)s->max_clusters * 32, 256);
+    const size_t smem = sizeof(float4) * (size_t)s->ntypes * s->ntypes;
+    long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
+              *fz = s->f[2].as<long long>();
+#define SOFIA_PAIR_ARGS                                                                    \
+    s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->slot_orig.as<int>(), \
+        s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,  \
+        s->ljtab.as<float4>(), k, fx, fy, fz, s->energy.as<double>(), ctx->d_status
+    if (precision == SOFIA_PREC_FP64) {
+        if (energy)
+            k_pair<double, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+        else
+            k_pair<double, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+    } else {
+        if (energy)
+            k_pair<float, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+        else
+            k_pair<float, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+    }
+#undef SOFIA_PAIR_ARGS
+    if (energy)
+        k_reduce_energy<<<1, 256, 0, st>>>(s->max_clusters, s->nclusters.as<int>(),
+                                           s->energy.as<double>(), s->red.as<double>());
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    return SOFIA_OK;
+}
+
+}  // namespace sofia
+
+using sofia::Sys;
+
+struct sofia_system {
+    Sys s;
+};
+
+extern "C" int sofia_system_create(sofia_nb_ctx *ctx, const sofia_system_desc *d,
+                                   sofia_system **out) {
+    if (!ctx || !d || !out) return SOFIA_EINVAL;
+    *out = nullptr;
+    if (d->np <= 0 || d->ntypes <= 0 || d->ntypes > 48 || !d->type || !d->q || !d->lj1 ||
+        !d->lj2 || !d->lj3 || !d->lj4 || !d->specbond || !d->num3bond || !(d->box > 0.0f) ||
+        !(d->cut_coul > 0.0f) || d->neighbor_pad < 0.0f)
+        return sofia::fail(ctx, SOFIA_EINVAL, "bad system description%s");
+    if (d->rcut != d->cut_coul)
+        return sofia::fail(ctx, SOFIA_EINVAL, "the cluster path needs rcut == cut_coul%s");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    sofia_system *ss = new sofia_system();
+    Sys *s = &ss->s;
+    s->ctx = ctx;
+    s->n = d->np;
+    s->ntypes = d->ntypes;
+    s->precision = d->precision;
+    s->box = d->box;
+    s->L = (double)d->box;
+    s->alpha = d->alpha;
+    s->rc = (double)d->cut_coul;
+    s->skin = (double)d->neighbor_pad;
+    s->rlist = s->rc + s->skin;
+    s->coulpre = 332.06371f;
+    sofia_dsf_constants(d->alpha, d->cut_coul, &s->e_shift, &s->f_shift);
+    if (s->rlist > 0.5 * s->L - 1.0) {
+        delete ss;
+        return sofia::fail(ctx, SOFIA_EINVAL, "box too small for rc + skin%s");
+    }
+    const double rho = (double)s->n / (s->L * s->L * s->L);
+    const double s_target = cbrt((double)sofia::CL / rho);
+    s->ncx = (int)fmax(1.0, floor(s->L / s_target));
+    s->s_col = s->L / s->ncx;
+    s->ncols = s->ncx * s->ncx;
+    s->ncol_reach = (int)ceil(s->rlist / s->s_col);
+    if (s->ncol_reach >= s->ncx) {
+        delete ss;
+        return sofia::fail(ctx, SOFIA_EINVAL, "box too small for the column grid%s");
+    }
+    s->max_clusters = s->n / sofia::CL + s->ncols + 1;
+    // expected j-clusters per row: bounding-box volume around rlist, plus headroom
+    const double reach = s->rlist + 1.5 * s_target;
+    s->jcap = (int)(4.19 * reach * reach * reach * rho / sofia::CL * 1.3) + 32;
+    int rc = sofia::sys_alloc(s);
+    if (!rc) rc = sofia::sys_alloc_list(s);
+    const size_t n = (size_t)s->n;
+    if (!rc) {
+        cudaStream_t st = ctx->stream;
+        rc = SOFIA_OK;
+        if (s->type.ensure(sizeof(int) * n) || s->q.ensure(sizeof(float) * n) ||
+            s->specbond.ensure(sizeof(int) * 12 * n) || s->num3bond.ensure(sizeof(int) * n) ||
+            s->ljtab.ensure(sizeof(float4) * (size_t)s->ntypes * s->ntypes) ||
+            s->invm.ensure(sizeof(double) * n) || s->mass.ensure(sizeof(double) * n))
+            rc = sofia::fail(ctx, SOFIA_ECUDA, "allocation failed%s");
+        if (!rc) {
+            cudaMemcpyAsync(s->type.p, d->type, sizeof(int) * n, cudaMemcpyDefault, st);
+            cudaMemcpyAsync(s->q.p, d->q, sizeof(float) * n, cudaMemcpyDefault, st);
+            cudaMemcpyAsync(s->specbond.p, d->specbond, sizeof(int) * 12 * n, cudaMemcpyDefault, st);
+            cudaMemcpyAsync(s->num3bond.p, d->num3bond, sizeof(int) * n, cudaMemcpyDefault, st);
+            const int nt2 = s->ntypes * s->ntypes;
+            float4 *tab = new float4[nt2];
+            float *h1 = new float[4 * nt2];
+            cudaMemcpy(h1, d->lj1, sizeof(float) * nt2, cudaMemcpyDefault);
+            cudaMemcpy(h1 + nt2, d->lj2, sizeof(float) * nt2, cudaMemcpyDefault);
+            cudaMemcpy(h1 + 2 * nt2, d->lj3, sizeof(float) * nt2, cudaMemcpyDefault);
+            cudaMemcpy(h1 + 3 * nt2, d->lj4, sizeof(float) * nt2, cudaMemcpyDefault);
+            for (int t = 0; t < nt2; ++t)
+                tab[t] = make_float4(h1[t], h1[nt2 + t], h1[2 * nt2 + t], h1[3 * nt2 + t]);
+            cudaMemcpy(s->ljtab.p, tab, sizeof(float4) * nt2, cudaMemcpyHostToDevice);
+            delete[] tab;
+            delete[] h1;
+            int *ht = new int[n];
+            cudaMemcpy(ht, d->type, sizeof(int) * n, cudaMemcpyDefault);
+            for (size_t i = 0; i < n; ++i)
+                if (ht[i] < 1 || ht[i] > s->ntypes) rc = sofia::fail(ctx, SOFIA_EINVAL, "atom type out of range%s");
+            if (d->mass && !rc) {
+                // per-atom masses and inverses from the per-type table
+                double *hm = new double[n], *hi = new double[n];
+                double *mt = new double[s->ntypes];
+                cudaMemcpy(mt, d->mass, sizeof(double) * s->ntypes, cudaMemcpyDefault);
+                for (size_t i = 0; i < n; ++i) {
+                    const int t = ht[i] - 1;
+                    hm[i] = (t >= 0 && t < s->ntypes) ? mt[t] : 1.0;
+                    hi[i] = 1.0 / hm[i];
+                }
+                cudaMemcpy(s->mass.p, hm, sizeof(double) * n, cudaMemcpyHostToDevice);
+                cudaMemcpy(s->invm.p, hi, sizeof(double) * n, cudaMemcpyHostToDevice);
+                delete[] hm;
+                delete[] hi;
+                delete[] mt;
+            }
+            delete[] ht;
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess && !rc) rc = sofia::cuda_fail(ctx, e, "system upload");
+        }
+    }
+    if (rc) {
+        sofia_system_destroy(ss);
+        return rc;
+    }
+    *out = ss;
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_system_destroy(sofia_system *ss) {
+    if (!ss) return SOFIA_OK;
+    Sys *s = &ss->s;
+    if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+    sofia::DevBuf *bufs[] = {&s->type, &s->q, &s->invm, &s->mass, &s->specbond, &s->num3bond,
+                             &s->ljtab, &s->col_count, &s->col_start, &s->col_fill, &s->col_atoms,
+                             &s->col_key, &s->cl_start, &s->slot_orig, &s->rec, &s->bb, &s->jlist,
+                             &s->jmask, &s->jcount, &s->nclusters, &s->status_local, &s->energy,
+                             &s->red, &s->flag, &s->stage_pos, &s->stage_ff};
+    for (auto *b : bufs) b->release();
+    for (int d = 0; d < 3; ++d) {
+        s->x[d].release();
+        s->v[d].release();
+        s->f[d].release();
+        s->xref[d].release();
+        s->img[d].release();
+    }
+    delete ss;
+    return SOFIA_OK;
+}
+
+// Drop-in for lj_cut_coul_dsf_nonewton over the production list: positions in
+// the reference's 16-byte AoS (host or device), real*4 forces out.
+extern "C" int sofia_force_nonbond_mixed(sofia_system *ss, const sofia_ainfo *position,
+                                         float *ff, double *potential, double *e_coul,
+                                         double *virial_diag3) {
+    if (!ss || !position || !ff) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const int n = s->n;
+    const void *dpos = position;
+    if (!sofia::is_device_ptr(position)) {
+        SOFIA_CUDA(ctx, s->stage_pos.ensure(sizeof(float4) * (size_t)n));
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(s->stage_pos.p, position, sizeof(float4) * (size_t)n,
+                                        cudaMemcpyHostToDevice, st));
+        dpos = s->stage_pos.p;
+    }
+    sofia::k_aos_to_soa<<<sofia::grid_for(n, 256), 256, 0, st>>>(
+        n, (const float4 *)dpos, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>());
+    const bool want_e = potential || e_coul || virial_diag3;
+    int rc = sofia::sys_eval(s, s->precision, want_e, false);
+    if (rc) return rc;
+    float *dff = ff;
+    const bool host_ff = !sofia::is_device_ptr(ff);
+    if (host_ff) {
+        SOFIA_CUDA(ctx, s->stage_ff.ensure(sizeof(float) * 3 * (size_t)n));
+        dff = s->stage_ff.as<float>();
+    }
+    sofia::k_fix_to_float<<<sofia::grid_for(n, 256), 256, 0, st>>>(
+        n, s->f[0].as<long long>(), s->f[1].as<long long>(), s->f[2].as<long long>(), dff);
+    if (host_ff)
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(ff, dff, sizeof(float) * 3 * (size_t)n,
+                                        cudaMemcpyDeviceToHost, st));
+    double e[5] = {0, 0, 0, 0, 0};
+    if (want_e)
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(e, s->red.p, sizeof(e), cudaMemcpyDeviceToHost, st));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    if (potential) *potential = e[0];
+    if (e_coul) *e_coul = e[1];
+    if (virial_diag3) {
+        virial_diag3[0] = e[2];
+        virial_diag3[1] = e[3];
+        virial_diag3[2] = e[4];
+    }
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_system_set_state(sofia_system *ss, const double *x, const double *v) {
+    if (!ss || !x) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = (size_t)s->n;
+    double *h = new double[3 * n];
+    SOFIA_CUDA(ctx, cudaMemcpy(h, x, sizeof(double) * 3 * n, cudaMemcpyDefault));
+    double *c = new double[n];
+    for (int d = 0; d < 3; ++d) {
+        for (size_t i = 0; i < n; ++i) c[i] = h[3 * i + d];
+        cudaMemcpy(s->x[d].p, c, sizeof(double) * n, cudaMemcpyHostToDevice);
+    }
+    if (v) {
+        SOFIA_CUDA(ctx, cudaMemcpy(h, v, sizeof(double) * 3 * n, cudaMemcpyDefault));
+        for (int d = 0; d < 3; ++d) {
+            for (size_t i = 0; i < n; ++i) c[i] = h[3 * i + d];
+            cudaMemcpy(s->v[d].p, c, sizeof(double) * n, cudaMemcpyHostToDevice);
+        }
+    }
+    delete[] h;
+    delete[] c;
+    s->built = 0;
+    SOFIA_CUDA(ctx, cudaDeviceSynchronize());
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_system_get_state(sofia_system *ss, double *x, double *v, double *f) {
+    if (!ss) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const size_t n = (size_t)s->n;
+    double *c = new double[n];
+    long long *cl = new long long[n];
+    for (int d = 0; d < 3; ++d) {
+        if (x) {
+            cudaMemcpy(c, s->x[d].p, sizeof(double) * n, cudaMemcpyDeviceToHost);
+            for (size_t i = 0; i < n; ++i) x[3 * i + d] = c[i];
+        }
+        if (v) {
+            cudaMemcpy(c, s->v[d].p, sizeof(double) * n, cudaMemcpyDeviceToHost);
+            for (size_t i = 0; i < n; ++i) v[3 * i + d] = c[i];
+        }
+        if (f) {
+            cudaMemcpy(cl, s->f[d].p, sizeof(long long) * n, cudaMemcpyDeviceToHost);
+            for (size_t i = 0; i < n; ++i) f[3 * i + d] = (double)cl[i] * sofia::FIX_INV;
+        }
+    }
+    delete[] c;
+    delete[] cl;
+    return SOFIA_OK;
+}
+
+// Forces on the resident positions; energies[5] = potential, e_coul, virial x,y,z.
+extern "C" int sofia_system_compute_forces(sofia_system *ss, int precision, int rebuild,
+                                           double *energies) {
+    if (!ss) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    int rc = sofia::sys_eval(s, precision, energies != nullptr, rebuild != 0);
+    if (rc) return rc;
+    if (energies) {
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(energies, s->red.p, sizeof(double) * 5,
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_system_stats(sofia_system *ss, int64_t *stats, int nstats) {
+    if (!ss || !stats || nstats <= 0) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int ncl = 0;
+    SOFIA_CUDA(ctx, cudaMemcpy(&ncl, s->nclusters.p, sizeof(int), cudaMemcpyDeviceToHost));
+    long long entries = 0;
+    if (ncl > 0) {
+        int *jc = new int[ncl];
+        cudaMemcpy(jc, s->jcount.p, sizeof(int) * ncl, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < ncl; ++i) entries += jc[i];
+        delete[] jc;
+    }
+    const int64_t vals[8] = {s->n_builds, ncl, entries, s->jcap, s->ncx, s->max_clusters,
+                             s->ncol_reach, 0};
+    for (int i = 0; i < nstats && i < 8; ++i) stats[i] = vals[i];
+    return SOFIA_OK;
+}

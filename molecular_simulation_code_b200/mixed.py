@@ -1,0 +1,110 @@
+"""Production (device-resident) nonbonded path over the C ABI.
+
+``System`` owns one ``sofia_system``: static per-atom data, FP64 positions,
+the cluster-pair list and 64-bit fixed-point forces live on the GPU.
+``forces_dropin`` is the drop-in form of ``lj_cut_coul_dsf_nonewton``
+(Source/mod_force_nonbond.f90:105-196): reference AoS positions in, real*4
+forces out, list maintenance (Source/mod_neighbor.f90:8-86) done inside.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import SOFIA_OK, SOFIA_PREC_FP64, SOFIA_PREC_MIXED, SofiaError, SofiaSystemDesc
+from .nonbond import Context, ptr
+
+MIXED = SOFIA_PREC_MIXED
+FP64 = SOFIA_PREC_FP64
+
+
+class System:
+    def __init__(self, ctx: Context, sysdata, alpha: float = 0.2, cut: float = 10.0,
+                 skin: float = 2.0, precision: int = MIXED):
+        self.ctx = ctx
+        self.n = sysdata.np_atoms
+        self._keep = [np.ascontiguousarray(sysdata.types, np.int32),
+                      np.ascontiguousarray(sysdata.q, np.float32),
+                      np.ascontiguousarray(sysdata.lj1, np.float32),
+                      np.ascontiguousarray(sysdata.lj2, np.float32),
+                      np.ascontiguousarray(sysdata.lj3, np.float32),
+                      np.ascontiguousarray(sysdata.lj4, np.float32),
+                      np.ascontiguousarray(sysdata.specbond, np.int32),
+                      np.ascontiguousarray(sysdata.num3bond, np.int32),
+                      np.ascontiguousarray(sysdata.mass_type, np.float64)]
+        k = self._keep
+        d = SofiaSystemDesc(self.n, sysdata.ntypes, np.float32(sysdata.box), float(alpha),
+                            np.float32(cut), np.float32(cut), np.float32(skin), precision,
+                            ptr(k[0]), ptr(k[1]), ptr(k[2]), ptr(k[3]), ptr(k[4]), ptr(k[5]),
+                            ptr(k[6]), ptr(k[7]), ptr(k[8]))
+        h = C.c_void_p()
+        ctx.check(ctx._lib.sofia_system_create(ctx.handle, C.byref(d), C.byref(h)))
+        self.handle = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx._lib.sofia_system_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forces_dropin(self, position, ff=None, energy: bool = True):
+        """Positions (np,4) float32 AoS or device tensor; returns (ff, pot, e_coul, virial)."""
+        if ff is None:
+            ff = np.zeros((self.n, 3), np.float32)
+        pot = C.c_double()
+        ec = C.c_double()
+        vir = np.zeros(3)
+        if energy:
+            args = (C.byref(pot), C.byref(ec), ptr(vir))
+        else:
+            args = (None, None, None)
+        self.ctx.check(self.ctx._lib.sofia_force_nonbond_mixed(self.handle, ptr(position),
+                                                               ptr(ff), *args))
+        return ff, pot.value, ec.value, vir
+
+    def set_state(self, x, v=None):
+        x = np.ascontiguousarray(x, np.float64)
+        v = None if v is None else np.ascontiguousarray(v, np.float64)
+        self.ctx.check(self.ctx._lib.sofia_system_set_state(self.handle, ptr(x), ptr(v)))
+
+    def get_state(self):
+        x = np.zeros((self.n, 3))
+        v = np.zeros((self.n, 3))
+        f = np.zeros((self.n, 3))
+        self.ctx.check(self.ctx._lib.sofia_system_get_state(self.handle, ptr(x), ptr(v), ptr(f)))
+        return x, v, f
+
+    def compute(self, precision: int | None = None, rebuild: bool = False, energy: bool = True):
+        e = np.zeros(5) if energy else None
+        p = self.precision if precision is None else precision
+        self.ctx.check(self.ctx._lib.sofia_system_compute_forces(self.handle, p, int(rebuild),
+                                                                 ptr(e)))
+        return e
+
+    def stats(self) -> dict:
+        st = np.zeros(8, np.int64)
+        self.ctx.check(self.ctx._lib.sofia_system_stats(self.handle, ptr(st), 8))
+        keys = ["builds", "clusters", "entries", "jcap", "ncx", "max_clusters", "reach"]
+        return {k: int(v) for k, v in zip(keys, st)}
+
+
+def force_rms_rel(f, fref) -> float:
+    """sqrt(sum |f - fref|^2 / sum |fref|^2) over all atoms."""
+    d = np.asarray(f, np.float64) - np.asarray(fref, np.float64)
+    return float(np.sqrt((d * d).sum() / (np.asarray(fref, np.float64) ** 2).sum()))
+
+
+def force_max_rel(f, fref) -> float:
+    """max_i |f_i - fref_i| / max_i |fref_i|."""
+    d = np.linalg.norm(np.asarray(f, np.float64) - np.asarray(fref, np.float64), axis=1)
+    return float(d.max() / np.linalg.norm(np.asarray(fref, np.float64), axis=1).max())
+
+
+__all__ = ["System", "MIXED", "FP64", "force_rms_rel", "force_max_rel", "SofiaError", "SOFIA_OK"]
