@@ -1,0 +1,467 @@
+#!/usr/bin/env python
+"""Throughput of the Sofia nonbonded hot path on B200 (atom-steps/s).
+
+Workload (default): the 275,000-atom glycine/water system (3,500 glycine +
+80,000 SPC/E water, 1.0 g/cm^3, L = 14.1 nm), rc = 10 A, skin 2 A, DSF
+alpha = 0.2 A^-1, seeded synthetic coordinates.  One step = advance the
+positions by one 2 fs ballistic step (device kernel), then the hot path:
+displacement check, list rebuild when an atom has moved more than skin/2,
+and the LJ + DSF forces, energies and virial of the mixed FP32-pair /
+64-bit fixed-point kernel.
+
+Printed (rank 0, one JSON line): value = device-resident atom-steps/s of
+the mixed path (max over ranks, replicas only); e2e = the same through the
+drop-in C ABI call with pinned host buffers (positions in, forces out every
+step); the plain FP64 variants; roofline of the pair kernel against a
+measured FP32 CUDA-core peak; the CPU baseline (oracle port, all host cores).
+
+``--impl reference`` times the CPU restatement of the reference path
+(oracle port, OpenMP over all host cores) on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 2.0            # fs
+CUT = 10.0          # A
+SKIN = 2.0          # A
+ALPHA = 0.2         # 1/A
+FLOP_PER_PAIR = 82  # algorithmic FLOP per unique pair within rc + skin
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="gly3500_wat80000_275k")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as td
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        td.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return rank, ws
+
+
+def allreduce_max(v: float, ws: int, device=None) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as td
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as td
+        td.barrier()
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, n in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def count_pairs_within(s, rv: float) -> int:
+    """Unique non-excluded atom pairs within rv (minimum image)."""
+    from scipy.spatial import cKDTree
+    L = float(s.box)
+    x = np.mod(s.xyz.astype(np.float64), L)
+    tree = cKDTree(x, boxsize=L)
+    total = int(tree.count_neighbors(tree, rv) - s.np_atoms) // 2
+    # excluded pairs (1-2/1-3/1-4) within rv are not listed
+    cols = np.arange(12)[None, :] < s.num3bond[:, None]
+    ii, ll = np.nonzero(cols)
+    jj = s.specbond[ii, ll] - 1
+    d = x[jj] - x[ii]
+    d -= L * np.round(d / L)
+    excl = int((np.einsum("ij,ij->i", d, d) < rv * rv).sum())
+    return total - excl // 2
+
+
+def measure_fp32_peak() -> float:
+    """FP32 CUDA-core TFLOP/s from cuBLAS SGEMM with TF32 disabled (8192^3)."""
+    import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    b = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def read_profile_traffic():
+    """Per-launch DRAM bytes of the pair kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_pair_mixed_275k.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def build_system(args, rank):
+    from molecular_simulation_code_b200.system import make_workload
+    return make_workload(args.workload, seed=1000 * 3 + rank)
+
+
+def cpu_baseline(s, rebuild_interval: float):
+    """Oracle port (OpenMP, all host threads): one list build + force evaluations,
+    per-step cost = force + build / rebuild_interval."""
+    from oracle import oracle as O
+    p = O.params(ALPHA, s.box, CUT, CUT, SKIN)
+    pos = s.position_aos()
+    lj = (s.lj1, s.lj2, s.lj3, s.lj4)
+    t0 = time.perf_counter()
+    nl, nn, na = O.neighbor_wrapper(p, pos, s.specbond, s.num3bond, 1024, fast=True)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    nf = 2
+    for _ in range(nf):
+        O.force_dsf(p, pos, s.q, lj, s.ntypes, nl, nn, na, fast=True)
+    t_force = (time.perf_counter() - t0) / nf
+    per_step = t_force + t_build / max(rebuild_interval, 1.0)
+    return {"value": s.np_atoms / per_step, "unit": "atom-steps/s", "cores": os.cpu_count(),
+            "kind": "port",
+            "sample": f"275k-atom workload: 1 reference list build ({t_build:.2f} s) + {nf} FP64 "
+                      f"force evaluations ({t_force:.2f} s each); per step = force + build/"
+                      f"{rebuild_interval:.1f} (the GPU run's rebuild interval)"}
+
+
+def run_reference(args, rank, ws):
+    """CPU restatement of the reference path (neighbor_wrapper on trigger +
+    lj_cut_coul_dsf_nonewton), all host threads, same workload and metric."""
+    from oracle import oracle as O
+    if rank != 0:
+        return
+    s = build_system(args, 0)
+    p = O.params(ALPHA, s.box, CUT, CUT, SKIN)
+    lj = (s.lj1, s.lj2, s.lj3, s.lj4)
+    x0 = s.xyz.astype(np.float64)
+    v = s.velocity.astype(np.float64)
+    n = s.np_atoms
+    pos = s.position_aos()
+    # bounded sample: each step evaluates a prefix of the atom rows if a full step
+    # would make the run longer than about three minutes
+    t0 = time.perf_counter()
+    nl, nn, na = O.neighbor_wrapper(p, pos, s.specbond, s.num3bond, 1024, fast=True)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.force_dsf(p, pos, s.q, lj, s.ntypes, nl, nn, na, fast=True)
+    t_force = time.perf_counter() - t0
+    budget = 180.0
+    nsteps = args.steps + args.warmup
+    frac = min(1.0, budget / (nsteps * (t_force + t_build / 10.0)))
+    rows = max(1024, int(n * frac))
+    import ctypes as C
+    L = O.lib(fast=True)
+    xref = x0.copy()
+    half2 = (0.5 * SKIN) ** 2
+    Lb = float(s.box)
+    elapsed = 0.0
+    builds = 0
+    for k in range(nsteps):
+        x = x0 + v * DT * (k + 1)
+        posk = pos.copy()
+        posk[:, :3] = np.mod(x, Lb).astype(np.float32)
+        posk[:, :3][posk[:, :3] <= 0] += np.float32(Lb)
+        t0 = time.perf_counter()
+        d = x - xref
+        d -= Lb * np.round(d / Lb)
+        if (np.einsum("ij,ij->i", d, d) > half2).any():
+            nl, nn, na = O.neighbor_wrapper(p, posk, s.specbond, s.num3bond, na, fast=True)
+            xref = x.copy()
+            builds += 1 if k >= args.warmup else 0
+        ff = np.zeros(rows * 3, np.float32)
+        pot = C.c_double()
+        ec = C.c_double()
+        L.orc_force_dsf_nonewton(C.byref(p), rows, posk, np.ascontiguousarray(s.q), lj[0], lj[1],
+                                 lj[2], lj[3], s.ntypes, nl, nn, na, ff, C.byref(pot),
+                                 C.byref(ec), np.zeros(3), None, 0)
+        dt_ = time.perf_counter() - t0
+        if k >= args.warmup:
+            elapsed += dt_
+    value = rows * args.steps / elapsed
+    out = {"impl": "reference", "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": args.workload, "atoms": n, "rc_A": CUT, "skin_A": SKIN},
+           "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": os.cpu_count(),
+                            "kind": "port",
+                            "sample": f"{rows} of {n} atom rows per step, {args.steps} steps, "
+                                      f"{builds} list rebuilds (half-skin trigger)"},
+           "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, rank, ws):
+    import torch
+
+    from molecular_simulation_code_b200 import mixed as M
+    from molecular_simulation_code_b200 import nonbond as nb
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    s = build_system(args, rank)
+    n = s.np_atoms
+    fp32_peak = measure_fp32_peak() if rank == 0 else 0.0
+    ctx = nb.Context(dev)
+    stream = torch.cuda.ExternalStream(ctx._lib.sofia_stream(ctx.handle))
+    sysm = M.System(ctx, s, alpha=ALPHA, cut=CUT, skin=SKIN, precision=M.MIXED)
+    x0 = s.xyz.astype(np.float64)
+    v0 = s.velocity.astype(np.float64)
+    sysm.set_state(x0, v0)
+
+    def timed_loop(precision, nsteps, warm):
+        sysm.set_state(x0, v0)
+        for _ in range(warm):
+            sysm.drift(DT)
+            sysm.compute(precision, energy=True)
+        b0 = sysm.stats()
+        sysm.timers(True)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(nsteps):
+            sysm.drift(DT)
+            sysm.compute(precision, energy=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        t = e0.elapsed_time(e1) / 1e3
+        tm = sysm.timers(False)
+        b1 = sysm.stats()
+        return t, tm, b1["builds"] - b0["builds"], b1["launches"] - b0["launches"], b1
+
+    with Clocks(dev) as clk:
+        t_mixed, tm, builds, launches, st = timed_loop(M.MIXED, args.steps, args.warmup)
+    t_max = allreduce_max(t_mixed, ws, device=torch.device("cuda", dev))
+    value = n * ws * args.steps / t_max
+
+    # plain FP64 twin of the same kernel and list
+    t_fp64 = None
+    if not args.no_fp64:
+        t_fp64, tm64, _, _, _ = timed_loop(M.FP64, args.steps, args.warmup)
+        t_fp64 = allreduce_max(t_fp64, ws, device=torch.device("cuda", dev))
+
+    # FP64 reference-semantics path (27-cell full list + FP64 pair kernel)
+    t_ref = None
+    if not args.no_fp64:
+        p = nb.DsfParams(alpha=ALPHA, box=s.box, cut_coul=CUT, rcut=CUT, neighbor_pad=SKIN)
+        lj = [torch.from_numpy(a).cuda() for a in (s.lj1, s.lj2, s.lj3, s.lj4)]
+        qd = torch.from_numpy(s.q).cuda()
+        sbd = torch.from_numpy(np.ascontiguousarray(s.specbond)).cuda()
+        n3d = torch.from_numpy(s.num3bond).cuda()
+        posd = torch.from_numpy(s.position_aos()).cuda()
+        L = float(s.box)
+        half2 = (0.5 * SKIN) ** 2
+        na = 1024
+        xref = x0.copy()
+        frames = []
+        for k in range(args.steps + args.warmup):
+            x = x0 + v0 * DT * (k + 1)
+            rb = False
+            d = x - xref
+            d -= L * np.round(d / L)
+            if k == 0 or (np.einsum("ij,ij->i", d, d) > half2).any():
+                rb = True
+                xref = x.copy()
+            xw = np.mod(x, L).astype(np.float32)
+            xw[xw <= 0] += np.float32(L)
+            frames.append((xw, rb))
+        ff = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        tot = 0.0
+        for k, (xw, rb) in enumerate(frames):
+            posd[:, :3] = torch.from_numpy(xw).cuda()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if rb:
+                _, _, na = nb.neighbor_wrapper(ctx, posd, sbd, n3d, p, na, want_host=False)
+            nb.lj_cut_coul_dsf_nonewton(ctx, posd, qd, lj, s.ntypes, None, None, na, p, ff=ff)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if k >= args.warmup:
+                tot += e0.elapsed_time(e1) / 1e3
+        t_ref = allreduce_max(tot, ws, device=torch.device("cuda", dev))
+        del lj, qd, sbd, n3d, posd, ff
+
+    # e2e: drop-in call with pinned host positions in and real*4 forces out each step
+    nf = args.steps + args.warmup
+    frames = torch.empty((nf, n, 4), dtype=torch.float32, pin_memory=True)
+    tbits = torch.from_numpy(s.types.view(np.float32).copy())
+    for k in range(nf):
+        frames[k, :, :3] = torch.from_numpy((x0 + v0 * DT * (k + 1)).astype(np.float32))
+        frames[k, :, 3] = tbits
+    ffh = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    drop = M.System(ctx, s, alpha=ALPHA, cut=CUT, skin=SKIN, precision=M.MIXED)
+    for k in range(args.warmup):
+        drop.forces_dropin(frames[k], ff=ffh)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.warmup, nf):
+        drop.forces_dropin(frames[k], ff=ffh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = allreduce_max(e0.elapsed_time(e1) / 1e3, ws, device=torch.device("cuda", dev))
+    drop.close()
+
+    if rank != 0:
+        return
+    P_rv = count_pairs_within(s, CUT + SKIN)
+    pair_ms = tm["pair_ms"] / max(tm["pairs"], 1)
+    achieved = FLOP_PER_PAIR * P_rv / (pair_ms / 1e3) / 1e12
+    rebuild_interval = args.steps / max(builds, 1)
+    cpu = None if args.no_cpu_baseline else cpu_baseline(s, rebuild_interval)
+    clocks = clk.summary()
+    out = {
+        "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "atoms_per_gpu": n, "rc_A": CUT, "skin_A": SKIN,
+                   "dt_fs": DT, "precision": "mixed FP32 pair / FP64 positions / int64 forces",
+                   "parallelism": f"replicas x{ws} (no exchange)",
+                   "l2": "inputs larger than L2 (cluster-pair list "
+                         f"{st['entries'] * 12 / 1e9:.2f} GB)",
+                   "step": "2 fs ballistic position update + displacement check + list rebuild "
+                           "on trigger + LJ/DSF forces, energies, virial"},
+        "fp64": {"cluster_atom_steps_per_s": (n * ws * args.steps / t_fp64) if t_fp64 else None,
+                 "reference_list_atom_steps_per_s": (n * ws * args.steps / t_ref) if t_ref else None,
+                 "mixed_over_fp64_cluster": (t_fp64 / t_max) if t_fp64 else None,
+                 "mixed_over_fp64_reference_list": (t_ref / t_max) if t_ref else None},
+        "e2e": {"value": n * ws * args.steps / t_e2e, "unit": "atom-steps/s",
+                "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 12 * n + 40},
+        "gpu_launches": launches,
+        "list": {"rebuilds": builds, "clusters": st["clusters"], "entries": st["entries"],
+                 "build_ms": tm["build_ms"] / max(tm["builds"], 1)},
+        "roofline": {"bound": "fp32", "kernel": "k_pair<float,energy>",
+                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak if fp32_peak else None,
+                     "traffic": read_profile_traffic(),
+                     "pair_ms": pair_ms, "pairs_P_rv": P_rv,
+                     "flop_per_pair": FLOP_PER_PAIR,
+                     "peak_source": "measured cuBLAS SGEMM 8192^3, TF32 off, on this GPU"},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank, ws = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, ws)
+        else:
+            run_ours(args, rank, ws)
+    finally:
+        if ws > 1:
+            import torch.distributed as td
+            td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

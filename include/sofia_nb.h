@@ -207,8 +207,14 @@ int sofia_system_get_state(sofia_system *sys, double *x, double *v, double *f);
 int sofia_system_compute_forces(sofia_system *sys, int precision, int rebuild,
                                 double *energies);
 /* stats[0..7]: list builds, clusters, list entries, row capacity, columns per
- * side, cluster capacity, column reach, 0. */
+ * side, cluster capacity, column reach, kernels launched so far. */
 int sofia_system_stats(sofia_system *sys, int64_t *stats, int nstats);
+/* Ballistic drift x += dt*v of the resident positions, nsteps times (no forces). */
+int sofia_system_drift(sofia_system *sys, double dt, int nsteps);
+/* CUDA-event timers of the list build and the pair kernel on the system's
+ * stream: returns and resets timers[4] = {build ms, builds, pair ms, pair
+ * launches}; enable != 0 keeps timing on. */
+int sofia_system_timers(sofia_system *sys, int enable, double *timers);
 
 #ifdef __cplusplus
 }

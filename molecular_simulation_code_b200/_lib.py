@@ -76,6 +76,8 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_system_get_state": (_I, [_P, _P, _P, _P]),
     "sofia_system_compute_forces": (_I, [_P, _I, _I, _P]),
     "sofia_system_stats": (_I, [_P, _P, _I]),
+    "sofia_system_drift": (_I, [_P, _D, _I]),
+    "sofia_system_timers": (_I, [_P, _I, _P]),
 }
 
 _lib = None

@@ -540,6 +540,18 @@ __global__ void k_reduce_energy(int maxcl, const int *__restrict__ ncl_dev,
     }
 }
 
+// Ballistic drift x += dt*v (FP64), used to move a system between
+// evaluations without forces (list maintenance and throughput checks).
+__global__ void k_drift(int n, double dt, double *__restrict__ x, double *__restrict__ y,
+                        double *__restrict__ z, const double *__restrict__ vx,
+                        const double *__restrict__ vy, const double *__restrict__ vz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] += dt * vx[i];
+    y[i] += dt * vy[i];
+    z[i] += dt * vz[i];
+}
+
 __global__ void k_aos_to_soa(int n, const float4 *__restrict__ pos, double *__restrict__ x,
                              double *__restrict__ y, double *__restrict__ z) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -677,9 +689,25 @@ static int sys_build(Sys *s) {
     a.status = s->status_local.as<int>();
     k_search<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(a);
     SOFIA_CUDA(ctx, cudaGetLastError());
+    s->launches += 8;
     s->n_builds++;
     s->built = 1;
     return SOFIA_OK;
+}
+
+// Folds finished event pairs into the timers (called after a stream sync).
+static void sys_collect_timers(Sys *s) {
+    float ms = 0.0f;
+    if (s->pending_build && cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]) == cudaSuccess) {
+        s->t_build_ms += ms;
+        s->n_build_timed++;
+    }
+    if (s->pending_pair && cudaEventElapsedTime(&ms, s->ev[2], s->ev[3]) == cudaSuccess) {
+        s->t_pair_ms += ms;
+        s->n_pair++;
+    }
+    cudaGetLastError();
+    s->pending_build = s->pending_pair = 0;
 }
 
 static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
@@ -733,16 +761,23 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
             n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
             s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(), s->L,
             half * half, s->flag.as<int>());
+        s->launches += 1;
         int h = 0;
         SOFIA_CUDA(ctx, cudaMemcpyAsync(&h, s->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
         build = h != 0;
     }
+    if (s->timing) sys_collect_timers(s);
     for (int attempt = 0; attempt < 4; ++attempt) {
         if (build) {
             SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * ST_NSLOTS, st));
+            if (s->timing) cudaEventRecord(s->ev[0], st);
             int rc = sys_build(s);
             if (rc) return rc;
+            if (s->timing) {
+                cudaEventRecord(s->ev[1], st);
+                s->pending_build = 1;
+            }
             int hs[ST_NSLOTS];
             SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs),
                                             cudaMemcpyDeviceToHost, st));
@@ -763,6 +798,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
                 s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
                 s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(),
                 s->type.as<int>(), s->L, s->rec.as<AtomRec>());
+            s->launches += 1;
         }
         break;
     }
@@ -775,6 +811,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
     s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->slot_orig.as<int>(), \
         s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,  \
         s->ljtab.as<float4>(), k, fx, fy, fz, s->energy.as<double>(), ctx->d_status
+    if (s->timing) cudaEventRecord(s->ev[2], st);
     if (precision == SOFIA_PREC_FP64) {
         if (energy)
             k_pair<double, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
@@ -787,9 +824,16 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
             k_pair<float, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
     }
 #undef SOFIA_PAIR_ARGS
-    if (energy)
+    if (s->timing) {
+        cudaEventRecord(s->ev[3], st);
+        s->pending_pair = 1;
+    }
+    s->launches += 1;
+    if (energy) {
         k_reduce_energy<<<1, 256, 0, st>>>(s->max_clusters, s->nclusters.as<int>(),
                                            s->energy.as<double>(), s->red.as<double>());
+        s->launches += 1;
+    }
     SOFIA_CUDA(ctx, cudaGetLastError());
     return SOFIA_OK;
 }
@@ -910,6 +954,8 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
     if (!ss) return SOFIA_OK;
     Sys *s = &ss->s;
     if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+    for (auto &e : s->ev)
+        if (e) cudaEventDestroy(e);
     sofia::DevBuf *bufs[] = {&s->type, &s->q, &s->invm, &s->mass, &s->specbond, &s->num3bond,
                              &s->ljtab, &s->col_count, &s->col_start, &s->col_fill, &s->col_atoms,
                              &s->col_key, &s->cl_start, &s->slot_orig, &s->rec, &s->bb, &s->jlist,
@@ -1062,7 +1108,44 @@ extern "C" int sofia_system_stats(sofia_system *ss, int64_t *stats, int nstats) 
         delete[] jc;
     }
     const int64_t vals[8] = {s->n_builds, ncl, entries, s->jcap, s->ncx, s->max_clusters,
-                             s->ncol_reach, 0};
+                             s->ncol_reach, s->launches};
     for (int i = 0; i < nstats && i < 8; ++i) stats[i] = vals[i];
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_system_drift(sofia_system *ss, double dt, int nsteps) {
+    if (!ss || nsteps < 0) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    for (int k = 0; k < nsteps; ++k) {
+        sofia::k_drift<<<sofia::grid_for(s->n, 256), 256, 0, ctx->stream>>>(
+            s->n, dt, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
+            s->v[0].as<double>(), s->v[1].as<double>(), s->v[2].as<double>());
+        s->launches += 1;
+    }
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    return SOFIA_OK;
+}
+
+// timers[0..3] = list-build ms, builds timed, pair-kernel ms, pair launches timed.
+extern "C" int sofia_system_timers(sofia_system *ss, int enable, double *timers) {
+    if (!ss) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (enable && !s->ev[0])
+        for (int k = 0; k < 4; ++k) SOFIA_CUDA(ctx, cudaEventCreate(&s->ev[k]));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (s->timing) sofia::sys_collect_timers(s);
+    if (timers) {
+        timers[0] = s->t_build_ms;
+        timers[1] = (double)s->n_build_timed;
+        timers[2] = s->t_pair_ms;
+        timers[3] = (double)s->n_pair;
+    }
+    s->t_build_ms = s->t_pair_ms = 0.0;
+    s->n_build_timed = s->n_pair = 0;
+    s->timing = enable ? 1 : 0;
     return SOFIA_OK;
 }

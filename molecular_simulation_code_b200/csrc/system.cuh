@@ -53,6 +53,13 @@ struct Sys {
     DevBuf stage_pos, stage_ff;
     int built = 0;
     long long n_builds = 0;
+    long long launches = 0;             // kernels launched by this system (all paths)
+    // optional CUDA-event timing of the list build and the pair kernel
+    int timing = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    double t_build_ms = 0.0, t_pair_ms = 0.0;
+    long long n_pair = 0, n_build_timed = 0;
+    int pending_build = 0, pending_pair = 0;
 };
 
 }  // namespace sofia

@@ -91,8 +91,17 @@ class System:
     def stats(self) -> dict:
         st = np.zeros(8, np.int64)
         self.ctx.check(self.ctx._lib.sofia_system_stats(self.handle, ptr(st), 8))
-        keys = ["builds", "clusters", "entries", "jcap", "ncx", "max_clusters", "reach"]
+        keys = ["builds", "clusters", "entries", "jcap", "ncx", "max_clusters", "reach",
+                "launches"]
         return {k: int(v) for k, v in zip(keys, st)}
+
+    def drift(self, dt: float, nsteps: int = 1):
+        self.ctx.check(self.ctx._lib.sofia_system_drift(self.handle, float(dt), int(nsteps)))
+
+    def timers(self, enable: bool = True) -> dict:
+        t = np.zeros(4)
+        self.ctx.check(self.ctx._lib.sofia_system_timers(self.handle, int(enable), ptr(t)))
+        return {"build_ms": t[0], "builds": int(t[1]), "pair_ms": t[2], "pairs": int(t[3])}
 
 
 def force_rms_rel(f, fref) -> float:
