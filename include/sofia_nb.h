@@ -206,8 +206,9 @@ int sofia_system_get_state(sofia_system *sys, double *x, double *v, double *f);
  * forces a list rebuild; energies[5] (may be NULL) = potential, e_coul, virial. */
 int sofia_system_compute_forces(sofia_system *sys, int precision, int rebuild,
                                 double *energies);
-/* stats[0..7]: list builds, clusters, list entries, row capacity, columns per
- * side, cluster capacity, column reach, kernels launched so far. */
+/* stats[0..9]: list builds, clusters, list entries, row capacity, columns per
+ * side, cluster capacity, column reach, kernels launched so far, prunes,
+ * entries of the pruned (rc + margin) list. */
 int sofia_system_stats(sofia_system *sys, int64_t *stats, int nstats);
 /* Ballistic drift x += dt*v of the resident positions, nsteps times (no forces). */
 int sofia_system_drift(sofia_system *sys, double dt, int nsteps);

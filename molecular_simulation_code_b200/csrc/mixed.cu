@@ -324,24 +324,46 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
 
 // Displacement trigger: flag a rebuild when any atom moved more than skin/2
 // (minimum image) since the last build.
+__device__ __forceinline__ double disp2(double x, double y, double z, double rx, double ry,
+                                        double rz, double L) {
+    double dx = x - rx, dy = y - ry, dz = z - rz;
+    dx -= L * rint(dx / L);
+    dy -= L * rint(dy / L);
+    dz -= L * rint(dz / L);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    return (d2 == d2) ? d2 : 1e300;  // non-finite positions force a rebuild
+}
+
+// Displacement triggers: bit 0 = some atom moved more than skin/2 since the
+// list build, bit 1 = more than margin/2 since the last prune.
 __global__ void k_disp_check(int n, const double *__restrict__ x, const double *__restrict__ y,
                              const double *__restrict__ z, const double *__restrict__ rx,
                              const double *__restrict__ ry, const double *__restrict__ rz,
-                             double L, double lim2, int *__restrict__ flag) {
+                             const double *__restrict__ px, const double *__restrict__ py,
+                             const double *__restrict__ pz, double L, double lim2,
+                             double plim2, int *__restrict__ flag) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool far = false;
+    bool far = false, pfar = false;
     if (i < n) {
-        double dx = x[i] - rx[i], dy = y[i] - ry[i], dz = z[i] - rz[i];
-        dx -= L * rint(dx / L);
-        dy -= L * rint(dy / L);
-        dz -= L * rint(dz / L);
-        far = (dx * dx + dy * dy + dz * dz) > lim2 || !(dx == dx && dy == dy && dz == dz);
+        far = disp2(x[i], y[i], z[i], rx[i], ry[i], rz[i], L) > lim2;
+        pfar = disp2(x[i], y[i], z[i], px[i], py[i], pz[i], L) > plim2;
     }
-    if (__any_sync(FULL, far) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+    const bool a = __any_sync(FULL, far), b = __any_sync(FULL, pfar);
+    if ((threadIdx.x & 31) == 0 && (a || b)) atomicOr(flag, (a ? 1 : 0) | (b ? 2 : 0));
+}
+
+__global__ void k_copy3(int n, const double *__restrict__ x, const double *__restrict__ y,
+                        const double *__restrict__ z, double *__restrict__ ox,
+                        double *__restrict__ oy, double *__restrict__ oz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ox[i] = x[i];
+    oy[i] = y[i];
+    oz[i] = z[i];
 }
 
 struct PairConst {
-    float rcut2, cut_coulsq, alpha2, pa, c2a, e_shift, f_shift, coulpre;
+    float rcut2, cut_coulsq, kexp, pa, c2a, e_shift, f_shift, coulpre;
     float A1, A2, A3, A4, A5;
     double rcut2d, cut_coulsqd, alphad, e_shiftd, f_shiftd, coulpred, MY_PIS_INV;
     double A1d, A2d, A3d, A4d, A5d, EWALD_Pd;
@@ -349,11 +371,30 @@ struct PairConst {
     int ntypes;
 };
 
+// Single-instruction MUFU approximations (hand-written PTX).
+__device__ __forceinline__ float rsqrt_a(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_a(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_a(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <typename T>
 struct PairMath;
 
 // FP32 pair: LJ 12-6 + DSF with the reference's polynomial erfc
-// (mod_force_nonbond.f90:152-175), using F*r = pref*(erfc + 2a/sqrt(pi) r e + f_shift r^2).
+// (mod_force_nonbond.f90:152-175), using
+//   F*r = pref * (erfc + (2 alpha/sqrt(pi)) r exp(-alpha^2 r^2) + f_shift r^2).
+// exp(-alpha^2 r^2) = 2^(kexp r^2) with kexp = -alpha^2 log2(e).
 template <>
 struct PairMath<float> {
     template <bool EN>
@@ -361,7 +402,7 @@ struct PairMath<float> {
                                                  float4 lj, bool on, const PairConst &k,
                                                  float &elj, float &ec) {
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float rinv = rsqrtf(r2);
+        const float rinv = rsqrt_a(r2);
         const float r2inv = rinv * rinv;
         const float r = r2 * rinv;
         const float dr6i = r2inv * r2inv * r2inv;
@@ -369,8 +410,8 @@ struct PairMath<float> {
         const bool c_on = on && r2 <= k.cut_coulsq;
         const float flj = dr6i * fmaf(lj.x, dr6i, -lj.y);
         const float pref = qiq * rinv;
-        const float ex = expf(-k.alpha2 * r2);
-        const float t = __fdividef(1.0f, fmaf(k.pa, r, 1.0f));
+        const float ex = ex2_a(k.kexp * r2);
+        const float t = rcp_a(fmaf(k.pa, r, 1.0f));
         const float poly = fmaf(t, fmaf(t, fmaf(t, fmaf(t, k.A5, k.A4), k.A3), k.A2), k.A1);
         const float erfcc = t * poly * ex;
         const float fc = pref * fmaf(k.f_shift, r2, fmaf(k.c2a * ex, r, erfcc));
@@ -413,11 +454,21 @@ struct PairMath<double> {
     }
 };
 
-__device__ __forceinline__ long long to_fix(double v) { return __double2ll_rn(v * FIX_SCALE); }
+template <typename T>
+__device__ __forceinline__ long long to_fix(T v);
+template <>
+__device__ __forceinline__ long long to_fix<float>(float v) {
+    return __float2ll_rn(v * 4294967296.0f);  // exact power-of-two scaling
+}
+template <>
+__device__ __forceinline__ long long to_fix<double>(double v) {
+    return __double2ll_rn(v * FIX_SCALE);
+}
 
-// Pair kernel: one warp per i-cluster; lane = li (i atom, 0..7) + 8*lj (j quarter).
+// Pair kernel: one warp per i-cluster; lane = li (i atom, 0..7) + 8*lj (j quarter,
+// each lane takes j atoms lj and lj+4 of every j-cluster).
 template <typename T, bool EN>
-__global__ void __launch_bounds__(256) k_pair(
+__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
     int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ slot_orig, const int *__restrict__ jlist,
     const unsigned long long *__restrict__ jmask, const int *__restrict__ jcount, int jcap,
@@ -425,7 +476,14 @@ __global__ void __launch_bounds__(256) k_pair(
     long long *__restrict__ fy, long long *__restrict__ fz, double *__restrict__ energy,
     int *__restrict__ status) {
     extern __shared__ float4 s_lj[];
+    __shared__ double s_sh[27 * 3];
     for (int t = threadIdx.x; t < k.ntypes * k.ntypes; t += blockDim.x) s_lj[t] = ljtab[t];
+    if (threadIdx.x < 27) {
+        const int im = threadIdx.x;
+        s_sh[im * 3 + 0] = (double)(im % 3 - 1) * k.L;
+        s_sh[im * 3 + 1] = (double)((im / 3) % 3 - 1) * k.L;
+        s_sh[im * 3 + 2] = (double)(im / 9 - 1) * k.L;
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int li = lane & 7, lj = lane >> 3;
@@ -438,25 +496,25 @@ __global__ void __launch_bounds__(256) k_pair(
     const int *row = jlist + (size_t)icl * jcap;
     const unsigned long long *mrow = jmask + (size_t)icl * jcap;
     T ax = 0, ay = 0, az = 0;
+    T a_lj = 0, a_c = 0, a_xx = 0, a_yy = 0, a_zz = 0;
     long long lx = 0, ly = 0, lz = 0;
     double e_lj = 0.0, e_c = 0.0, vxx = 0.0, vyy = 0.0, vzz = 0.0;
-    const double L = k.L;
     for (int e = 0; e < n; ++e) {
         const int w = row[e];
-        const unsigned long long mask = mrow[e];
+        const unsigned mb = (unsigned)(mrow[e] >> (li * CL)) & 0xffu;
         const int jc = w & ((1 << IMG_SHIFT) - 1);
         const int img = w >> IMG_SHIFT;
-        const double sx = (double)(img % 3 - 1) * L;
-        const double sy = (double)((img / 3) % 3 - 1) * L;
-        const double sz = (double)(img / 9 - 1) * L;
+        const double xis = ri.x - s_sh[img * 3 + 0];
+        const double yis = ri.y - s_sh[img * 3 + 1];
+        const double zis = ri.z - s_sh[img * 3 + 2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int jj = lj + 4 * h;
             const AtomRec rj = rec[jc * CL + jj];
-            const T dx = (T)(ri.x - (rj.x + sx));
-            const T dy = (T)(ri.y - (rj.y + sy));
-            const T dz = (T)(ri.z - (rj.z + sz));
-            const bool on = (mask >> (li * CL + jj)) & 1ull;
+            const T dx = (T)(xis - rj.x);
+            const T dy = (T)(yis - rj.y);
+            const T dz = (T)(zis - rj.z);
+            const bool on = (mb >> jj) & 1u;
             const float4 ljp = s_lj[ti + rj.type];
             T elj = 0, ec = 0;
             const T fs = PairMath<T>::template eval<EN>(dx, dy, dz, qiq * (T)rj.q, ljp, on, k,
@@ -465,23 +523,31 @@ __global__ void __launch_bounds__(256) k_pair(
             ay += dy * fs;
             az += dz * fs;
             if (EN) {
-                e_lj += (double)elj;
-                e_c += (double)ec;
-                vxx += (double)(dx * dx * fs);
-                vyy += (double)(dy * dy * fs);
-                vzz += (double)(dz * dz * fs);
+                a_lj += elj;
+                a_c += ec;
+                a_xx += dx * dx * fs;
+                a_yy += dy * dy * fs;
+                a_zz += dz * dz * fs;
             }
         }
         if ((e & (FLUSH - 1)) == FLUSH - 1) {
-            lx += to_fix((double)ax);
-            ly += to_fix((double)ay);
-            lz += to_fix((double)az);
+            lx += to_fix<T>(ax);
+            ly += to_fix<T>(ay);
+            lz += to_fix<T>(az);
             ax = ay = az = 0;
+            if (EN) {
+                e_lj += (double)a_lj;
+                e_c += (double)a_c;
+                vxx += (double)a_xx;
+                vyy += (double)a_yy;
+                vzz += (double)a_zz;
+                a_lj = a_c = a_xx = a_yy = a_zz = 0;
+            }
         }
     }
-    lx += to_fix((double)ax);
-    ly += to_fix((double)ay);
-    lz += to_fix((double)az);
+    lx += to_fix<T>(ax);
+    ly += to_fix<T>(ay);
+    lz += to_fix<T>(az);
 #pragma unroll
     for (int off = 8; off <= 16; off <<= 1) {
         lx += __shfl_xor_sync(FULL, lx, off);
@@ -500,6 +566,11 @@ __global__ void __launch_bounds__(256) k_pair(
         }
     }
     if (EN) {
+        e_lj += (double)a_lj;
+        e_c += (double)a_c;
+        vxx += (double)a_xx;
+        vyy += (double)a_yy;
+        vzz += (double)a_zz;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             e_lj += __shfl_xor_sync(FULL, e_lj, off);
@@ -519,23 +590,96 @@ __global__ void __launch_bounds__(256) k_pair(
     }
 }
 
-__global__ void k_reduce_energy(int maxcl, const int *__restrict__ ncl_dev,
-                                const double *__restrict__ pe, double *__restrict__ out) {
+// Dynamic pruning: keep the outer-list entries that have at least one unmasked
+// atom pair within r_in = rc + margin at the current positions.  Valid until an
+// atom moves more than margin/2 (checked like the rebuild trigger).
+__global__ void __launch_bounds__(256) k_prune(
+    int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
+    const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
+    const int *__restrict__ jcount, int jcap, double L, float rin2, int *__restrict__ ilist,
+    unsigned long long *__restrict__ imask, int *__restrict__ icount) {
+    __shared__ double s_sh[27 * 3];
+    if (threadIdx.x < 27) {
+        const int im = threadIdx.x;
+        s_sh[im * 3 + 0] = (double)(im % 3 - 1) * L;
+        s_sh[im * 3 + 1] = (double)((im / 3) % 3 - 1) * L;
+        s_sh[im * 3 + 2] = (double)(im / 9 - 1) * L;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int li = lane & 7, lj = lane >> 3;
+    const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (icl >= maxcl || icl >= ncl_dev[0]) return;
+    const AtomRec ri = rec[icl * CL + li];
+    const int n = jcount[icl];
+    const int *row = jlist + (size_t)icl * jcap;
+    const unsigned long long *mrow = jmask + (size_t)icl * jcap;
+    int *orow = ilist + (size_t)icl * jcap;
+    unsigned long long *omrow = imask + (size_t)icl * jcap;
+    int kept = 0;
+    for (int e = 0; e < n; ++e) {
+        const int w = row[e];
+        const unsigned long long m = mrow[e];
+        const unsigned mb = (unsigned)(m >> (li * CL)) & 0xffu;
+        const int jc = w & ((1 << IMG_SHIFT) - 1);
+        const int img = w >> IMG_SHIFT;
+        const double xis = ri.x - s_sh[img * 3 + 0];
+        const double yis = ri.y - s_sh[img * 3 + 1];
+        const double zis = ri.z - s_sh[img * 3 + 2];
+        bool any = false;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int jj = lj + 4 * h;
+            const AtomRec rj = rec[jc * CL + jj];
+            const float dx = (float)(xis - rj.x), dy = (float)(yis - rj.y),
+                        dz = (float)(zis - rj.z);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            any |= ((mb >> jj) & 1u) && r2 < rin2;
+        }
+        if (__any_sync(FULL, any)) {
+            if (lane == 0) {
+                orow[kept] = w;
+                omrow[kept] = m;
+            }
+            ++kept;
+        }
+    }
+    if (lane == 0) icount[icl] = kept;
+}
+
+// Two-stage deterministic column sums: stage 1 = fixed grid of blocks over
+// contiguous ranges (coalesced), stage 2 = one block over the partials.
+constexpr int RED_BLOCKS = 128;
+__global__ void k_red_stage1(int n, int w, const int *__restrict__ ncl_dev,
+                             const double *__restrict__ in, double *__restrict__ part) {
     __shared__ double s[256];
-    const int t = threadIdx.x;
-    const int n = min(maxcl, ncl_dev[0]);
-    const int chunk = (n + 255) / 256;
-    for (int c = 0; c < 5; ++c) {
+    const int nn = ncl_dev ? min(n, ncl_dev[0]) : n;
+    const int chunk = (nn + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * chunk, b1 = min(nn, b0 + chunk);
+    for (int c = 0; c < w; ++c) {
         double acc = 0.0;
-        const int b = t * chunk, e = min(n, b + chunk);
-        for (int i = b; i < e; ++i) acc += pe[(size_t)i * 5 + c];
-        s[t] = acc;
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) acc += in[(size_t)i * w + c];
+        s[threadIdx.x] = acc;
         __syncthreads();
         for (int off = 128; off > 0; off >>= 1) {
-            if (t < off) s[t] += s[t + off];
+            if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
             __syncthreads();
         }
-        if (t == 0) out[c] = 0.5 * s[0];
+        if (threadIdx.x == 0) part[blockIdx.x * w + c] = s[0];
+        __syncthreads();
+    }
+}
+__global__ void k_red_stage2(int nblk, int w, const double *__restrict__ part,
+                             double *__restrict__ out, double scale) {
+    __shared__ double s[256];
+    for (int c = 0; c < w; ++c) {
+        s[threadIdx.x] = (threadIdx.x < nblk) ? part[threadIdx.x * w + c] : 0.0;
+        __syncthreads();
+        for (int off = 128; off > 0; off >>= 1) {
+            if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[c] = scale * s[0];
         __syncthreads();
     }
 }
@@ -572,23 +716,6 @@ __global__ void k_fix_to_float(int n, const long long *__restrict__ fx,
     ff[3 * i + 2] = (float)((double)fz[i] * FIX_INV);
 }
 
-__global__ void k_fix_to_double(int n, const long long *__restrict__ fx,
-                                const long long *__restrict__ fy,
-                                const long long *__restrict__ fz, double *__restrict__ f) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    f[3 * i + 0] = (double)fx[i] * FIX_INV;
-    f[3 * i + 1] = (double)fy[i] * FIX_INV;
-    f[3 * i + 2] = (double)fz[i] * FIX_INV;
-}
-
-// Early-exit wrapper: the build kernels run only when the flag is set, so the
-// whole evaluation can be launched (or graph-captured) without a host round trip.
-__global__ void k_clear_if_flag(const int *__restrict__ flag, int *__restrict__ a, int n) {
-    if (!flag[0]) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = 0;
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -620,6 +747,9 @@ static int sys_alloc(Sys *s) {
     SOFIA_CUDA(ctx, s->red.ensure(sizeof(double) * 8));
     SOFIA_CUDA(ctx, s->flag.ensure(sizeof(int) * 4));
     SOFIA_CUDA(ctx, s->status_local.ensure(sizeof(int) * ST_NSLOTS));
+    for (int d = 0; d < 3; ++d) SOFIA_CUDA(ctx, s->xprn[d].ensure(sizeof(double) * n));
+    SOFIA_CUDA(ctx, s->icount.ensure(sizeof(int) * maxcl));
+    SOFIA_CUDA(ctx, s->part.ensure(sizeof(double) * 8 * RED_BLOCKS));
     return SOFIA_OK;
 }
 
@@ -627,6 +757,8 @@ static int sys_alloc_list(Sys *s) {
     const size_t maxcl = (size_t)s->max_clusters;
     SOFIA_CUDA(s->ctx, s->jlist.ensure(sizeof(int) * maxcl * s->jcap));
     SOFIA_CUDA(s->ctx, s->jmask.ensure(sizeof(unsigned long long) * maxcl * s->jcap));
+    SOFIA_CUDA(s->ctx, s->ilist.ensure(sizeof(int) * maxcl * s->jcap));
+    SOFIA_CUDA(s->ctx, s->imask.ensure(sizeof(unsigned long long) * maxcl * s->jcap));
     return SOFIA_OK;
 }
 
@@ -719,7 +851,7 @@ static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
     k.rcut2 = (float)rcut2;
     k.cut_coulsq = (float)rcut2;
     k.alphad = s->alpha;
-    k.alpha2 = (float)(s->alpha * s->alpha);
+    k.kexp = (float)(-(s->alpha * s->alpha) * 1.4426950408889634);  // -alpha^2 log2(e)
     const double EP = (double)0.3275911f;
     k.EWALD_Pd = EP;
     k.pa = (float)(EP * s->alpha);
@@ -749,23 +881,54 @@ static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
 
 // Launches: displacement check, conditional rebuild, pack, pair kernel.
 // `force_build` rebuilds regardless of the trigger.
+static void sys_prune(Sys *s) {
+    cudaStream_t st = s->ctx->stream;
+    const float rin = (float)(s->rc + s->margin);
+    k_prune<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(
+        s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->jlist.as<int>(),
+        s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap, s->L, rin * rin,
+        s->ilist.as<int>(), s->imask.as<unsigned long long>(), s->icount.as<int>());
+    k_copy3<<<grid_for(s->n, 256), 256, 0, st>>>(s->n, s->x[0].as<double>(), s->x[1].as<double>(),
+                                                 s->x[2].as<double>(), s->xprn[0].as<double>(),
+                                                 s->xprn[1].as<double>(), s->xprn[2].as<double>());
+    s->launches += 2;
+    s->n_prunes++;
+}
+
+static void sys_pack(Sys *s) {
+    cudaStream_t st = s->ctx->stream;
+    const int nslots = s->max_clusters * CL;
+    k_pack<<<grid_for(nslots, 256), 256, 0, st>>>(
+        nslots, s->nclusters.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(),
+        s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
+        s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
+        s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
+        s->rec.as<AtomRec>());
+    s->launches += 1;
+}
+
+// One evaluation: displacement triggers, list rebuild or prune when due, pack,
+// pair kernel on the pruned list, deterministic energy reduction.
 int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     const int n = s->n;
     bool build = force_build || !s->built;
+    bool prune = build;
     if (!build) {
-        const double half = 0.5 * s->skin;
+        const double half = 0.5 * s->skin, phalf = 0.5 * s->margin;
         SOFIA_CUDA(ctx, cudaMemsetAsync(s->flag.p, 0, sizeof(int), st));
         k_disp_check<<<grid_for(n, 256), 256, 0, st>>>(
             n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
-            s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(), s->L,
-            half * half, s->flag.as<int>());
+            s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(),
+            s->xprn[0].as<double>(), s->xprn[1].as<double>(), s->xprn[2].as<double>(), s->L,
+            half * half, phalf * phalf, s->flag.as<int>());
         s->launches += 1;
         int h = 0;
         SOFIA_CUDA(ctx, cudaMemcpyAsync(&h, s->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
-        build = h != 0;
+        build = (h & 1) != 0;
+        prune = h != 0;
     }
     if (s->timing) sys_collect_timers(s);
     for (int attempt = 0; attempt < 4; ++attempt) {
@@ -782,7 +945,8 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
             SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs),
                                             cudaMemcpyDeviceToHost, st));
             SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
-            if (hs[ST_CELLOVER]) return fail(ctx, SOFIA_EINVAL, "an xy column holds more than 2048 atoms%s");
+            if (hs[ST_CELLOVER])
+                return fail(ctx, SOFIA_EINVAL, "an xy column holds more than 2048 atoms%s");
             if (hs[ST_NCLUSTER] > s->jcap) {
                 // redo with a larger row capacity, like the reference's list regrow
                 s->jcap = (int)(hs[ST_NCLUSTER] * 1.2) + 16;
@@ -791,17 +955,11 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
                 continue;
             }
         } else {
-            const int nslots = s->max_clusters * CL;
-            k_pack<<<grid_for(nslots, 256), 256, 0, st>>>(
-                nslots, s->nclusters.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(),
-                s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
-                s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
-                s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(),
-                s->type.as<int>(), s->L, s->rec.as<AtomRec>());
-            s->launches += 1;
+            sys_pack(s);
         }
         break;
     }
+    if (prune) sys_prune(s);
     PairConst k = make_pair_const(s, nullptr);
     const int blocks = grid_for((long)s->max_clusters * 32, 256);
     const size_t smem = sizeof(float4) * (size_t)s->ntypes * s->ntypes;
@@ -809,7 +967,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
               *fz = s->f[2].as<long long>();
 #define SOFIA_PAIR_ARGS                                                                    \
     s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->slot_orig.as<int>(), \
-        s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,  \
+        s->ilist.as<int>(), s->imask.as<unsigned long long>(), s->icount.as<int>(), s->jcap,  \
         s->ljtab.as<float4>(), k, fx, fy, fz, s->energy.as<double>(), ctx->d_status
     if (s->timing) cudaEventRecord(s->ev[2], st);
     if (precision == SOFIA_PREC_FP64) {
@@ -830,9 +988,11 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
     }
     s->launches += 1;
     if (energy) {
-        k_reduce_energy<<<1, 256, 0, st>>>(s->max_clusters, s->nclusters.as<int>(),
-                                           s->energy.as<double>(), s->red.as<double>());
-        s->launches += 1;
+        k_red_stage1<<<RED_BLOCKS, 256, 0, st>>>(s->max_clusters, 5, s->nclusters.as<int>(),
+                                                 s->energy.as<double>(), s->part.as<double>());
+        k_red_stage2<<<1, 256, 0, st>>>(RED_BLOCKS, 5, s->part.as<double>(), s->red.as<double>(),
+                                        0.5);
+        s->launches += 2;
     }
     SOFIA_CUDA(ctx, cudaGetLastError());
     return SOFIA_OK;
@@ -956,6 +1116,11 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
     if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
     for (auto &e : s->ev)
         if (e) cudaEventDestroy(e);
+    for (int d = 0; d < 3; ++d) s->xprn[d].release();
+    s->ilist.release();
+    s->imask.release();
+    s->icount.release();
+    s->part.release();
     sofia::DevBuf *bufs[] = {&s->type, &s->q, &s->invm, &s->mass, &s->specbond, &s->num3bond,
                              &s->ljtab, &s->col_count, &s->col_start, &s->col_fill, &s->col_atoms,
                              &s->col_key, &s->cl_start, &s->slot_orig, &s->rec, &s->bb, &s->jlist,
@@ -1107,9 +1272,16 @@ extern "C" int sofia_system_stats(sofia_system *ss, int64_t *stats, int nstats) 
         for (int i = 0; i < ncl; ++i) entries += jc[i];
         delete[] jc;
     }
-    const int64_t vals[8] = {s->n_builds, ncl, entries, s->jcap, s->ncx, s->max_clusters,
-                             s->ncol_reach, s->launches};
-    for (int i = 0; i < nstats && i < 8; ++i) stats[i] = vals[i];
+    long long inner = 0;
+    if (ncl > 0) {
+        int *jc = new int[ncl];
+        cudaMemcpy(jc, s->icount.p, sizeof(int) * ncl, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < ncl; ++i) inner += jc[i];
+        delete[] jc;
+    }
+    const int64_t vals[10] = {s->n_builds, ncl, entries, s->jcap, s->ncx, s->max_clusters,
+                              s->ncol_reach, s->launches, s->n_prunes, inner};
+    for (int i = 0; i < nstats && i < 10; ++i) stats[i] = vals[i];
     return SOFIA_OK;
 }
 

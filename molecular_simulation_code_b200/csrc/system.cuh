@@ -51,6 +51,10 @@ struct Sys {
     DevBuf red;                         // reduced energies
     DevBuf flag;                        // rebuild flag (int)
     DevBuf stage_pos, stage_ff;
+    // pruned inner list (rc + margin) and the positions it was pruned at
+    DevBuf ilist, imask, icount, xprn[3], part;
+    double margin = 0.6;
+    long long n_prunes = 0;
     int built = 0;
     long long n_builds = 0;
     long long launches = 0;             // kernels launched by this system (all paths)
