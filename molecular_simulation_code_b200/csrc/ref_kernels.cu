@@ -329,27 +329,48 @@ __global__ void __launch_bounds__(256) k_force_ref(
     }
 }
 
-// Fixed-order reduction of per-item partials: pe[n][w] -> out[w].  One block,
-// each thread sums a contiguous chunk, then a shared-memory tree.
-__global__ void k_reduce_cols(int n, int w, const double *__restrict__ pe,
-                              double *__restrict__ out, double scale) {
+// Fixed-order reduction of per-item partials pe[n][w] -> out[w]: a fixed grid
+// of blocks sums contiguous ranges (coalesced), then one block sums the
+// partials, so the result does not depend on scheduling.
+constexpr int RED_BLOCKS = 128;
+__global__ void k_red1(int n, int w, const double *__restrict__ pe, double *__restrict__ part) {
     __shared__ double s[256];
-    const int t = threadIdx.x;
-    const int chunk = (n + 255) / 256;
+    const int chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
     for (int c = 0; c < w; ++c) {
         double acc = 0.0;
-        const int b = t * chunk;
-        const int e = min(n, b + chunk);
-        for (int k = b; k < e; ++k) acc += pe[(size_t)k * w + c];
-        s[t] = acc;
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) acc += pe[(size_t)i * w + c];
+        s[threadIdx.x] = acc;
         __syncthreads();
         for (int off = 128; off > 0; off >>= 1) {
-            if (t < off) s[t] += s[t + off];
+            if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
             __syncthreads();
         }
-        if (t == 0) out[c] = scale * s[0];
+        if (threadIdx.x == 0) part[blockIdx.x * w + c] = s[0];
         __syncthreads();
     }
+}
+__global__ void k_red2(int w, const double *__restrict__ part, double *__restrict__ out,
+                       double scale) {
+    __shared__ double s[256];
+    for (int c = 0; c < w; ++c) {
+        s[threadIdx.x] = (threadIdx.x < RED_BLOCKS) ? part[threadIdx.x * w + c] : 0.0;
+        __syncthreads();
+        for (int off = 128; off > 0; off >>= 1) {
+            if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[c] = scale * s[0];
+        __syncthreads();
+    }
+}
+
+// pe[n][w] -> out[w] (out = red_out, partials after it)
+inline void reduce_cols(cudaStream_t st, int n, int w, const double *pe, double *out,
+                        double scale) {
+    double *part = out + 16;
+    k_red1<<<RED_BLOCKS, 256, 0, st>>>(n, w, pe, part);
+    k_red2<<<1, 256, 0, st>>>(w, part, out, scale);
 }
 
 // Minimum image of mod_minimg.f90:5-15: d - box*nint(ibox*d), box*nint() in real*4.
@@ -774,15 +795,14 @@ extern "C" int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ai
     sofia::OutArg o_ff;
     if ((rc = sofia::stage_out(ctx, ff, sizeof(float) * 3 * (size_t)np, 8, &o_ff))) return rc;
     SOFIA_CUDA(ctx, ctx->pe_atom.ensure(sizeof(double) * 5 * (size_t)np));
-    SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * 16));
+    SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * (16 + 8 * RED_BLOCKS)));
     DsfConst k = make_const(box, ibox, rcut2, cut_coulsq, alpha, e_shift, f_shift, coulpre);
     const long threads = (long)np * 32;
     k_force_ref<<<sofia::grid_for(threads, 256), 256, 0, st>>>(
         np, (const float4 *)dpos, (const float *)dq, (const float *)d1, (const float *)d2,
         (const float *)d3, (const float *)d4, ntypes, (const int *)dl, (const int *)dn,
         neigh_alloc, k, (float *)o_ff.dev, ctx->pe_atom.as<double>());
-    k_reduce_cols<<<1, 256, 0, st>>>(np, 5, ctx->pe_atom.as<double>(), ctx->red_out.as<double>(),
-                                     0.5);
+    reduce_cols(st, np, 5, ctx->pe_atom.as<double>(), ctx->red_out.as<double>(), 0.5);
     SOFIA_CUDA(ctx, cudaGetLastError());
     if ((rc = sofia::finish_out(ctx, o_ff))) return rc;
     SOFIA_CUDA(ctx, cudaMemcpyAsync(ctx->h_red, ctx->red_out.p, sizeof(double) * 5,
@@ -825,7 +845,7 @@ extern "C" int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
     if ((rc = sofia::stage_out(ctx, ffh, sizeof(float) * 3 * (size_t)np, 5, &o_ff, true))) return rc;
     SOFIA_CUDA(ctx, ctx->acc64.ensure(sizeof(double) * 3 * (size_t)np));
     SOFIA_CUDA(ctx, ctx->pe_atom.ensure(sizeof(double) * 3 * (size_t)ndihed));
-    SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * 16));
+    SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * (16 + 8 * RED_BLOCKS)));
     SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->acc64.p, 0, sizeof(double) * 3 * (size_t)np, st));
     SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
     DsfConst k = make_const(box, ibox, rcut2, cut_coulsq, alpha, e_shift, f_shift, coulpre);
@@ -833,8 +853,7 @@ extern "C" int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
         ndihed, np, (const float4 *)dpos, (const float *)dq, ntypes, (const double *)dlj,
         (const int *)ddl, (const double *)ddc, ndihedtypes, k, box, ibox,
         ctx->acc64.as<double>(), ctx->pe_atom.as<double>(), ctx->d_status);
-    k_reduce_cols<<<1, 256, 0, st>>>(ndihed, 3, ctx->pe_atom.as<double>(),
-                                     ctx->red_out.as<double>(), 1.0);
+    reduce_cols(st, ndihed, 3, ctx->pe_atom.as<double>(), ctx->red_out.as<double>(), 1.0);
     k_add_to_float<<<sofia::grid_for(3L * np, 256), 256, 0, st>>>(3L * np, ctx->acc64.as<double>(),
                                                                   (float *)o_ff.dev);
     SOFIA_CUDA(ctx, cudaGetLastError());
@@ -872,7 +891,7 @@ extern "C" int sofia_correct_1x(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
     if ((rc = sofia::stage_out(ctx, ffc, sizeof(float) * 3 * (size_t)np, 3, &o_ff, true))) return rc;
     SOFIA_CUDA(ctx, ctx->acc64.ensure(sizeof(double) * 3 * (size_t)np));
     SOFIA_CUDA(ctx, ctx->pe_atom.ensure(sizeof(double) * 4 * (size_t)npairs));
-    SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * 16));
+    SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * (16 + 8 * RED_BLOCKS)));
     SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->acc64.p, 0, sizeof(double) * 3 * (size_t)np, st));
     DsfConst k = make_const(box, ibox, 0.0, cut_coulsq, 0.0, 0.0, 0.0, coulpre);
     SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
@@ -880,8 +899,7 @@ extern "C" int sofia_correct_1x(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
         npairs, np, (const float4 *)dpos, (const float *)dq, (const int *)dlist, stride, col_a,
         col_b, k, gewald, fudge, coulpre, ctx->acc64.as<double>(), ctx->pe_atom.as<double>(),
         ctx->d_status);
-    k_reduce_cols<<<1, 256, 0, st>>>(npairs, 4, ctx->pe_atom.as<double>(),
-                                     ctx->red_out.as<double>(), 1.0);
+    reduce_cols(st, npairs, 4, ctx->pe_atom.as<double>(), ctx->red_out.as<double>(), 1.0);
     k_add_to_float<<<sofia::grid_for(3L * np, 256), 256, 0, st>>>(3L * np, ctx->acc64.as<double>(),
                                                                   (float *)o_ff.dev);
     SOFIA_CUDA(ctx, cudaGetLastError());
