@@ -202,10 +202,13 @@ int sofia_force_nonbond_mixed(sofia_system *sys, const sofia_ainfo *position, fl
 /* Resident state: x, v as [np*3] doubles (host or device). */
 int sofia_system_set_state(sofia_system *sys, const double *x, const double *v);
 int sofia_system_get_state(sofia_system *sys, double *x, double *v, double *f);
-/* Forces on the resident positions with the given precision; rebuild != 0
- * forces a list rebuild; energies[5] (may be NULL) = potential, e_coul, virial. */
-int sofia_system_compute_forces(sofia_system *sys, int precision, int rebuild,
-                                double *energies);
+/* Forces on the resident positions with the given precision.  flags:
+ * SOFIA_EVAL_REBUILD forces a list rebuild, SOFIA_EVAL_VIRIAL adds the
+ * diagonal virial.  energies[5] (may be NULL; energies are computed only when
+ * given) = potential, e_coul, virial x, y, z. */
+#define SOFIA_EVAL_REBUILD 1
+#define SOFIA_EVAL_VIRIAL 2
+int sofia_system_compute_forces(sofia_system *sys, int precision, int flags, double *energies);
 /* stats[0..9]: list builds, clusters, list entries, row capacity, columns per
  * side, cluster capacity, column reach, kernels launched so far, prunes,
  * entries of the pruned (rc + margin) list. */

@@ -158,7 +158,7 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
                        const double *__restrict__ rz, const double *__restrict__ ix,
                        const double *__restrict__ iy, const double *__restrict__ iz,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
-                       AtomRec *__restrict__ rec) {
+                       AtomRec *__restrict__ rec, float4 *__restrict__ recf) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nslots || s >= ncl_dev[0] * CL) return;
     const int o = slot_orig[s];
@@ -182,6 +182,7 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
         r.type = 0;
     }
     rec[s] = r;
+    recf[s] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.0f);
 }
 
 __global__ void k_bbox(int maxcl, const int *__restrict__ ncl_dev,
@@ -466,8 +467,11 @@ __device__ __forceinline__ long long to_fix<double>(double v) {
 }
 
 // Pair kernel: one warp per i-cluster; lane = li (i atom, 0..7) + 8*lj (j quarter,
-// each lane takes j atoms lj and lj+4 of every j-cluster).
-template <typename T, bool EN>
+// each lane takes j atoms lj and lj+4 of every j-cluster).  List rows are read 32
+// entries at a time with coalesced loads and broadcast to the warp by shuffles;
+// the j atoms are read with 8-lane broadcast loads.  EN adds the LJ and Coulomb
+// energies, VIR the diagonal virial.
+template <typename T, bool EN, bool VIR>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
     int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ slot_orig, const int *__restrict__ jlist,
@@ -499,49 +503,59 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
     T a_lj = 0, a_c = 0, a_xx = 0, a_yy = 0, a_zz = 0;
     long long lx = 0, ly = 0, lz = 0;
     double e_lj = 0.0, e_c = 0.0, vxx = 0.0, vyy = 0.0, vzz = 0.0;
-    for (int e = 0; e < n; ++e) {
-        const int w = row[e];
-        const unsigned mb = (unsigned)(mrow[e] >> (li * CL)) & 0xffu;
-        const int jc = w & ((1 << IMG_SHIFT) - 1);
-        const int img = w >> IMG_SHIFT;
-        const double xis = ri.x - s_sh[img * 3 + 0];
-        const double yis = ri.y - s_sh[img * 3 + 1];
-        const double zis = ri.z - s_sh[img * 3 + 2];
+    for (int base = 0; base < n; base += 32) {
+        const int cnt = min(32, n - base);
+        const int myw = (lane < cnt) ? row[base + lane] : 0;
+        const unsigned long long mym = (lane < cnt) ? mrow[base + lane] : 0ull;
+        for (int e = 0; e < cnt; ++e) {
+            const int w = __shfl_sync(FULL, myw, e);
+            const unsigned mb = (unsigned)(__shfl_sync(FULL, mym, e) >> (li * CL)) & 0xffu;
+            const int jc = w & ((1 << IMG_SHIFT) - 1);
+            const int img = w >> IMG_SHIFT;
+            const double xis = ri.x - s_sh[img * 3 + 0];
+            const double yis = ri.y - s_sh[img * 3 + 1];
+            const double zis = ri.z - s_sh[img * 3 + 2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int jj = lj + 4 * h;
-            const AtomRec rj = rec[jc * CL + jj];
-            const T dx = (T)(xis - rj.x);
-            const T dy = (T)(yis - rj.y);
-            const T dz = (T)(zis - rj.z);
-            const bool on = (mb >> jj) & 1u;
-            const float4 ljp = s_lj[ti + rj.type];
-            T elj = 0, ec = 0;
-            const T fs = PairMath<T>::template eval<EN>(dx, dy, dz, qiq * (T)rj.q, ljp, on, k,
-                                                        elj, ec);
-            ax += dx * fs;
-            ay += dy * fs;
-            az += dz * fs;
-            if (EN) {
-                a_lj += elj;
-                a_c += ec;
-                a_xx += dx * dx * fs;
-                a_yy += dy * dy * fs;
-                a_zz += dz * dz * fs;
+            for (int h = 0; h < 2; ++h) {
+                const int jj = lj + 4 * h;
+                const AtomRec rj = rec[jc * CL + jj];
+                const T dx = (T)(xis - rj.x);
+                const T dy = (T)(yis - rj.y);
+                const T dz = (T)(zis - rj.z);
+                const bool on = (mb >> jj) & 1u;
+                const float4 ljp = s_lj[ti + rj.type];
+                T elj = 0, ec = 0;
+                const T fs = PairMath<T>::template eval<EN>(dx, dy, dz, qiq * (T)rj.q, ljp, on,
+                                                            k, elj, ec);
+                ax += dx * fs;
+                ay += dy * fs;
+                az += dz * fs;
+                if (EN) {
+                    a_lj += elj;
+                    a_c += ec;
+                }
+                if (VIR) {
+                    a_xx += dx * dx * fs;
+                    a_yy += dy * dy * fs;
+                    a_zz += dz * dz * fs;
+                }
             }
-        }
-        if ((e & (FLUSH - 1)) == FLUSH - 1) {
-            lx += to_fix<T>(ax);
-            ly += to_fix<T>(ay);
-            lz += to_fix<T>(az);
-            ax = ay = az = 0;
-            if (EN) {
-                e_lj += (double)a_lj;
-                e_c += (double)a_c;
-                vxx += (double)a_xx;
-                vyy += (double)a_yy;
-                vzz += (double)a_zz;
-                a_lj = a_c = a_xx = a_yy = a_zz = 0;
+            if (((base + e) & (FLUSH - 1)) == FLUSH - 1) {
+                lx += to_fix<T>(ax);
+                ly += to_fix<T>(ay);
+                lz += to_fix<T>(az);
+                ax = ay = az = 0;
+                if (EN) {
+                    e_lj += (double)a_lj;
+                    e_c += (double)a_c;
+                    a_lj = a_c = 0;
+                }
+                if (VIR) {
+                    vxx += (double)a_xx;
+                    vyy += (double)a_yy;
+                    vzz += (double)a_zz;
+                    a_xx = a_yy = a_zz = 0;
+                }
             }
         }
     }
@@ -565,7 +579,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
                 atomicAdd(&status[ST_FIXED_OVF], 1);
         }
     }
-    if (EN) {
+    if (EN || VIR) {
         e_lj += (double)a_lj;
         e_c += (double)a_c;
         vxx += (double)a_xx;
@@ -592,57 +606,58 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
 
 // Dynamic pruning: keep the outer-list entries that have at least one unmasked
 // atom pair within r_in = rc + margin at the current positions.  Valid until an
-// atom moves more than margin/2 (checked like the rebuild trigger).
+// atom moves more than margin/2 (checked like the rebuild trigger).  Distances
+// here only select entries, so FP32 copies of the positions suffice (the
+// squared radius carries a 1e-3 A safety margin).
 __global__ void __launch_bounds__(256) k_prune(
-    int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
+    int maxcl, const int *__restrict__ ncl_dev, const float4 *__restrict__ recf,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
-    const int *__restrict__ jcount, int jcap, double L, float rin2, int *__restrict__ ilist,
+    const int *__restrict__ jcount, int jcap, float L, float rin2, int *__restrict__ ilist,
     unsigned long long *__restrict__ imask, int *__restrict__ icount) {
-    __shared__ double s_sh[27 * 3];
-    if (threadIdx.x < 27) {
-        const int im = threadIdx.x;
-        s_sh[im * 3 + 0] = (double)(im % 3 - 1) * L;
-        s_sh[im * 3 + 1] = (double)((im / 3) % 3 - 1) * L;
-        s_sh[im * 3 + 2] = (double)(im / 9 - 1) * L;
-    }
-    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int li = lane & 7, lj = lane >> 3;
     const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (icl >= maxcl || icl >= ncl_dev[0]) return;
-    const AtomRec ri = rec[icl * CL + li];
+    const float4 pi = recf[icl * CL + li];
     const int n = jcount[icl];
     const int *row = jlist + (size_t)icl * jcap;
     const unsigned long long *mrow = jmask + (size_t)icl * jcap;
     int *orow = ilist + (size_t)icl * jcap;
     unsigned long long *omrow = imask + (size_t)icl * jcap;
     int kept = 0;
-    for (int e = 0; e < n; ++e) {
-        const int w = row[e];
-        const unsigned long long m = mrow[e];
-        const unsigned mb = (unsigned)(m >> (li * CL)) & 0xffu;
-        const int jc = w & ((1 << IMG_SHIFT) - 1);
-        const int img = w >> IMG_SHIFT;
-        const double xis = ri.x - s_sh[img * 3 + 0];
-        const double yis = ri.y - s_sh[img * 3 + 1];
-        const double zis = ri.z - s_sh[img * 3 + 2];
-        bool any = false;
+    for (int base = 0; base < n; base += 32) {
+        const int cnt = min(32, n - base);
+        const int myw = (lane < cnt) ? row[base + lane] : 0;
+        const unsigned long long mym = (lane < cnt) ? mrow[base + lane] : 0ull;
+        unsigned keepbits = 0;
+        for (int e = 0; e < cnt; ++e) {
+            const int w = __shfl_sync(FULL, myw, e);
+            const unsigned long long m = __shfl_sync(FULL, mym, e);
+            const unsigned mb = (unsigned)(m >> (li * CL)) & 0xffu;
+            const int jc = w & ((1 << IMG_SHIFT) - 1);
+            const int img = w >> IMG_SHIFT;
+            const float sx = (float)(img % 3 - 1) * L, sy = (float)((img / 3) % 3 - 1) * L,
+                        sz = (float)(img / 9 - 1) * L;
+            bool any = false;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int jj = lj + 4 * h;
-            const AtomRec rj = rec[jc * CL + jj];
-            const float dx = (float)(xis - rj.x), dy = (float)(yis - rj.y),
-                        dz = (float)(zis - rj.z);
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            any |= ((mb >> jj) & 1u) && r2 < rin2;
-        }
-        if (__any_sync(FULL, any)) {
-            if (lane == 0) {
-                orow[kept] = w;
-                omrow[kept] = m;
+            for (int h = 0; h < 2; ++h) {
+                const int jj = lj + 4 * h;
+                const float4 pj = recf[jc * CL + jj];
+                const float dx = pi.x - (pj.x + sx), dy = pi.y - (pj.y + sy),
+                            dz = pi.z - (pj.z + sz);
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                any |= ((mb >> jj) & 1u) && r2 < rin2;
             }
-            ++kept;
+            if (__any_sync(FULL, any)) keepbits |= 1u << e;
         }
+        // compact the kept entries of this batch in order
+        const bool mine = (keepbits >> lane) & 1u;
+        const int at = kept + __popc(keepbits & ((1u << lane) - 1u));
+        if (mine) {
+            orow[at] = myw;
+            omrow[at] = mym;
+        }
+        kept += __popc(keepbits);
     }
     if (lane == 0) icount[icl] = kept;
 }
@@ -740,6 +755,7 @@ static int sys_alloc(Sys *s) {
     const size_t maxcl = (size_t)s->max_clusters;
     SOFIA_CUDA(ctx, s->slot_orig.ensure(sizeof(int) * maxcl * CL + sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, s->rec.ensure(sizeof(AtomRec) * maxcl * CL));
+    SOFIA_CUDA(ctx, s->recf.ensure(sizeof(float4) * maxcl * CL));
     SOFIA_CUDA(ctx, s->bb.ensure(sizeof(float4) * 2 * maxcl));
     SOFIA_CUDA(ctx, s->jcount.ensure(sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, s->nclusters.ensure(sizeof(int) * 4));
@@ -794,7 +810,7 @@ static int sys_build(Sys *s) {
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
         s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
-        s->rec.as<AtomRec>());
+        s->rec.as<AtomRec>(), s->recf.as<float4>());
     k_bbox<<<grid_for(s->max_clusters, 128), 128, 0, st>>>(
         s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->slot_orig.as<int>(),
         s->bb.as<float4>());
@@ -884,9 +900,10 @@ static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
 static void sys_prune(Sys *s) {
     cudaStream_t st = s->ctx->stream;
     const float rin = (float)(s->rc + s->margin);
+    const float rin2 = rin * rin + 1e-3f;
     k_prune<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(
-        s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->jlist.as<int>(),
-        s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap, s->L, rin * rin,
+        s->max_clusters, s->nclusters.as<int>(), s->recf.as<float4>(), s->jlist.as<int>(),
+        s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap, (float)s->L, rin2,
         s->ilist.as<int>(), s->imask.as<unsigned long long>(), s->icount.as<int>());
     k_copy3<<<grid_for(s->n, 256), 256, 0, st>>>(s->n, s->x[0].as<double>(), s->x[1].as<double>(),
                                                  s->x[2].as<double>(), s->xprn[0].as<double>(),
@@ -903,13 +920,13 @@ static void sys_pack(Sys *s) {
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
         s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
-        s->rec.as<AtomRec>());
+        s->rec.as<AtomRec>(), s->recf.as<float4>());
     s->launches += 1;
 }
 
 // One evaluation: displacement triggers, list rebuild or prune when due, pack,
 // pair kernel on the pruned list, deterministic energy reduction.
-int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
+int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) {
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     const int n = s->n;
@@ -971,15 +988,19 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
         s->ljtab.as<float4>(), k, fx, fy, fz, s->energy.as<double>(), ctx->d_status
     if (s->timing) cudaEventRecord(s->ev[2], st);
     if (precision == SOFIA_PREC_FP64) {
-        if (energy)
-            k_pair<double, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+        if (virial)
+            k_pair<double, true, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+        else if (energy)
+            k_pair<double, true, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
         else
-            k_pair<double, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            k_pair<double, false, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
     } else {
-        if (energy)
-            k_pair<float, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+        if (virial)
+            k_pair<float, true, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+        else if (energy)
+            k_pair<float, true, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
         else
-            k_pair<float, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            k_pair<float, false, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
     }
 #undef SOFIA_PAIR_ARGS
     if (s->timing) {
@@ -987,7 +1008,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool force_build) {
         s->pending_pair = 1;
     }
     s->launches += 1;
-    if (energy) {
+    if (energy || virial) {
         k_red_stage1<<<RED_BLOCKS, 256, 0, st>>>(s->max_clusters, 5, s->nclusters.as<int>(),
                                                  s->energy.as<double>(), s->part.as<double>());
         k_red_stage2<<<1, 256, 0, st>>>(RED_BLOCKS, 5, s->part.as<double>(), s->red.as<double>(),
@@ -1119,6 +1140,7 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
     for (int d = 0; d < 3; ++d) s->xprn[d].release();
     s->ilist.release();
     s->imask.release();
+    s->recf.release();
     s->icount.release();
     s->part.release();
     sofia::DevBuf *bufs[] = {&s->type, &s->q, &s->invm, &s->mass, &s->specbond, &s->num3bond,
@@ -1159,7 +1181,7 @@ extern "C" int sofia_force_nonbond_mixed(sofia_system *ss, const sofia_ainfo *po
     sofia::k_aos_to_soa<<<sofia::grid_for(n, 256), 256, 0, st>>>(
         n, (const float4 *)dpos, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>());
     const bool want_e = potential || e_coul || virial_diag3;
-    int rc = sofia::sys_eval(s, s->precision, want_e, false);
+    int rc = sofia::sys_eval(s, s->precision, want_e, virial_diag3 != nullptr, false);
     if (rc) return rc;
     float *dff = ff;
     const bool host_ff = !sofia::is_device_ptr(ff);
@@ -1242,13 +1264,15 @@ extern "C" int sofia_system_get_state(sofia_system *ss, double *x, double *v, do
 }
 
 // Forces on the resident positions; energies[5] = potential, e_coul, virial x,y,z.
-extern "C" int sofia_system_compute_forces(sofia_system *ss, int precision, int rebuild,
+extern "C" int sofia_system_compute_forces(sofia_system *ss, int precision, int flags,
                                            double *energies) {
     if (!ss) return SOFIA_EINVAL;
     Sys *s = &ss->s;
     sofia_nb_ctx *ctx = s->ctx;
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
-    int rc = sofia::sys_eval(s, precision, energies != nullptr, rebuild != 0);
+    int rc = sofia::sys_eval(s, precision, energies != nullptr,
+                             energies != nullptr && (flags & SOFIA_EVAL_VIRIAL),
+                             (flags & SOFIA_EVAL_REBUILD) != 0);
     if (rc) return rc;
     if (energies) {
         SOFIA_CUDA(ctx, cudaMemcpyAsync(energies, s->red.p, sizeof(double) * 5,

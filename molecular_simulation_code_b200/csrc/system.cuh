@@ -45,7 +45,7 @@ struct Sys {
     DevBuf ljtab;                      // float4 {lj1,lj2,lj3,lj4} per type pair
     // cluster structures
     DevBuf col_count, col_start, col_fill, col_atoms, col_key, cl_start;
-    DevBuf slot_orig, rec, bb, jlist, jmask, jcount, nclusters;
+    DevBuf slot_orig, rec, recf, bb, jlist, jmask, jcount, nclusters;
     DevBuf status_local;
     DevBuf energy;                      // per-i-cluster energy partials (pot, ecoul, vir x,y,z)
     DevBuf red;                         // reduced energies

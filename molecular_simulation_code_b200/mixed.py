@@ -81,11 +81,12 @@ class System:
         self.ctx.check(self.ctx._lib.sofia_system_get_state(self.handle, ptr(x), ptr(v), ptr(f)))
         return x, v, f
 
-    def compute(self, precision: int | None = None, rebuild: bool = False, energy: bool = True):
+    def compute(self, precision: int | None = None, rebuild: bool = False, energy: bool = True,
+                virial: bool = True):
         e = np.zeros(5) if energy else None
         p = self.precision if precision is None else precision
-        self.ctx.check(self.ctx._lib.sofia_system_compute_forces(self.handle, p, int(rebuild),
-                                                                 ptr(e)))
+        flags = (1 if rebuild else 0) | (2 if virial else 0)
+        self.ctx.check(self.ctx._lib.sofia_system_compute_forces(self.handle, p, flags, ptr(e)))
         return e
 
     def stats(self) -> dict:
