@@ -34,6 +34,7 @@ extern "C" {
 #define SOFIA_ECUDA 3     /* CUDA runtime error */
 #define SOFIA_ETIMEOUT 4  /* a bounded device wait gave up */
 #define SOFIA_ESTATE 5    /* device state check failed (non-finite values, SHAKE failure, ...) */
+#define SOFIA_ETOOBIG 6   /* size beyond the fixed capacity of an allocation-free call */
 
 /* type(ainfo) of Source/global.f90:82-85: {real*4 x,y,z; integer type}, 16 bytes. */
 typedef struct {
@@ -112,6 +113,40 @@ int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *positi
                             float box, float ibox, double rcut2, double cut_coulsq, double alpha,
                             double e_shift, double f_shift, float coulpre, float *ff,
                             double *potential, double *e_coul, double *virial_diag3);
+
+/*
+ * Allocation-free form of sofia_force_nonbond_dsf.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot allocate device
+ * memory when they need forces: work being captured into a CUDA graph (where
+ * cudaMalloc is not allowed), hosts that give the library a fixed device arena
+ * or enforce a memory budget from outside, and drivers that keep every device
+ * array themselves.  It needs no context and allocates nothing: no cudaMalloc,
+ * no cudaFree, no allocating library routine.
+ *   - stream: the caller's cudaStream_t (NULL = the legacy default stream).
+ *   - position, q, lj1..lj4, nlist, numneigh and ff must be device memory
+ *     (host pointers are rejected with SOFIA_EINVAL, because copying them would
+ *     need a device buffer); potential, e_coul, virial_diag3 are host scalars
+ *     and may be NULL.  Meaning of every argument as in sofia_force_nonbond_dsf.
+ *   - np may be at most SOFIA_NOALLOC_MAX_ATOMS; larger systems get
+ *     SOFIA_ETOOBIG.  The per-atom energy partials live in a fixed array of
+ *     (5*SOFIA_NOALLOC_MAX_ATOMS + 1040) doubles (about 2.6 MB) compiled into
+ *     the library, which every GPU that loads the library holds until exit.
+ *   - The first call on a device looks up that array's device address and
+ *     caches it; make this first call before any stream capture begins.
+ *   - All calls share the one array: calls that overlap on the GPU (on
+ *     different streams, threads or processes sharing the context) race and
+ *     corrupt each other's energies; order them on one stream or serialise.
+ *   - Returns after the energies are on the host (the stream is synchronised).
+ */
+#define SOFIA_NOALLOC_MAX_ATOMS 65536
+int sofia_force_nonbond_dsf_noalloc(void *stream, int np, const sofia_ainfo *position,
+                                    const float *q, const float *lj1, const float *lj2,
+                                    const float *lj3, const float *lj4, int ntypes,
+                                    const int32_t *nlist, const int32_t *numneigh,
+                                    int32_t neigh_alloc, float box, float ibox, double rcut2,
+                                    double cut_coulsq, double alpha, double e_shift,
+                                    double f_shift, float coulpre, float *ff, double *potential,
+                                    double *e_coul, double *virial_diag3);
 
 /*
  * dihedral_opls_DSF (Source/mod_force_dihed.f90:816-1092): OPLS torsion with

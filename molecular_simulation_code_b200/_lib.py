@@ -17,6 +17,8 @@ SOFIA_EINVAL = 2
 SOFIA_ECUDA = 3
 SOFIA_ETIMEOUT = 4
 SOFIA_ESTATE = 5
+SOFIA_ETOOBIG = 6
+SOFIA_NOALLOC_MAX_ATOMS = 65536
 
 
 class SofiaError(RuntimeError):
@@ -63,6 +65,9 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_force_nonbond_dsf": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, C.c_int32, _F,
                                      _F, _D, _D, _D, _D, _D, _F, _P, C.POINTER(_D),
                                      C.POINTER(_D), _P]),
+    "sofia_force_nonbond_dsf_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P,
+                                             C.c_int32, _F, _F, _D, _D, _D, _D, _D, _F, _P,
+                                             C.POINTER(_D), C.POINTER(_D), _P]),
     "sofia_pair14_dsf": (_I, [_P, _I, _P, _P, _I, _P, _I, _P, _P, _I, _F, _F, _D, _D, _D, _D, _D, _F,
                               _P, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
     "sofia_correct_1x": (_I, [_P, _I, _P, _P, _I, _P, _I, _I, _I, _F, _F, _D, _D, _D, _F, _P,

@@ -11,6 +11,7 @@
 // candidate sweep, neighbour rows of neigh_alloc int32 per atom (Fortran
 // nlist(neigh_alloc*(i-1)+j)).
 #include <climits>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -914,6 +915,101 @@ extern "C" int sofia_correct_1x(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
         virial3[0] += ctx->h_red[1];
         virial3[1] += ctx->h_red[2];
         virial3[2] += ctx->h_red[3];
+    }
+    return SOFIA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of sofia_force_nonbond_dsf.
+//
+// Some callers cannot allocate device memory at the time they need forces:
+// code running while a CUDA stream is being captured into a graph (cudaMalloc
+// is not capturable), hosts that hand the library a fixed device arena or run
+// under a memory budget enforced outside the library, and Fortran drivers that
+// keep every device array in their own module and never expect a library to
+// allocate behind their back.  For them this entry point takes only caller-owned
+// device buffers and keeps its per-atom energy partials in a fixed array that
+// lives in the library image.
+//
+// The scratch array below is defined at file scope in device memory, so every
+// GPU that loads this library holds it until the process exits.  Its host-side
+// name is only a stand-in for the device symbol: host code must never pass it
+// to a kernel; the device address is looked up once per device with
+// cudaGetSymbolAddress and cached.
+namespace {
+
+constexpr size_t NOALLOC_DOUBLES = (size_t)SOFIA_NOALLOC_MAX_ATOMS * 5 + 16 + 8 * RED_BLOCKS;
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Device address of the scratch array on the current device (looked up once).
+int noalloc_scratch(double **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        cudaGetLastError();
+        return SOFIA_ECUDA;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return SOFIA_ECUDA;
+        }
+        g_noalloc_addr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return SOFIA_OK;
+}
+
+}  // namespace
+
+extern "C" int sofia_force_nonbond_dsf_noalloc(
+    void *stream, int np, const sofia_ainfo *position, const float *q, const float *lj1,
+    const float *lj2, const float *lj3, const float *lj4, int ntypes, const int32_t *nlist,
+    const int32_t *numneigh, int32_t neigh_alloc, float box, float ibox, double rcut2,
+    double cut_coulsq, double alpha, double e_shift, double f_shift, float coulpre, float *ff,
+    double *potential, double *e_coul, double *virial_diag3) {
+    if (np <= 0 || ntypes <= 0 || neigh_alloc <= 0 || !position || !q || !lj1 || !lj2 || !lj3 ||
+        !lj4 || !nlist || !numneigh || !ff)
+        return SOFIA_EINVAL;
+    if (np > SOFIA_NOALLOC_MAX_ATOMS) return SOFIA_ETOOBIG;
+    // every array must already be in device memory: staging would need an allocation
+    const void *ptrs[] = {position, q, lj1, lj2, lj3, lj4, nlist, numneigh, ff};
+    for (const void *p : ptrs)
+        if (!sofia::is_device_ptr(p)) return SOFIA_EINVAL;
+    double *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double *pe = scratch;
+    double *out = scratch + (size_t)SOFIA_NOALLOC_MAX_ATOMS * 5;
+    // every scratch element this call reads is first written by this call
+    // (k_force_ref fills pe[0..5*np), the reduction fills its partials and out),
+    // so nothing needs clearing between calls
+    DsfConst k = make_const(box, ibox, rcut2, cut_coulsq, alpha, e_shift, f_shift, coulpre);
+    const long threads = (long)np * 32;
+    k_force_ref<<<sofia::grid_for(threads, 256), 256, 0, st>>>(
+        np, (const float4 *)position, q, lj1, lj2, lj3, lj4, ntypes, nlist, numneigh, neigh_alloc,
+        k, ff, pe);
+    reduce_cols(st, np, 5, pe, out, 0.5);
+    double h[5];
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return SOFIA_ECUDA;
+    }
+    if (potential) *potential = h[0];
+    if (e_coul) *e_coul = h[1];
+    if (virial_diag3) {
+        virial_diag3[0] = h[2];
+        virial_diag3[1] = h[3];
+        virial_diag3[2] = h[4];
     }
     return SOFIA_OK;
 }
