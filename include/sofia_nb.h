@@ -255,6 +255,59 @@ int sofia_system_drift(sofia_system *sys, double dt, int nsteps);
  * launches}; enable != 0 keeps timing on. */
 int sofia_system_timers(sofia_system *sys, int enable, double *timers);
 
+/* ------------------------------------------------------------------------ */
+/*
+ * Device-resident MD around the production path (residency kernels): velocity
+ * Verlet (Source/mod_ensemble.f90:11-87), force-form Langevin
+ * (Source/mod_langevin.f90:15-43; counter-based Philox4x32-10 noise keyed by
+ * seed, atom and step instead of the reference's clock-seeded MT19937),
+ * SHAKE (Source/mod_shake.f90:8-913), harmonic bonds and angles
+ * (Source/mod_force_bond.f90:6-75, Source/mod_force_angle.f90:10-122), OPLS
+ * torsions with their 0.5-scaled DSF/LJ 1-4 pairs
+ * (Source/mod_force_dihed.f90:816-1092).  Step order of the reference loop
+ * (Source/mod_integrate.f90:270-298).  Lists are 1-based like the reference's
+ * bondlist(3,:), anglelist(4,:), dihedlist(5,:), shakeatom.
+ */
+#define SOFIA_TERM_BOND 1
+#define SOFIA_TERM_ANGLE 2
+#define SOFIA_TERM_TORSION 4
+#define SOFIA_TERM_PAIR14 8
+#define SOFIA_MD_NE 12 /* lj, coul, self, bond, angle, torsion, coul14, lj14, kinetic, total, T(K), step */
+
+typedef struct {
+    double dt;          /* fs */
+    double temperature; /* K (Langevin bath) */
+    double gamma;       /* Langevin friction, 1/fs (0 = NVE) */
+    uint64_t seed;      /* Langevin noise stream */
+    int terms;          /* SOFIA_TERM_* bitmask */
+    int nbond;
+    const int32_t *bonds;      /* [nbond*3] i1, i2, type */
+    int nbondtypes;
+    const double *bond_coeff;  /* [nbondtypes*2] k (kcal/mol/A^2), r0 (A) */
+    int nangle;
+    const int32_t *angles;     /* [nangle*4] i1, i2 (middle), i3, type */
+    int nangletypes;
+    const double *angle_coeff; /* [nangletypes*2] k (kcal/mol/rad^2), theta0 (rad) */
+    int ndihed;
+    const int32_t *dihedrals;  /* [ndihed*5] i1..i4, type */
+    int ndihedtypes;
+    const double *dihed_coeff; /* [ndihedtypes*4] OPLS k1..k4 */
+    const double *lj14;        /* [4*ntypes*ntypes] lj14_1..4 (needed for SOFIA_TERM_PAIR14) */
+    int nshake;
+    const int32_t *shake;      /* [nshake*5] num (1, 3, 4, -3), atoms */
+    const double *shake_bond;  /* [nshake*3] bond lengths */
+    int shake_maxiter;         /* 0 = 25 like the reference */
+    double shake_tol;          /* 0 = 1e-4 like the reference */
+} sofia_md_desc;
+
+int sofia_system_md_setup(sofia_system *sys, const sofia_md_desc *md);
+/* Runs nsteps steps on the device (use_graph != 0: one CUDA graph per step kind);
+ * energies (may be NULL) receive the last step's SOFIA_MD_NE values when
+ * energy_every > 0.  Positions and velocities stay resident
+ * (sofia_system_get_state / set_state move them). */
+int sofia_system_md_run(sofia_system *sys, int nsteps, int energy_every, int use_graph,
+                        double *energies);
+
 #ifdef __cplusplus
 }
 #endif

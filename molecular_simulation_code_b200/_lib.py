@@ -35,6 +35,22 @@ SOFIA_PREC_MIXED = 0
 SOFIA_PREC_FP64 = 1
 
 
+class SofiaMdDesc(C.Structure):
+    _fields_ = [("dt", C.c_double), ("temperature", C.c_double), ("gamma", C.c_double),
+                ("seed", C.c_uint64), ("terms", C.c_int), ("nbond", C.c_int),
+                ("bonds", C.c_void_p), ("nbondtypes", C.c_int), ("bond_coeff", C.c_void_p),
+                ("nangle", C.c_int), ("angles", C.c_void_p), ("nangletypes", C.c_int),
+                ("angle_coeff", C.c_void_p), ("ndihed", C.c_int), ("dihedrals", C.c_void_p),
+                ("ndihedtypes", C.c_int), ("dihed_coeff", C.c_void_p), ("lj14", C.c_void_p),
+                ("nshake", C.c_int), ("shake", C.c_void_p), ("shake_bond", C.c_void_p),
+                ("shake_maxiter", C.c_int), ("shake_tol", C.c_double)]
+
+
+SOFIA_MD_NE = 12
+MD_ENERGY_NAMES = ["lj", "coul", "self", "bond", "angle", "torsion", "coul14", "lj14", "kinetic",
+                   "total", "temperature", "step"]
+
+
 class SofiaSystemDesc(C.Structure):
     _fields_ = [("np", C.c_int), ("ntypes", C.c_int), ("box", C.c_float), ("alpha", C.c_double),
                 ("cut_coul", C.c_float), ("rcut", C.c_float), ("neighbor_pad", C.c_float),
@@ -82,6 +98,8 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_system_compute_forces": (_I, [_P, _I, _I, _P]),
     "sofia_system_stats": (_I, [_P, _P, _I]),
     "sofia_system_drift": (_I, [_P, _D, _I]),
+    "sofia_system_md_setup": (_I, [_P, C.POINTER(SofiaMdDesc)]),
+    "sofia_system_md_run": (_I, [_P, _I, _I, _I, _P]),
     "sofia_system_timers": (_I, [_P, _I, _P]),
 }
 

@@ -1,0 +1,813 @@
+// md.cu -- device-resident MD step: velocity Verlet, force-form Langevin,
+// SHAKE and bonded terms around the nonbonded path, so a trajectory segment
+// runs without host round trips (and is captured once into a CUDA graph).
+//
+// Step order follows the reference's NVE loop (Source/mod_integrate.f90:270-298):
+// nve_v(dt/2), nve_x, [list maintenance], forces, shake(1), nve_v(dt/2).
+//   nve_v / nve_x          Source/mod_ensemble.f90:11-87
+//   Langevin force          Source/mod_langevin.f90:15-43 (force form, gconst of
+//                           Source/get_started.f90:81-84); the reference draws
+//                           clock-seeded MT19937 uniforms, here a counter-based
+//                           Philox4x32-10 keyed by (seed, atom, step)
+//   SHAKE                   Source/mod_shake.f90:8-913 (shake2/3/4/3angle)
+//   bond / angle            Source/mod_force_bond.f90:6-75, mod_force_angle.f90:10-122
+//   torsion + 1-4 pair      Source/mod_force_dihed.f90:816-1092
+// The reference's DSF driver drops the bond, angle and improper forces
+// (Source/mod_force.f90:549-553); here every enabled term acts on the atoms.
+// State is FP64 (positions, velocities) with 64-bit fixed-point forces; all
+// force contributions are added in integers, so a step is bit-reproducible.
+#include <cmath>
+
+#include "system.cuh"
+
+namespace sofia {
+namespace {
+
+constexpr double KCAL2AMU = (double)0.0004184f;  // real*4 literal (get_started.f90:32)
+constexpr double KBOLTZ = (double)0.001987204181f;  // real*4 variable (global.f90:133)
+
+__device__ __forceinline__ long long fixd(double v) { return __double2ll_rn(v * FIX_SCALE); }
+__device__ __forceinline__ double unfix(long long v) { return (double)v * FIX_INV; }
+
+__device__ __forceinline__ void fadd(long long *f, double v) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(f), (unsigned long long)fixd(v));
+}
+
+__device__ __forceinline__ double mimg(double d, double L) { return d - L * rint(d / L); }
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter-based RNG.
+__device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const unsigned lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const unsigned lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+__device__ __forceinline__ double u01m(unsigned b) {  // uniform in [-1/2, 1/2)
+    return (double)(b >> 8) * (1.0 / 16777216.0) - 0.5;
+}
+
+// nve_v: v += (dt/2) * kcal2amu * f / m
+__global__ void k_kick(int n, double h, const double *__restrict__ invm,
+                       const long long *__restrict__ fx, const long long *__restrict__ fy,
+                       const long long *__restrict__ fz, double *__restrict__ vx,
+                       double *__restrict__ vy, double *__restrict__ vz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double c = h * invm[i];
+    vx[i] += c * unfix(fx[i]);
+    vy[i] += c * unfix(fy[i]);
+    vz[i] += c * unfix(fz[i]);
+}
+
+// nve_x: x += dt * v
+__global__ void k_stream(int n, double dt, double *__restrict__ x, double *__restrict__ y,
+                         double *__restrict__ z, const double *__restrict__ vx,
+                         const double *__restrict__ vy, const double *__restrict__ vz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] += dt * vx[i];
+    y[i] += dt * vy[i];
+    z[i] += dt * vz[i];
+}
+
+// Force-form Langevin: f += -gamma m v / kcal2amu + sqrt(12 * 2 m gamma kT kcal2amu / dt) U / kcal2amu
+__global__ void k_langevin(int n, double gamma, double gsig, unsigned long long seed,
+                           const long long *__restrict__ step_dev, const double *__restrict__ mass,
+                           const double *__restrict__ vx, const double *__restrict__ vy,
+                           const double *__restrict__ vz, long long *__restrict__ fx,
+                           long long *__restrict__ fy, long long *__restrict__ fz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long step = step_dev[0];
+    const uint4 r = philox(make_uint4((unsigned)i, (unsigned)step, (unsigned)(step >> 32), 0x5EED5EEDu),
+                           make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
+    const double m = mass[i];
+    const double g1 = -gamma * m / KCAL2AMU;
+    const double g2 = gsig * sqrt(m);
+    fx[i] += fixd(g1 * vx[i] + g2 * u01m(r.x));
+    fy[i] += fixd(g1 * vy[i] + g2 * u01m(r.y));
+    fz[i] += fixd(g1 * vz[i] + g2 * u01m(r.z));
+}
+
+template <bool EN>
+__global__ void k_bond(int nb, const int *__restrict__ bl, const double *__restrict__ bc,
+                       const double *__restrict__ x, const double *__restrict__ y,
+                       const double *__restrict__ z, double L, long long *__restrict__ fx,
+                       long long *__restrict__ fy, long long *__restrict__ fz,
+                       double *__restrict__ e) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nb) return;
+    const int i1 = bl[3 * m] - 1, i2 = bl[3 * m + 1] - 1, t = bl[3 * m + 2] - 1;
+    const double dx = mimg(x[i1] - x[i2], L), dy = mimg(y[i1] - y[i2], L), dz = mimg(z[i1] - z[i2], L);
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double dr = r - bc[2 * t + 1];
+    const double rk = bc[2 * t] * dr;
+    const double force = (r > 0.0) ? -2.0 * rk / r : 0.0;
+    fadd(&fx[i1], dx * force);
+    fadd(&fy[i1], dy * force);
+    fadd(&fz[i1], dz * force);
+    fadd(&fx[i2], -dx * force);
+    fadd(&fy[i2], -dy * force);
+    fadd(&fz[i2], -dz * force);
+    if (EN) e[m] = rk * dr;
+}
+
+template <bool EN>
+__global__ void k_angle(int na, const int *__restrict__ al, const double *__restrict__ ac,
+                        const double *__restrict__ x, const double *__restrict__ y,
+                        const double *__restrict__ z, double L, long long *__restrict__ fx,
+                        long long *__restrict__ fy, long long *__restrict__ fz,
+                        double *__restrict__ e) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= na) return;
+    const int i1 = al[4 * m] - 1, i2 = al[4 * m + 1] - 1, i3 = al[4 * m + 2] - 1,
+              t = al[4 * m + 3] - 1;
+    const double dx1 = mimg(x[i1] - x[i2], L), dy1 = mimg(y[i1] - y[i2], L),
+                 dz1 = mimg(z[i1] - z[i2], L);
+    const double dx2 = mimg(x[i3] - x[i2], L), dy2 = mimg(y[i3] - y[i2], L),
+                 dz2 = mimg(z[i3] - z[i2], L);
+    const double rsq1 = dx1 * dx1 + dy1 * dy1 + dz1 * dz1, r1 = sqrt(rsq1);
+    const double rsq2 = dx2 * dx2 + dy2 * dy2 + dz2 * dz2, r2 = sqrt(rsq2);
+    double c = (dx1 * dx2 + dy1 * dy2 + dz1 * dz2) / (r1 * r2);
+    c = fmin(1.0, fmax(-1.0, c));
+    double s = sqrt(1.0 - c * c);
+    if (s < 0.001) s = 0.001;
+    s = 1.0 / s;
+    const double dtheta = acos(c) - ac[2 * t + 1];
+    const double tk = ac[2 * t] * dtheta;
+    const double a = 2.0 * tk * s;
+    const double a11 = a * c / rsq1, a12 = -a / (r1 * r2), a22 = a * c / rsq2;
+    const double vx1 = a11 * dx1 + a12 * dx2, vx2 = a22 * dx2 + a12 * dx1;
+    const double vy1 = a11 * dy1 + a12 * dy2, vy2 = a22 * dy2 + a12 * dy1;
+    const double vz1 = a11 * dz1 + a12 * dz2, vz2 = a22 * dz2 + a12 * dz1;
+    fadd(&fx[i1], -vx1);
+    fadd(&fy[i1], -vy1);
+    fadd(&fz[i1], -vz1);
+    fadd(&fx[i2], vx2 + vx1);
+    fadd(&fy[i2], vy2 + vy1);
+    fadd(&fz[i2], vz2 + vz1);
+    fadd(&fx[i3], -vx2);
+    fadd(&fy[i3], -vy2);
+    fadd(&fz[i3], -vz2);
+    if (EN) e[m] = tk * dtheta;
+}
+
+struct DihArgs {
+    int nd, ntypes, terms;
+    const int *dl;
+    const double *dc, *lj14;
+    const double *x, *y, *z;
+    const int *type;
+    const float *q;
+    double L, alpha, EWALD_P, A1, A2, A3, A4, A5, MY_PIS, e_shift, f_shift, cut_coulsq, rcut2;
+    float coulpre;
+    long long *fx, *fy, *fz;
+    double *e;  // [nd][3] torsion, coul14, lj14
+};
+
+// dihedral_opls_DSF (mod_force_dihed.f90:849-1068) on the FP64 state.
+template <bool EN>
+__global__ void k_dihedral(DihArgs a) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nd) return;
+    const int i1 = a.dl[5 * n] - 1, i2 = a.dl[5 * n + 1] - 1, i3 = a.dl[5 * n + 2] - 1,
+              i4 = a.dl[5 * n + 3] - 1, type = a.dl[5 * n + 4] - 1;
+    const double *x = a.x, *y = a.y, *z = a.z;
+    const double L = a.L;
+    const double vb1x = mimg(x[i1] - x[i2], L), vb1y = mimg(y[i1] - y[i2], L), vb1z = mimg(z[i1] - z[i2], L);
+    const double vb2x = mimg(x[i3] - x[i2], L), vb2y = mimg(y[i3] - y[i2], L), vb2z = mimg(z[i3] - z[i2], L);
+    const double vb2xm = -vb2x, vb2ym = -vb2y, vb2zm = -vb2z;
+    const double vb3x = mimg(x[i4] - x[i3], L), vb3y = mimg(y[i4] - y[i3], L), vb3z = mimg(z[i4] - z[i3], L);
+    double f1[3] = {0, 0, 0}, f2[3] = {0, 0, 0}, f3[3] = {0, 0, 0}, f4[3] = {0, 0, 0};
+    double pp = 0.0;
+    if (a.terms & 4) {
+        const double sb1 = 1.0 / (vb1x * vb1x + vb1y * vb1y + vb1z * vb1z);
+        const double sb2 = 1.0 / (vb2x * vb2x + vb2y * vb2y + vb2z * vb2z);
+        const double sb3 = 1.0 / (vb3x * vb3x + vb3y * vb3y + vb3z * vb3z);
+        const double rb1 = sqrt(sb1), rb3 = sqrt(sb3);
+        const double c0 = (vb1x * vb3x + vb1y * vb3y + vb1z * vb3z) * rb1 * rb3;
+        const double b1mag = sqrt(vb1x * vb1x + vb1y * vb1y + vb1z * vb1z);
+        const double b2mag = sqrt(vb2x * vb2x + vb2y * vb2y + vb2z * vb2z);
+        const double b3mag = sqrt(vb3x * vb3x + vb3y * vb3y + vb3z * vb3z);
+        const double r12c1 = 1.0 / (b1mag * b2mag);
+        const double c1mag = (vb1x * vb2x + vb1y * vb2y + vb1z * vb2z) * r12c1;
+        const double r12c2 = 1.0 / (b2mag * b3mag);
+        const double c2mag = (vb2xm * vb3x + vb2ym * vb3y + vb2zm * vb3z) * r12c2;
+        double sc1 = sqrt(fmax(1.0 - c1mag * c1mag, 0.0));
+        if (sc1 < 0.001) sc1 = 0.001;
+        sc1 = 1.0 / sc1;
+        double sc2 = sqrt(fmax(1.0 - c2mag * c2mag, 0.0));
+        if (sc2 < 0.001) sc2 = 0.001;
+        sc2 = 1.0 / sc2;
+        const double s1 = sc1 * sc1, s2 = sc2 * sc2;
+        double s12 = sc1 * sc2;
+        double c = (c0 + c1mag * c2mag) * s12;
+        c = fmin(1.0, fmax(-1.0, c));
+        const double phi = acos(c);
+        double si = sin(phi);
+        if (fabs(si) < 0.0001) si = 0.0001;
+        const double siinv = 1.0 / si;
+        const double *kc = a.dc + 4 * type;
+        pp = kc[0] * (1.0 + c) + kc[1] * (1.0 - cos(2.0 * phi)) + kc[2] * (1.0 + cos(3.0 * phi)) +
+             kc[3] * (1.0 - cos(4.0 * phi));
+        const double pd = kc[0] - 2.0 * kc[1] * sin(2.0 * phi) * siinv +
+                          3.0 * kc[2] * sin(3.0 * phi) * siinv - 4.0 * kc[3] * sin(4.0 * phi) * siinv;
+        c *= pd;
+        s12 *= pd;
+        const double a11 = c * sb1 * s1, a22 = -sb2 * (2.0 * c0 * s12 - c * (s1 + s2)),
+                     a33 = c * sb3 * s2;
+        const double a12 = -r12c1 * (c1mag * c * s1 + c2mag * s12), a13 = -rb1 * rb3 * s12,
+                     a23 = r12c2 * (c2mag * c * s2 + c1mag * s12);
+        const double sx2 = a12 * vb1x + a22 * vb2x + a23 * vb3x;
+        const double sy2 = a12 * vb1y + a22 * vb2y + a23 * vb3y;
+        const double sz2 = a12 * vb1z + a22 * vb2z + a23 * vb3z;
+        f1[0] = a11 * vb1x + a12 * vb2x + a13 * vb3x;
+        f1[1] = a11 * vb1y + a12 * vb2y + a13 * vb3y;
+        f1[2] = a11 * vb1z + a12 * vb2z + a13 * vb3z;
+        f2[0] = -sx2 - f1[0];
+        f2[1] = -sy2 - f1[1];
+        f2[2] = -sz2 - f1[2];
+        f4[0] = a13 * vb1x + a23 * vb2x + a33 * vb3x;
+        f4[1] = a13 * vb1y + a23 * vb2y + a33 * vb3y;
+        f4[2] = a13 * vb1z + a23 * vb2z + a33 * vb3z;
+        f3[0] = sx2 - f4[0];
+        f3[1] = sy2 - f4[1];
+        f3[2] = sz2 - f4[2];
+    }
+    double ec14 = 0.0, p14 = 0.0;
+    if (a.terms & 8) {
+        const double ddx = mimg(x[i1] - x[i4], L), ddy = mimg(y[i1] - y[i4], L),
+                     ddz = mimg(z[i1] - z[i4], L);
+        const double dr2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        double force = 0.0;
+        if (dr2 < a.cut_coulsq) {
+            const double r = sqrt(dr2), dr2i = 1.0 / dr2;
+            const double pref = (double)a.coulpre * (double)a.q[i1] * (double)a.q[i4] / r;
+            const double erfcd = exp(-a.alpha * a.alpha * dr2);
+            const double t = 1.0 / (1.0 + a.EWALD_P * a.alpha * r);
+            const double erfcc = t * (a.A1 + t * (a.A2 + t * (a.A3 + t * (a.A4 + t * a.A5)))) * erfcd;
+            const double fc = 0.5 * pref * (erfcc / r + 2.0 * a.alpha / a.MY_PIS * erfcd + r * a.f_shift) * r;
+            ec14 = 0.5 * pref * (erfcc - r * a.e_shift - dr2 * a.f_shift);
+            double flj = 0.0;
+            if (dr2 < a.rcut2) {
+                const double dr6i = dr2i * dr2i * dr2i;
+                const size_t o = (size_t)(a.type[i1] - 1) * a.ntypes + (size_t)(a.type[i4] - 1);
+                const size_t tn = (size_t)a.ntypes * a.ntypes;
+                flj = dr6i * (a.lj14[o] * dr6i - a.lj14[tn + o]);
+                p14 = dr6i * (dr6i * a.lj14[2 * tn + o] - a.lj14[3 * tn + o]);
+            }
+            force = (fc + flj) * dr2i;
+        }
+        f1[0] += ddx * force;
+        f1[1] += ddy * force;
+        f1[2] += ddz * force;
+        f4[0] -= ddx * force;
+        f4[1] -= ddy * force;
+        f4[2] -= ddz * force;
+    }
+    long long *F[3] = {a.fx, a.fy, a.fz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        fadd(&F[d][i1], f1[d]);
+        fadd(&F[d][i2], f2[d]);
+        fadd(&F[d][i3], f3[d]);
+        fadd(&F[d][i4], f4[d]);
+    }
+    if (EN) {
+        a.e[3 * n] = pp;
+        a.e[3 * n + 1] = ec14;
+        a.e[3 * n + 2] = p14;
+    }
+}
+
+// SHAKE (force form) per group; each atom belongs to at most one group, so the
+// owning thread adds its constraint forces without atomics.
+__global__ void k_shake(int ns, const int *__restrict__ sa, const double *__restrict__ sb,
+                        const double *__restrict__ x, const double *__restrict__ y,
+                        const double *__restrict__ z, const double *__restrict__ vx,
+                        const double *__restrict__ vy, const double *__restrict__ vz,
+                        const double *__restrict__ invm, double L, double dt, double dtsq,
+                        int maxiter, double tol, long long *__restrict__ fx,
+                        long long *__restrict__ fy, long long *__restrict__ fz,
+                        int *__restrict__ status) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ns) return;
+    const int num = sa[5 * g];
+    int at[4] = {sa[5 * g + 1] - 1, sa[5 * g + 2] - 1, sa[5 * g + 3] - 1, sa[5 * g + 4] - 1};
+    int nc, cp[3], cq[3], na;
+    double bl[3];
+    if (num == 1) {
+        nc = 1; na = 2; cp[0] = 0; cq[0] = 1; bl[0] = sb[3 * g];
+    } else if (num == 3) {
+        nc = 2; na = 3; cp[0] = 0; cq[0] = 1; cp[1] = 0; cq[1] = 2; bl[0] = sb[3 * g]; bl[1] = sb[3 * g + 1];
+    } else if (num == 4) {
+        nc = 3; na = 4;
+        for (int k = 0; k < 3; ++k) { cp[k] = 0; cq[k] = k + 1; bl[k] = sb[3 * g + k]; }
+    } else if (num == -3) {
+        nc = 3; na = 3; cp[0] = 0; cq[0] = 1; cp[1] = 0; cq[1] = 2; cp[2] = 1; cq[2] = 2;
+        for (int k = 0; k < 3; ++k) bl[k] = sb[3 * g + k];
+    } else {
+        return;
+    }
+    double im[4], xs[4][3], xc[4][3];
+    for (int a = 0; a < na; ++a) {
+        const int i = at[a];
+        im[a] = invm[i];
+        const double c = dtsq * im[a];
+        xc[a][0] = x[i];
+        xc[a][1] = y[i];
+        xc[a][2] = z[i];
+        xs[a][0] = x[i] + dt * vx[i] + c * unfix(fx[i]);
+        xs[a][1] = y[i] + dt * vy[i] + c * unfix(fy[i]);
+        xs[a][2] = z[i] + dt * vz[i] + c * unfix(fz[i]);
+    }
+    double r[3][3], s[3][3], C[3][3];
+    for (int c = 0; c < nc; ++c)
+        for (int d = 0; d < 3; ++d) {
+            r[c][d] = mimg(xc[cp[c]][d] - xc[cq[c]][d], L);
+            s[c][d] = mimg(xs[cp[c]][d] - xs[cq[c]][d], L);
+        }
+    for (int c = 0; c < nc; ++c)
+        for (int d = 0; d < nc; ++d) {
+            double e = 0.0;
+            if (cp[c] == cp[d]) e += im[cp[c]];
+            if (cp[c] == cq[d]) e -= im[cp[c]];
+            if (cq[c] == cp[d]) e -= im[cq[c]];
+            if (cq[c] == cq[d]) e += im[cq[c]];
+            C[c][d] = e;
+        }
+    double lam[3] = {0.0, 0.0, 0.0};
+    if (nc == 1) {
+        const double rr = r[0][0] * r[0][0] + r[0][1] * r[0][1] + r[0][2] * r[0][2];
+        const double ss = s[0][0] * s[0][0] + s[0][1] * s[0][1] + s[0][2] * s[0][2];
+        const double sr = s[0][0] * r[0][0] + s[0][1] * r[0][1] + s[0][2] * r[0][2];
+        const double aa = C[0][0] * C[0][0] * rr, bb = 2.0 * C[0][0] * sr, cc = ss - bl[0] * bl[0];
+        double det = bb * bb - 4.0 * aa * cc;
+        if (det < 0.0) {
+            atomicAdd(&status[ST_SHAKE], 1);
+            det = 0.0;
+        }
+        const double l1 = (-bb + sqrt(det)) / (2.0 * aa), l2 = (-bb - sqrt(det)) / (2.0 * aa);
+        lam[0] = (fabs(l1) <= fabs(l2)) ? l1 : l2;
+    } else {
+        double A[3][3], Ai[3][3], ss[3], rd[3][3];
+        for (int c = 0; c < nc; ++c) {
+            ss[c] = s[c][0] * s[c][0] + s[c][1] * s[c][1] + s[c][2] * s[c][2];
+            for (int d = 0; d < nc; ++d) {
+                A[c][d] = 2.0 * C[c][d] * (s[c][0] * r[d][0] + s[c][1] * r[d][1] + s[c][2] * r[d][2]);
+                rd[c][d] = r[c][0] * r[d][0] + r[c][1] * r[d][1] + r[c][2] * r[d][2];
+            }
+        }
+        if (nc == 2) {
+            const double det = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+            if (det == 0.0) {
+                atomicAdd(&status[ST_SHAKE], 1);
+                return;
+            }
+            const double di = 1.0 / det;
+            Ai[0][0] = A[1][1] * di; Ai[0][1] = -A[0][1] * di;
+            Ai[1][0] = -A[1][0] * di; Ai[1][1] = A[0][0] * di;
+        } else {
+            const double det = A[0][0] * A[1][1] * A[2][2] + A[0][1] * A[1][2] * A[2][0] +
+                               A[0][2] * A[1][0] * A[2][1] - A[0][0] * A[1][2] * A[2][1] -
+                               A[0][1] * A[1][0] * A[2][2] - A[0][2] * A[1][1] * A[2][0];
+            if (det == 0.0) {
+                atomicAdd(&status[ST_SHAKE], 1);
+                return;
+            }
+            const double di = 1.0 / det;
+            Ai[0][0] = di * (A[1][1] * A[2][2] - A[1][2] * A[2][1]);
+            Ai[0][1] = -di * (A[0][1] * A[2][2] - A[0][2] * A[2][1]);
+            Ai[0][2] = di * (A[0][1] * A[1][2] - A[0][2] * A[1][1]);
+            Ai[1][0] = -di * (A[1][0] * A[2][2] - A[1][2] * A[2][0]);
+            Ai[1][1] = di * (A[0][0] * A[2][2] - A[0][2] * A[2][0]);
+            Ai[1][2] = -di * (A[0][0] * A[1][2] - A[0][2] * A[1][0]);
+            Ai[2][0] = di * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+            Ai[2][1] = -di * (A[0][0] * A[2][1] - A[0][1] * A[2][0]);
+            Ai[2][2] = di * (A[0][0] * A[1][1] - A[0][1] * A[1][0]);
+        }
+        bool done = false;
+        for (int it = 0; it < maxiter && !done; ++it) {
+            double bvec[3], ln[3];
+            for (int c = 0; c < nc; ++c) {
+                double qd = 0.0;
+                for (int d = 0; d < nc; ++d)
+                    for (int e = 0; e < nc; ++e) qd += C[c][d] * C[c][e] * rd[d][e] * lam[d] * lam[e];
+                bvec[c] = bl[c] * bl[c] - ss[c] - qd;
+            }
+            done = true;
+            for (int c = 0; c < nc; ++c) {
+                ln[c] = 0.0;
+                for (int d = 0; d < nc; ++d) ln[c] += Ai[c][d] * bvec[d];
+                if (fabs(ln[c] - lam[c]) > tol) done = false;
+            }
+            for (int c = 0; c < nc; ++c) lam[c] = ln[c];
+        }
+        if (!done) atomicAdd(&status[ST_SHAKE], 1);
+    }
+    long long *F[3] = {fx, fy, fz};
+    for (int c = 0; c < nc; ++c) {
+        const double l = lam[c] / dtsq;
+        for (int d = 0; d < 3; ++d) {
+            F[d][at[cp[c]]] += fixd(l * r[c][d]);
+            F[d][at[cq[c]]] -= fixd(l * r[c][d]);
+        }
+    }
+}
+
+__global__ void k_ke(int n, const double *__restrict__ mass, const double *__restrict__ vx,
+                     const double *__restrict__ vy, const double *__restrict__ vz,
+                     double *__restrict__ ke) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ke[i] = 0.5 * mass[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]) / KCAL2AMU;
+}
+
+__global__ void k_step_inc(long long *__restrict__ step) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) step[0] += 1;
+}
+
+// Two-stage deterministic sum of column c of in[n][w] into out[slot].
+constexpr int MRED = 64;
+__global__ void k_mred1(int n, int w, int c, const double *__restrict__ in,
+                        double *__restrict__ part) {
+    __shared__ double s[256];
+    const int chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+    double acc = 0.0;
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) acc += in[(size_t)i * w + c];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = 128; off > 0; off >>= 1) {
+        if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+__global__ void k_mred2(const double *__restrict__ part, double *__restrict__ out) {
+    __shared__ double s[MRED];
+    s[threadIdx.x] = part[threadIdx.x];
+    __syncthreads();
+    for (int off = MRED / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = s[0];
+}
+
+}  // namespace
+
+static void md_reduce(cudaStream_t st, int n, int w, int c, const double *in, double *part,
+                      double *out) {
+    if (n <= 0) return;
+    k_mred1<<<MRED, 256, 0, st>>>(n, w, c, in, part);
+    k_mred2<<<1, MRED, 0, st>>>(part, out);
+}
+
+// energies slots in md.ered: 0 lj, 1 coul, (2..4 pair virial), 5 bond, 6 angle,
+// 7 torsion, 8 coul14, 9 lj14, 10 kinetic; partials after slot 16.
+static int md_forces(Sys *s, bool energy, bool force_build) {
+    Md &md = s->md;
+    cudaStream_t st = s->ctx->stream;
+    int rc = sys_step_forces(s, s->precision, energy, false, force_build);
+    if (rc) return rc;
+    long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
+              *fz = s->f[2].as<long long>();
+    const double *x = s->x[0].as<double>(), *y = s->x[1].as<double>(), *z = s->x[2].as<double>();
+    double *et = md.eterm.as<double>();
+    const int nb = md.nbond, na = md.nangle, nd = md.ndihed;
+    if ((md.terms & 1) && nb) {
+        if (energy)
+            k_bond<true><<<grid_for(nb, 128), 128, 0, st>>>(nb, md.bonds.as<int>(), md.bcoef.as<double>(), x, y, z, s->L, fx, fy, fz, et);
+        else
+            k_bond<false><<<grid_for(nb, 128), 128, 0, st>>>(nb, md.bonds.as<int>(), md.bcoef.as<double>(), x, y, z, s->L, fx, fy, fz, et);
+    }
+    if ((md.terms & 2) && na) {
+        if (energy)
+            k_angle<true><<<grid_for(na, 128), 128, 0, st>>>(na, md.angles.as<int>(), md.acoef.as<double>(), x, y, z, s->L, fx, fy, fz, et + nb);
+        else
+            k_angle<false><<<grid_for(na, 128), 128, 0, st>>>(na, md.angles.as<int>(), md.acoef.as<double>(), x, y, z, s->L, fx, fy, fz, et + nb);
+    }
+    if ((md.terms & 12) && nd) {
+        DihArgs a;
+        a.nd = nd;
+        a.ntypes = s->ntypes;
+        a.terms = md.terms;
+        a.dl = md.diheds.as<int>();
+        a.dc = md.dcoef.as<double>();
+        a.lj14 = md.lj14.as<double>();
+        a.x = x;
+        a.y = y;
+        a.z = z;
+        a.type = s->type.as<int>();
+        a.q = s->q.as<float>();
+        a.L = s->L;
+        a.alpha = s->alpha;
+        a.EWALD_P = (double)0.3275911f;
+        a.A1 = (double)0.254829592f;
+        a.A2 = (double)-0.284496736f;
+        a.A3 = (double)1.421413741f;
+        a.A4 = (double)-1.453152027f;
+        a.A5 = (double)1.061405429f;
+        a.MY_PIS = (double)1.77245385090551602729f;
+        a.e_shift = s->e_shift;
+        a.f_shift = s->f_shift;
+        a.cut_coulsq = (double)(float)(s->rc * s->rc);
+        a.rcut2 = a.cut_coulsq;
+        a.coulpre = s->coulpre;
+        a.fx = fx;
+        a.fy = fy;
+        a.fz = fz;
+        a.e = et + nb + na;
+        if (energy)
+            k_dihedral<true><<<grid_for(nd, 128), 128, 0, st>>>(a);
+        else
+            k_dihedral<false><<<grid_for(nd, 128), 128, 0, st>>>(a);
+    }
+    if (md.gamma > 0.0) {
+        const double kT = KBOLTZ * md.temperature;
+        const double gsig = sqrt(12.0 * 2.0 * md.gamma * kT * KCAL2AMU / md.dt) / KCAL2AMU;
+        k_langevin<<<grid_for(s->n, 256), 256, 0, st>>>(
+            s->n, md.gamma, gsig, md.seed, md.step_dev.as<long long>(), s->mass.as<double>(),
+            s->v[0].as<double>(), s->v[1].as<double>(), s->v[2].as<double>(), fx, fy, fz);
+    }
+    if (md.nshake) {
+        k_shake<<<grid_for(md.nshake, 128), 128, 0, st>>>(
+            md.nshake, md.shake.as<int>(), md.sbond.as<double>(), x, y, z, s->v[0].as<double>(),
+            s->v[1].as<double>(), s->v[2].as<double>(), s->invm.as<double>(), s->L, md.dt,
+            md.dt * md.dt * KCAL2AMU, md.shake_maxiter, md.shake_tol, fx, fy, fz,
+            s->status_local.as<int>());
+    }
+    SOFIA_CUDA(s->ctx, cudaGetLastError());
+    return SOFIA_OK;
+}
+
+static void md_energy_reduce(Sys *s) {
+    Md &md = s->md;
+    cudaStream_t st = s->ctx->stream;
+    double *red = md.ered.as<double>();
+    double *part = red + 16;
+    double *et = md.eterm.as<double>();
+    // nonbonded pair energies were reduced into s->red by the pair path
+    cudaMemcpyAsync(red, s->red.p, sizeof(double) * 5, cudaMemcpyDeviceToDevice, st);
+    if (md.nbond && (md.terms & 1)) md_reduce(st, md.nbond, 1, 0, et, part, red + 5);
+    if (md.nangle && (md.terms & 2)) md_reduce(st, md.nangle, 1, 0, et + md.nbond, part, red + 6);
+    if (md.ndihed && (md.terms & 12)) {
+        const double *ed = et + md.nbond + md.nangle;
+        md_reduce(st, md.ndihed, 3, 0, ed, part, red + 7);
+        md_reduce(st, md.ndihed, 3, 1, ed, part, red + 8);
+        md_reduce(st, md.ndihed, 3, 2, ed, part, red + 9);
+    }
+    double *ke = md.eterm.as<double>() + (md.nbond + md.nangle + 3 * (size_t)md.ndihed);
+    k_ke<<<grid_for(s->n, 256), 256, 0, st>>>(s->n, s->mass.as<double>(), s->v[0].as<double>(),
+                                              s->v[1].as<double>(), s->v[2].as<double>(), ke);
+    md_reduce(st, s->n, 1, 0, ke, part, red + 10);
+}
+
+// One MD step (all device work; capturable).
+static int md_step(Sys *s, bool energy) {
+    Md &md = s->md;
+    cudaStream_t st = s->ctx->stream;
+    const int n = s->n;
+    const double h = 0.5 * md.dt * KCAL2AMU;
+    double *vx = s->v[0].as<double>(), *vy = s->v[1].as<double>(), *vz = s->v[2].as<double>();
+    const long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
+                    *fz = s->f[2].as<long long>();
+    k_kick<<<grid_for(n, 256), 256, 0, st>>>(n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz);
+    k_stream<<<grid_for(n, 256), 256, 0, st>>>(n, md.dt, s->x[0].as<double>(), s->x[1].as<double>(),
+                                               s->x[2].as<double>(), vx, vy, vz);
+    k_step_inc<<<1, 32, 0, st>>>(md.step_dev.as<long long>());
+    int rc = md_forces(s, energy, false);
+    if (rc) return rc;
+    k_kick<<<grid_for(n, 256), 256, 0, st>>>(n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz);
+    if (energy) md_energy_reduce(s);
+    s->launches += 8;
+    SOFIA_CUDA(s->ctx, cudaGetLastError());
+    return SOFIA_OK;
+}
+
+static void md_drop_graphs(Sys *s) {
+    for (auto &g : s->md.graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    s->md.graph_ok = 0;
+}
+
+static int md_capture(Sys *s) {
+    md_drop_graphs(s);
+    cudaStream_t st = s->ctx->stream;
+    const int timing = s->timing;
+    s->timing = 0;  // no event records inside the graph
+    for (int e = 0; e < 2; ++e) {
+        cudaGraph_t g = nullptr;
+        const long long l0 = s->launches;
+        SOFIA_CUDA(s->ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int rc = md_step(s, e == 1);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        s->md.graph_launches[e] = s->launches - l0;
+        s->launches = l0;
+        s->timing = timing;
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return cuda_fail(s->ctx, ce, "cudaStreamEndCapture");
+        ce = cudaGraphInstantiate(&s->md.graph[e], g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return cuda_fail(s->ctx, ce, "cudaGraphInstantiate");
+    }
+    s->md.graph_ok = 1;
+    return SOFIA_OK;
+}
+
+}  // namespace sofia
+
+using sofia::Md;
+using sofia::Sys;
+
+template <class T>
+static int up(sofia_nb_ctx *ctx, sofia::DevBuf &b, const T *src, size_t count) {
+    SOFIA_CUDA(ctx, b.ensure(sizeof(T) * (count ? count : 1)));
+    if (count && src)
+        SOFIA_CUDA(ctx, cudaMemcpy(b.p, src, sizeof(T) * count, cudaMemcpyDefault));
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_system_md_setup(sofia_system *ss, const sofia_md_desc *d) {
+    if (!ss || !d || !(d->dt > 0.0) || d->temperature < 0.0 || d->gamma < 0.0) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    Md &md = s->md;
+    sofia::md_drop_graphs(s);
+    md.dt = d->dt;
+    md.temperature = d->temperature;
+    md.gamma = d->gamma;
+    md.seed = d->seed;
+    md.nbond = d->bonds ? d->nbond : 0;
+    md.nangle = d->angles ? d->nangle : 0;
+    md.ndihed = d->dihedrals ? d->ndihed : 0;
+    md.nshake = d->shake ? d->nshake : 0;
+    md.terms = d->terms;
+    md.shake_maxiter = d->shake_maxiter > 0 ? d->shake_maxiter : 25;
+    md.shake_tol = d->shake_tol > 0.0 ? d->shake_tol : (double)0.0001f;
+    int rc;
+    if ((rc = up(ctx, md.bonds, d->bonds, (size_t)md.nbond * 3))) return rc;
+    if ((rc = up(ctx, md.bcoef, d->bond_coeff, (size_t)(d->nbondtypes > 0 ? d->nbondtypes : 0) * 2))) return rc;
+    if ((rc = up(ctx, md.angles, d->angles, (size_t)md.nangle * 4))) return rc;
+    if ((rc = up(ctx, md.acoef, d->angle_coeff, (size_t)(d->nangletypes > 0 ? d->nangletypes : 0) * 2))) return rc;
+    if ((rc = up(ctx, md.diheds, d->dihedrals, (size_t)md.ndihed * 5))) return rc;
+    if ((rc = up(ctx, md.dcoef, d->dihed_coeff, (size_t)(d->ndihedtypes > 0 ? d->ndihedtypes : 0) * 4))) return rc;
+    if ((rc = up(ctx, md.lj14, d->lj14, d->lj14 ? (size_t)4 * s->ntypes * s->ntypes : 0))) return rc;
+    if ((rc = up(ctx, md.shake, d->shake, (size_t)md.nshake * 5))) return rc;
+    if ((rc = up(ctx, md.sbond, d->shake_bond, (size_t)md.nshake * 3))) return rc;
+    // validate indices on the host (no kernel ever sees an out-of-range id)
+    {
+        const int n = s->n;
+        auto bad = [n](const int32_t *l, int cnt, int stride, int nid, int tcol, int ntyp) {
+            for (int m = 0; m < cnt; ++m) {
+                for (int k = 0; k < nid; ++k)
+                    if (l[m * stride + k] < 1 || l[m * stride + k] > n) return true;
+                if (tcol >= 0 && (l[m * stride + tcol] < 1 || l[m * stride + tcol] > ntyp)) return true;
+            }
+            return false;
+        };
+        if ((md.nbond && bad(d->bonds, md.nbond, 3, 2, 2, d->nbondtypes)) ||
+            (md.nangle && bad(d->angles, md.nangle, 4, 3, 3, d->nangletypes)) ||
+            (md.ndihed && bad(d->dihedrals, md.ndihed, 5, 4, 4, d->ndihedtypes)))
+            return sofia::fail(ctx, SOFIA_EINVAL, "bonded list index or type out of range%s");
+        if ((md.terms & 8) && md.ndihed && !d->lj14)
+            return sofia::fail(ctx, SOFIA_EINVAL, "1-4 pairs need lj14 tables%s");
+        for (int g = 0; g < md.nshake; ++g) {
+            const int num = d->shake[5 * g];
+            const int na = (num == 1) ? 2 : (num == 4 ? 4 : 3);
+            if (num != 1 && num != 3 && num != 4 && num != -3)
+                return sofia::fail(ctx, SOFIA_EINVAL, "unknown SHAKE group kind%s");
+            for (int k = 0; k < na; ++k)
+                if (d->shake[5 * g + 1 + k] < 1 || d->shake[5 * g + 1 + k] > n)
+                    return sofia::fail(ctx, SOFIA_EINVAL, "SHAKE atom index out of range%s");
+        }
+    }
+    const size_t nterm = (size_t)md.nbond + md.nangle + 3 * (size_t)md.ndihed + (size_t)s->n;
+    SOFIA_CUDA(ctx, md.eterm.ensure(sizeof(double) * nterm));
+    SOFIA_CUDA(ctx, md.ered.ensure(sizeof(double) * (16 + sofia::MRED)));
+    SOFIA_CUDA(ctx, cudaMemset(md.ered.p, 0, sizeof(double) * 16));
+    SOFIA_CUDA(ctx, md.step_dev.ensure(sizeof(long long)));
+    SOFIA_CUDA(ctx, cudaMemset(md.step_dev.p, 0, sizeof(long long)));
+    for (int k = 0; k < 6; ++k) SOFIA_CUDA(ctx, md.snap[k].ensure(sizeof(double) * s->n));
+    SOFIA_CUDA(ctx, md.snap[6].ensure(sizeof(long long)));
+    // DSF self energy (Source/mod_assign_types.f90:59-62) and degrees of freedom
+    {
+        float *hq = new float[s->n];
+        cudaMemcpy(hq, s->q.p, sizeof(float) * s->n, cudaMemcpyDeviceToHost);
+        const double my_pis = (double)1.77245385090551602729f;
+        double es = 0.0;
+        for (int i = 0; i < s->n; ++i)
+            es -= (0.5 * s->e_shift + s->alpha / my_pis) * (double)hq[i] * (double)hq[i] *
+                  (double)s->coulpre;
+        delete[] hq;
+        md.e_self = es;
+        int ncons = 0;
+        for (int g = 0; g < md.nshake; ++g) {
+            const int num = d->shake[5 * g];
+            ncons += (num == 1) ? 1 : (num == 3 ? 2 : 3);
+        }
+        md.ndof = 3 * s->n - ncons - 3;
+    }
+    md.step = 0;
+    md.forces_valid = 0;
+    md.ready = 1;
+    return SOFIA_OK;
+}
+
+// Runs nsteps MD steps on the device.  energies[SOFIA_MD_NE] receives the
+// energies of the last step (if energy_every > 0 and it divides the step).
+extern "C" int sofia_system_md_run(sofia_system *ss, int nsteps, int energy_every, int use_graph,
+                                   double *energies) {
+    if (!ss || nsteps < 0) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    Md &md = s->md;
+    if (!md.ready) return sofia::fail(ctx, SOFIA_EINVAL, "sofia_system_md_setup first%s");
+    if (!s->mass.p) return sofia::fail(ctx, SOFIA_EINVAL, "system created without masses%s");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t nb = sizeof(double) * (size_t)s->n;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        // snapshot for a redo after a list-capacity overflow
+        for (int d = 0; d < 3; ++d) {
+            SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[d].p, s->x[d].p, nb, cudaMemcpyDeviceToDevice, st));
+            SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[3 + d].p, s->v[d].p, nb, cudaMemcpyDeviceToDevice, st));
+        }
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[6].p, md.step_dev.p, sizeof(long long), cudaMemcpyDeviceToDevice, st));
+        SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * sofia::ST_NSLOTS, st));
+        const int had_forces = md.forces_valid;
+        int rc = SOFIA_OK;
+        if (!md.forces_valid) {
+            // initial forces (force_driver(0) + shake(1) before the loop, mod_integrate.f90:237-240)
+            rc = sofia::md_forces(s, false, true);
+            if (rc) return rc;
+            md.forces_valid = 1;
+        }
+        if (use_graph && !md.graph_ok) {
+            rc = sofia::md_capture(s);
+            if (rc) return rc;
+        }
+        for (int k = 0; k < nsteps; ++k) {
+            const bool en = energy_every > 0 && ((k + 1) % energy_every == 0 || k + 1 == nsteps);
+            if (use_graph) {
+                SOFIA_CUDA(ctx, cudaGraphLaunch(md.graph[en ? 1 : 0], st));
+                s->launches += md.graph_launches[en ? 1 : 0];
+            } else {
+                rc = sofia::md_step(s, en);
+                if (rc) return rc;
+            }
+        }
+        rc = sofia::sys_list_overflow(s);
+        if (rc == SOFIA_ENEEDGROW) {
+            // list row capacity grew: restore the segment start and run it again
+            sofia::md_drop_graphs(s);
+            for (int d = 0; d < 3; ++d) {
+                SOFIA_CUDA(ctx, cudaMemcpyAsync(s->x[d].p, md.snap[d].p, nb, cudaMemcpyDeviceToDevice, st));
+                SOFIA_CUDA(ctx, cudaMemcpyAsync(s->v[d].p, md.snap[3 + d].p, nb, cudaMemcpyDeviceToDevice, st));
+            }
+            SOFIA_CUDA(ctx, cudaMemcpyAsync(md.step_dev.p, md.snap[6].p, sizeof(long long), cudaMemcpyDeviceToDevice, st));
+            md.forces_valid = had_forces ? 0 : 0;
+            continue;
+        }
+        if (rc) return rc;
+        int hs[sofia::ST_NSLOTS];
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
+        SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+        if (hs[sofia::ST_SHAKE])
+            return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE did not converge (or negative determinant)%s");
+        md.step += nsteps;
+        if (energies && energy_every > 0) {
+            double e[16];
+            SOFIA_CUDA(ctx, cudaMemcpy(e, md.ered.p, sizeof(double) * 16, cudaMemcpyDeviceToHost));
+            const double pot = e[0] + e[1] + md.e_self + e[5] + e[6] + e[7] + e[8] + e[9];
+            energies[0] = e[0];
+            energies[1] = e[1];
+            energies[2] = md.e_self;
+            energies[3] = e[5];
+            energies[4] = e[6];
+            energies[5] = e[7];
+            energies[6] = e[8];
+            energies[7] = e[9];
+            energies[8] = e[10];
+            energies[9] = pot + e[10];
+            energies[10] = 2.0 * e[10] / ((double)md.ndof * sofia::KBOLTZ);
+            energies[11] = (double)md.step;
+        }
+        return SOFIA_OK;
+    }
+    return sofia::fail(ctx, SOFIA_ENEEDGROW, "list capacity kept overflowing%s");
+}

@@ -25,7 +25,13 @@ namespace sofia {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int MAX_COL = 2048;  // atoms per xy column handled by the in-column sort
+constexpr int MAX_COL = 2048;
+
+// Build and prune kernels take an optional device flag: when `cond` is given
+// they return at once unless (cond[0] & cmask) != 0, so a whole step can be
+// launched (or captured into a CUDA graph) without a host round trip.
+#define SOFIA_COND_RETURN \
+    if (cond && !(cond[0] & cmask)) return  // atoms per xy column handled by the in-column sort
 constexpr int FLUSH = 4;       // j-clusters between FP32 -> fixed-point flushes
 
 __device__ __forceinline__ double wrap_shift(double x, double L) {
@@ -33,13 +39,15 @@ __device__ __forceinline__ double wrap_shift(double x, double L) {
     return -L * floor(x / L);
 }
 
-__global__ void k_wrap_bin(int n, const double *__restrict__ x, const double *__restrict__ y,
+__global__ void k_wrap_bin(const int *__restrict__ cond, int cmask, int n,
+                           const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ z, double L, double s_col, int ncx,
                            double *__restrict__ ix, double *__restrict__ iy,
                            double *__restrict__ iz, double *__restrict__ rx,
                            double *__restrict__ ry, double *__restrict__ rz,
                            int *__restrict__ col_of, int *__restrict__ col_count,
                            float *__restrict__ zkey) {
+    SOFIA_COND_RETURN;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double px = x[i], py = y[i], pz = z[i];
@@ -65,7 +73,9 @@ __global__ void k_wrap_bin(int n, const double *__restrict__ x, const double *__
     atomicAdd(&col_count[c], 1);
 }
 
-__global__ void k_scan1(int n, const int *__restrict__ in, int *__restrict__ out, int round8) {
+__global__ void k_scan1(const int *__restrict__ cond, int cmask, int n, const int *__restrict__ in,
+                        int *__restrict__ out, int round8) {
+    SOFIA_COND_RETURN;
     __shared__ int s[1024];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
@@ -90,9 +100,11 @@ __global__ void k_scan1(int n, const int *__restrict__ in, int *__restrict__ out
     if (threadIdx.x == 0) out[n] = carry;
 }
 
-__global__ void k_col_scatter(int n, const int *__restrict__ col_of,
+__global__ void k_col_scatter(const int *__restrict__ cond, int cmask, int n,
+                              const int *__restrict__ col_of,
                               const int *__restrict__ col_start, int *__restrict__ col_fill,
                               int *__restrict__ col_atoms) {
+    SOFIA_COND_RETURN;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int c = col_of[i];
@@ -101,10 +113,12 @@ __global__ void k_col_scatter(int n, const int *__restrict__ col_of,
 }
 
 // Sort each column by (z, index); then lay the column out as clusters of 8.
-__global__ void k_col_sort_assign(int ncols, const int *__restrict__ col_start,
+__global__ void k_col_sort_assign(const int *__restrict__ cond, int cmask, int ncols,
+                                  const int *__restrict__ col_start,
                                   int *__restrict__ col_atoms, const float *__restrict__ zkey,
                                   const int *__restrict__ cl_start, int *__restrict__ slot_orig,
                                   int *__restrict__ cl_col, int *__restrict__ status) {
+    SOFIA_COND_RETURN;
     __shared__ unsigned long long s[MAX_COL];
     const int c = blockIdx.x;
     if (c >= ncols) return;
@@ -185,9 +199,11 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
     recf[s] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.0f);
 }
 
-__global__ void k_bbox(int maxcl, const int *__restrict__ ncl_dev,
+__global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
+                       const int *__restrict__ ncl_dev,
                        const AtomRec *__restrict__ rec, const int *__restrict__ slot_orig,
                        float4 *__restrict__ bb) {
+    SOFIA_COND_RETURN;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= maxcl || c >= ncl_dev[0]) return;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -212,6 +228,8 @@ __device__ __forceinline__ float gap(float alo, float ahi, float blo, float bhi)
 }
 
 struct SearchArgs {
+    const int *cond;
+    int cmask;
     int maxcl, ncx, reach, jcap;
     float L, s_col, rl2, rexcl2;
     const int *ncl_dev, *cl_start, *cl_col, *slot_orig, *specbond, *num3bond;
@@ -225,6 +243,7 @@ struct SearchArgs {
 // included), test every cluster's bounding box in three z images, compact the
 // accepted (cluster, image) pairs in visiting order and attach the pair mask.
 __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
+    if (a.cond && !(a.cond[0] & a.cmask)) return;
     const int lane = threadIdx.x & 31;
     const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (icl >= a.maxcl || icl >= a.ncl_dev[0]) return;
@@ -353,9 +372,11 @@ __global__ void k_disp_check(int n, const double *__restrict__ x, const double *
     if ((threadIdx.x & 31) == 0 && (a || b)) atomicOr(flag, (a ? 1 : 0) | (b ? 2 : 0));
 }
 
-__global__ void k_copy3(int n, const double *__restrict__ x, const double *__restrict__ y,
+__global__ void k_copy3(const int *__restrict__ cond, int cmask, int n,
+                        const double *__restrict__ x, const double *__restrict__ y,
                         const double *__restrict__ z, double *__restrict__ ox,
                         double *__restrict__ oy, double *__restrict__ oz) {
+    SOFIA_COND_RETURN;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     ox[i] = x[i];
@@ -610,10 +631,12 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
 // here only select entries, so FP32 copies of the positions suffice (the
 // squared radius carries a 1e-3 A safety margin).
 __global__ void __launch_bounds__(256) k_prune(
-    int maxcl, const int *__restrict__ ncl_dev, const float4 *__restrict__ recf,
+    const int *__restrict__ cond, int cmask, int maxcl, const int *__restrict__ ncl_dev,
+    const float4 *__restrict__ recf,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
     const int *__restrict__ jcount, int jcap, float L, float rin2, int *__restrict__ ilist,
     unsigned long long *__restrict__ imask, int *__restrict__ icount) {
+    SOFIA_COND_RETURN;
     const int lane = threadIdx.x & 31;
     const int li = lane & 7, lj = lane >> 3;
     const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -660,6 +683,39 @@ __global__ void __launch_bounds__(256) k_prune(
         kept += __popc(keepbits);
     }
     if (lane == 0) icount[icl] = kept;
+}
+
+// Conditional list-build preparation: clear the column counters and mark
+// every slot as padding.
+__global__ void k_build_prep(const int *__restrict__ cond, int cmask, int ncols1,
+                             int *__restrict__ col_count, int *__restrict__ col_fill, int nslots,
+                             int *__restrict__ slot_orig) {
+    SOFIA_COND_RETURN;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += gridDim.x * blockDim.x) {
+        slot_orig[i] = -1;
+        if (i < ncols1) {
+            col_count[i] = 0;
+            col_fill[i] = 0;
+        }
+    }
+}
+
+__global__ void k_set_ncl(const int *__restrict__ cond, int cmask, const int *__restrict__ src,
+                          int *__restrict__ dst) {
+    SOFIA_COND_RETURN;
+    if (threadIdx.x == 0 && blockIdx.x == 0) dst[0] = src[0];
+}
+
+__global__ void k_set_flag(int *__restrict__ flag, int v) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) flag[0] = v;
+}
+
+// Device-side counters of list builds and prunes (for statistics).
+__global__ void k_count_events(const int *__restrict__ flag, long long *__restrict__ cnt) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        if (flag[0] & 1) cnt[0] += 1;
+        if (flag[0] & 3) cnt[1] += 1;
+    }
 }
 
 // Two-stage deterministic column sums: stage 1 = fixed grid of blocks over
@@ -766,6 +822,9 @@ static int sys_alloc(Sys *s) {
     for (int d = 0; d < 3; ++d) SOFIA_CUDA(ctx, s->xprn[d].ensure(sizeof(double) * n));
     SOFIA_CUDA(ctx, s->icount.ensure(sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, s->part.ensure(sizeof(double) * 8 * RED_BLOCKS));
+    SOFIA_CUDA(ctx, s->dcount.ensure(sizeof(long long) * 4));
+    SOFIA_CUDA(ctx, cudaMemset(s->dcount.p, 0, sizeof(long long) * 4));
+    SOFIA_CUDA(ctx, cudaMemset(s->status_local.p, 0, sizeof(int) * ST_NSLOTS));
     return SOFIA_OK;
 }
 
@@ -778,32 +837,8 @@ static int sys_alloc_list(Sys *s) {
     return SOFIA_OK;
 }
 
-// Launch the list build (unconditionally).  Errors and overflows land in status_local.
-static int sys_build(Sys *s) {
-    sofia_nb_ctx *ctx = s->ctx;
-    cudaStream_t st = ctx->stream;
-    const int n = s->n;
-    int *col_of = s->col_atoms.as<int>() + n;
-    SOFIA_CUDA(ctx, cudaMemsetAsync(s->col_count.p, 0, sizeof(int) * (s->ncols + 1), st));
-    SOFIA_CUDA(ctx, cudaMemsetAsync(s->col_fill.p, 0, sizeof(int) * (s->ncols + 1), st));
-    k_wrap_bin<<<grid_for(n, 256), 256, 0, st>>>(
-        n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(), s->L, s->s_col,
-        s->ncx, s->img[0].as<double>(), s->img[1].as<double>(), s->img[2].as<double>(),
-        s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(), col_of,
-        s->col_count.as<int>(), s->col_key.as<float>());
-    k_scan1<<<1, 1024, 0, st>>>(s->ncols, s->col_count.as<int>(), s->col_start.as<int>(), 0);
-    k_scan1<<<1, 1024, 0, st>>>(s->ncols, s->col_count.as<int>(), s->cl_start.as<int>(), 1);
-    k_col_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, col_of, s->col_start.as<int>(),
-                                                    s->col_fill.as<int>(), s->col_atoms.as<int>());
-    int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
-    SOFIA_CUDA(ctx, cudaMemsetAsync(s->slot_orig.p, 0xff, sizeof(int) * (size_t)s->max_clusters * CL, st));
-    k_col_sort_assign<<<s->ncols, 256, 0, st>>>(s->ncols, s->col_start.as<int>(),
-                                                s->col_atoms.as<int>(), s->col_key.as<float>(),
-                                                s->cl_start.as<int>(), s->slot_orig.as<int>(),
-                                                cl_col, s->status_local.as<int>());
-    // number of clusters = cl_start[ncols]
-    SOFIA_CUDA(ctx, cudaMemcpyAsync(s->nclusters.p, s->cl_start.as<int>() + s->ncols, sizeof(int),
-                                    cudaMemcpyDeviceToDevice, st));
+static void sys_pack(Sys *s) {
+    cudaStream_t st = s->ctx->stream;
     const int nslots = s->max_clusters * CL;
     k_pack<<<grid_for(nslots, 256), 256, 0, st>>>(
         nslots, s->nclusters.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(),
@@ -811,10 +846,50 @@ static int sys_build(Sys *s) {
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
         s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
         s->rec.as<AtomRec>(), s->recf.as<float4>());
+    s->launches += 1;
+}
+
+// Launch the list build.  With cond == nullptr it always runs; otherwise every
+// kernel returns at once unless (cond[0] & 1).  The records are packed in the
+// middle (the bounding boxes and the search need them), so after this call the
+// records are current whether or not the list was rebuilt.
+static int sys_build(Sys *s, const int *cond) {
+    sofia_nb_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = s->n;
+    const int cm = 1;
+    int *col_of = s->col_atoms.as<int>() + n;
+    int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
+    const int nslots = s->max_clusters * CL;
+    k_build_prep<<<grid_for(nslots, 256), 256, 0, st>>>(cond, cm, s->ncols + 1,
+                                                        s->col_count.as<int>(),
+                                                        s->col_fill.as<int>(), nslots,
+                                                        s->slot_orig.as<int>());
+    k_wrap_bin<<<grid_for(n, 256), 256, 0, st>>>(
+        cond, cm, n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(), s->L,
+        s->s_col, s->ncx, s->img[0].as<double>(), s->img[1].as<double>(), s->img[2].as<double>(),
+        s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(), col_of,
+        s->col_count.as<int>(), s->col_key.as<float>());
+    k_scan1<<<1, 1024, 0, st>>>(cond, cm, s->ncols, s->col_count.as<int>(),
+                                s->col_start.as<int>(), 0);
+    k_scan1<<<1, 1024, 0, st>>>(cond, cm, s->ncols, s->col_count.as<int>(),
+                                s->cl_start.as<int>(), 1);
+    k_col_scatter<<<grid_for(n, 256), 256, 0, st>>>(cond, cm, n, col_of, s->col_start.as<int>(),
+                                                    s->col_fill.as<int>(),
+                                                    s->col_atoms.as<int>());
+    k_col_sort_assign<<<s->ncols, 256, 0, st>>>(cond, cm, s->ncols, s->col_start.as<int>(),
+                                                s->col_atoms.as<int>(), s->col_key.as<float>(),
+                                                s->cl_start.as<int>(), s->slot_orig.as<int>(),
+                                                cl_col, s->status_local.as<int>());
+    k_set_ncl<<<1, 32, 0, st>>>(cond, cm, s->cl_start.as<int>() + s->ncols,
+                                s->nclusters.as<int>());
+    sys_pack(s);
     k_bbox<<<grid_for(s->max_clusters, 128), 128, 0, st>>>(
-        s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->slot_orig.as<int>(),
-        s->bb.as<float4>());
+        cond, cm, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
+        s->slot_orig.as<int>(), s->bb.as<float4>());
     SearchArgs a;
+    a.cond = cond;
+    a.cmask = cm;
     a.maxcl = s->max_clusters;
     a.ncx = s->ncx;
     a.reach = s->ncol_reach;
@@ -837,8 +912,8 @@ static int sys_build(Sys *s) {
     a.status = s->status_local.as<int>();
     k_search<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(a);
     SOFIA_CUDA(ctx, cudaGetLastError());
-    s->launches += 8;
-    s->n_builds++;
+    s->launches += 10;
+    if (!cond) s->n_builds++;
     s->built = 1;
     return SOFIA_OK;
 }
@@ -897,32 +972,23 @@ static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
 
 // Launches: displacement check, conditional rebuild, pack, pair kernel.
 // `force_build` rebuilds regardless of the trigger.
-static void sys_prune(Sys *s) {
+static void sys_prune(Sys *s, const int *cond) {
     cudaStream_t st = s->ctx->stream;
     const float rin = (float)(s->rc + s->margin);
     const float rin2 = rin * rin + 1e-3f;
     k_prune<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(
-        s->max_clusters, s->nclusters.as<int>(), s->recf.as<float4>(), s->jlist.as<int>(),
-        s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap, (float)s->L, rin2,
-        s->ilist.as<int>(), s->imask.as<unsigned long long>(), s->icount.as<int>());
-    k_copy3<<<grid_for(s->n, 256), 256, 0, st>>>(s->n, s->x[0].as<double>(), s->x[1].as<double>(),
-                                                 s->x[2].as<double>(), s->xprn[0].as<double>(),
-                                                 s->xprn[1].as<double>(), s->xprn[2].as<double>());
+        cond, 3, s->max_clusters, s->nclusters.as<int>(), s->recf.as<float4>(),
+        s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,
+        (float)s->L, rin2, s->ilist.as<int>(), s->imask.as<unsigned long long>(),
+        s->icount.as<int>());
+    k_copy3<<<grid_for(s->n, 256), 256, 0, st>>>(cond, 3, s->n, s->x[0].as<double>(),
+                                                 s->x[1].as<double>(), s->x[2].as<double>(),
+                                                 s->xprn[0].as<double>(), s->xprn[1].as<double>(),
+                                                 s->xprn[2].as<double>());
     s->launches += 2;
-    s->n_prunes++;
+    if (!cond) s->n_prunes++;
 }
 
-static void sys_pack(Sys *s) {
-    cudaStream_t st = s->ctx->stream;
-    const int nslots = s->max_clusters * CL;
-    k_pack<<<grid_for(nslots, 256), 256, 0, st>>>(
-        nslots, s->nclusters.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(),
-        s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
-        s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
-        s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
-        s->rec.as<AtomRec>(), s->recf.as<float4>());
-    s->launches += 1;
-}
 
 // One evaluation: displacement triggers, list rebuild or prune when due, pack,
 // pair kernel on the pruned list, deterministic energy reduction.
@@ -952,7 +1018,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
         if (build) {
             SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * ST_NSLOTS, st));
             if (s->timing) cudaEventRecord(s->ev[0], st);
-            int rc = sys_build(s);
+            int rc = sys_build(s, nullptr);
             if (rc) return rc;
             if (s->timing) {
                 cudaEventRecord(s->ev[1], st);
@@ -976,7 +1042,14 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
         }
         break;
     }
-    if (prune) sys_prune(s);
+    if (prune) sys_prune(s, nullptr);
+    return sys_pair(s, precision, energy, virial);
+}
+
+// Pair kernel (+ energy reduction) on the pruned list.
+int sys_pair(Sys *s, int precision, bool energy, bool virial) {
+    sofia_nb_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
     PairConst k = make_pair_const(s, nullptr);
     const int blocks = grid_for((long)s->max_clusters * 32, 256);
     const size_t smem = sizeof(float4) * (size_t)s->ntypes * s->ntypes;
@@ -1019,13 +1092,57 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
     return SOFIA_OK;
 }
 
+// Device-only evaluation, no host round trip (graph-capturable): displacement
+// triggers (or a forced build), conditional rebuild, pack, conditional prune,
+// pair kernel.  Row-capacity overflow is recorded in status_local and checked
+// by the caller after the segment (sys_list_overflow).
+int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build) {
+    sofia_nb_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = s->n;
+    int *flag = s->flag.as<int>();
+    if (force_build || !s->built) {
+        k_set_flag<<<1, 32, 0, st>>>(flag, 3);
+    } else {
+        const double half = 0.5 * s->skin, phalf = 0.5 * s->margin;
+        k_set_flag<<<1, 32, 0, st>>>(flag, 0);
+        k_disp_check<<<grid_for(n, 256), 256, 0, st>>>(
+            n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
+            s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(),
+            s->xprn[0].as<double>(), s->xprn[1].as<double>(), s->xprn[2].as<double>(), s->L,
+            half * half, phalf * phalf, flag);
+    }
+    int rc = sys_build(s, flag);
+    if (rc) return rc;
+    sys_prune(s, flag);
+    k_count_events<<<1, 32, 0, st>>>(flag, s->dcount.as<long long>());
+    s->launches += 3;
+    return sys_pair(s, precision, energy, virial);
+}
+
+// After a device-only segment: SOFIA_ENEEDGROW (and a larger row capacity) if
+// some list row overflowed; SOFIA_EINVAL if a column overflowed.
+int sys_list_overflow(Sys *s) {
+    sofia_nb_ctx *ctx = s->ctx;
+    int hs[ST_NSLOTS];
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (hs[ST_CELLOVER]) return fail(ctx, SOFIA_EINVAL, "an xy column holds more than 2048 atoms%s");
+    if (hs[ST_NCLUSTER] > s->jcap) {
+        s->jcap = (int)(hs[ST_NCLUSTER] * 1.2) + 16;
+        int r2 = sys_alloc_list(s);
+        if (r2) return r2;
+        SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * ST_NSLOTS, ctx->stream));
+        s->built = 0;
+        return SOFIA_ENEEDGROW;
+    }
+    return SOFIA_OK;
+}
+
 }  // namespace sofia
 
 using sofia::Sys;
-
-struct sofia_system {
-    Sys s;
-};
 
 extern "C" int sofia_system_create(sofia_nb_ctx *ctx, const sofia_system_desc *d,
                                    sofia_system **out) {
@@ -1141,6 +1258,7 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
     s->ilist.release();
     s->imask.release();
     s->recf.release();
+    s->dcount.release();
     s->icount.release();
     s->part.release();
     sofia::DevBuf *bufs[] = {&s->type, &s->q, &s->invm, &s->mass, &s->specbond, &s->num3bond,
@@ -1231,6 +1349,7 @@ extern "C" int sofia_system_set_state(sofia_system *ss, const double *x, const d
     delete[] h;
     delete[] c;
     s->built = 0;
+    s->md.forces_valid = 0;
     SOFIA_CUDA(ctx, cudaDeviceSynchronize());
     return SOFIA_OK;
 }
@@ -1303,8 +1422,11 @@ extern "C" int sofia_system_stats(sofia_system *ss, int64_t *stats, int nstats) 
         for (int i = 0; i < ncl; ++i) inner += jc[i];
         delete[] jc;
     }
-    const int64_t vals[10] = {s->n_builds, ncl, entries, s->jcap, s->ncx, s->max_clusters,
-                              s->ncol_reach, s->launches, s->n_prunes, inner};
+    long long dc[2] = {0, 0};
+    cudaMemcpy(dc, s->dcount.p, sizeof(dc), cudaMemcpyDeviceToHost);
+    const int64_t vals[10] = {s->n_builds + dc[0], ncl, entries, s->jcap, s->ncx,
+                              s->max_clusters, s->ncol_reach, s->launches, s->n_prunes + dc[1],
+                              inner};
     for (int i = 0; i < nstats && i < 10; ++i) stats[i] = vals[i];
     return SOFIA_OK;
 }

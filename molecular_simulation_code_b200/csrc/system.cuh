@@ -28,6 +28,31 @@ struct __align__(16) AtomRec {
     int type;
 };
 
+// Device-resident MD state (velocity Verlet + force-form Langevin + SHAKE +
+// bonded terms) of one system.
+struct Md {
+    int ready = 0;
+    double dt = 2.0, temperature = 300.0, gamma = 0.0;  // fs, K, 1/fs
+    unsigned long long seed = 0;
+    int nbond = 0, nangle = 0, ndihed = 0, nshake = 0;
+    int nbt = 0, nat = 0, ndt = 0;
+    DevBuf bonds, bcoef, angles, acoef, diheds, dcoef, lj14, shake, sbond;
+    int shake_maxiter = 25;
+    double shake_tol = 1e-4;
+    int terms = 15;
+    DevBuf eterm;          // per-term energy partials
+    DevBuf ered;           // reduced energies
+    DevBuf step_dev;       // device step counter (RNG counter inside graphs)
+    DevBuf snap[7];        // x, v (3 each) and the step counter at segment start
+    double e_self = 0.0;
+    int ndof = 0;
+    long long step = 0;
+    int forces_valid = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    long long graph_launches[2] = {0, 0};
+    int graph_ok = 0;
+};
+
 struct Sys {
     sofia_nb_ctx *ctx = nullptr;
     int n = 0, ntypes = 0, precision = 0;
@@ -52,7 +77,7 @@ struct Sys {
     DevBuf flag;                        // rebuild flag (int)
     DevBuf stage_pos, stage_ff;
     // pruned inner list (rc + margin) and the positions it was pruned at
-    DevBuf ilist, imask, icount, xprn[3], part;
+    DevBuf ilist, imask, icount, xprn[3], part, dcount;
     double margin = 0.6;
     long long n_prunes = 0;
     int built = 0;
@@ -64,6 +89,17 @@ struct Sys {
     double t_build_ms = 0.0, t_pair_ms = 0.0;
     long long n_pair = 0, n_build_timed = 0;
     int pending_build = 0, pending_pair = 0;
+    Md md;
 };
 
+// evaluation entry points (mixed.cu)
+int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build);
+int sys_pair(Sys *s, int precision, bool energy, bool virial);
+int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build);
+int sys_list_overflow(Sys *s);
+
 }  // namespace sofia
+
+struct sofia_system {
+    sofia::Sys s;
+};

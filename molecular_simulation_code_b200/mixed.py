@@ -12,7 +12,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import SOFIA_OK, SOFIA_PREC_FP64, SOFIA_PREC_MIXED, SofiaError, SofiaSystemDesc
+from ._lib import (MD_ENERGY_NAMES, SOFIA_MD_NE, SOFIA_OK, SOFIA_PREC_FP64, SOFIA_PREC_MIXED,
+                   SofiaError, SofiaMdDesc, SofiaSystemDesc)
 from .nonbond import Context, ptr
 
 MIXED = SOFIA_PREC_MIXED
@@ -98,6 +99,34 @@ class System:
 
     def drift(self, dt: float, nsteps: int = 1):
         self.ctx.check(self.ctx._lib.sofia_system_drift(self.handle, float(dt), int(nsteps)))
+
+    def md_setup(self, sysdata, dt: float = 2.0, temperature: float = 300.0,
+                 gamma: float = 0.001, seed: int = 1, terms: int = 15, shake: bool = True,
+                 shake_maxiter: int = 0, shake_tol: float = 0.0):
+        """Bonded lists, SHAKE groups and thermostat of the device-resident MD."""
+        k = [np.ascontiguousarray(a) for a in (
+            sysdata.bonds.astype(np.int32), sysdata.bond_coeff.astype(np.float64),
+            sysdata.angles.astype(np.int32), sysdata.angle_coeff.astype(np.float64),
+            sysdata.dihedrals.astype(np.int32), sysdata.dihed_coeff.astype(np.float64),
+            np.ascontiguousarray(sysdata.lj14, np.float64).reshape(-1),
+            sysdata.shake.astype(np.int32), sysdata.shake_bond.astype(np.float64))]
+        self._md_keep = k
+        ns = k[7].shape[0] if shake else 0
+        d = SofiaMdDesc(float(dt), float(temperature), float(gamma), int(seed), int(terms),
+                        k[0].shape[0], ptr(k[0]), k[1].shape[0], ptr(k[1]),
+                        k[2].shape[0], ptr(k[2]), k[3].shape[0], ptr(k[3]),
+                        k[4].shape[0], ptr(k[4]), k[5].shape[0], ptr(k[5]), ptr(k[6]),
+                        ns, ptr(k[7]), ptr(k[8]), int(shake_maxiter), float(shake_tol))
+        self.ctx.check(self.ctx._lib.sofia_system_md_setup(self.handle, C.byref(d)))
+
+    def md_run(self, nsteps: int, energy_every: int = 0, use_graph: bool = True) -> dict | None:
+        e = np.zeros(SOFIA_MD_NE)
+        self.ctx.check(self.ctx._lib.sofia_system_md_run(self.handle, int(nsteps),
+                                                         int(energy_every), int(use_graph),
+                                                         ptr(e)))
+        if energy_every <= 0:
+            return None
+        return dict(zip(MD_ENERGY_NAMES, e.tolist()))
 
     def timers(self, enable: bool = True) -> dict:
         t = np.zeros(4)

@@ -1,0 +1,98 @@
+"""GPU tests of the device-resident MD step (residency kernels around the hot path)."""
+import numpy as np
+import pytest
+
+from molecular_simulation_code_b200 import mixed as M
+from molecular_simulation_code_b200.system import make_system
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(ctx, s, precision=M.MIXED, **md):
+    sysm = M.System(ctx, s, cut=8.0, skin=2.0, precision=precision)
+    sysm.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
+    sysm.md_setup(s, **md)
+    return sysm
+
+
+@pytest.fixture(scope="module")
+def small():
+    return make_system(20, 900, 21)
+
+
+def _constraint_err(s, x):
+    L = float(s.box)
+    worst = 0.0
+    for g, b in zip(s.shake, s.shake_bond):
+        num, a = int(g[0]), g[1:] - 1
+        pairs = {1: [(0, 1)], 3: [(0, 1), (0, 2)], 4: [(0, 1), (0, 2), (0, 3)],
+                 -3: [(0, 1), (0, 2), (1, 2)]}[num]
+        for k, (u, w) in enumerate(pairs):
+            d = x[a[u]] - x[a[w]]
+            d -= L * np.round(d / L)
+            worst = max(worst, abs(np.linalg.norm(d) - b[k]))
+    return worst
+
+
+def test_md_deterministic_and_graph_equals_eager(ctx, small):
+    s = small
+    a = _system(ctx, s, dt=1.0, gamma=0.01, seed=7)
+    a.md_run(30, use_graph=True)
+    xa, va, fa = a.get_state()
+    b = _system(ctx, s, dt=1.0, gamma=0.01, seed=7)
+    b.md_run(30, use_graph=False)
+    xb, vb, fb = b.get_state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb) and np.array_equal(fa, fb)
+    c = _system(ctx, s, dt=1.0, gamma=0.01, seed=8)
+    c.md_run(30)
+    xc, _, _ = c.get_state()
+    assert not np.array_equal(xa, xc)  # another noise stream
+    for o in (a, b, c):
+        o.close()
+
+
+def test_md_shake_keeps_constraints(ctx, small):
+    s = small
+    a = _system(ctx, s, dt=1.0, gamma=0.02, seed=3, shake_maxiter=200, shake_tol=1e-10)
+    a.md_run(50)
+    x, _, _ = a.get_state()
+    assert _constraint_err(s, x) < 1e-5
+    a.close()
+
+
+def test_md_langevin_thermalises_and_stays_finite(ctx, small):
+    s = small
+    a = _system(ctx, s, dt=1.0, gamma=0.05, seed=5, temperature=300.0)
+    e = None
+    for _ in range(8):
+        e = a.md_run(50, energy_every=50)
+    assert np.isfinite(e["total"])
+    assert 200.0 < e["temperature"] < 420.0, e
+    x, v, f = a.get_state()
+    assert np.all(np.isfinite(x)) and np.all(np.isfinite(v))
+    a.close()
+
+
+def test_md_nve_conserves_energy_short(ctx, small):
+    s = small
+    a = _system(ctx, s, dt=1.0, gamma=0.05, seed=9, shake_maxiter=100, shake_tol=1e-10)
+    a.md_run(300)  # relax the lattice start under the thermostat
+    a.md_setup(s, dt=1.0, gamma=0.0, seed=9, shake_maxiter=100, shake_tol=1e-10)
+    es = [a.md_run(20, energy_every=20)["total"] for _ in range(10)]
+    ke = a.md_run(1, energy_every=1)["kinetic"]
+    spread = max(es) - min(es)
+    assert spread < 0.01 * ke, (es, ke)
+    a.close()
+
+
+def test_md_fp64_and_mixed_trajectories_stay_close(ctx, small):
+    s = small
+    a = _system(ctx, s, dt=1.0, gamma=0.0, seed=1)
+    b = _system(ctx, s, precision=M.FP64, dt=1.0, gamma=0.0, seed=1)
+    a.md_run(10)
+    b.md_run(10)
+    xa, _, _ = a.get_state()
+    xb, _, _ = b.get_state()
+    assert np.abs(xa - xb).max() < 1e-3
+    a.close()
+    b.close()
