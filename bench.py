@@ -3,17 +3,22 @@
 
 Workload (default): the 275,000-atom glycine/water system (3,500 glycine +
 80,000 SPC/E water, 1.0 g/cm^3, L = 14.1 nm), rc = 10 A, skin 2 A, DSF
-alpha = 0.2 A^-1, seeded synthetic coordinates.  One step = advance the
-positions by one 2 fs ballistic step (device kernel), then the hot path:
-displacement check, list rebuild when an atom has moved more than skin/2,
-and the LJ + DSF forces, energies and virial of the mixed FP32-pair /
-64-bit fixed-point kernel.
+alpha = 0.2 A^-1, seeded synthetic coordinates, 2 fs steps, Langevin 300 K
+with gamma = 1/ps, SHAKE on X-H bonds and rigid water.
 
-Printed (rank 0, one JSON line): value = device-resident atom-steps/s of
-the mixed path (max over ranks, replicas only); e2e = the same through the
-drop-in C ABI call with pinned host buffers (positions in, forces out every
-step); the plain FP64 variants; roofline of the pair kernel against a
-measured FP32 CUDA-core peak; the CPU baseline (oracle port, all host cores).
+value: device-resident MD atom-steps/s of the mixed path (FP64 positions,
+FP32 pair arithmetic, 64-bit fixed-point forces): each step is velocity
+Verlet + Langevin + SHAKE + bonded/1-4 terms + the nonbonded hot path
+(displacement check, list rebuild/prune on trigger, LJ + DSF forces), the
+steps captured as one CUDA graph, energies on the last step of the timed
+segment; max over ranks (replicas only, no exchange).
+e2e: the reference-facing drop-in call (sofia_force_nonbond_mixed) with
+pinned host buffers: positions in, real*4 forces and energies out, every
+step, on a ballistic trajectory.
+Also reported: the plain FP64 variants (same MD in FP64, and the FP64
+reference-semantics path), the nonbonded-only hot path, the roofline of the
+pair kernel against a measured FP32 CUDA-core peak, and the CPU baseline
+(oracle port, all host cores).
 
 ``--impl reference`` times the CPU restatement of the reference path
 (oracle port, OpenMP over all host cores) on the same workload and metric.
@@ -35,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 DT = 2.0            # fs
+RELAX_STEPS = 100   # untimed damped steps from the lattice start
 CUT = 10.0          # A
 SKIN = 2.0          # A
 ALPHA = 0.2         # 1/A
@@ -306,6 +312,30 @@ def run_ours(args, rank, ws):
     v0 = s.velocity.astype(np.float64)
     sysm.set_state(x0, v0)
 
+    def md_loop(precision, nsteps, warm):
+        """Device-resident MD: relax (untimed), warm up, then time nsteps in one graph segment."""
+        m = M.System(ctx, s, alpha=ALPHA, cut=CUT, skin=SKIN, precision=precision)
+        m.set_state(x0, v0)
+        m.md_setup(s, dt=1.0, temperature=300.0, gamma=0.02, seed=11)
+        m.md_run(RELAX_STEPS)  # lattice start: short strongly damped relaxation
+        m.md_setup(s, dt=DT, temperature=300.0, gamma=0.001, seed=12)
+        m.md_run(max(warm, 1))
+        b0 = m.stats()
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        en = m.md_run(nsteps, energy_every=nsteps, use_graph=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        b1 = m.stats()
+        t = e0.elapsed_time(e1) / 1e3
+        m.close()
+        return t, en, b1["builds"] - b0["builds"], b1["prunes"] - b0["prunes"], \
+            b1["launches"] - b0["launches"]
+
     def timed_loop(precision, nsteps, warm):
         sysm.set_state(x0, v0)
         for _ in range(warm):
@@ -330,9 +360,18 @@ def run_ours(args, rank, ws):
         return t, tm, b1["builds"] - b0["builds"], b1["launches"] - b0["launches"], b1
 
     with Clocks(dev) as clk:
-        t_mixed, tm, builds, launches, st = timed_loop(M.MIXED, args.steps, args.warmup)
-    t_max = allreduce_max(t_mixed, ws, device=torch.device("cuda", dev))
+        t_md, md_en, md_builds, md_prunes, md_launches = md_loop(M.MIXED, args.steps,
+                                                                 args.warmup)
+    t_max = allreduce_max(t_md, ws, device=torch.device("cuda", dev))
     value = n * ws * args.steps / t_max
+    t_md64 = None
+    if not args.no_fp64:
+        t_md64, _, _, _, _ = md_loop(M.FP64, args.steps, args.warmup)
+        t_md64 = allreduce_max(t_md64, ws, device=torch.device("cuda", dev))
+
+    # nonbonded hot path only (ballistic drift between evaluations), with kernel timers
+    t_hot, tm, builds, launches, st = timed_loop(M.MIXED, args.steps, args.warmup)
+    t_hot = allreduce_max(t_hot, ws, device=torch.device("cuda", dev))
 
     # plain FP64 twin of the same kernel and list
     t_fp64 = None
@@ -412,7 +451,7 @@ def run_ours(args, rank, ws):
     P_rv = count_pairs_within(s, CUT + SKIN)
     pair_ms = tm["pair_ms"] / max(tm["pairs"], 1)
     achieved = FLOP_PER_PAIR * P_rv / (pair_ms / 1e3) / 1e12
-    rebuild_interval = args.steps / max(builds, 1)
+    rebuild_interval = args.steps / max(md_builds, 1)
     cpu = None if args.no_cpu_baseline else cpu_baseline(s, rebuild_interval)
     clocks = clk.summary()
     out = {
@@ -425,16 +464,22 @@ def run_ours(args, rank, ws):
                    "parallelism": f"replicas x{ws} (no exchange)",
                    "l2": "inputs larger than L2 (cluster-pair list "
                          f"{st['entries'] * 12 / 1e9:.2f} GB)",
-                   "step": "2 fs ballistic position update + displacement check + list rebuild "
-                           "or prune on trigger + LJ/DSF forces and energies (no virial, as the "
-                           "reference DSF path)"},
-        "fp64": {"cluster_atom_steps_per_s": (n * ws * args.steps / t_fp64) if t_fp64 else None,
-                 "reference_list_atom_steps_per_s": (n * ws * args.steps / t_ref) if t_ref else None,
-                 "mixed_over_fp64_cluster": (t_fp64 / t_max) if t_fp64 else None,
-                 "mixed_over_fp64_reference_list": (t_ref / t_max) if t_ref else None},
+                   "step": "2 fs MD step: velocity Verlet + Langevin 300 K + SHAKE + bonded/1-4 + "
+                           "nonbonded LJ/DSF (list rebuild/prune on device triggers), CUDA graph"},
+        "md": {"energies_last_step": md_en, "list_rebuilds": md_builds, "prunes": md_prunes,
+               "ns_per_day": DT * 1e-6 * args.steps / t_max * 86400.0},
+        "fp64": {"md_atom_steps_per_s": (n * ws * args.steps / t_md64) if t_md64 else None,
+                 "mixed_over_fp64_md": (t_md64 / t_max) if t_md64 else None,
+                 "hot_path_cluster_atom_steps_per_s": (n * ws * args.steps / t_fp64) if t_fp64 else None,
+                 "hot_path_reference_list_atom_steps_per_s": (n * ws * args.steps / t_ref) if t_ref else None,
+                 "hot_path_mixed_over_fp64_cluster": (t_fp64 / t_hot) if t_fp64 else None,
+                 "hot_path_mixed_over_fp64_reference_list": (t_ref / t_hot) if t_ref else None},
+        "hot_path": {"atom_steps_per_s": n * ws * args.steps / t_hot,
+                     "step": "2 fs ballistic update + displacement check + rebuild/prune on "
+                             "trigger + LJ/DSF forces and energies"},
         "e2e": {"value": n * ws * args.steps / t_e2e, "unit": "atom-steps/s",
                 "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 12 * n + 40},
-        "gpu_launches": launches,
+        "gpu_launches": md_launches,
         "list": {"rebuilds": builds, "clusters": st["clusters"], "entries": st["entries"],
                  "pruned_entries": st["inner_entries"], "prunes": st["prunes"],
                  "build_ms": tm["build_ms"] / max(tm["builds"], 1)},

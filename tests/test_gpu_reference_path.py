@@ -224,3 +224,17 @@ def test_greatest_cluster_bit_exact(ctx, seed, crystal, greatest_in):
         assert gsz == osz and gg == og
         assert np.array_equal(gd, od) and np.array_equal(gb, ob)
         assert np.array_equal(pt_g, pt_o)
+
+
+def test_neighbor_list_sets_bit_exact_90k(ctx):
+    """The 90,000-atom configuration (rc 10 A, skin 2 A): identical sorted rows."""
+    from molecular_simulation_code_b200.system import make_workload
+    s = make_workload("gly1500_wat25000_90k", seed=2000)
+    p = ref_params(s, cut=10.0, pad=2.0)
+    pos = s.position_aos()
+    nl, nn, na = nb.neighbor_wrapper(ctx, pos, s.specbond, s.num3bond, p, 1024)
+    onl, onn, ona = O.neighbor_wrapper(_orc_params(p), pos, s.specbond, s.num3bond, 1024)
+    assert np.array_equal(nn, onn)
+    rows_gpu = [np.sort(nl[i * na:i * na + nn[i]]) for i in range(0, s.np_atoms, 7)]
+    rows_orc = [np.sort(onl[i * ona:i * ona + onn[i]]) for i in range(0, s.np_atoms, 7)]
+    assert all(np.array_equal(g, o) for g, o in zip(rows_gpu, rows_orc))
