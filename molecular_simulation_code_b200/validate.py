@@ -82,9 +82,14 @@ def main(argv=None):
             es.append(e["total"])
         ts = np.array(ts)
         es = np.array(es)
-        slope = float(np.polyfit(ts, es, 1)[0])  # kcal/mol/ns
+        coef = np.polyfit(ts, es, 1)
+        slope = float(coef[0])  # kcal/mol/ns
+        resid = es - np.polyval(coef, ts)
+        # standard error of the least-squares slope (independent residuals)
+        se = float(np.sqrt((resid ** 2).sum() / max(len(ts) - 2, 1) / ((ts - ts.mean()) ** 2).sum()))
         drift[name] = {"kT_per_ns_per_atom": slope / kT / n,
-                       "energy_rms_fluct_kcal": float(np.std(es - np.polyval(np.polyfit(ts, es, 1), ts))),
+                       "stderr_kT_per_ns_per_atom": se / kT / n,
+                       "energy_rms_fluct_kcal": float(np.std(resid)),
                        "ps": args.nve_ps, "last_temperature_K": e["temperature"]}
         sysn.close()
     out = {"workload": args.workload, "atoms": n, "snapshots": args.snapshots,
