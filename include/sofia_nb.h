@@ -308,6 +308,21 @@ int sofia_system_md_setup(sofia_system *sys, const sofia_md_desc *md);
 int sofia_system_md_run(sofia_system *sys, int nsteps, int energy_every, int use_graph,
                         double *energies);
 
+/*
+ * Batches of independent replicas (no reference counterpart: the reference
+ * runs one replica per MPI rank, Source/MD.f90:26-44, with no exchange).
+ * Every system must have its own context (stream) on the batch's device for
+ * the replicas to overlap; one CUDA graph per step kind forks one step of
+ * every replica and joins it.  energies = [n][SOFIA_MD_NE].
+ */
+typedef struct sofia_batch sofia_batch;
+int sofia_batch_create(sofia_nb_ctx *ctx, sofia_system *const *systems, int n, sofia_batch **out);
+int sofia_batch_destroy(sofia_batch *batch);
+int sofia_batch_md_run(sofia_batch *batch, int nsteps, int energy_every, double *energies);
+/* Prune margin (A) of the pruned inner list (default 0.6): the tuning knob
+ * the autotuner picks per size class. */
+int sofia_system_set_margin(sofia_system *sys, double margin);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,10 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_system_drift": (_I, [_P, _D, _I]),
     "sofia_system_md_setup": (_I, [_P, C.POINTER(SofiaMdDesc)]),
     "sofia_system_md_run": (_I, [_P, _I, _I, _I, _P]),
+    "sofia_batch_create": (_I, [_P, _P, _I, C.POINTER(_P)]),
+    "sofia_batch_destroy": (_I, [_P]),
+    "sofia_batch_md_run": (_I, [_P, _I, _I, _P]),
+    "sofia_system_set_margin": (_I, [_P, _D]),
     "sofia_system_timers": (_I, [_P, _I, _P]),
 }
 

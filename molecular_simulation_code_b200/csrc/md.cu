@@ -17,6 +17,7 @@
 // State is FP64 (positions, velocities) with 64-bit fixed-point forces; all
 // force contributions are added in integers, so a step is bit-reproducible.
 #include <cmath>
+#include <vector>
 
 #include "system.cuh"
 
@@ -810,4 +811,225 @@ extern "C" int sofia_system_md_run(sofia_system *ss, int nsteps, int energy_ever
         return SOFIA_OK;
     }
     return sofia::fail(ctx, SOFIA_ENEEDGROW, "list capacity kept overflowing%s");
+}
+
+// ---------------------------------------------------------------------------
+// Batches of independent replicas.  Every replica keeps its own resident state
+// and list on its own context stream; one CUDA graph per step kind forks from
+// the batch stream into every replica stream, records each replica's MD step
+// there, and joins back, so a whole multi-replica step is one graph launch and
+// replicas of different sizes overlap on the GPU.  Replicas never exchange
+// data: each result is bit-identical to the same replica run alone.
+struct sofia_batch {
+    sofia_nb_ctx *ctx = nullptr;
+    std::vector<sofia_system *> sys;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    long long graph_launches[2] = {0, 0};
+    int graph_ok = 0;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+};
+
+static void batch_drop_graphs(sofia_batch *b) {
+    for (auto &g : b->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    b->graph_ok = 0;
+}
+
+extern "C" int sofia_batch_create(sofia_nb_ctx *ctx, sofia_system *const *systems, int n,
+                                  sofia_batch **out) {
+    if (!ctx || !systems || n <= 0 || !out) return SOFIA_EINVAL;
+    *out = nullptr;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    for (int i = 0; i < n; ++i) {
+        if (!systems[i]) return sofia::fail(ctx, SOFIA_EINVAL, "null system in batch%s");
+        if (systems[i]->s.ctx->device != ctx->device)
+            return sofia::fail(ctx, SOFIA_EINVAL, "batch systems must share the device%s");
+        if (!systems[i]->s.md.ready)
+            return sofia::fail(ctx, SOFIA_EINVAL, "sofia_system_md_setup every system first%s");
+        for (int j = 0; j < i; ++j)
+            if (systems[j] == systems[i]) return sofia::fail(ctx, SOFIA_EINVAL, "system listed twice%s");
+    }
+    sofia_batch *b = new sofia_batch();
+    b->ctx = ctx;
+    b->sys.assign(systems, systems + n);
+    b->join.resize(n, nullptr);
+    cudaError_t e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int i = 0; i < n && e == cudaSuccess; ++i)
+        e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        sofia_batch_destroy(b);
+        return sofia::cuda_fail(ctx, e, "batch events");
+    }
+    *out = b;
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_batch_destroy(sofia_batch *b) {
+    if (!b) return SOFIA_OK;
+    if (b->ctx) cudaStreamSynchronize(b->ctx->stream);
+    batch_drop_graphs(b);
+    if (b->fork) cudaEventDestroy(b->fork);
+    for (auto e : b->join)
+        if (e) cudaEventDestroy(e);
+    delete b;
+    return SOFIA_OK;
+}
+
+static int batch_capture(sofia_batch *b) {
+    batch_drop_graphs(b);
+    sofia_nb_ctx *ctx = b->ctx;
+    cudaStream_t ms = ctx->stream;
+    for (int e = 0; e < 2; ++e) {
+        cudaGraph_t g = nullptr;
+        long long launches = 0;
+        SOFIA_CUDA(ctx, cudaStreamBeginCapture(ms, cudaStreamCaptureModeRelaxed));
+        int rc = SOFIA_OK;
+        if (cudaEventRecord(b->fork, ms) != cudaSuccess) rc = SOFIA_ECUDA;
+        for (size_t i = 0; i < b->sys.size() && !rc; ++i) {
+            Sys *s = &b->sys[i]->s;
+            cudaStream_t st = s->ctx->stream;
+            if (st != ms && cudaStreamWaitEvent(st, b->fork, 0) != cudaSuccess) {
+                rc = SOFIA_ECUDA;
+                break;
+            }
+            const int timing = s->timing;
+            s->timing = 0;
+            const long long l0 = s->launches;
+            rc = sofia::md_step(s, e == 1);
+            launches += s->launches - l0;
+            s->launches = l0;
+            s->timing = timing;
+            if (!rc && st != ms) {
+                if (cudaEventRecord(b->join[i], st) != cudaSuccess ||
+                    cudaStreamWaitEvent(ms, b->join[i], 0) != cudaSuccess)
+                    rc = SOFIA_ECUDA;
+            }
+        }
+        cudaError_t ce = cudaStreamEndCapture(ms, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc == SOFIA_ECUDA ? sofia::fail(ctx, rc, "batch capture failed%s") : rc;
+        }
+        if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaStreamEndCapture (batch)");
+        ce = cudaGraphInstantiate(&b->graph[e], g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaGraphInstantiate (batch)");
+        b->graph_launches[e] = launches;
+    }
+    b->graph_ok = 1;
+    return SOFIA_OK;
+}
+
+// Runs nsteps steps of every replica.  energies[n*SOFIA_MD_NE] (may be NULL)
+// receive each replica's last-step energies when energy_every > 0.
+extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
+                                  double *energies) {
+    if (!b || nsteps < 0) return SOFIA_EINVAL;
+    sofia_nb_ctx *ctx = b->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t ms = ctx->stream;
+    const int n = (int)b->sys.size();
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        for (int i = 0; i < n; ++i) {
+            Sys *s = &b->sys[i]->s;
+            Md &md = s->md;
+            cudaStream_t st = s->ctx->stream;
+            const size_t nb = sizeof(double) * (size_t)s->n;
+            for (int d = 0; d < 3; ++d) {
+                SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[d].p, s->x[d].p, nb, cudaMemcpyDeviceToDevice, st));
+                SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[3 + d].p, s->v[d].p, nb, cudaMemcpyDeviceToDevice, st));
+            }
+            SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[6].p, md.step_dev.p, sizeof(long long), cudaMemcpyDeviceToDevice, st));
+            SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * sofia::ST_NSLOTS, st));
+            if (!md.forces_valid) {
+                int rc = sofia::md_forces(s, false, true);
+                if (rc) return rc;
+                md.forces_valid = 1;
+            }
+            SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+        }
+        if (!b->graph_ok) {
+            int rc = batch_capture(b);
+            if (rc) return rc;
+        }
+        for (int k = 0; k < nsteps; ++k) {
+            const bool en = energy_every > 0 && ((k + 1) % energy_every == 0 || k + 1 == nsteps);
+            SOFIA_CUDA(ctx, cudaGraphLaunch(b->graph[en ? 1 : 0], ms));
+        }
+        SOFIA_CUDA(ctx, cudaStreamSynchronize(ms));
+        bool regrow = false;
+        for (int i = 0; i < n; ++i) {
+            Sys *s = &b->sys[i]->s;
+            s->launches += (long long)nsteps * (b->graph_launches[0]) / (n > 0 ? n : 1);
+            const int rc = sofia::sys_list_overflow(s);
+            if (rc == SOFIA_ENEEDGROW) {
+                regrow = true;
+                continue;
+            }
+            if (rc) return rc;
+        }
+        if (regrow) {
+            batch_drop_graphs(b);
+            for (int i = 0; i < n; ++i) {
+                Sys *s = &b->sys[i]->s;
+                Md &md = s->md;
+                cudaStream_t st = s->ctx->stream;
+                const size_t nb = sizeof(double) * (size_t)s->n;
+                sofia::md_drop_graphs(s);
+                for (int d = 0; d < 3; ++d) {
+                    SOFIA_CUDA(ctx, cudaMemcpyAsync(s->x[d].p, md.snap[d].p, nb, cudaMemcpyDeviceToDevice, st));
+                    SOFIA_CUDA(ctx, cudaMemcpyAsync(s->v[d].p, md.snap[3 + d].p, nb, cudaMemcpyDeviceToDevice, st));
+                }
+                SOFIA_CUDA(ctx, cudaMemcpyAsync(md.step_dev.p, md.snap[6].p, sizeof(long long), cudaMemcpyDeviceToDevice, st));
+                md.forces_valid = 0;
+                s->built = 0;
+                SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+            }
+            continue;
+        }
+        for (int i = 0; i < n; ++i) {
+            Sys *s = &b->sys[i]->s;
+            Md &md = s->md;
+            int hs[sofia::ST_NSLOTS];
+            SOFIA_CUDA(ctx, cudaMemcpy(hs, s->status_local.p, sizeof(hs), cudaMemcpyDeviceToHost));
+            if (hs[sofia::ST_SHAKE])
+                return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE did not converge in a batch replica%s");
+            md.step += nsteps;
+            if (energies && energy_every > 0) {
+                double e[16];
+                SOFIA_CUDA(ctx, cudaMemcpy(e, md.ered.p, sizeof(double) * 16, cudaMemcpyDeviceToHost));
+                double *o = energies + (size_t)i * SOFIA_MD_NE;
+                const double pot = e[0] + e[1] + md.e_self + e[5] + e[6] + e[7] + e[8] + e[9];
+                o[0] = e[0];
+                o[1] = e[1];
+                o[2] = md.e_self;
+                o[3] = e[5];
+                o[4] = e[6];
+                o[5] = e[7];
+                o[6] = e[8];
+                o[7] = e[9];
+                o[8] = e[10];
+                o[9] = pot + e[10];
+                o[10] = 2.0 * e[10] / ((double)md.ndof * sofia::KBOLTZ);
+                o[11] = (double)md.step;
+            }
+        }
+        return SOFIA_OK;
+    }
+    return sofia::fail(ctx, SOFIA_ENEEDGROW, "list capacity kept overflowing (batch)%s");
+}
+
+// Prune margin (A) of the pruned inner list: the per-size-class tuning knob.
+extern "C" int sofia_system_set_margin(sofia_system *ss, double margin) {
+    if (!ss || !(margin >= 0.05) || !(margin <= ss->s.skin)) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    s->margin = margin;
+    s->built = 0;
+    sofia::md_drop_graphs(s);
+    return SOFIA_OK;
 }

@@ -1,0 +1,97 @@
+"""GPU tests: replica batches and the continuous-batching segment server.
+
+Bar: a replica's trajectory is bit-identical alone and inside a batch (and
+across segment boundaries), so each served result is the same alone and in
+the mix (tolerance: exact).
+"""
+import numpy as np
+import pytest
+
+from molecular_simulation_code_b200 import mixed as M
+from molecular_simulation_code_b200 import nonbond as nb
+from molecular_simulation_code_b200.batch import Batch, autotune_margin, set_margin
+from molecular_simulation_code_b200.serve import Request, Server, estimate_bytes, run_stream
+from molecular_simulation_code_b200.system import make_system
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def replicas():
+    return [make_system(6, 700, 31), make_system(12, 1100, 32), make_system(4, 600, 33)]
+
+
+def _prep(ctx, s, seed):
+    m = M.System(ctx, s, cut=8.0, skin=2.0)
+    m.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
+    m.md_setup(s, dt=1.0, gamma=0.01, seed=seed)
+    return m
+
+
+def test_batch_equals_alone(ctx, replicas):
+    alone = []
+    for k, s in enumerate(replicas):
+        c = nb.Context(0)
+        m = _prep(c, s, 100 + k)
+        m.md_run(40)
+        alone.append(m.get_state()[0])
+        m.close()
+        c.close()
+    ctxs = [nb.Context(0) for _ in replicas]
+    systems = [_prep(c, s, 100 + k) for k, (c, s) in enumerate(zip(ctxs, replicas))]
+    b = Batch(ctx, systems)
+    b.run(15)
+    e = b.run(25, energy_every=25)
+    assert len(e) == len(replicas) and all(np.isfinite(r["total"]) for r in e)
+    for k, m in enumerate(systems):
+        assert np.array_equal(m.get_state()[0], alone[k]), f"replica {k} differs"
+    b.close()
+    for m in systems:
+        m.close()
+    for c in ctxs:
+        c.close()
+
+
+def test_segments_compose(ctx, replicas):
+    s = replicas[0]
+    a = _prep(ctx, s, 5)
+    a.md_run(30)
+    a.md_run(30)
+    b = _prep(ctx, s, 5)
+    b.md_run(60)
+    assert np.array_equal(a.get_state()[0], b.get_state()[0])
+    a.close()
+    b.close()
+
+
+def test_autotune_returns_a_candidate(ctx, replicas):
+    best, times = autotune_margin(ctx, replicas[1], margins=(0.4, 0.8), steps=10, cut=8.0)
+    assert best in (0.4, 0.8) and all(t > 0 for t in times.values())
+    m = M.System(ctx, replicas[1], cut=8.0, skin=2.0)
+    with pytest.raises(Exception):
+        set_margin(m, 5.0)  # larger than the skin
+    m.close()
+
+
+def test_server_serves_and_continues(replicas):
+    srv = Server(max_active=2, hbm_budget=2 * estimate_bytes(6000), chunk_steps=20, cut=8.0,
+                 dt=1.0, gamma=0.01)
+    reqs = [Request(k, 0.0, s, 40) for k, s in enumerate(replicas)]
+    reqs.append(Request(10, 0.0, replicas[0], 20, continues=0))
+    stats = run_stream(srv, reqs)
+    assert stats["requests"] == 4
+    got = {r.rid: r for r in srv.results}
+    assert set(got) == {0, 1, 2, 10}
+    assert all(r.cluster_size >= 0 and r.latency > 0 for r in srv.results)
+    # the continuation resumed replica 0: its state equals 60 steps run alone
+    cont = srv.parked[10]
+    x_served = cont.system.get_state()[0]
+    srv.close()
+    c = nb.Context(0)
+    m = M.System(c, replicas[0], cut=8.0, skin=2.0)
+    m.set_state(replicas[0].xyz.astype(np.float64), replicas[0].velocity.astype(np.float64))
+    m.md_setup(replicas[0], dt=1.0, gamma=0.01, seed=1000003 * 1)
+    m.md_run(60)
+    assert np.array_equal(m.get_state()[0], x_served)
+    m.close()
+    c.close()
