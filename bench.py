@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--workload", default="gly3500_wat80000_275k")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--only-hot", action="store_true",
+                    help="time only the nonbonded hot path (profiling runs)")
     return ap.parse_args()
 
 
@@ -359,6 +361,12 @@ def run_ours(args, rank, ws):
         b1 = sysm.stats()
         return t, tm, b1["builds"] - b0["builds"], b1["launches"] - b0["launches"], b1
 
+    if args.only_hot:
+        t_hot, tm, builds, launches, st = timed_loop(M.MIXED, args.steps, args.warmup)
+        print(json.dumps({"mode": "hot path only", "atom_steps_per_s": n * args.steps / t_hot,
+                          "pair_ms": tm["pair_ms"] / max(tm["pairs"], 1), "list": st}),
+              flush=True)
+        return
     with Clocks(dev) as clk:
         t_md, md_en, md_builds, md_prunes, md_launches = md_loop(M.MIXED, args.steps,
                                                                  args.warmup)

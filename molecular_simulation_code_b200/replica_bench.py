@@ -1,0 +1,143 @@
+"""Throughput and latency of batched replicas and of the segment server.
+
+batch:  64 seeded replicas, N ~ U[3,000, 30,000] atoms, glycine 5-20 % of
+        molecules, own cubic box at 1.0 g/cm^3; 100-step segments (one graph
+        launch per step for all replicas); prune margin autotuned per size
+        class; mixed and FP64 atom-steps/s.
+serve:  Poisson request stream (default 200 requests/s), systems of
+        N ~ U[2,000, 60,000] atoms, U[500, 5,000] steps times --steps-scale,
+        up to 64 concurrent replicas, largest-cluster analysis at the end of
+        every segment; p50/p99 latency and replica-steps/s, mixed and FP64.
+
+Prints one JSON line per mode:
+    python -m molecular_simulation_code_b200.replica_bench --mode batch|serve
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+
+def bench_batch(args):
+    import torch
+
+    from . import mixed as M
+    from .batch import Batch, Tuner, make_replicas, set_margin, size_class
+    from .nonbond import Context
+
+    reps = make_replicas(args.replicas, seed=args.seed, n_min=3000, n_max=30000,
+                         processes=args.procs)
+    master = Context(0)
+    out = {"mode": "batch", "replicas": len(reps),
+           "atoms_total": int(sum(r.np_atoms for r in reps)),
+           "atoms_min": int(min(r.np_atoms for r in reps)),
+           "atoms_max": int(max(r.np_atoms for r in reps)), "segment_steps": args.segment}
+    tuner = Tuner()
+    if args.tune:
+        for r in reps:
+            tuner.margin_for(master, r, steps=20)
+        out["tuned_margin_per_class"] = {str(k): v for k, v in tuner.choice.items()}
+    stream = torch.cuda.ExternalStream(master._lib.sofia_stream(master.handle))
+    for name, prec in (("mixed", M.MIXED), ("fp64", M.FP64)):
+        ctxs = [Context(0) for _ in reps]
+        systems = []
+        for c, r in zip(ctxs, reps):
+            m = M.System(c, r, precision=prec)
+            if args.tune:
+                set_margin(m, tuner.choice[size_class(r.np_atoms)])
+            m.set_state(r.xyz.astype(np.float64), r.velocity.astype(np.float64))
+            m.md_setup(r, dt=1.0, gamma=0.02, seed=7)
+            systems.append(m)
+        b = Batch(master, systems)
+        b.run(50)  # damped relaxation from the lattice start
+        for m, r in zip(systems, reps):
+            m.md_setup(r, dt=2.0, gamma=0.001, seed=8)
+        b.close()
+        b = Batch(master, systems)
+        b.run(args.segment)  # warm-up segment (also captures the graphs)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.segments):
+            b.run(args.segment, energy_every=args.segment)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        steps = args.segments * args.segment
+        out[name] = {"atom_steps_per_s": out["atoms_total"] * steps / t,
+                     "replica_steps_per_s": len(reps) * steps / t,
+                     "ms_per_batch_step": 1e3 * t / steps}
+        b.close()
+        for m in systems:
+            m.close()
+        for c in ctxs:
+            c.close()
+    out["mixed_over_fp64"] = out["mixed"]["atom_steps_per_s"] / out["fp64"]["atom_steps_per_s"]
+    return out
+
+
+def bench_serve(args):
+    from . import mixed as M
+    from .batch import make_replicas
+    from .serve import Request, Server, poisson_arrivals, run_stream
+
+    rng = np.random.default_rng(args.seed)
+    systems = make_replicas(args.requests, seed=args.seed + 1, n_min=2000, n_max=60000,
+                            processes=args.procs)
+    arrivals = poisson_arrivals(args.rate, args.requests, seed=args.seed + 2)
+    steps = (rng.integers(500, 5001, size=args.requests) * args.steps_scale).astype(int)
+    steps = np.maximum(steps // args.chunk, 1) * args.chunk
+    out = {"mode": "serve", "requests": args.requests, "rate_per_s": args.rate,
+           "steps_scale": args.steps_scale, "max_active": args.max_active,
+           "atoms_range": [int(min(s.np_atoms for s in systems)),
+                           int(max(s.np_atoms for s in systems))]}
+    for name, prec in (("mixed", M.MIXED), ("fp64", M.FP64)):
+        srv = Server(max_active=args.max_active, hbm_budget=int(args.budget_gb * (1 << 30)),
+                     chunk_steps=args.chunk, precision=prec)
+        reqs = [Request(k, float(arrivals[k]), systems[k], int(steps[k]))
+                for k in range(args.requests)]
+        stats = run_stream(srv, reqs)
+        per_step = np.array([r.service / r.nsteps for r in srv.results])
+        stats["per_step_service_p50_ms"] = float(np.percentile(per_step, 50) * 1e3)
+        stats["per_step_service_p99_ms"] = float(np.percentile(per_step, 99) * 1e3)
+        stats["cluster_sizes"] = sorted(int(r.cluster_size) for r in srv.results)[-5:]
+        out[name] = stats
+        srv.close()
+    out["mixed_over_fp64_replica_steps"] = (out["mixed"]["replica_steps_per_s"] /
+                                            out["fp64"]["replica_steps_per_s"])
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--mode", choices=["batch", "serve"], default="batch")
+    ap.add_argument("--replicas", type=int, default=64)
+    ap.add_argument("--segment", type=int, default=100)
+    ap.add_argument("--segments", type=int, default=3)
+    ap.add_argument("--tune", action="store_true")
+    ap.add_argument("--requests", type=int, default=128)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--steps-scale", type=float, default=0.2)
+    ap.add_argument("--chunk", type=int, default=50)
+    ap.add_argument("--max-active", type=int, default=64)
+    ap.add_argument("--budget-gb", type=float, default=64.0)
+    ap.add_argument("--seed", type=int, default=5000)
+    ap.add_argument("--procs", type=int, default=min(16, os.cpu_count() or 1))
+    args = ap.parse_args(argv)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    t0 = time.time()
+    out = bench_batch(args) if args.mode == "batch" else bench_serve(args)
+    out["wall_s"] = time.time() - t0
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

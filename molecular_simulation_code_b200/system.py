@@ -286,6 +286,8 @@ def _push_apart(xyz: np.ndarray, mol: np.ndarray, n_mol: int, L: float,
         d = x[pairs[:, 0]] - x[pairs[:, 1]]
         d -= L * np.round(d / L)
         r = np.linalg.norm(d, axis=1)
+        if r.min() > d_min - 0.4:
+            break  # no clash left (closest contact >= d_min - 0.4 A)
         r = np.maximum(r, 1e-3)
         push = (0.5 * (d_min - r) / r)[:, None] * d
         disp = np.zeros((n_mol, 3))
