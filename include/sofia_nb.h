@@ -244,9 +244,10 @@ int sofia_system_get_state(sofia_system *sys, double *x, double *v, double *f);
 #define SOFIA_EVAL_REBUILD 1
 #define SOFIA_EVAL_VIRIAL 2
 int sofia_system_compute_forces(sofia_system *sys, int precision, int flags, double *energies);
-/* stats[0..9]: list builds, clusters, list entries, row capacity, columns per
+/* stats[0..10]: list builds, clusters, list entries, row capacity, columns per
  * side, cluster capacity, column reach, kernels launched so far, prunes,
- * entries of the pruned (rc + margin) list. */
+ * entries of the pruned (rc + margin) list, SHAKE groups that reached maxiter
+ * (a warning, as the reference prints, Source/mod_shake.f90:322-324). */
 int sofia_system_stats(sofia_system *sys, int64_t *stats, int nstats);
 /* Ballistic drift x += dt*v of the resident positions, nsteps times (no forces). */
 int sofia_system_drift(sofia_system *sys, double dt, int nsteps);

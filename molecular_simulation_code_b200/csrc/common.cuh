@@ -46,6 +46,7 @@ enum StatusSlot {
     ST_REBUILD = 7,      // rebuild flag set by the displacement check
     ST_NCLUSTER = 8,     // cluster-pair list fill
     ST_FIXED_OVF = 9,    // fixed-point force range exceeded
+    ST_SHAKE_NC = 10,    // SHAKE groups that hit maxiter (warning, as the reference prints)
     ST_NSLOTS = 16
 };
 

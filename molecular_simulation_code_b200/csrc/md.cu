@@ -409,7 +409,7 @@ __global__ void k_shake(int ns, const int *__restrict__ sa, const double *__rest
             }
             for (int c = 0; c < nc; ++c) lam[c] = ln[c];
         }
-        if (!done) atomicAdd(&status[ST_SHAKE], 1);
+        if (!done) atomicAdd(&status[ST_SHAKE_NC], 1);  // warning only (mod_shake.f90:322-324)
     }
     long long *F[3] = {fx, fy, fz};
     for (int c = 0; c < nc; ++c) {
@@ -789,7 +789,8 @@ extern "C" int sofia_system_md_run(sofia_system *ss, int nsteps, int energy_ever
         SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
         SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
         if (hs[sofia::ST_SHAKE])
-            return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE did not converge (or negative determinant)%s");
+            return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE determinant <= 0 (mod_shake.f90:146-153, :267)%s");
+        s->shake_nc += hs[sofia::ST_SHAKE_NC];
         md.step += nsteps;
         if (energies && energy_every > 0) {
             double e[16];
@@ -998,7 +999,8 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
             int hs[sofia::ST_NSLOTS];
             SOFIA_CUDA(ctx, cudaMemcpy(hs, s->status_local.p, sizeof(hs), cudaMemcpyDeviceToHost));
             if (hs[sofia::ST_SHAKE])
-                return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE did not converge in a batch replica%s");
+                return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE determinant <= 0 in a batch replica%s");
+            s->shake_nc += hs[sofia::ST_SHAKE_NC];
             md.step += nsteps;
             if (energies && energy_every > 0) {
                 double e[16];

@@ -1424,10 +1424,10 @@ extern "C" int sofia_system_stats(sofia_system *ss, int64_t *stats, int nstats) 
     }
     long long dc[2] = {0, 0};
     cudaMemcpy(dc, s->dcount.p, sizeof(dc), cudaMemcpyDeviceToHost);
-    const int64_t vals[10] = {s->n_builds + dc[0], ncl, entries, s->jcap, s->ncx,
+    const int64_t vals[11] = {s->n_builds + dc[0], ncl, entries, s->jcap, s->ncx,
                               s->max_clusters, s->ncol_reach, s->launches, s->n_prunes + dc[1],
-                              inner};
-    for (int i = 0; i < nstats && i < 10; ++i) stats[i] = vals[i];
+                              inner, s->shake_nc};
+    for (int i = 0; i < nstats && i < 11; ++i) stats[i] = vals[i];
     return SOFIA_OK;
 }
 

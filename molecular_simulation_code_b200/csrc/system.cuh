@@ -83,6 +83,7 @@ struct Sys {
     int built = 0;
     long long n_builds = 0;
     long long launches = 0;             // kernels launched by this system (all paths)
+    long long shake_nc = 0;             // SHAKE groups that reached maxiter (warnings)
     // optional CUDA-event timing of the list build and the pair kernel
     int timing = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};

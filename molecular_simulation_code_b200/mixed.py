@@ -91,10 +91,10 @@ class System:
         return e
 
     def stats(self) -> dict:
-        st = np.zeros(10, np.int64)
-        self.ctx.check(self.ctx._lib.sofia_system_stats(self.handle, ptr(st), 10))
+        st = np.zeros(11, np.int64)
+        self.ctx.check(self.ctx._lib.sofia_system_stats(self.handle, ptr(st), 11))
         keys = ["builds", "clusters", "entries", "jcap", "ncx", "max_clusters", "reach",
-                "launches", "prunes", "inner_entries"]
+                "launches", "prunes", "inner_entries", "shake_maxiter_hits"]
         return {k: int(v) for k, v in zip(keys, st)}
 
     def drift(self, dt: float, nsteps: int = 1):

@@ -88,7 +88,7 @@ class Server:
                  chunk_steps: int = 100, precision: int = M.MIXED, tune: bool = False,
                  cut: float = 10.0, skin: float = 2.0, dt: float = 2.0,
                  temperature: float = 300.0, gamma: float = 0.001,
-                 cluster=(9.0, 5.0, 11)):
+                 cluster=(9.0, 5.0, 11), warm_in: int = 50):
         self.device = device
         self.ctx = Context(device)
         self.max_active = max_active
@@ -98,6 +98,7 @@ class Server:
         self.cut, self.skin, self.dt = cut, skin, dt
         self.temperature, self.gamma = temperature, gamma
         self.mrcut, self.denscut, self.densmin = cluster
+        self.warm_in = warm_in
         self.tuner = Tuner() if tune else None
         self.queue: collections.deque[Request] = collections.deque()
         self.active: list[_Replica] = []
@@ -129,6 +130,11 @@ class Server:
             set_margin(m, self.tuner.margin_for(ctx, s, cut=self.cut, skin=self.skin,
                                                 precision=self.precision))
         m.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
+        if self.warm_in:
+            # damped warm-in from a lattice start (part of the request's service time)
+            m.md_setup(s, dt=1.0, temperature=self.temperature, gamma=0.02,
+                       seed=7 * (req.rid + 1))
+            m.md_run(self.warm_in)
         m.md_setup(s, dt=self.dt, temperature=self.temperature, gamma=self.gamma,
                    seed=1000003 * (req.rid + 1))
         return _Replica(req, ctx, m, self.now())

@@ -75,7 +75,7 @@ def test_autotune_returns_a_candidate(ctx, replicas):
 
 def test_server_serves_and_continues(replicas):
     srv = Server(max_active=2, hbm_budget=2 * estimate_bytes(6000), chunk_steps=20, cut=8.0,
-                 dt=1.0, gamma=0.01)
+                 dt=1.0, gamma=0.01, warm_in=0)
     reqs = [Request(k, 0.0, s, 40) for k, s in enumerate(replicas)]
     reqs.append(Request(10, 0.0, replicas[0], 20, continues=0))
     stats = run_stream(srv, reqs)
