@@ -98,6 +98,14 @@ int sofia_neighbor_build(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
                          int32_t neigh_alloc, int32_t *needed_alloc);
 
 /*
+ * check_neighbor (Source/mod_neighbor.f90:895-913): *nflag = 1 if any atom's
+ * accumulated displacement (real*4 drx, dry, drz) has drx^2+dry^2+drz^2 >= rvrc2
+ * (rvrc2 = neighbor_pad^2, the full skin, Source/get_started.f90:47-48).
+ */
+int sofia_check_neighbor(sofia_nb_ctx *ctx, int np, const float *drx, const float *dry,
+                         const float *drz, double rvrc2, int32_t *nflag);
+
+/*
  * lj_cut_coul_dsf_nonewton_NOMIC (Source/mod_force_nonbond.f90:105-196): LJ
  * 12-6 + damped-shifted-force Coulomb over the full list, FP64 pair arithmetic
  * on the real*4 arrays.  lj1..lj4 are [ntypes*ntypes] real*4 tables indexed

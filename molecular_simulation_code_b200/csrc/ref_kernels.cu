@@ -1013,3 +1013,41 @@ extern "C" int sofia_force_nonbond_dsf_noalloc(
     }
     return SOFIA_OK;
 }
+
+// check_neighbor (Source/mod_neighbor.f90:895-913): rebuild flag when any atom's
+// accumulated real*4 displacement satisfies drx^2+dry^2+drz^2 >= rvrc2.
+namespace {
+__global__ void k_check_neighbor(int np, const float *__restrict__ drx,
+                                 const float *__restrict__ dry, const float *__restrict__ drz,
+                                 double rvrc2, int *__restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool far = false;
+    if (i < np) {
+        const float d2 = drx[i] * drx[i] + dry[i] * dry[i] + drz[i] * drz[i];
+        far = (double)d2 >= rvrc2;
+    }
+    if (__any_sync(FULL, far) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+}  // namespace
+
+extern "C" int sofia_check_neighbor(sofia_nb_ctx *ctx, int np, const float *drx,
+                                    const float *dry, const float *drz, double rvrc2,
+                                    int32_t *nflag) {
+    if (!ctx) return SOFIA_EINVAL;
+    if (np <= 0 || !drx || !dry || !drz || !nflag) return sofia::fail(ctx, SOFIA_EINVAL, "bad args%s");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int rc;
+    const void *dx, *dy, *dz;
+    if ((rc = sofia::stage_in(ctx, drx, sizeof(float) * (size_t)np, 0, &dx))) return rc;
+    if ((rc = sofia::stage_in(ctx, dry, sizeof(float) * (size_t)np, 1, &dy))) return rc;
+    if ((rc = sofia::stage_in(ctx, drz, sizeof(float) * (size_t)np, 2, &dz))) return rc;
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
+    k_check_neighbor<<<sofia::grid_for(np, 256), 256, 0, st>>>(np, (const float *)dx, (const float *)dy,
+                                                               (const float *)dz, rvrc2,
+                                                               ctx->d_status + sofia::ST_REBUILD);
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    if ((rc = check_status(ctx))) return rc;
+    *nflag = ctx->h_status[sofia::ST_REBUILD] ? 1 : 0;
+    return SOFIA_OK;
+}

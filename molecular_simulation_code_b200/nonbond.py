@@ -166,6 +166,14 @@ def neighbor_wrapper(ctx: Context, position, specbond, num3bond, p: DsfParams,
         return nlist, numneigh, neigh_alloc
 
 
+def check_neighbor(ctx: Context, drx, dry, drz, rvrc2: float) -> int:
+    """check_neighbor (Source/mod_neighbor.f90:895-913): 1 if a rebuild is due."""
+    flag = C.c_int32()
+    ctx.check(ctx._lib.sofia_check_neighbor(ctx.handle, int(len(drx)), ptr(drx), ptr(dry),
+                                            ptr(drz), float(rvrc2), C.byref(flag)))
+    return flag.value
+
+
 def lj_cut_coul_dsf_nonewton(ctx: Context, position, q, lj, ntypes: int, nlist, numneigh,
                              neigh_alloc: int, p: DsfParams, ff=None):
     """FP64 LJ + DSF over the full list.  ``nlist=None`` uses the resident list.

@@ -238,3 +238,18 @@ def test_neighbor_list_sets_bit_exact_90k(ctx):
     rows_gpu = [np.sort(nl[i * na:i * na + nn[i]]) for i in range(0, s.np_atoms, 7)]
     rows_orc = [np.sort(onl[i * ona:i * ona + onn[i]]) for i in range(0, s.np_atoms, 7)]
     assert all(np.array_equal(g, o) for g, o in zip(rows_gpu, rows_orc))
+
+
+def test_check_neighbor_matches_oracle(ctx):
+    import ctypes as C
+    rng = np.random.default_rng(4)
+    for scale in (0.3, 1.0, 1.49, 1.51):
+        d = (rng.normal(size=(3, 5000)) * scale / np.sqrt(3)).astype(np.float32)
+        L = O.lib()
+        L.orc_check_neighbor.argtypes = [C.c_int, np.ctypeslib.ndpointer(np.float32),
+                                         np.ctypeslib.ndpointer(np.float32),
+                                         np.ctypeslib.ndpointer(np.float32), C.c_double]
+        L.orc_check_neighbor.restype = C.c_int
+        want = L.orc_check_neighbor(5000, d[0].copy(), d[1].copy(), d[2].copy(), 1.5 ** 2)
+        got = nb.check_neighbor(ctx, d[0].copy(), d[1].copy(), d[2].copy(), 1.5 ** 2)
+        assert got == want
