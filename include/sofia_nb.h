@@ -332,6 +332,25 @@ int sofia_batch_md_run(sofia_batch *batch, int nsteps, int energy_every, double 
  * the autotuner picks per size class. */
 int sofia_system_set_margin(sofia_system *sys, double margin);
 
+/*
+ * Snapshot / rollback of the resident replica state, replacing the in-memory
+ * copies nuc_move makes before a trial segment and restores on rejection
+ * (Source/mod_nucleation.f90:318-389 and :453-531).  The snapshot holds
+ * positions, velocities and the thermostat step counter.  Both calls make the
+ * next evaluation rebuild the neighbor structures and recompute the forces
+ * from the (saved) positions, so the run continued after a snapshot and the
+ * run repeated after a rollback take bit-identical steps.
+ * sofia_system_rollback returns SOFIA_ESTATE when no snapshot was taken.
+ */
+int sofia_system_snapshot(sofia_system *sys);
+int sofia_system_rollback(sofia_system *sys);
+/* Thermostat step counter (counter of the Langevin noise).  Reading it with
+ * the state and setting it on resume continues the same noise sequence; the
+ * reference restart (read_dump_global_id_v, Source/mod_datadump.f90:216-252)
+ * holds no such counter.  SOFIA_ESTATE before sofia_system_md_setup. */
+int sofia_system_md_get_step(sofia_system *sys, long long *step);
+int sofia_system_md_set_step(sofia_system *sys, long long step);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,6 +106,10 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_batch_md_run": (_I, [_P, _I, _I, _P]),
     "sofia_system_set_margin": (_I, [_P, _D]),
     "sofia_system_timers": (_I, [_P, _I, _P]),
+    "sofia_system_snapshot": (_I, [_P]),
+    "sofia_system_rollback": (_I, [_P]),
+    "sofia_system_md_get_step": (_I, [_P, _P]),
+    "sofia_system_md_set_step": (_I, [_P, C.c_longlong]),
 }
 
 _lib = None

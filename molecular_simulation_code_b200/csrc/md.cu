@@ -781,7 +781,7 @@ extern "C" int sofia_system_md_run(sofia_system *ss, int nsteps, int energy_ever
                 SOFIA_CUDA(ctx, cudaMemcpyAsync(s->v[d].p, md.snap[3 + d].p, nb, cudaMemcpyDeviceToDevice, st));
             }
             SOFIA_CUDA(ctx, cudaMemcpyAsync(md.step_dev.p, md.snap[6].p, sizeof(long long), cudaMemcpyDeviceToDevice, st));
-            md.forces_valid = had_forces ? 0 : 0;
+            md.forces_valid = 0;
             continue;
         }
         if (rc) return rc;
@@ -1033,5 +1033,90 @@ extern "C" int sofia_system_set_margin(sofia_system *ss, double margin) {
     s->margin = margin;
     s->built = 0;
     sofia::md_drop_graphs(s);
+    return SOFIA_OK;
+}
+
+// In-memory snapshot / rollback of one replica, the accept/reject pattern of
+// nuc_move (mod_nucleation.f90:318-389 saves position, v and the lists;
+// :453-531 restores them on reject).  The snapshot holds positions, velocities
+// and the thermostat step counter on the device; the lists are rebuilt from
+// the saved positions after the snapshot and after a rollback alike, so
+// nothing else needs saving.
+extern "C" int sofia_system_snapshot(sofia_system *ss) {
+    if (!ss) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia::Md &md = s->md;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t nb = sizeof(double) * (size_t)s->n;
+    cudaStream_t st = ctx->stream;
+    for (int d = 0; d < 3; ++d) {
+        SOFIA_CUDA(ctx, md.keep[d].ensure(nb));
+        SOFIA_CUDA(ctx, md.keep[3 + d].ensure(nb));
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(md.keep[d].p, s->x[d].p, nb, cudaMemcpyDeviceToDevice, st));
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(md.keep[3 + d].p, s->v[d].p, nb, cudaMemcpyDeviceToDevice, st));
+    }
+    SOFIA_CUDA(ctx, md.keep[6].ensure(sizeof(long long)));
+    if (md.ready) {
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(md.keep[6].p, md.step_dev.p, sizeof(long long),
+                                        cudaMemcpyDeviceToDevice, st));
+    }
+    md.keep_step = md.step;
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    md.has_keep = 1;
+    // The snapshot is a restart point: the next evaluation rebuilds the lists
+    // and recomputes the forces from these positions, exactly as it will after
+    // a rollback, so both continuations take identical steps.
+    s->built = 0;
+    md.forces_valid = 0;
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_system_rollback(sofia_system *ss) {
+    if (!ss) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia::Md &md = s->md;
+    sofia_nb_ctx *ctx = s->ctx;
+    if (!md.has_keep) return sofia::fail(ctx, SOFIA_ESTATE, "rollback: no snapshot was taken");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t nb = sizeof(double) * (size_t)s->n;
+    cudaStream_t st = ctx->stream;
+    for (int d = 0; d < 3; ++d) {
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(s->x[d].p, md.keep[d].p, nb, cudaMemcpyDeviceToDevice, st));
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(s->v[d].p, md.keep[3 + d].p, nb, cudaMemcpyDeviceToDevice, st));
+    }
+    if (md.ready) {
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(md.step_dev.p, md.keep[6].p, sizeof(long long),
+                                        cudaMemcpyDeviceToDevice, st));
+    }
+    md.step = md.keep_step;
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    s->built = 0;
+    md.forces_valid = 0;
+    return SOFIA_OK;
+}
+
+// Thermostat step counter (the Philox counter of the Langevin noise): read it
+// for a checkpoint, set it when resuming one so the noise sequence continues.
+extern "C" int sofia_system_md_get_step(sofia_system *ss, long long *step) {
+    if (!ss || !step) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    if (!s->md.ready) return sofia::fail(s->ctx, SOFIA_ESTATE, "md_get_step: MD is not set up");
+    SOFIA_CUDA(s->ctx, cudaSetDevice(s->ctx->device));
+    SOFIA_CUDA(s->ctx, cudaMemcpyAsync(step, s->md.step_dev.p, sizeof(long long),
+                                       cudaMemcpyDeviceToHost, s->ctx->stream));
+    SOFIA_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_system_md_set_step(sofia_system *ss, long long step) {
+    if (!ss || step < 0) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    if (!s->md.ready) return sofia::fail(s->ctx, SOFIA_ESTATE, "md_set_step: MD is not set up");
+    SOFIA_CUDA(s->ctx, cudaSetDevice(s->ctx->device));
+    SOFIA_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    SOFIA_CUDA(s->ctx, cudaMemcpy(s->md.step_dev.p, &step, sizeof(long long),
+                                  cudaMemcpyHostToDevice));
+    s->md.step = step;
     return SOFIA_OK;
 }

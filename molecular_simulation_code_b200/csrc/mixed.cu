@@ -18,6 +18,7 @@
 // build (checked every evaluation on the device; the reference triggers at the
 // full skin, Source/mod_neighbor.f90:895-913).
 #include <cmath>
+#include <vector>
 
 #include "system.cuh"
 
@@ -1331,26 +1332,22 @@ extern "C" int sofia_system_set_state(sofia_system *ss, const double *x, const d
     Sys *s = &ss->s;
     sofia_nb_ctx *ctx = s->ctx;
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     const size_t n = (size_t)s->n;
-    double *h = new double[3 * n];
-    SOFIA_CUDA(ctx, cudaMemcpy(h, x, sizeof(double) * 3 * n, cudaMemcpyDefault));
-    double *c = new double[n];
-    for (int d = 0; d < 3; ++d) {
-        for (size_t i = 0; i < n; ++i) c[i] = h[3 * i + d];
-        cudaMemcpy(s->x[d].p, c, sizeof(double) * n, cudaMemcpyHostToDevice);
-    }
-    if (v) {
-        SOFIA_CUDA(ctx, cudaMemcpy(h, v, sizeof(double) * 3 * n, cudaMemcpyDefault));
+    std::vector<double> h(3 * n), c(n);
+    const double *src[2] = {x, v};
+    sofia::DevBuf *dst[2] = {s->x, s->v};
+    for (int k = 0; k < 2; ++k) {
+        if (!src[k]) continue;
+        SOFIA_CUDA(ctx, cudaMemcpy(h.data(), src[k], sizeof(double) * 3 * n, cudaMemcpyDefault));
         for (int d = 0; d < 3; ++d) {
             for (size_t i = 0; i < n; ++i) c[i] = h[3 * i + d];
-            cudaMemcpy(s->v[d].p, c, sizeof(double) * n, cudaMemcpyHostToDevice);
+            SOFIA_CUDA(ctx, cudaMemcpy(dst[k][d].p, c.data(), sizeof(double) * n,
+                                       cudaMemcpyHostToDevice));
         }
     }
-    delete[] h;
-    delete[] c;
     s->built = 0;
     s->md.forces_valid = 0;
-    SOFIA_CUDA(ctx, cudaDeviceSynchronize());
     return SOFIA_OK;
 }
 
@@ -1361,24 +1358,25 @@ extern "C" int sofia_system_get_state(sofia_system *ss, double *x, double *v, do
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
     SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     const size_t n = (size_t)s->n;
-    double *c = new double[n];
-    long long *cl = new long long[n];
+    std::vector<double> c(n);
+    std::vector<long long> cl(n);
     for (int d = 0; d < 3; ++d) {
         if (x) {
-            cudaMemcpy(c, s->x[d].p, sizeof(double) * n, cudaMemcpyDeviceToHost);
+            SOFIA_CUDA(ctx, cudaMemcpy(c.data(), s->x[d].p, sizeof(double) * n,
+                                       cudaMemcpyDeviceToHost));
             for (size_t i = 0; i < n; ++i) x[3 * i + d] = c[i];
         }
         if (v) {
-            cudaMemcpy(c, s->v[d].p, sizeof(double) * n, cudaMemcpyDeviceToHost);
+            SOFIA_CUDA(ctx, cudaMemcpy(c.data(), s->v[d].p, sizeof(double) * n,
+                                       cudaMemcpyDeviceToHost));
             for (size_t i = 0; i < n; ++i) v[3 * i + d] = c[i];
         }
         if (f) {
-            cudaMemcpy(cl, s->f[d].p, sizeof(long long) * n, cudaMemcpyDeviceToHost);
+            SOFIA_CUDA(ctx, cudaMemcpy(cl.data(), s->f[d].p, sizeof(long long) * n,
+                                       cudaMemcpyDeviceToHost));
             for (size_t i = 0; i < n; ++i) f[3 * i + d] = (double)cl[i] * sofia::FIX_INV;
         }
     }
-    delete[] c;
-    delete[] cl;
     return SOFIA_OK;
 }
 

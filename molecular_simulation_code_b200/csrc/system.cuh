@@ -44,6 +44,9 @@ struct Md {
     DevBuf ered;           // reduced energies
     DevBuf step_dev;       // device step counter (RNG counter inside graphs)
     DevBuf snap[7];        // x, v (3 each) and the step counter at segment start
+    DevBuf keep[7];        // caller-requested snapshot (same layout), for rollback
+    long long keep_step = 0;
+    int has_keep = 0;
     double e_self = 0.0;
     int ndof = 0;
     long long step = 0;

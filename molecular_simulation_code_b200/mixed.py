@@ -128,6 +128,22 @@ class System:
             return None
         return dict(zip(MD_ENERGY_NAMES, e.tolist()))
 
+    def snapshot(self):
+        """Device copy of x, v and the thermostat step (nuc_move's save)."""
+        self.ctx.check(self.ctx._lib.sofia_system_snapshot(self.handle))
+
+    def rollback(self):
+        """Restore the last snapshot (nuc_move's reject branch)."""
+        self.ctx.check(self.ctx._lib.sofia_system_rollback(self.handle))
+
+    def md_step(self) -> int:
+        st = C.c_longlong()
+        self.ctx.check(self.ctx._lib.sofia_system_md_get_step(self.handle, C.byref(st)))
+        return int(st.value)
+
+    def set_md_step(self, step: int):
+        self.ctx.check(self.ctx._lib.sofia_system_md_set_step(self.handle, int(step)))
+
     def timers(self, enable: bool = True) -> dict:
         t = np.zeros(4)
         self.ctx.check(self.ctx._lib.sofia_system_timers(self.handle, int(enable), ptr(t)))
