@@ -123,6 +123,25 @@ int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *positi
                             double *potential, double *e_coul, double *virial_diag3);
 
 /*
+ * lj_cut_coul_long_nonewton_NOMIC (Source/mod_force_nonbond.f90:300-400; the
+ * _MIC variant at :201-298 computes the same): the real-space Ewald term of
+ * the PME path (coul_flag = 2) with LJ, over the same full list.  Pair
+ * arithmetic is real*4 as in the reference, promoted to double where the
+ * reference's mixed-mode statements promote; the A&S 7.1.26 erfc uses
+ * gewald (calculate_gewald, Source/get_started.f90:153-173).  Outputs and list
+ * handling as in sofia_force_nonbond_dsf; the reciprocal-space part
+ * (cal_e_pme_kspace) and the excluded-pair corrections (sofia_correct_1x)
+ * are separate calls.
+ */
+int sofia_force_nonbond_long(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
+                             const float *q, const float *lj1, const float *lj2,
+                             const float *lj3, const float *lj4, int ntypes,
+                             const int32_t *nlist, const int32_t *numneigh, int32_t neigh_alloc,
+                             float box, float ibox, double rcut2, double cut_coulsq,
+                             double gewald, float coulpre, float *ff, double *potential,
+                             double *e_coul, double *virial_diag3);
+
+/*
  * Allocation-free form of sofia_force_nonbond_dsf.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot allocate device
  * memory when they need forces: work being captured into a CUDA graph (where

@@ -81,6 +81,9 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_force_nonbond_dsf": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, C.c_int32, _F,
                                      _F, _D, _D, _D, _D, _D, _F, _P, C.POINTER(_D),
                                      C.POINTER(_D), _P]),
+    "sofia_force_nonbond_long": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, C.c_int32,
+                                      _F, _F, _D, _D, _D, _F, _P, C.POINTER(_D), C.POINTER(_D),
+                                      _P]),
     "sofia_check_neighbor": (_I, [_P, _I, _P, _P, _P, _D, C.POINTER(C.c_int32)]),
     "sofia_force_nonbond_dsf_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P,
                                              C.c_int32, _F, _F, _D, _D, _D, _D, _D, _F, _P,

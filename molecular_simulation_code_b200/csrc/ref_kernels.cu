@@ -221,6 +221,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 struct DsfConst {
     double box, ibox, rcut2, cut_coulsq, alpha, e_shift, f_shift, coulpre;
+    float boxf, iboxf, coulpref;  // real*4 copies for the real*4 real-space kernel
+    double gewald;
     double EWALD_P, A1, A2, A3, A4, A5, MY_PIS, MY_PIS_INV, EWALD_F;
 };
 
@@ -235,6 +237,10 @@ __host__ DsfConst make_const(float box, float ibox, double rcut2, double cut_cou
     c.e_shift = e_shift;
     c.f_shift = f_shift;
     c.coulpre = (double)coulpre;
+    c.boxf = box;
+    c.iboxf = ibox;
+    c.coulpref = coulpre;
+    c.gewald = 0.0;
     c.EWALD_F = (double)1.12837917f;
     c.EWALD_P = (double)0.3275911f;
     c.A1 = (double)0.254829592f;
@@ -308,6 +314,91 @@ __global__ void __launch_bounds__(256) k_force_ref(
         vx = vx + dx * dx * force;
         vy = vy + dy * dy * force;
         vz = vz + dz * dz * force;
+    }
+    ffx = warp_sum(ffx);
+    ffy = warp_sum(ffy);
+    ffz = warp_sum(ffz);
+    pot = warp_sum(pot);
+    ec = warp_sum(ec);
+    vx = warp_sum(vx);
+    vy = warp_sum(vy);
+    vz = warp_sum(vz);
+    if (lane == 0) {
+        ff[(size_t)i * 3 + 0] = (float)ffx;
+        ff[(size_t)i * 3 + 1] = (float)ffy;
+        ff[(size_t)i * 3 + 2] = (float)ffz;
+        double *o = pe + (size_t)i * 5;
+        o[0] = pot;
+        o[1] = ec;
+        o[2] = vx;
+        o[3] = vy;
+        o[4] = vz;
+    }
+}
+
+// lj_cut_coul_long_nonewton_NOMIC / _MIC (mod_force_nonbond.f90:300-400, :201-298):
+// the real-space Ewald term of the PME path.  Same warp-per-atom layout as
+// k_force_ref, but every pair quantity is real*4 as in the reference; the
+// mixed-mode statements are promoted to double where Fortran promotes them
+// (dr2i = 1.0d0/dr2, grij = gewald*r, t, the erfc polynomial, forcecoul) and
+// force/virial products are added into double sums.  This unit is compiled
+// without FMA contraction, so each float operation rounds as written.  The
+// real*4 exp is the correctly rounded single-precision value obtained by
+// rounding the double-precision exp.
+__global__ void __launch_bounds__(256) k_force_long_ref(
+    int np, const float4 *__restrict__ pos, const float *__restrict__ q,
+    const float *__restrict__ lj1, const float *__restrict__ lj2, const float *__restrict__ lj3,
+    const float *__restrict__ lj4, int ntypes, const int *__restrict__ nlist,
+    const int *__restrict__ numneigh, int neigh_alloc, DsfConst k, float *__restrict__ ff,
+    double *__restrict__ pe) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= np) return;
+    const float4 pi = pos[i];
+    const int itype = __float_as_int(pi.w);
+    const float qtmp = q[i];
+    const int ioffset = (itype - 1) * ntypes;
+    const int num = min(numneigh[i], neigh_alloc);
+    const int *row = nlist + (size_t)i * (size_t)neigh_alloc;
+    const bool itype_ok = (unsigned)(itype - 1) < (unsigned)ntypes;
+    const float box = k.boxf, ibox = k.iboxf, coulpre = k.coulpref;
+    double ffx = 0.0, ffy = 0.0, ffz = 0.0, pot = 0.0, ec = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
+    for (int j = lane; j < num; j += 32) {
+        const int neigh = row[j] - 1;
+        if ((unsigned)neigh >= (unsigned)np) continue;
+        const float4 pj = pos[neigh];
+        const int jtype = __float_as_int(pj.w);
+        if (!itype_ok || (unsigned)(jtype - 1) >= (unsigned)ntypes) continue;
+        float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        // (b + sign(2^23,b)) - sign(2^23,dx) is rint(b) in real*4 for |b| < 2^22
+        dx = dx - box * rintf(dx * ibox);
+        dy = dy - box * rintf(dy * ibox);
+        dz = dz - box * rintf(dz * ibox);
+        const float dr2 = dx * dx + dy * dy + dz * dz;
+        const float dr2i = (float)(1.0 / (double)dr2);
+        float dr6i = dr2i * dr2i * dr2i;
+        if ((double)dr2 > k.rcut2) dr6i = 0.0f;
+        const int off = ioffset + jtype - 1;
+        const float forcelj = dr6i * (lj1[off] * dr6i - lj2[off]);
+        pot = pot + (double)(dr6i * (dr6i * lj3[off] - lj4[off]));
+        const float r = sqrtf(dr2);
+        float prefactor = coulpre * qtmp * q[neigh] / r;
+        const float grij = (float)(k.gewald * (double)r);
+        const float expm2 = (float)exp((double)(-(grij * grij)));
+        const double t = (double)(float)(1.0 / (1.0 + k.EWALD_P * (double)grij));
+        const float erfc_ =
+            (float)(t * (k.A1 + t * (k.A2 + t * (k.A3 + t * (k.A4 + t * k.A5)))) * (double)expm2);
+        if ((double)dr2 > k.cut_coulsq) prefactor = 0.0f;
+        const float forcecoul =
+            (float)((double)prefactor * ((double)erfc_ + k.EWALD_F * (double)grij * (double)expm2));
+        ec = ec + (double)(prefactor * erfc_);
+        const float force = (forcecoul + forcelj) * dr2i;
+        ffx = ffx + (double)(dx * force);
+        ffy = ffy + (double)(dy * force);
+        ffz = ffz + (double)(dz * force);
+        vx = vx + (double)(dx * dx * force);
+        vy = vy + (double)(dy * dy * force);
+        vz = vz + (double)(dz * dz * force);
     }
     ffx = warp_sum(ffx);
     ffy = warp_sum(ffy);
@@ -757,15 +848,15 @@ extern "C" int sofia_neighbor_build(sofia_nb_ctx *ctx, int np, const sofia_ainfo
     return SOFIA_OK;
 }
 
-extern "C" int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
-                                       const float *q, const float *lj1, const float *lj2,
-                                       const float *lj3, const float *lj4, int ntypes,
-                                       const int32_t *nlist, const int32_t *numneigh,
-                                       int32_t neigh_alloc, float box, float ibox, double rcut2,
-                                       double cut_coulsq, double alpha, double e_shift,
-                                       double f_shift, float coulpre, float *ff,
-                                       double *potential, double *e_coul,
-                                       double *virial_diag3) {
+// Shared body of the two reference-semantics force entry points: stage the
+// module arrays, run the pair kernel (DSF in FP64 or real-space Ewald in
+// real*4), reduce the per-atom partials in fixed order and halve them.
+static int force_ref_run(sofia_nb_ctx *ctx, bool long_range, int np,
+                         const sofia_ainfo *position, const float *q, const float *lj1,
+                         const float *lj2, const float *lj3, const float *lj4, int ntypes,
+                         const int32_t *nlist, const int32_t *numneigh, int32_t neigh_alloc,
+                         const DsfConst &k, float *ff, double *potential, double *e_coul,
+                         double *virial_diag3) {
     if (!ctx) return SOFIA_EINVAL;
     if (np <= 0 || !position || !q || !lj1 || !lj2 || !lj3 || !lj4 || ntypes <= 0 || !ff)
         return sofia::fail(ctx, SOFIA_EINVAL, "bad args%s");
@@ -797,12 +888,17 @@ extern "C" int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ai
     if ((rc = sofia::stage_out(ctx, ff, sizeof(float) * 3 * (size_t)np, 8, &o_ff))) return rc;
     SOFIA_CUDA(ctx, ctx->pe_atom.ensure(sizeof(double) * 5 * (size_t)np));
     SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * (16 + 8 * RED_BLOCKS)));
-    DsfConst k = make_const(box, ibox, rcut2, cut_coulsq, alpha, e_shift, f_shift, coulpre);
     const long threads = (long)np * 32;
-    k_force_ref<<<sofia::grid_for(threads, 256), 256, 0, st>>>(
-        np, (const float4 *)dpos, (const float *)dq, (const float *)d1, (const float *)d2,
-        (const float *)d3, (const float *)d4, ntypes, (const int *)dl, (const int *)dn,
-        neigh_alloc, k, (float *)o_ff.dev, ctx->pe_atom.as<double>());
+    if (long_range)
+        k_force_long_ref<<<sofia::grid_for(threads, 256), 256, 0, st>>>(
+            np, (const float4 *)dpos, (const float *)dq, (const float *)d1, (const float *)d2,
+            (const float *)d3, (const float *)d4, ntypes, (const int *)dl, (const int *)dn,
+            neigh_alloc, k, (float *)o_ff.dev, ctx->pe_atom.as<double>());
+    else
+        k_force_ref<<<sofia::grid_for(threads, 256), 256, 0, st>>>(
+            np, (const float4 *)dpos, (const float *)dq, (const float *)d1, (const float *)d2,
+            (const float *)d3, (const float *)d4, ntypes, (const int *)dl, (const int *)dn,
+            neigh_alloc, k, (float *)o_ff.dev, ctx->pe_atom.as<double>());
     reduce_cols(st, np, 5, ctx->pe_atom.as<double>(), ctx->red_out.as<double>(), 0.5);
     SOFIA_CUDA(ctx, cudaGetLastError());
     if ((rc = sofia::finish_out(ctx, o_ff))) return rc;
@@ -817,6 +913,35 @@ extern "C" int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ai
         virial_diag3[2] = ctx->h_red[4];
     }
     return SOFIA_OK;
+}
+
+extern "C" int sofia_force_nonbond_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
+                                       const float *q, const float *lj1, const float *lj2,
+                                       const float *lj3, const float *lj4, int ntypes,
+                                       const int32_t *nlist, const int32_t *numneigh,
+                                       int32_t neigh_alloc, float box, float ibox, double rcut2,
+                                       double cut_coulsq, double alpha, double e_shift,
+                                       double f_shift, float coulpre, float *ff,
+                                       double *potential, double *e_coul,
+                                       double *virial_diag3) {
+    const DsfConst k = make_const(box, ibox, rcut2, cut_coulsq, alpha, e_shift, f_shift, coulpre);
+    return force_ref_run(ctx, false, np, position, q, lj1, lj2, lj3, lj4, ntypes, nlist,
+                         numneigh, neigh_alloc, k, ff, potential, e_coul, virial_diag3);
+}
+
+extern "C" int sofia_force_nonbond_long(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
+                                        const float *q, const float *lj1, const float *lj2,
+                                        const float *lj3, const float *lj4, int ntypes,
+                                        const int32_t *nlist, const int32_t *numneigh,
+                                        int32_t neigh_alloc, float box, float ibox, double rcut2,
+                                        double cut_coulsq, double gewald, float coulpre,
+                                        float *ff, double *potential, double *e_coul,
+                                        double *virial_diag3) {
+    if (ctx && !(gewald > 0.0)) return sofia::fail(ctx, SOFIA_EINVAL, "gewald must be > 0%s");
+    DsfConst k = make_const(box, ibox, rcut2, cut_coulsq, 0.0, 0.0, 0.0, coulpre);
+    k.gewald = gewald;
+    return force_ref_run(ctx, true, np, position, q, lj1, lj2, lj3, lj4, ntypes, nlist,
+                         numneigh, neigh_alloc, k, ff, potential, e_coul, virial_diag3);
 }
 
 extern "C" int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,

@@ -17,6 +17,7 @@ reference's offload transfers) or CUDA torch tensors (used in place).
 from __future__ import annotations
 
 import ctypes as C
+import math
 import dataclasses
 
 import numpy as np
@@ -189,6 +190,38 @@ def lj_cut_coul_dsf_nonewton(ctx: Context, position, q, lj, ntypes: int, nlist, 
         ntypes, ptr(nlist), ptr(numneigh), int(neigh_alloc), p.box, p.ibox, p.rcut2,
         p.cut_coulsq, float(p.alpha), p.e_shift, p.f_shift, p.coulpre, ptr(ff), C.byref(pot),
         C.byref(ec), ptr(vir)))
+    return ff, pot.value, ec.value, vir
+
+
+def calculate_gewald(cut_coul: float) -> float:
+    """Ewald splitting parameter of calculate_gewald (Source/get_started.f90:153-173):
+    100 bisection steps on [0, 1] for erfc(g*cut_coul)/cut_coul = 1e-6 (real*4 tolerance)."""
+    cc = float(np.float32(cut_coul))
+    tol = float(np.float32(0.000001))
+    lo, hi, g = 0.0, 1.0, 1.0
+    for _ in range(100):
+        g = 0.5 * (lo + hi)
+        if math.erfc(g * cc) / cc > tol:
+            lo = g
+        else:
+            hi = g
+    return g
+
+
+def lj_cut_coul_long_nonewton(ctx: Context, position, q, lj, ntypes: int, nlist, numneigh,
+                              neigh_alloc: int, p: DsfParams, gewald: float, ff=None):
+    """Real-space Ewald + LJ over the full list (the PME path's pair term), real*4
+    pair arithmetic.  Returns (ff (np,3) float32, potential, e_coul, virial_diag3)."""
+    n = int(position.shape[0])
+    if ff is None:
+        ff = np.zeros((n, 3), np.float32)
+    pot = C.c_double()
+    ec = C.c_double()
+    vir = np.zeros(3, np.float64)
+    ctx.check(ctx._lib.sofia_force_nonbond_long(
+        ctx.handle, n, ptr(position), ptr(q), ptr(lj[0]), ptr(lj[1]), ptr(lj[2]), ptr(lj[3]),
+        ntypes, ptr(nlist), ptr(numneigh), int(neigh_alloc), p.box, p.ibox, p.rcut2,
+        p.cut_coulsq, float(gewald), p.coulpre, ptr(ff), C.byref(pot), C.byref(ec), ptr(vir)))
     return ff, pot.value, ec.value, vir
 
 

@@ -66,6 +66,10 @@ def lib(fast: bool = False) -> C.CDLL:
                                          _f32p, _f32p, _f32p, C.c_int, _i32p, _i32p, C.c_int,
                                          _f32p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                          _f64p, C.c_void_p, C.c_int]
+    L.orc_force_long_nonewton.argtypes = [C.POINTER(OrcParams), C.c_int, _f32p, _f32p, _f32p,
+                                          _f32p, _f32p, _f32p, C.c_int, _i32p, _i32p, C.c_int,
+                                          C.c_double, _f32p, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), _f64p, C.c_void_p, C.c_int]
     L.orc_force_dsf_n2.argtypes = [C.POINTER(OrcParams), C.c_int, _f32p, _f32p, _f32p, _f32p,
                                    _f32p, _f32p, C.c_int, _i32p, _i32p, _i32p, _i32p, _f64p,
                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -184,6 +188,24 @@ def force_dsf(p: OrcParams, pos, q, lj, ntypes, nlist, numneigh, neigh_alloc, nt
                                      lj[3], ntypes, nlist, numneigh, neigh_alloc, ff,
                                      C.byref(pot), C.byref(ec), vir,
                                      ff64.ctypes.data_as(C.c_void_p), nthreads)
+    return ff.reshape(n, 3), ff64.reshape(n, 3), pot.value, ec.value, vir
+
+
+def force_long(p: OrcParams, pos, q, lj, ntypes, nlist, numneigh, neigh_alloc, gewald: float,
+               nthreads=0, fast: bool = False):
+    """lj_cut_coul_long_nonewton (real-space Ewald): ff (float32), ff64, potential,
+    e_coul, virial3."""
+    n = pos.shape[0]
+    ff = np.zeros(n * 3, np.float32)
+    ff64 = np.zeros(n * 3, np.float64)
+    pot = C.c_double()
+    ec = C.c_double()
+    vir = np.zeros(3, np.float64)
+    lib(fast).orc_force_long_nonewton(C.byref(p), n, np.ascontiguousarray(pos, np.float32),
+                                      np.ascontiguousarray(q, np.float32), lj[0], lj[1], lj[2],
+                                      lj[3], ntypes, nlist, numneigh, neigh_alloc, float(gewald),
+                                      ff, C.byref(pot), C.byref(ec), vir,
+                                      ff64.ctypes.data_as(C.c_void_p), nthreads)
     return ff.reshape(n, 3), ff64.reshape(n, 3), pot.value, ec.value, vir
 
 

@@ -391,6 +391,111 @@ void orc_force_dsf_nonewton(const orc_params *p, int np, const orc_ainfo *pos, c
     }
 }
 
+/* mod_force_nonbond.f90:300-400 (lj_cut_coul_long_nonewton_NOMIC; the _MIC
+ * variant at :201-298 has the same arithmetic): real-space Ewald/PME pair term
+ * with LJ over the full list, all pair arithmetic in real*4.  Mixed-mode
+ * statements follow Fortran promotion: dr2i = 1.0d0/dr2, grij = gewald*r,
+ * t = 1.0/(1.0+EWALD_P*grij), the erfc polynomial and forcecoul are computed
+ * in double and stored to real*4; the real*4 exp(-grij*grij) is taken as the
+ * correctly rounded single-precision exponential, (float)exp((double)x).
+ * Force and virial terms are real*4 products added into double sums. */
+void orc_force_long_nonewton(const orc_params *p, int np, const orc_ainfo *pos, const float *q,
+                             const float *lj1, const float *lj2, const float *lj3,
+                             const float *lj4, int ntypes, const int32_t *nlist,
+                             const int32_t *numneigh, int neigh_alloc, double gewald, float *ff,
+                             double *potential, double *e_coul, double *virial3,
+                             double *ff64, int nthreads) {
+    const float box = p->box, ibox = p->ibox, coulpre = p->coulpre;
+    const double rcut2 = p->rcut2, cut_coulsq = p->cut_coulsq;
+    const double EWALD_F = p->EWALD_F, EWALD_P = p->EWALD_P, A1 = p->A1, A2 = p->A2,
+                 A3 = p->A3, A4 = p->A4, A5 = p->A5;
+    const float TWO23 = 8388608.0f; /* 1/epsilon(real*4) */
+    double *pe = (double *)malloc(sizeof(double) * (size_t)np * 5);
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 32) num_threads(nthreads)
+#endif
+    for (int i = 1; i <= np; ++i) {
+        const float x1 = pos[i - 1].x, y1 = pos[i - 1].y, z1 = pos[i - 1].z;
+        const int itype = pos[i - 1].type;
+        const float qtmp = q[i - 1];
+        const int ioffset = (itype - 1) * ntypes;
+        const size_t neigh_off = (size_t)neigh_alloc * (size_t)(i - 1);
+        const int num = numneigh[i - 1];
+        double ffx = 0.0, ffy = 0.0, ffz = 0.0, pot = 0.0, ec = 0.0;
+        double vx = 0.0, vy = 0.0, vz = 0.0;
+        for (int j = 1; j <= num; ++j) {
+            const int neigh = nlist[neigh_off + j - 1];
+            float dx = x1 - pos[neigh - 1].x;
+            float dy = y1 - pos[neigh - 1].y;
+            float dz = z1 - pos[neigh - 1].z;
+            const int jtype = pos[neigh - 1].type;
+            float bx = dx * ibox, by = dy * ibox, bz = dz * ibox;
+            bx = (bx + copysignf(TWO23, bx)) - copysignf(TWO23, dx);
+            by = (by + copysignf(TWO23, by)) - copysignf(TWO23, dy);
+            bz = (bz + copysignf(TWO23, bz)) - copysignf(TWO23, dz);
+            dx = dx - box * bx;
+            dy = dy - box * by;
+            dz = dz - box * bz;
+            const float dr2 = dx * dx + dy * dy + dz * dz;
+            const float dr2i = (float)(1.0 / (double)dr2);
+            float dr6i = dr2i * dr2i * dr2i;
+            if ((double)dr2 > rcut2) dr6i = 0.0f;
+            const int offset = ioffset + jtype - 1;
+            const float forcelj = dr6i * (lj1[offset] * dr6i - lj2[offset]);
+            pot = pot + (double)(dr6i * (dr6i * lj3[offset] - lj4[offset]));
+            const float r = sqrtf(dr2);
+            float prefactor = coulpre * qtmp * q[neigh - 1] / r;
+            const float grij = (float)(gewald * (double)r);
+            const float expm2 = (float)exp((double)(-(grij * grij)));
+            const float t = (float)(1.0 / (1.0 + EWALD_P * (double)grij));
+            const double td = (double)t;
+            const float erfc_ = (float)(td * (A1 + td * (A2 + td * (A3 + td * (A4 + td * A5)))) *
+                                        (double)expm2);
+            if ((double)dr2 > cut_coulsq) prefactor = 0.0f;
+            const float forcecoul = (float)((double)prefactor *
+                                            ((double)erfc_ + EWALD_F * (double)grij * (double)expm2));
+            ec = ec + (double)(prefactor * erfc_);
+            const float force = (forcecoul + forcelj) * dr2i;
+            ffx = ffx + (double)(dx * force);
+            ffy = ffy + (double)(dy * force);
+            ffz = ffz + (double)(dz * force);
+            vx += (double)(dx * dx * force);
+            vy += (double)(dy * dy * force);
+            vz += (double)(dz * dz * force);
+        }
+        ff[(size_t)(i - 1) * 3 + 0] = (float)ffx;
+        ff[(size_t)(i - 1) * 3 + 1] = (float)ffy;
+        ff[(size_t)(i - 1) * 3 + 2] = (float)ffz;
+        if (ff64) {
+            ff64[(size_t)(i - 1) * 3 + 0] = ffx;
+            ff64[(size_t)(i - 1) * 3 + 1] = ffy;
+            ff64[(size_t)(i - 1) * 3 + 2] = ffz;
+        }
+        pe[(size_t)(i - 1) * 5 + 0] = pot;
+        pe[(size_t)(i - 1) * 5 + 1] = ec;
+        pe[(size_t)(i - 1) * 5 + 2] = vx;
+        pe[(size_t)(i - 1) * 5 + 3] = vy;
+        pe[(size_t)(i - 1) * 5 + 4] = vz;
+    }
+    double sp = 0.0, se = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int i = 0; i < np; ++i) {
+        sp += pe[(size_t)i * 5 + 0];
+        se += pe[(size_t)i * 5 + 1];
+        sx += pe[(size_t)i * 5 + 2];
+        sy += pe[(size_t)i * 5 + 3];
+        sz += pe[(size_t)i * 5 + 4];
+    }
+    free(pe);
+    *potential = 0.50 * sp; /* :395-397 */
+    *e_coul = 0.50 * se;
+    if (virial3) {
+        virial3[0] = 0.5 * sx; /* virialx = 0.50*vvx, :387-389 */
+        virial3[1] = 0.5 * sy;
+        virial3[2] = 0.5 * sz;
+    }
+}
+
 /* mod_force_nonbond.f90:409-502 (lj_cut_coul_dsf_N2): O(N^2) pairs i<j with
  * NINT minimum image, a single dr2 < rcut2 gate, 1-2/1-3 weight 0 and 1-4
  * weight 0.5 from specbond.  Accumulates in double (the reference rounds ff to

@@ -78,6 +78,13 @@ void orc_force_dsf_nonewton(const orc_params *p, int np, const orc_ainfo *pos, c
                             double *potential, double *e_coul, double *virial3,
                             double *ff64 /* optional (np,3) double accumulators */,
                             int nthreads);
+/* lj_cut_coul_long_nonewton_NOMIC (mod_force_nonbond.f90:300-400): real*4 real-space Ewald */
+void orc_force_long_nonewton(const orc_params *p, int np, const orc_ainfo *pos, const float *q,
+                             const float *lj1, const float *lj2, const float *lj3,
+                             const float *lj4, int ntypes, const int32_t *nlist,
+                             const int32_t *numneigh, int neigh_alloc, double gewald, float *ff,
+                             double *potential, double *e_coul, double *virial3,
+                             double *ff64, int nthreads);
 void orc_force_dsf_n2(const orc_params *p, int np, const orc_ainfo *pos, const float *q,
                       const float *lj1, const float *lj2, const float *lj3, const float *lj4,
                       int ntypes, const int32_t *specbond, const int32_t *num1bond,

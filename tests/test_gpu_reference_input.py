@@ -63,6 +63,20 @@ def test_fp64_forces_match_oracle(ctx, ref):
     assert np.abs(ff - off).max() <= 2 * np.spacing(np.abs(off).max())
 
 
+def test_real_space_ewald_matches_oracle(ctx, ref):
+    """The PME path's pair term on the reference input (gewald of cut_coul 12 A)."""
+    s, _, p, op, pos, (onl, onn, ona) = ref
+    lj = (s.lj1, s.lj2, s.lj3, s.lj4)
+    g = nb.calculate_gewald(p.cut_coul)
+    off, _, opot, oec, ovir = O.force_long(op, pos, s.q, lj, s.ntypes, onl, onn, ona, g)
+    ff, pot, ec, vir = nb.lj_cut_coul_long_nonewton(ctx, pos, s.q, lj, s.ntypes, onl, onn, ona,
+                                                    p, g)
+    assert abs(pot - opot) <= FP64_TOL * abs(opot)
+    assert abs(ec - oec) <= FP64_TOL * abs(oec)
+    assert np.abs(vir - ovir).max() <= FP64_TOL * np.abs(ovir).max()
+    assert np.abs(ff - off).max() <= 2 * np.spacing(np.abs(off).max())
+
+
 def test_cluster_pair_path(ctx, ref):
     """Production path on the reference system: FP64 within 1e-10 of the oracle,
     mixed within 1e-6 RMS of FP64."""

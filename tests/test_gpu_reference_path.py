@@ -123,6 +123,33 @@ def test_force_fp64_matches_oracle(ctx):
     assert np.abs(ff - off).max() <= 2 * ulp
 
 
+@pytest.mark.parametrize("cut,pad", [(7.0, 1.5), (5.0, 2.0)])
+def test_force_long_matches_oracle(ctx, cut, pad):
+    """Real-space Ewald (real*4 pair arithmetic): FP64 sums within 1e-10, real*4
+    forces within two ulps of the largest force."""
+    s = small_system()
+    p = ref_params(s, cut=cut, pad=pad)
+    pos = s.position_aos()
+    lj = (s.lj1, s.lj2, s.lj3, s.lj4)
+    g = nb.calculate_gewald(cut)
+    onl, onn, ona = O.neighbor_wrapper(_orc_params(p), pos, s.specbond, s.num3bond, 512)
+    off, _, opot, oec, ovir = O.force_long(_orc_params(p), pos, s.q, lj, s.ntypes, onl, onn,
+                                           ona, g)
+    ff, pot, ec, vir = nb.lj_cut_coul_long_nonewton(ctx, pos, s.q, lj, s.ntypes, onl, onn, ona,
+                                                    p, g)
+    assert abs(pot - opot) <= FP64_TOL * abs(opot)
+    assert abs(ec - oec) <= FP64_TOL * abs(oec)
+    assert rel_err(vir, ovir) <= FP64_TOL
+    assert np.abs(ff - off).max() <= 2 * np.spacing(np.abs(off).max())
+    # resident list path gives the same result
+    _, _, na2 = nb.neighbor_wrapper(ctx, pos, s.specbond, s.num3bond, p, 512, want_host=False)
+    ff2, pot2, ec2, _ = nb.lj_cut_coul_long_nonewton(ctx, pos, s.q, lj, s.ntypes, None, None,
+                                                     na2, p, g)
+    assert abs(pot2 - opot) <= FP64_TOL * abs(opot) and abs(ec2 - oec) <= FP64_TOL * abs(oec)
+    with pytest.raises(RuntimeError):
+        nb.lj_cut_coul_long_nonewton(ctx, pos, s.q, lj, s.ntypes, onl, onn, ona, p, 0.0)
+
+
 def test_force_resident_list_equals_host_list(ctx):
     s = small_system()
     p = ref_params(s)

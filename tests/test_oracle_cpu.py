@@ -246,3 +246,67 @@ def test_cluster_stale_last_atom_quirk():
     assert np.all(np.isclose(ptta[:269], pos[:269, :3], atol=1e-4) |
                   np.isclose(np.abs(ptta[:269] - pos[:269, :3]), float(box), atol=1e-3))
     assert not np.allclose(ptta[269], pos[269, :3], atol=1e-3)
+
+
+def _long_fp64(p, pos, q, lj, ntypes, nl, nn, na, g, cut):
+    """Independent FP64 real-space Ewald + LJ with the exact erfc, over the list."""
+    from scipy.special import erfc
+    x = pos[:, :3].astype(np.float64)
+    t = pos[:, 3].view(np.int32) - 1
+    L = float(p.box)
+    n = x.shape[0]
+    ii = np.repeat(np.arange(n), nn)
+    jj = np.concatenate([nl[i * na:i * na + nn[i]] for i in range(n)]) - 1
+    d = x[ii] - x[jj]
+    d -= L * np.round(d / L)
+    r2 = (d * d).sum(axis=1)
+    r = np.sqrt(r2)
+    off = t[ii] * ntypes + t[jj]
+    dr6i = np.where(r2 > cut * cut, 0.0, 1.0 / r2 ** 3)
+    flj = dr6i * (lj[0][off] * dr6i - lj[1][off])
+    elj = dr6i * (dr6i * lj[2][off] - lj[3][off])
+    pref = np.where(r2 > cut * cut, 0.0, float(p.coulpre) * q[ii].astype(np.float64) * q[jj] / r)
+    ec = pref * erfc(g * r)
+    fc = pref * (erfc(g * r) + 2.0 / math.sqrt(math.pi) * g * r * np.exp(-(g * r) ** 2))
+    fr = (fc + flj) / r2
+    f = np.zeros((n, 3))
+    np.add.at(f, ii, d * fr[:, None])
+    return f, 0.5 * elj.sum(), 0.5 * ec.sum(), 0.5 * np.abs(ec).sum()
+
+
+def test_long_range_real_space_vs_exact_fp64():
+    """The real*4 restatement with the A&S 7.1.26 erfc (|error| <= 1.5e-7) against
+    an FP64 evaluation with the exact erfc: real*4-level agreement."""
+    s = small_system()
+    p = _p(s, cut=7.0, pad=1.5)
+    pos = s.position_aos()
+    lj = (s.lj1, s.lj2, s.lj3, s.lj4)
+    g = O.calculate_gewald(7.0)
+    nl, nn, na = O.neighbor_wrapper(p, pos, s.specbond, s.num3bond, 512)
+    ff, ff64, pot, ec, vir = O.force_long(p, pos, s.q, lj, s.ntypes, nl, nn, na, g)
+    f_ref, pot_ref, ec_ref, ec_abs = _long_fp64(p, pos, s.q, lj, s.ntypes, nl, nn, na, g, 7.0)
+    assert pot == pytest.approx(pot_ref, rel=1e-5)
+    # e_coul cancels strongly; bound its error by the sum of |pair terms|
+    assert abs(ec - ec_ref) <= 1e-5 * ec_abs
+    assert rel_err(ff64, f_ref) < 1e-5
+    assert np.array_equal(ff, ff64.astype(np.float32))
+    # the full list holds each pair twice: the net force vanishes to rounding
+    assert np.abs(ff64.sum(axis=0)).max() < 1e-4 * np.abs(ff64).max()
+
+
+def test_long_range_thread_count_invariant():
+    s = small_system()
+    p = _p(s)
+    pos = s.position_aos()
+    lj = (s.lj1, s.lj2, s.lj3, s.lj4)
+    g = O.calculate_gewald(7.0)
+    a = O.neighbor_wrapper(p, pos, s.specbond, s.num3bond, 512)
+    fa = O.force_long(p, pos, s.q, lj, s.ntypes, *a, g, nthreads=1)
+    fb = O.force_long(p, pos, s.q, lj, s.ntypes, *a, g, nthreads=4)
+    assert np.array_equal(fa[0], fb[0]) and fa[2] == fb[2] and fa[3] == fb[3]
+
+
+def test_product_gewald_equals_oracle():
+    from molecular_simulation_code_b200.nonbond import calculate_gewald
+    for c in (8.0, 9.5, 10.0, 12.0):
+        assert calculate_gewald(c) == O.calculate_gewald(c)
