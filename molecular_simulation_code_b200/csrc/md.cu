@@ -750,7 +750,6 @@ extern "C" int sofia_system_md_run(sofia_system *ss, int nsteps, int energy_ever
         }
         SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[6].p, md.step_dev.p, sizeof(long long), cudaMemcpyDeviceToDevice, st));
         SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * sofia::ST_NSLOTS, st));
-        const int had_forces = md.forces_valid;
         int rc = SOFIA_OK;
         if (!md.forces_valid) {
             // initial forces (force_driver(0) + shake(1) before the loop, mod_integrate.f90:237-240)

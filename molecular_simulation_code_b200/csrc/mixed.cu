@@ -173,9 +173,14 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
                        const double *__restrict__ rz, const double *__restrict__ ix,
                        const double *__restrict__ iy, const double *__restrict__ iz,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
-                       AtomRec *__restrict__ rec, float4 *__restrict__ recf) {
+                       AtomRec *__restrict__ rec, float4 *__restrict__ recf,
+                       long long *__restrict__ fslot) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nslots || s >= ncl_dev[0] * CL) return;
+    // the pair kernel adds into the slot-ordered accumulators: start them at zero
+    fslot[s] = 0;
+    fslot[nslots + s] = 0;
+    fslot[2 * nslots + s] = 0;
     const int o = slot_orig[s];
     AtomRec r;
     if (o >= 0) {
@@ -240,9 +245,21 @@ struct SearchArgs {
     int *status;
 };
 
+// Half list: the cluster pair (ci, cj, image) and its mirror (cj, ci, -image)
+// are the same atom pairs, so exactly one of them is kept.  Distinct clusters
+// split by index parity (each row keeps about half of its partners, which
+// balances the rows); a cluster with its own image keeps the positive image;
+// a cluster with itself (no image) keeps one entry with the upper-triangle
+// mask.
+__device__ __forceinline__ bool half_keep(int ci, int cj, int img) {
+    if (ci != cj) return (ci < cj) != (((ci + cj) & 1) != 0);
+    return img >= 13;
+}
+
 // One warp per i-cluster: visit the xy columns within reach (periodic images
 // included), test every cluster's bounding box in three z images, compact the
-// accepted (cluster, image) pairs in visiting order and attach the pair mask.
+// accepted (cluster, image) pairs of the half list in visiting order and
+// attach the pair mask.
 __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
     if (a.cond && !(a.cond[0] & a.cmask)) return;
     const int lane = threadIdx.x & 31;
@@ -284,7 +301,8 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
                         const float ey = gap(ilo.y, ihi.y, jlo.y + sy, jhi.y + sy);
                         const float ez = gap(ilo.z, ihi.z, jlo.z + sz, jhi.z + sz);
                         const float d2 = ex * ex + ey * ey + ez * ez;
-                        acc = d2 < a.rl2;
+                        const int img = (imx + 1) + 3 * (imy + 1) + 9 * (imz + 1);
+                        acc = d2 < a.rl2 && half_keep(icl, jc, img);
                         if (acc) {
                             need_excl = d2 < a.rexcl2;
                             unsigned jreal = 0;
@@ -294,9 +312,11 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
 #pragma unroll
                             for (int ii = 0; ii < CL; ++ii)
                                 if ((ireal >> ii) & 1u) mask |= (unsigned long long)jreal << (ii * CL);
-                            if (jc == icl && imx == 0 && imy == 0 && imz == 0) {
+                            if (jc == icl && img == 13) {
+                                // the cluster with itself: pairs ii < jj only
 #pragma unroll
-                                for (int ii = 0; ii < CL; ++ii) mask &= ~(1ull << (ii * CL + ii));
+                                for (int ii = 0; ii < CL; ++ii)
+                                    mask &= ~(((2ull << ii) - 1ull) << (ii * CL));
                             }
                         }
                     }
@@ -488,19 +508,51 @@ __device__ __forceinline__ long long to_fix<double>(double v) {
     return __double2ll_rn(v * FIX_SCALE);
 }
 
-// Pair kernel: one warp per i-cluster; lane = li (i atom, 0..7) + 8*lj (j quarter,
-// each lane takes j atoms lj and lj+4 of every j-cluster).  List rows are read 32
-// entries at a time with coalesced loads and broadcast to the warp by shuffles;
-// the j atoms are read with 8-lane broadcast loads.  EN adds the LJ and Coulomb
-// energies, VIR the diagonal virial.
+// The j-force values of one entry, v[3h + c] (component c of j atom lj + 4h),
+// summed over the 8 lanes that share lj (lane bits 0..2) by reduce-scatter:
+// each butterfly level keeps half of the values and trades the other half.
+// Afterwards lane (b2 b1 b0) holds component 2*b1 + b0 (3 = none) of j atom
+// lj + 4*b2.  6 shuffles instead of 18 for a full butterfly of 6 values.
+template <typename T>
+__device__ __forceinline__ T reduce_scatter_j(const T (&v)[6], int lane) {
+    const bool u2 = lane & 4, u1 = lane & 2, u0 = lane & 1;
+    T s0, s1, s2;
+    {
+        const T k0 = u2 ? v[3] : v[0], k1 = u2 ? v[4] : v[1], k2 = u2 ? v[5] : v[2];
+        const T o0 = u2 ? v[0] : v[3], o1 = u2 ? v[1] : v[4], o2 = u2 ? v[2] : v[5];
+        s0 = k0 + __shfl_xor_sync(FULL, o0, 4);
+        s1 = k1 + __shfl_xor_sync(FULL, o1, 4);
+        s2 = k2 + __shfl_xor_sync(FULL, o2, 4);
+    }
+    T t0, t1;
+    {
+        const T k0 = u1 ? s2 : s0, k1 = u1 ? (T)0 : s1;
+        const T o0 = u1 ? s0 : s2, o1 = u1 ? s1 : (T)0;
+        t0 = k0 + __shfl_xor_sync(FULL, o0, 2);
+        t1 = k1 + __shfl_xor_sync(FULL, o1, 2);
+    }
+    const T k0 = u0 ? t1 : t0, o0 = u0 ? t0 : t1;
+    return k0 + __shfl_xor_sync(FULL, o0, 1);
+}
+
+// Pair kernel on the half cluster-pair list (each atom pair once, Newton's
+// third law).  One warp per i-cluster; lane = li (i atom, 0..7) + 8*lj (each
+// lane takes j atoms lj and lj+4 of every j-cluster).  List rows are read 32
+// entries at a time with coalesced loads and broadcast by shuffles.
+//   * i forces stay in registers (flushed from FP32 to 64-bit fixed point every
+//     FLUSH entries) and are added once at the end;
+//   * the j forces of each entry are reduced over the 8 lanes of a j atom
+//     (reduce_scatter_j) and added to the slot-ordered fixed-point
+//     accumulators, 24 lanes x one 64-bit atomic add into one j-cluster's
+//     contiguous slots.  Integer addition makes the sums independent of the
+//     order of the atomics, so results stay bit-reproducible.
+// EN adds the LJ and Coulomb energies, VIR the diagonal virial (each pair once).
 template <typename T, bool EN, bool VIR>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
     int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
-    const int *__restrict__ slot_orig, const int *__restrict__ jlist,
-    const unsigned long long *__restrict__ jmask, const int *__restrict__ jcount, int jcap,
-    const float4 *__restrict__ ljtab, PairConst k, long long *__restrict__ fx,
-    long long *__restrict__ fy, long long *__restrict__ fz, double *__restrict__ energy,
-    int *__restrict__ status) {
+    const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
+    const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
+    unsigned long long *__restrict__ fslot, double *__restrict__ energy) {
     extern __shared__ float4 s_lj[];
     __shared__ double s_sh[27 * 3];
     for (int t = threadIdx.x; t < k.ntypes * k.ntypes; t += blockDim.x) s_lj[t] = ljtab[t];
@@ -515,6 +567,11 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
     const int li = lane & 7, lj = lane >> 3;
     const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (icl >= maxcl || icl >= ncl_dev[0]) return;
+    const size_t stride = (size_t)maxcl * CL;
+    // this lane's share of the reduced j force: component jcomp of j atom jslot
+    const int jcomp = 2 * ((lane >> 1) & 1) + (lane & 1);
+    const int jslot = lj + 4 * ((lane >> 2) & 1);
+    unsigned long long *jdst = fslot + (size_t)(jcomp < 3 ? jcomp : 0) * stride;
     const AtomRec ri = rec[icl * CL + li];
     const T qiq = (T)k.coulpre * (T)ri.q;
     const int ti = ri.type * k.ntypes;
@@ -537,6 +594,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
             const double xis = ri.x - s_sh[img * 3 + 0];
             const double yis = ri.y - s_sh[img * 3 + 1];
             const double zis = ri.z - s_sh[img * 3 + 2];
+            T v[6];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int jj = lj + 4 * h;
@@ -549,19 +607,26 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
                 T elj = 0, ec = 0;
                 const T fs = PairMath<T>::template eval<EN>(dx, dy, dz, qiq * (T)rj.q, ljp, on,
                                                             k, elj, ec);
-                ax += dx * fs;
-                ay += dy * fs;
-                az += dz * fs;
+                const T px = dx * fs, py = dy * fs, pz = dz * fs;
+                ax += px;
+                ay += py;
+                az += pz;
+                v[3 * h + 0] = px;
+                v[3 * h + 1] = py;
+                v[3 * h + 2] = pz;
                 if (EN) {
                     a_lj += elj;
                     a_c += ec;
                 }
                 if (VIR) {
-                    a_xx += dx * dx * fs;
-                    a_yy += dy * dy * fs;
-                    a_zz += dz * dz * fs;
+                    a_xx += dx * px;
+                    a_yy += dy * py;
+                    a_zz += dz * pz;
                 }
             }
+            const T fj = reduce_scatter_j<T>(v, lane);
+            if (jcomp < 3 && fj != (T)0)
+                atomicAdd(jdst + jc * CL + jslot, (unsigned long long)(-to_fix<T>(fj)));
             if (((base + e) & (FLUSH - 1)) == FLUSH - 1) {
                 lx += to_fix<T>(ax);
                 ly += to_fix<T>(ay);
@@ -591,15 +656,10 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
         lz += __shfl_xor_sync(FULL, lz, off);
     }
     if (lj == 0) {
-        const int o = slot_orig[icl * CL + li];
-        if (o >= 0) {
-            fx[o] = lx;
-            fy[o] = ly;
-            fz[o] = lz;
-            const long long lim = 1ll << 62;
-            if (lx > lim || lx < -lim || ly > lim || ly < -lim || lz > lim || lz < -lim)
-                atomicAdd(&status[ST_FIXED_OVF], 1);
-        }
+        const size_t si = (size_t)icl * CL + li;
+        if (lx) atomicAdd(fslot + si, (unsigned long long)lx);
+        if (ly) atomicAdd(fslot + stride + si, (unsigned long long)ly);
+        if (lz) atomicAdd(fslot + 2 * stride + si, (unsigned long long)lz);
     }
     if (EN || VIR) {
         e_lj += (double)a_lj;
@@ -624,6 +684,26 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
             o[4] = vzz;
         }
     }
+}
+
+// Slot-ordered fixed-point pair forces -> the caller's atom order (sets the
+// force arrays; bonded terms add to them afterwards).  Flags sums outside the
+// fixed-point range.
+__global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
+                         const int *__restrict__ slot_orig, const long long *__restrict__ fslot,
+                         long long *__restrict__ fx, long long *__restrict__ fy,
+                         long long *__restrict__ fz, int *__restrict__ status) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots || s >= ncl_dev[0] * CL) return;
+    const int o = slot_orig[s];
+    if (o < 0) return;
+    const long long a = fslot[s], b = fslot[nslots + s], c = fslot[2 * (size_t)nslots + s];
+    fx[o] = a;
+    fy[o] = b;
+    fz[o] = c;
+    const long long lim = 1ll << 62;
+    if (a > lim || a < -lim || b > lim || b < -lim || c > lim || c < -lim)
+        atomicAdd(&status[ST_FIXED_OVF], 1);
 }
 
 // Dynamic pruning: keep the outer-list entries that have at least one unmasked
@@ -813,6 +893,7 @@ static int sys_alloc(Sys *s) {
     SOFIA_CUDA(ctx, s->slot_orig.ensure(sizeof(int) * maxcl * CL + sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, s->rec.ensure(sizeof(AtomRec) * maxcl * CL));
     SOFIA_CUDA(ctx, s->recf.ensure(sizeof(float4) * maxcl * CL));
+    SOFIA_CUDA(ctx, s->fslot.ensure(sizeof(long long) * 3 * maxcl * CL));
     SOFIA_CUDA(ctx, s->bb.ensure(sizeof(float4) * 2 * maxcl));
     SOFIA_CUDA(ctx, s->jcount.ensure(sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, s->nclusters.ensure(sizeof(int) * 4));
@@ -846,7 +927,7 @@ static void sys_pack(Sys *s) {
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
         s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
-        s->rec.as<AtomRec>(), s->recf.as<float4>());
+        s->rec.as<AtomRec>(), s->recf.as<float4>(), s->fslot.as<long long>());
     s->launches += 1;
 }
 
@@ -1056,10 +1137,10 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial) {
     const size_t smem = sizeof(float4) * (size_t)s->ntypes * s->ntypes;
     long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
               *fz = s->f[2].as<long long>();
-#define SOFIA_PAIR_ARGS                                                                    \
-    s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->slot_orig.as<int>(), \
-        s->ilist.as<int>(), s->imask.as<unsigned long long>(), s->icount.as<int>(), s->jcap,  \
-        s->ljtab.as<float4>(), k, fx, fy, fz, s->energy.as<double>(), ctx->d_status
+#define SOFIA_PAIR_ARGS                                                                   \
+    s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(), s->ilist.as<int>(),    \
+        s->imask.as<unsigned long long>(), s->icount.as<int>(), s->jcap,                  \
+        s->ljtab.as<float4>(), k, s->fslot.as<unsigned long long>(), s->energy.as<double>()
     if (s->timing) cudaEventRecord(s->ev[2], st);
     if (precision == SOFIA_PREC_FP64) {
         if (virial)
@@ -1081,12 +1162,18 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial) {
         cudaEventRecord(s->ev[3], st);
         s->pending_pair = 1;
     }
-    s->launches += 1;
+    const int nslots = s->max_clusters * CL;
+    k_unpack<<<grid_for(nslots, 256), 256, 0, st>>>(nslots, s->nclusters.as<int>(),
+                                                    s->slot_orig.as<int>(),
+                                                    s->fslot.as<long long>(), fx, fy, fz,
+                                                    ctx->d_status);
+    s->launches += 2;
     if (energy || virial) {
         k_red_stage1<<<RED_BLOCKS, 256, 0, st>>>(s->max_clusters, 5, s->nclusters.as<int>(),
                                                  s->energy.as<double>(), s->part.as<double>());
+        // the half list holds each pair once: no halving
         k_red_stage2<<<1, 256, 0, st>>>(RED_BLOCKS, 5, s->part.as<double>(), s->red.as<double>(),
-                                        0.5);
+                                        1.0);
         s->launches += 2;
     }
     SOFIA_CUDA(ctx, cudaGetLastError());
@@ -1259,6 +1346,7 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
     s->ilist.release();
     s->imask.release();
     s->recf.release();
+    s->fslot.release();
     s->dcount.release();
     s->icount.release();
     s->part.release();
