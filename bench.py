@@ -41,6 +41,7 @@ sys.path.insert(0, ROOT)
 
 DT = 2.0            # fs
 RELAX_STEPS = 100   # untimed damped steps from the lattice start
+EQUIL_STEPS = 400   # untimed 2 fs steps with strong Langevin coupling: brings the lattice start to 300 K
 CUT = 10.0          # A
 SKIN = 2.0          # A
 ALPHA = 0.2         # 1/A
@@ -320,6 +321,8 @@ def run_ours(args, rank, ws):
         m.set_state(x0, v0)
         m.md_setup(s, dt=1.0, temperature=300.0, gamma=0.02, seed=11)
         m.md_run(RELAX_STEPS)  # lattice start: short strongly damped relaxation
+        m.md_setup(s, dt=DT, temperature=300.0, gamma=0.02, seed=13)
+        m.md_run(EQUIL_STEPS)  # release the lattice energy into the bath (tau = 50 fs)
         m.md_setup(s, dt=DT, temperature=300.0, gamma=0.001, seed=12)
         m.md_run(max(warm, 1))
         b0 = m.stats()

@@ -118,7 +118,8 @@ __global__ void k_col_sort_assign(const int *__restrict__ cond, int cmask, int n
                                   const int *__restrict__ col_start,
                                   int *__restrict__ col_atoms, const float *__restrict__ zkey,
                                   const int *__restrict__ cl_start, int *__restrict__ slot_orig,
-                                  int *__restrict__ cl_col, int *__restrict__ status) {
+                                  int *__restrict__ cl_col, int *__restrict__ atom_slot,
+                                  int *__restrict__ status) {
     SOFIA_COND_RETURN;
     __shared__ unsigned long long s[MAX_COL];
     const int c = blockIdx.x;
@@ -158,7 +159,9 @@ __global__ void k_col_sort_assign(const int *__restrict__ cond, int cmask, int n
     }
     const int c0 = cl_start[c], ncl = cl_start[c + 1] - c0;
     for (int t = threadIdx.x; t < ncl * CL; t += blockDim.x) {
-        slot_orig[c0 * CL + t] = (t < nc) ? (int)(s[t] & 0xffffffffu) : -1;
+        const int o = (t < nc) ? (int)(s[t] & 0xffffffffu) : -1;
+        slot_orig[c0 * CL + t] = o;
+        if (o >= 0) atom_slot[o] = c0 * CL + t;
         if ((t & (CL - 1)) == 0) cl_col[c0 + t / CL] = c;
     }
 }
@@ -236,9 +239,9 @@ __device__ __forceinline__ float gap(float alo, float ahi, float blo, float bhi)
 struct SearchArgs {
     const int *cond;
     int cmask;
-    int maxcl, ncx, reach, jcap;
-    float L, s_col, rl2, rexcl2;
-    const int *ncl_dev, *cl_start, *cl_col, *slot_orig, *specbond, *num3bond;
+    int maxcl, ncx, reach, jcap, n;
+    float L, s_col, rl, rl2, rexcl2;
+    const int *ncl_dev, *cl_start, *cl_col, *slot_orig, *specbond, *num3bond, *atom_slot;
     const float4 *bb;
     int *jlist, *jcount;
     unsigned long long *jmask;
@@ -271,6 +274,22 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
     // i-cluster atoms: real-atom bits and orig ids (lanes 0..7 hold one each)
     const int my_io = a.slot_orig[icl * CL + (lane & 7)];
     const unsigned ireal = __ballot_sync(FULL, my_io >= 0) & 0xffu;
+    // the exclusion partners of the 8 i atoms as cluster slots, 96 items
+    // (i atom b / 12, partner b % 12) spread 3 per lane
+    int ex_slot[3], ex_bit[3];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const int b = lane + 32 * t;
+        const int ii = b / 12, l = b - 12 * (b / 12);
+        const int io = a.slot_orig[icl * CL + ii];
+        int ps = -1;
+        if (io >= 0 && l < min(a.num3bond[io], 12)) {
+            const int po = a.specbond[io * 12 + l] - 1;
+            if (po >= 0 && po < a.n) ps = a.atom_slot[po];
+        }
+        ex_slot[t] = ps;
+        ex_bit[t] = ii * CL + (ps & (CL - 1));
+    }
     int count = 0;
     int *row = a.jlist + (size_t)icl * a.jcap;
     unsigned long long *mrow = a.jmask + (size_t)icl * a.jcap;
@@ -291,6 +310,9 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
             const int jc0 = a.cl_start[cx + cy * a.ncx], jc1 = a.cl_start[cx + cy * a.ncx + 1];
             for (int imz = -1; imz <= 1; ++imz) {
                 const float sz = imz * a.L;
+                // the column image spans z in [sz, sz + L): skip images out of reach
+                const float gz = gap(ilo.z, ihi.z, sz, sz + a.L);
+                if (gx * gx + gy * gy + gz * gz >= a.rl2) continue;
                 for (int base = jc0; base < jc1; base += 32) {
                     const int jc = base + lane;
                     bool acc = false, need_excl = false;
@@ -321,28 +343,20 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
                         }
                     }
                     const unsigned ballot = __ballot_sync(FULL, acc);
-                    // exclusions: the warp resolves each nearby accepted entry together
+                    // exclusions: for each nearby accepted entry the warp ORs the bits of
+                    // the i atoms' partners that sit in that j-cluster
                     unsigned todo = __ballot_sync(FULL, need_excl);
                     while (todo) {
                         const int src = __ffs(todo) - 1;
                         todo &= todo - 1;
                         const int jsrc = __shfl_sync(FULL, jc, src);
-                        unsigned bits[2];
+                        unsigned long long m = 0ull;
 #pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int b = lane + 32 * h;
-                            const int io = a.slot_orig[icl * CL + (b >> 3)];
-                            const int jo = a.slot_orig[jsrc * CL + (b & 7)];
-                            bool ex = false;
-                            if (io >= 0 && jo >= 0) {
-                                const int n3 = a.num3bond[io];
-                                for (int l = 0; l < n3 && l < 12; ++l)
-                                    ex |= (a.specbond[io * 12 + l] == jo + 1);
-                            }
-                            bits[h] = __ballot_sync(FULL, ex);
-                        }
-                        if (lane == src)
-                            mask &= ~((unsigned long long)bits[0] | ((unsigned long long)bits[1] << 32));
+                        for (int t = 0; t < 3; ++t)
+                            if (ex_slot[t] >= 0 && (ex_slot[t] >> 3) == jsrc) m |= 1ull << ex_bit[t];
+                        const unsigned lo = __reduce_or_sync(FULL, (unsigned)m);
+                        const unsigned hi = __reduce_or_sync(FULL, (unsigned)(m >> 32));
+                        if (lane == src) mask &= ~((unsigned long long)lo | ((unsigned long long)hi << 32));
                     }
                     if (acc) {
                         const int at = count + __popc(ballot & ((1u << lane) - 1u));
@@ -588,21 +602,25 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
         const unsigned long long mym = (lane < cnt) ? mrow[base + lane] : 0ull;
         for (int e = 0; e < cnt; ++e) {
             const int w = __shfl_sync(FULL, myw, e);
-            const unsigned mb = (unsigned)(__shfl_sync(FULL, mym, e) >> (li * CL)) & 0xffu;
+            const unsigned long long mm = __shfl_sync(FULL, mym, e);
             const int jc = w & ((1 << IMG_SHIFT) - 1);
             const int img = w >> IMG_SHIFT;
             const double xis = ri.x - s_sh[img * 3 + 0];
             const double yis = ri.y - s_sh[img * 3 + 1];
             const double zis = ri.z - s_sh[img * 3 + 2];
-            T v[6];
+            T v[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
+                // pruned mask, lane layout: bit h*32 + lane; a j half with no pair in
+                // range is skipped by the whole warp
+                const unsigned mh = (unsigned)(mm >> (32 * h));
+                if (mh == 0u) continue;
                 const int jj = lj + 4 * h;
                 const AtomRec rj = rec[jc * CL + jj];
                 const T dx = (T)(xis - rj.x);
                 const T dy = (T)(yis - rj.y);
                 const T dz = (T)(zis - rj.z);
-                const bool on = (mb >> jj) & 1u;
+                const bool on = (mh >> lane) & 1u;
                 const float4 ljp = s_lj[ti + rj.type];
                 T elj = 0, ec = 0;
                 const T fs = PairMath<T>::template eval<EN>(dx, dy, dz, qiq * (T)rj.q, ljp, on,
@@ -707,10 +725,13 @@ __global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
 }
 
 // Dynamic pruning: keep the outer-list entries that have at least one unmasked
-// atom pair within r_in = rc + margin at the current positions.  Valid until an
-// atom moves more than margin/2 (checked like the rebuild trigger).  Distances
-// here only select entries, so FP32 copies of the positions suffice (the
-// squared radius carries a 1e-3 A safety margin).
+// atom pair within r_in = rc + margin at the current positions, and replace
+// their pair mask by the in-range bits in the pair kernel's lane layout (bit
+// h*32 + lane = pair (i atom lane&7, j atom (lane>>3) + 4h)).  Valid until an
+// atom moves more than margin/2 (checked like the rebuild trigger): a pair
+// out of range now cannot come within rc before the next prune.  Distances
+// here only select pairs, so FP32 copies of the positions suffice (the squared
+// radius carries a 1e-3 A^2 safety margin).
 __global__ void __launch_bounds__(256) k_prune(
     const int *__restrict__ cond, int cmask, int maxcl, const int *__restrict__ ncl_dev,
     const float4 *__restrict__ recf,
@@ -718,6 +739,14 @@ __global__ void __launch_bounds__(256) k_prune(
     const int *__restrict__ jcount, int jcap, float L, float rin2, int *__restrict__ ilist,
     unsigned long long *__restrict__ imask, int *__restrict__ icount) {
     SOFIA_COND_RETURN;
+    __shared__ float s_shf[27 * 3];
+    if (threadIdx.x < 27) {
+        const int im = threadIdx.x;
+        s_shf[im * 3 + 0] = (float)(im % 3 - 1) * L;
+        s_shf[im * 3 + 1] = (float)((im / 3) % 3 - 1) * L;
+        s_shf[im * 3 + 2] = (float)(im / 9 - 1) * L;
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int li = lane & 7, lj = lane >> 3;
     const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -734,32 +763,34 @@ __global__ void __launch_bounds__(256) k_prune(
         const int myw = (lane < cnt) ? row[base + lane] : 0;
         const unsigned long long mym = (lane < cnt) ? mrow[base + lane] : 0ull;
         unsigned keepbits = 0;
+        unsigned long long newm = 0ull;
+#pragma unroll 2
         for (int e = 0; e < cnt; ++e) {
             const int w = __shfl_sync(FULL, myw, e);
             const unsigned long long m = __shfl_sync(FULL, mym, e);
             const unsigned mb = (unsigned)(m >> (li * CL)) & 0xffu;
             const int jc = w & ((1 << IMG_SHIFT) - 1);
             const int img = w >> IMG_SHIFT;
-            const float sx = (float)(img % 3 - 1) * L, sy = (float)((img / 3) % 3 - 1) * L,
-                        sz = (float)(img / 9 - 1) * L;
-            bool any = false;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int jj = lj + 4 * h;
-                const float4 pj = recf[jc * CL + jj];
-                const float dx = pi.x - (pj.x + sx), dy = pi.y - (pj.y + sy),
-                            dz = pi.z - (pj.z + sz);
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                any |= ((mb >> jj) & 1u) && r2 < rin2;
+            const float sx = s_shf[img * 3 + 0], sy = s_shf[img * 3 + 1], sz = s_shf[img * 3 + 2];
+            const float4 pj0 = recf[jc * CL + lj], pj1 = recf[jc * CL + lj + 4];
+            float dx = pi.x - (pj0.x + sx), dy = pi.y - (pj0.y + sy), dz = pi.z - (pj0.z + sz);
+            const bool in0 = ((mb >> lj) & 1u) && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rin2;
+            dx = pi.x - (pj1.x + sx);
+            dy = pi.y - (pj1.y + sy);
+            dz = pi.z - (pj1.z + sz);
+            const bool in1 = ((mb >> (lj + 4)) & 1u) && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rin2;
+            const unsigned b0 = __ballot_sync(FULL, in0), b1 = __ballot_sync(FULL, in1);
+            if (b0 | b1) {
+                keepbits |= 1u << e;
+                if (lane == e) newm = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
             }
-            if (__any_sync(FULL, any)) keepbits |= 1u << e;
         }
         // compact the kept entries of this batch in order
         const bool mine = (keepbits >> lane) & 1u;
         const int at = kept + __popc(keepbits & ((1u << lane) - 1u));
         if (mine) {
             orow[at] = myw;
-            omrow[at] = mym;
+            omrow[at] = newm;
         }
         kept += __popc(keepbits);
     }
@@ -894,6 +925,7 @@ static int sys_alloc(Sys *s) {
     SOFIA_CUDA(ctx, s->rec.ensure(sizeof(AtomRec) * maxcl * CL));
     SOFIA_CUDA(ctx, s->recf.ensure(sizeof(float4) * maxcl * CL));
     SOFIA_CUDA(ctx, s->fslot.ensure(sizeof(long long) * 3 * maxcl * CL));
+    SOFIA_CUDA(ctx, s->atom_slot.ensure(sizeof(int) * n));
     SOFIA_CUDA(ctx, s->bb.ensure(sizeof(float4) * 2 * maxcl));
     SOFIA_CUDA(ctx, s->jcount.ensure(sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, s->nclusters.ensure(sizeof(int) * 4));
@@ -962,7 +994,8 @@ static int sys_build(Sys *s, const int *cond) {
     k_col_sort_assign<<<s->ncols, 256, 0, st>>>(cond, cm, s->ncols, s->col_start.as<int>(),
                                                 s->col_atoms.as<int>(), s->col_key.as<float>(),
                                                 s->cl_start.as<int>(), s->slot_orig.as<int>(),
-                                                cl_col, s->status_local.as<int>());
+                                                cl_col, s->atom_slot.as<int>(),
+                                                s->status_local.as<int>());
     k_set_ncl<<<1, 32, 0, st>>>(cond, cm, s->cl_start.as<int>() + s->ncols,
                                 s->nclusters.as<int>());
     sys_pack(s);
@@ -979,6 +1012,7 @@ static int sys_build(Sys *s, const int *cond) {
     a.L = (float)s->L;
     a.s_col = (float)s->s_col;
     const float rl = (float)s->rlist + 1e-3f;
+    a.rl = rl;
     a.rl2 = rl * rl;
     a.rexcl2 = (float)(s->r_excl * s->r_excl);
     a.ncl_dev = s->nclusters.as<int>();
@@ -987,6 +1021,8 @@ static int sys_build(Sys *s, const int *cond) {
     a.slot_orig = s->slot_orig.as<int>();
     a.specbond = s->specbond.as<int>();
     a.num3bond = s->num3bond.as<int>();
+    a.atom_slot = s->atom_slot.as<int>();
+    a.n = s->n;
     a.bb = s->bb.as<float4>();
     a.jlist = s->jlist.as<int>();
     a.jcount = s->jcount.as<int>();
@@ -1347,6 +1383,7 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
     s->imask.release();
     s->recf.release();
     s->fslot.release();
+    s->atom_slot.release();
     s->dcount.release();
     s->icount.release();
     s->part.release();

@@ -75,6 +75,7 @@ struct Sys {
     DevBuf col_count, col_start, col_fill, col_atoms, col_key, cl_start;
     DevBuf slot_orig, rec, recf, bb, jlist, jmask, jcount, nclusters;
     DevBuf fslot;                       // pair forces in cluster-slot order, 64-bit fixed point [3][slots]
+    DevBuf atom_slot;                   // cluster slot of every atom (inverse of slot_orig)
     DevBuf status_local;
     DevBuf energy;                      // per-i-cluster energy partials (pot, ecoul, vir x,y,z)
     DevBuf red;                         // reduced energies
