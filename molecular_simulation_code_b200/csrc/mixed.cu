@@ -454,7 +454,8 @@ struct PairMath;
 // exp(-alpha^2 r^2) = 2^(kexp r^2) with kexp = -alpha^2 log2(e).
 template <>
 struct PairMath<float> {
-    template <bool EN>
+    // SAME: the LJ and Coulomb cut-offs are equal, so one test gates both terms
+    template <bool EN, bool SAME>
     __device__ __forceinline__ static float eval(float dx, float dy, float dz, float qiq,
                                                  float4 lj, bool on, const PairConst &k,
                                                  float &elj, float &ec) {
@@ -464,7 +465,7 @@ struct PairMath<float> {
         const float r = r2 * rinv;
         const float dr6i = r2inv * r2inv * r2inv;
         const bool lj_on = on && r2 <= k.rcut2;
-        const bool c_on = on && r2 <= k.cut_coulsq;
+        const bool c_on = SAME ? lj_on : (on && r2 <= k.cut_coulsq);
         const float flj = dr6i * fmaf(lj.x, dr6i, -lj.y);
         const float pref = qiq * rinv;
         const float ex = ex2_a(k.kexp * r2);
@@ -477,6 +478,7 @@ struct PairMath<float> {
             elj = lj_on ? dr6i * fmaf(dr6i, lj.z, -lj.w) : 0.0f;
             ec = c_on ? pref * (erfcc - fmaf(r, k.e_shift, r2 * k.f_shift)) : 0.0f;
         }
+        if (SAME) return lj_on ? (fc + flj) * r2inv : 0.0f;
         const float fs = ((c_on ? fc : 0.0f) + (lj_on ? flj : 0.0f)) * r2inv;
         return on ? fs : 0.0f;
     }
@@ -484,7 +486,7 @@ struct PairMath<float> {
 
 template <>
 struct PairMath<double> {
-    template <bool EN>
+    template <bool EN, bool SAME>
     __device__ __forceinline__ static double eval(double dx, double dy, double dz, double qiq,
                                                   float4 lj, bool on, const PairConst &k,
                                                   double &elj, double &ec) {
@@ -561,7 +563,7 @@ __device__ __forceinline__ T reduce_scatter_j(const T (&v)[6], int lane) {
 //     contiguous slots.  Integer addition makes the sums independent of the
 //     order of the atomics, so results stay bit-reproducible.
 // EN adds the LJ and Coulomb energies, VIR the diagonal virial (each pair once).
-template <typename T, bool EN, bool VIR>
+template <typename T, bool EN, bool VIR, bool SAME>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
     int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
@@ -623,8 +625,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
                 const bool on = (mh >> lane) & 1u;
                 const float4 ljp = s_lj[ti + rj.type];
                 T elj = 0, ec = 0;
-                const T fs = PairMath<T>::template eval<EN>(dx, dy, dz, qiq * (T)rj.q, ljp, on,
-                                                            k, elj, ec);
+                const T fs = PairMath<T>::template eval<EN, SAME>(dx, dy, dz, qiq * (T)rj.q, ljp,
+                                                                  on, k, elj, ec);
                 const T px = dx * fs, py = dy * fs, pz = dz * fs;
                 ax += px;
                 ay += py;
@@ -1178,20 +1180,21 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial) {
         s->imask.as<unsigned long long>(), s->icount.as<int>(), s->jcap,                  \
         s->ljtab.as<float4>(), k, s->fslot.as<unsigned long long>(), s->energy.as<double>()
     if (s->timing) cudaEventRecord(s->ev[2], st);
+    // sofia_system_create requires rcut == cut_coul: one cut-off gates both terms
     if (precision == SOFIA_PREC_FP64) {
         if (virial)
-            k_pair<double, true, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            k_pair<double, true, true, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
         else if (energy)
-            k_pair<double, true, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            k_pair<double, true, false, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
         else
-            k_pair<double, false, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            k_pair<double, false, false, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
     } else {
         if (virial)
-            k_pair<float, true, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            k_pair<float, true, true, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
         else if (energy)
-            k_pair<float, true, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            k_pair<float, true, false, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
         else
-            k_pair<float, false, false><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            k_pair<float, false, false, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
     }
 #undef SOFIA_PAIR_ARGS
     if (s->timing) {
