@@ -965,11 +965,11 @@ static void sys_pack(Sys *s) {
     s->launches += 1;
 }
 
-// Launch the list build.  With cond == nullptr it always runs; otherwise every
-// kernel returns at once unless (cond[0] & 1).  The records are packed in the
-// middle (the bounding boxes and the search need them), so after this call the
-// records are current whether or not the list was rebuilt.
-static int sys_build(Sys *s, const int *cond) {
+// The list build, in two parts around the record pack (the bounding boxes and
+// the search need current records).  With cond == nullptr the kernels always
+// run; otherwise every kernel returns at once unless (cond[0] & 1).
+// Part 1: bin atoms into xy columns, sort each column by z, assign cluster slots.
+static void sys_build_bin(Sys *s, const int *cond) {
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     const int n = s->n;
@@ -1000,7 +1000,15 @@ static int sys_build(Sys *s, const int *cond) {
                                                 s->status_local.as<int>());
     k_set_ncl<<<1, 32, 0, st>>>(cond, cm, s->cl_start.as<int>() + s->ncols,
                                 s->nclusters.as<int>());
-    sys_pack(s);
+    s->launches += 7;
+}
+
+// Part 2: cluster bounding boxes and the cluster-pair search.
+static int sys_build_search(Sys *s, const int *cond) {
+    sofia_nb_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int cm = 1;
+    int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
     k_bbox<<<grid_for(s->max_clusters, 128), 128, 0, st>>>(
         cond, cm, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
         s->slot_orig.as<int>(), s->bb.as<float4>());
@@ -1032,10 +1040,18 @@ static int sys_build(Sys *s, const int *cond) {
     a.status = s->status_local.as<int>();
     k_search<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(a);
     SOFIA_CUDA(ctx, cudaGetLastError());
-    s->launches += 10;
+    s->launches += 2;
     if (!cond) s->n_builds++;
     s->built = 1;
     return SOFIA_OK;
+}
+
+// The whole build; the records are current afterwards whether or not the
+// list was rebuilt.
+static int sys_build(Sys *s, const int *cond) {
+    sys_build_bin(s, cond);
+    sys_pack(s);
+    return sys_build_search(s, cond);
 }
 
 // Folds finished event pairs into the timers (called after a stream sync).

@@ -51,6 +51,26 @@ def test_md_deterministic_and_graph_equals_eager(ctx, small):
         o.close()
 
 
+def test_graph_conditional_build_and_prune_equal_eager(ctx, small):
+    """Long enough for several list rebuilds and prunes: the captured step (build
+    and prune as conditional graph nodes) takes exactly the eager path's steps."""
+    s = small
+    a = _system(ctx, s, dt=2.0, gamma=0.01, seed=5)
+    a0 = a.stats()
+    a.md_run(150, use_graph=True)
+    a1 = a.stats()
+    b = _system(ctx, s, dt=2.0, gamma=0.01, seed=5)
+    b.md_run(150, use_graph=False)
+    b1 = b.stats()
+    assert a1["builds"] - a0["builds"] >= 2 and a1["prunes"] - a0["prunes"] >= 2
+    assert (a1["builds"], a1["prunes"]) == (b1["builds"], b1["prunes"])
+    xa, va, _ = a.get_state()
+    xb, vb, _ = b.get_state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+    a.close()
+    b.close()
+
+
 def test_md_shake_keeps_constraints(ctx, small):
     s = small
     a = _system(ctx, s, dt=1.0, gamma=0.02, seed=3, shake_maxiter=200, shake_tol=1e-10)
