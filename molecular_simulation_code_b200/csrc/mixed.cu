@@ -216,8 +216,10 @@ __global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= maxcl || c >= ncl_dev[0]) return;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    int real = 0;
     for (int k = 0; k < CL; ++k) {
         if (slot_orig[c * CL + k] < 0) continue;
+        real |= 1 << k;
         const AtomRec r = rec[c * CL + k];
         lo[0] = fmin(lo[0], r.x);
         lo[1] = fmin(lo[1], r.y);
@@ -226,8 +228,9 @@ __global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
         hi[1] = fmax(hi[1], r.y);
         hi[2] = fmax(hi[2], r.z);
     }
+    // w of the low corner carries the cluster's real-atom bits (padding slots clear)
     bb[2 * c] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
-                            __double2float_rd(lo[2]), 0.0f);
+                            __double2float_rd(lo[2]), __int_as_float(real));
     bb[2 * c + 1] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
                                 __double2float_ru(hi[2]), 0.0f);
 }
@@ -272,8 +275,12 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
     const int col = a.cl_col[icl];
     const int cxi = col % a.ncx, cyi = col / a.ncx;
     // i-cluster atoms: real-atom bits and orig ids (lanes 0..7 hold one each)
-    const int my_io = a.slot_orig[icl * CL + (lane & 7)];
-    const unsigned ireal = __ballot_sync(FULL, my_io >= 0) & 0xffu;
+    const unsigned ireal = (unsigned)__float_as_int(ilo.w) & 0xffu;
+    // byte ii of iexp is 0xff when i atom ii is real
+    unsigned long long iexp = 0ull;
+#pragma unroll
+    for (int ii = 0; ii < CL; ++ii)
+        if ((ireal >> ii) & 1u) iexp |= 0xffull << (ii * CL);
     // the exclusion partners of the 8 i atoms as cluster slots, 96 items
     // (i atom b / 12, partner b % 12) spread 3 per lane
     int ex_slot[3], ex_bit[3];
@@ -327,13 +334,9 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
                         acc = d2 < a.rl2 && half_keep(icl, jc, img);
                         if (acc) {
                             need_excl = d2 < a.rexcl2;
-                            unsigned jreal = 0;
-#pragma unroll
-                            for (int k = 0; k < CL; ++k)
-                                jreal |= (a.slot_orig[jc * CL + k] >= 0 ? 1u : 0u) << k;
-#pragma unroll
-                            for (int ii = 0; ii < CL; ++ii)
-                                if ((ireal >> ii) & 1u) mask |= (unsigned long long)jreal << (ii * CL);
+                            const unsigned long long jreal =
+                                (unsigned long long)((unsigned)__float_as_int(jlo.w) & 0xffu);
+                            mask = (jreal * 0x0101010101010101ull) & iexp;
                             if (jc == icl && img == 13) {
                                 // the cluster with itself: pairs ii < jj only
 #pragma unroll
@@ -726,14 +729,29 @@ __global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
         atomicAdd(&status[ST_FIXED_OVF], 1);
 }
 
+// 8x8 bit-matrix transpose: bit (r*8 + c) -> bit (c*8 + r)  (three swap rounds).
+__device__ __forceinline__ unsigned long long transpose8(unsigned long long x) {
+    unsigned long long t;
+    t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+    x = x ^ t ^ (t << 7);
+    t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+    x = x ^ t ^ (t << 14);
+    t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+    x = x ^ t ^ (t << 28);
+    return x;
+}
+
 // Dynamic pruning: keep the outer-list entries that have at least one unmasked
 // atom pair within r_in = rc + margin at the current positions, and replace
 // their pair mask by the in-range bits in the pair kernel's lane layout (bit
-// h*32 + lane = pair (i atom lane&7, j atom (lane>>3) + 4h)).  Valid until an
-// atom moves more than margin/2 (checked like the rebuild trigger): a pair
-// out of range now cannot come within rc before the next prune.  Distances
-// here only select pairs, so FP32 copies of the positions suffice (the squared
-// radius carries a 1e-3 A^2 safety margin).
+// 8*jj + ii = pair (i atom ii, j atom jj), i.e. bit h*32 + lane for pair
+// (lane & 7, (lane >> 3) + 4h)).  Valid until an atom moves more than margin/2
+// (checked like the rebuild trigger): a pair out of range now cannot come
+// within rc before the next prune.  One warp per i-cluster, one lane per list
+// entry: the i atoms sit in registers and every lane checks its entry's 64
+// pairs, so entries need no shuffles or ballots.  Distances here only select
+// pairs, so FP32 copies of the positions suffice (the squared radius carries a
+// 1e-3 A^2 safety margin).
 __global__ void __launch_bounds__(256) k_prune(
     const int *__restrict__ cond, int cmask, int maxcl, const int *__restrict__ ncl_dev,
     const float4 *__restrict__ recf,
@@ -750,10 +768,16 @@ __global__ void __launch_bounds__(256) k_prune(
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int li = lane & 7, lj = lane >> 3;
     const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (icl >= maxcl || icl >= ncl_dev[0]) return;
-    const float4 pi = recf[icl * CL + li];
+    float xi[CL], yi[CL], zi[CL];
+#pragma unroll
+    for (int ii = 0; ii < CL; ++ii) {
+        const float4 p = recf[icl * CL + ii];
+        xi[ii] = p.x;
+        yi[ii] = p.y;
+        zi[ii] = p.z;
+    }
     const int n = jcount[icl];
     const int *row = jlist + (size_t)icl * jcap;
     const unsigned long long *mrow = jmask + (size_t)icl * jcap;
@@ -761,40 +785,38 @@ __global__ void __launch_bounds__(256) k_prune(
     unsigned long long *omrow = imask + (size_t)icl * jcap;
     int kept = 0;
     for (int base = 0; base < n; base += 32) {
-        const int cnt = min(32, n - base);
-        const int myw = (lane < cnt) ? row[base + lane] : 0;
-        const unsigned long long mym = (lane < cnt) ? mrow[base + lane] : 0ull;
-        unsigned keepbits = 0;
-        unsigned long long newm = 0ull;
-#pragma unroll 2
-        for (int e = 0; e < cnt; ++e) {
-            const int w = __shfl_sync(FULL, myw, e);
-            const unsigned long long m = __shfl_sync(FULL, mym, e);
-            const unsigned mb = (unsigned)(m >> (li * CL)) & 0xffu;
+        const int e = base + lane;
+        const bool active = e < n;
+        const int w = active ? row[e] : 0;
+        const unsigned long long m = active ? mrow[e] : 0ull;
+        unsigned lo = 0u, hi = 0u;  // in-range bits 8*jj + ii, jj < 4 and jj >= 4
+        if (active) {
             const int jc = w & ((1 << IMG_SHIFT) - 1);
             const int img = w >> IMG_SHIFT;
             const float sx = s_shf[img * 3 + 0], sy = s_shf[img * 3 + 1], sz = s_shf[img * 3 + 2];
-            const float4 pj0 = recf[jc * CL + lj], pj1 = recf[jc * CL + lj + 4];
-            float dx = pi.x - (pj0.x + sx), dy = pi.y - (pj0.y + sy), dz = pi.z - (pj0.z + sz);
-            const bool in0 = ((mb >> lj) & 1u) && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rin2;
-            dx = pi.x - (pj1.x + sx);
-            dy = pi.y - (pj1.y + sy);
-            dz = pi.z - (pj1.z + sz);
-            const bool in1 = ((mb >> (lj + 4)) & 1u) && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rin2;
-            const unsigned b0 = __ballot_sync(FULL, in0), b1 = __ballot_sync(FULL, in1);
-            if (b0 | b1) {
-                keepbits |= 1u << e;
-                if (lane == e) newm = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
+#pragma unroll
+            for (int jj = 0; jj < CL; ++jj) {
+                const float4 pj = recf[jc * CL + jj];
+                const float xs = pj.x + sx, ys = pj.y + sy, zs = pj.z + sz;
+#pragma unroll
+                for (int ii = 0; ii < CL; ++ii) {
+                    const float dx = xi[ii] - xs, dy = yi[ii] - ys, dz = zi[ii] - zs;
+                    const bool in = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rin2;
+                    if (jj < 4) lo |= in ? (1u << (8 * jj + ii)) : 0u;
+                    else hi |= in ? (1u << (8 * (jj - 4) + ii)) : 0u;
+                }
             }
         }
-        // compact the kept entries of this batch in order
-        const bool mine = (keepbits >> lane) & 1u;
-        const int at = kept + __popc(keepbits & ((1u << lane) - 1u));
-        if (mine) {
-            orow[at] = myw;
+        const unsigned long long newm =
+            (((unsigned long long)hi << 32) | lo) & transpose8(m);
+        const bool keep = newm != 0ull;
+        const unsigned kb = __ballot_sync(FULL, keep);
+        if (keep) {
+            const int at = kept + __popc(kb & ((1u << lane) - 1u));
+            orow[at] = w;
             omrow[at] = newm;
         }
-        kept += __popc(keepbits);
+        kept += __popc(kb);
     }
     if (lane == 0) icount[icl] = kept;
 }
