@@ -142,6 +142,20 @@ int sofia_force_nonbond_long(sofia_nb_ctx *ctx, int np, const sofia_ainfo *posit
                              double *e_coul, double *virial_diag3);
 
 /*
+ * improper_harmonic_lammps14 (Source/mod_force_dihed.f90:1546-1724): harmonic
+ * improper torsions E = k (omega - omega0)^2 over improlist[nimpro*5] (i1..i4,
+ * type; 1-based), improcoeff[nimprotypes*2] = (k, omega0 in rad).  Forces are
+ * ADDED to ff_impro (real*4 [np][3], the reference's ff_impro), the energy to
+ * *e_improper and the diagonal virial to virial3 (may be NULL).  The reference
+ * reads no omega0 from its topology (read_topol leaves theta0 unset,
+ * Source/mod_readfile.f90:433), so the caller supplies it.
+ */
+int sofia_improper_harmonic(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position, int nimpro,
+                            const int32_t *improlist, const double *improcoeff, int nimprotypes,
+                            float box, float ibox, float *ff_impro, double *e_improper,
+                            double *virial3);
+
+/*
  * Allocation-free form of sofia_force_nonbond_dsf.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot allocate device
  * memory when they need forces: work being captured into a CUDA graph (where
@@ -300,7 +314,8 @@ int sofia_system_timers(sofia_system *sys, int enable, double *timers);
 #define SOFIA_TERM_ANGLE 2
 #define SOFIA_TERM_TORSION 4
 #define SOFIA_TERM_PAIR14 8
-#define SOFIA_MD_NE 12 /* lj, coul, self, bond, angle, torsion, coul14, lj14, kinetic, total, T(K), step */
+#define SOFIA_TERM_IMPROPER 16
+#define SOFIA_MD_NE 13 /* lj, coul, self, bond, angle, torsion, coul14, lj14, kinetic, total, T(K), step, improper */
 
 typedef struct {
     double dt;          /* fs */
@@ -326,6 +341,10 @@ typedef struct {
     const double *shake_bond;  /* [nshake*3] bond lengths */
     int shake_maxiter;         /* 0 = 25 like the reference */
     double shake_tol;          /* 0 = 1e-4 like the reference */
+    int nimpro;                /* harmonic impropers (SOFIA_TERM_IMPROPER) */
+    const int32_t *impropers;  /* [nimpro*5] i1..i4, type */
+    int nimprotypes;
+    const double *impro_coeff; /* [nimprotypes*2] k (kcal/mol/rad^2), omega0 (rad) */
 } sofia_md_desc;
 
 int sofia_system_md_setup(sofia_system *sys, const sofia_md_desc *md);

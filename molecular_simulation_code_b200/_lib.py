@@ -43,12 +43,14 @@ class SofiaMdDesc(C.Structure):
                 ("angle_coeff", C.c_void_p), ("ndihed", C.c_int), ("dihedrals", C.c_void_p),
                 ("ndihedtypes", C.c_int), ("dihed_coeff", C.c_void_p), ("lj14", C.c_void_p),
                 ("nshake", C.c_int), ("shake", C.c_void_p), ("shake_bond", C.c_void_p),
-                ("shake_maxiter", C.c_int), ("shake_tol", C.c_double)]
+                ("shake_maxiter", C.c_int), ("shake_tol", C.c_double),
+                ("nimpro", C.c_int), ("impropers", C.c_void_p), ("nimprotypes", C.c_int),
+                ("impro_coeff", C.c_void_p)]
 
 
-SOFIA_MD_NE = 12
+SOFIA_MD_NE = 13
 MD_ENERGY_NAMES = ["lj", "coul", "self", "bond", "angle", "torsion", "coul14", "lj14", "kinetic",
-                   "total", "temperature", "step"]
+                   "total", "temperature", "step", "improper"]
 
 
 class SofiaSystemDesc(C.Structure):
@@ -85,6 +87,8 @@ SIGNATURES: dict[str, tuple] = {
                                       _F, _F, _D, _D, _D, _F, _P, C.POINTER(_D), C.POINTER(_D),
                                       _P]),
     "sofia_check_neighbor": (_I, [_P, _I, _P, _P, _P, _D, C.POINTER(C.c_int32)]),
+    "sofia_improper_harmonic": (_I, [_P, _I, _P, _I, _P, _P, _I, _F, _F, _P, C.POINTER(_D),
+                                     _P]),
     "sofia_force_nonbond_dsf_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P,
                                              C.c_int32, _F, _F, _D, _D, _D, _D, _D, _F, _P,
                                              C.POINTER(_D), C.POINTER(_D), _P]),

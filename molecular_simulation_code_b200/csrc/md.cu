@@ -19,6 +19,7 @@
 #include <cmath>
 #include <vector>
 
+#include "improper.cuh"
 #include "system.cuh"
 
 namespace sofia {
@@ -156,6 +157,31 @@ __global__ void k_angle(int na, const int *__restrict__ al, const double *__rest
     fadd(&fy[i3], -vy2);
     fadd(&fz[i3], -vz2);
     if (EN) e[m] = tk * dtheta;
+}
+
+// improper_harmonic_lammps14 (mod_force_dihed.f90:1546-1724) on the FP64 state.
+template <bool EN>
+__global__ void k_improper(int ni, const int *__restrict__ il, const double *__restrict__ ic,
+                           const double *__restrict__ x, const double *__restrict__ y,
+                           const double *__restrict__ z, double L, long long *__restrict__ fx,
+                           long long *__restrict__ fy, long long *__restrict__ fz,
+                           double *__restrict__ e) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= ni) return;
+    const int i1 = il[5 * m] - 1, i2 = il[5 * m + 1] - 1, i3 = il[5 * m + 2] - 1,
+              i4 = il[5 * m + 3] - 1, t = il[5 * m + 4] - 1;
+    const double v1[3] = {mimg(x[i1] - x[i2], L), mimg(y[i1] - y[i2], L), mimg(z[i1] - z[i2], L)};
+    const double v2[3] = {mimg(x[i3] - x[i2], L), mimg(y[i3] - y[i2], L), mimg(z[i3] - z[i2], L)};
+    const double v3[3] = {mimg(x[i4] - x[i3], L), mimg(y[i4] - y[i3], L), mimg(z[i4] - z[i3], L)};
+    const ImproperOut r = improper_harmonic(v1, v2, v3, ic[2 * t], ic[2 * t + 1]);
+    long long *f[3] = {fx, fy, fz};
+    for (int d = 0; d < 3; ++d) {
+        fadd(&f[d][i1], r.f1[d]);
+        fadd(&f[d][i2], r.f2[d]);
+        fadd(&f[d][i3], r.f3[d]);
+        fadd(&f[d][i4], r.f4[d]);
+    }
+    if (EN) e[m] = r.e;
 }
 
 struct DihArgs {
@@ -530,6 +556,13 @@ static int md_forces(Sys *s, bool energy, bool force_build) {
         else
             k_dihedral<false><<<grid_for(nd, 128), 128, 0, st>>>(a);
     }
+    if ((md.terms & 16) && md.nimpro) {
+        double *ei = et + nb + na + 3 * (size_t)nd;
+        if (energy)
+            k_improper<true><<<grid_for(md.nimpro, 128), 128, 0, st>>>(md.nimpro, md.impros.as<int>(), md.icoef.as<double>(), x, y, z, s->L, fx, fy, fz, ei);
+        else
+            k_improper<false><<<grid_for(md.nimpro, 128), 128, 0, st>>>(md.nimpro, md.impros.as<int>(), md.icoef.as<double>(), x, y, z, s->L, fx, fy, fz, ei);
+    }
     if (md.gamma > 0.0) {
         const double kT = KBOLTZ * md.temperature;
         const double gsig = sqrt(12.0 * 2.0 * md.gamma * kT * KCAL2AMU / md.dt) / KCAL2AMU;
@@ -564,10 +597,33 @@ static void md_energy_reduce(Sys *s) {
         md_reduce(st, md.ndihed, 3, 1, ed, part, red + 8);
         md_reduce(st, md.ndihed, 3, 2, ed, part, red + 9);
     }
-    double *ke = md.eterm.as<double>() + (md.nbond + md.nangle + 3 * (size_t)md.ndihed);
+    if (md.nimpro && (md.terms & 16))
+        md_reduce(st, md.nimpro, 1, 0, et + md.nbond + md.nangle + 3 * (size_t)md.ndihed, part,
+                  red + 11);
+    double *ke = md.eterm.as<double>() + (md.nbond + md.nangle + 3 * (size_t)md.ndihed +
+                                          (size_t)md.nimpro);
     k_ke<<<grid_for(s->n, 256), 256, 0, st>>>(s->n, s->mass.as<double>(), s->v[0].as<double>(),
                                               s->v[1].as<double>(), s->v[2].as<double>(), ke);
     md_reduce(st, s->n, 1, 0, ke, part, red + 10);
+}
+
+// Reduced device energies (red slots: 0-1 pair, 5 bond, 6 angle, 7-9 torsion,
+// coul14, lj14, 10 kinetic, 11 improper) -> the SOFIA_MD_NE output layout.
+static void md_fill_energies(const Md &md, const double *e, double *o) {
+    const double pot = e[0] + e[1] + md.e_self + e[5] + e[6] + e[7] + e[8] + e[9] + e[11];
+    o[0] = e[0];
+    o[1] = e[1];
+    o[2] = md.e_self;
+    o[3] = e[5];
+    o[4] = e[6];
+    o[5] = e[7];
+    o[6] = e[8];
+    o[7] = e[9];
+    o[8] = e[10];
+    o[9] = pot + e[10];
+    o[10] = 2.0 * e[10] / ((double)md.ndof * KBOLTZ);
+    o[11] = (double)md.step;
+    o[12] = e[11];
 }
 
 // One MD step (all device work; capturable).
@@ -657,6 +713,7 @@ extern "C" int sofia_system_md_setup(sofia_system *ss, const sofia_md_desc *d) {
     md.nangle = d->angles ? d->nangle : 0;
     md.ndihed = d->dihedrals ? d->ndihed : 0;
     md.nshake = d->shake ? d->nshake : 0;
+    md.nimpro = d->impropers ? d->nimpro : 0;
     md.terms = d->terms;
     md.shake_maxiter = d->shake_maxiter > 0 ? d->shake_maxiter : 25;
     md.shake_tol = d->shake_tol > 0.0 ? d->shake_tol : (double)0.0001f;
@@ -670,6 +727,8 @@ extern "C" int sofia_system_md_setup(sofia_system *ss, const sofia_md_desc *d) {
     if ((rc = up(ctx, md.lj14, d->lj14, d->lj14 ? (size_t)4 * s->ntypes * s->ntypes : 0))) return rc;
     if ((rc = up(ctx, md.shake, d->shake, (size_t)md.nshake * 5))) return rc;
     if ((rc = up(ctx, md.sbond, d->shake_bond, (size_t)md.nshake * 3))) return rc;
+    if ((rc = up(ctx, md.impros, d->impropers, (size_t)md.nimpro * 5))) return rc;
+    if ((rc = up(ctx, md.icoef, d->impro_coeff, (size_t)(d->nimprotypes > 0 ? d->nimprotypes : 0) * 2))) return rc;
     // validate indices on the host (no kernel ever sees an out-of-range id)
     {
         const int n = s->n;
@@ -683,7 +742,8 @@ extern "C" int sofia_system_md_setup(sofia_system *ss, const sofia_md_desc *d) {
         };
         if ((md.nbond && bad(d->bonds, md.nbond, 3, 2, 2, d->nbondtypes)) ||
             (md.nangle && bad(d->angles, md.nangle, 4, 3, 3, d->nangletypes)) ||
-            (md.ndihed && bad(d->dihedrals, md.ndihed, 5, 4, 4, d->ndihedtypes)))
+            (md.ndihed && bad(d->dihedrals, md.ndihed, 5, 4, 4, d->ndihedtypes)) ||
+            (md.nimpro && bad(d->impropers, md.nimpro, 5, 4, 4, d->nimprotypes)))
             return sofia::fail(ctx, SOFIA_EINVAL, "bonded list index or type out of range%s");
         if ((md.terms & 8) && md.ndihed && !d->lj14)
             return sofia::fail(ctx, SOFIA_EINVAL, "1-4 pairs need lj14 tables%s");
@@ -697,7 +757,8 @@ extern "C" int sofia_system_md_setup(sofia_system *ss, const sofia_md_desc *d) {
                     return sofia::fail(ctx, SOFIA_EINVAL, "SHAKE atom index out of range%s");
         }
     }
-    const size_t nterm = (size_t)md.nbond + md.nangle + 3 * (size_t)md.ndihed + (size_t)s->n;
+    const size_t nterm = (size_t)md.nbond + md.nangle + 3 * (size_t)md.ndihed +
+                         (size_t)md.nimpro + (size_t)s->n;
     SOFIA_CUDA(ctx, md.eterm.ensure(sizeof(double) * nterm));
     SOFIA_CUDA(ctx, md.ered.ensure(sizeof(double) * (16 + sofia::MRED)));
     SOFIA_CUDA(ctx, cudaMemset(md.ered.p, 0, sizeof(double) * 16));
@@ -794,19 +855,7 @@ extern "C" int sofia_system_md_run(sofia_system *ss, int nsteps, int energy_ever
         if (energies && energy_every > 0) {
             double e[16];
             SOFIA_CUDA(ctx, cudaMemcpy(e, md.ered.p, sizeof(double) * 16, cudaMemcpyDeviceToHost));
-            const double pot = e[0] + e[1] + md.e_self + e[5] + e[6] + e[7] + e[8] + e[9];
-            energies[0] = e[0];
-            energies[1] = e[1];
-            energies[2] = md.e_self;
-            energies[3] = e[5];
-            energies[4] = e[6];
-            energies[5] = e[7];
-            energies[6] = e[8];
-            energies[7] = e[9];
-            energies[8] = e[10];
-            energies[9] = pot + e[10];
-            energies[10] = 2.0 * e[10] / ((double)md.ndof * sofia::KBOLTZ);
-            energies[11] = (double)md.step;
+            sofia::md_fill_energies(md, e, energies);
         }
         return SOFIA_OK;
     }
@@ -1005,19 +1054,7 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
                 double e[16];
                 SOFIA_CUDA(ctx, cudaMemcpy(e, md.ered.p, sizeof(double) * 16, cudaMemcpyDeviceToHost));
                 double *o = energies + (size_t)i * SOFIA_MD_NE;
-                const double pot = e[0] + e[1] + md.e_self + e[5] + e[6] + e[7] + e[8] + e[9];
-                o[0] = e[0];
-                o[1] = e[1];
-                o[2] = md.e_self;
-                o[3] = e[5];
-                o[4] = e[6];
-                o[5] = e[7];
-                o[6] = e[8];
-                o[7] = e[9];
-                o[8] = e[10];
-                o[9] = pot + e[10];
-                o[10] = 2.0 * e[10] / ((double)md.ndof * sofia::KBOLTZ);
-                o[11] = (double)md.step;
+                sofia::md_fill_energies(md, e, o);
             }
         }
         return SOFIA_OK;

@@ -14,6 +14,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "improper.cuh"
 
 namespace {
 
@@ -992,6 +993,97 @@ extern "C" int sofia_pair14_dsf(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
     if (e_dihedral) *e_dihedral += ctx->h_red[0];
     if (e_coul_14) *e_coul_14 += ctx->h_red[1];
     if (pot_14) *pot_14 += ctx->h_red[2];
+    return SOFIA_OK;
+}
+
+// improper_harmonic_lammps14 (mod_force_dihed.f90:1546-1724), one thread per
+// improper: real*4 coordinate differences with the NINT minimum image, FP64
+// angle math (sofia::improper_harmonic); forces into FP64 accumulators,
+// energy and virial per improper for a fixed-order reduction.
+__global__ void k_improper_ref(int nimpro, int np, const float4 *__restrict__ pos,
+                               const int *__restrict__ il, const double *__restrict__ ic,
+                               int nimprotypes, float box, float ibox, double *__restrict__ acc,
+                               double *__restrict__ pe, int *__restrict__ status) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nimpro) return;
+    const int i1 = il[5 * m] - 1, i2 = il[5 * m + 1] - 1, i3 = il[5 * m + 2] - 1,
+              i4 = il[5 * m + 3] - 1, t = il[5 * m + 4] - 1;
+    double *o = pe + (size_t)m * 4;
+    if ((unsigned)i1 >= (unsigned)np || (unsigned)i2 >= (unsigned)np ||
+        (unsigned)i3 >= (unsigned)np || (unsigned)i4 >= (unsigned)np ||
+        (unsigned)t >= (unsigned)nimprotypes) {
+        atomicAdd(&status[sofia::ST_BADBIN], 1);
+        o[0] = o[1] = o[2] = o[3] = 0.0;
+        return;
+    }
+    const float4 p1 = pos[i1], p2 = pos[i2], p3 = pos[i3], p4 = pos[i4];
+    const double v1[3] = {minimg1((double)(p1.x - p2.x), box, ibox),
+                          minimg1((double)(p1.y - p2.y), box, ibox),
+                          minimg1((double)(p1.z - p2.z), box, ibox)};
+    const double v2[3] = {minimg1((double)(p3.x - p2.x), box, ibox),
+                          minimg1((double)(p3.y - p2.y), box, ibox),
+                          minimg1((double)(p3.z - p2.z), box, ibox)};
+    const double v3[3] = {minimg1((double)(p4.x - p3.x), box, ibox),
+                          minimg1((double)(p4.y - p3.y), box, ibox),
+                          minimg1((double)(p4.z - p3.z), box, ibox)};
+    const sofia::ImproperOut r = sofia::improper_harmonic(v1, v2, v3, ic[2 * t], ic[2 * t + 1]);
+    for (int d = 0; d < 3; ++d) {
+        atomicAdd(&acc[3 * i1 + d], r.f1[d]);
+        atomicAdd(&acc[3 * i2 + d], r.f2[d]);
+        atomicAdd(&acc[3 * i3 + d], r.f3[d]);
+        atomicAdd(&acc[3 * i4 + d], r.f4[d]);
+    }
+    o[0] = r.e;
+    o[1] = r.vir[0];
+    o[2] = r.vir[1];
+    o[3] = r.vir[2];
+}
+
+extern "C" int sofia_improper_harmonic(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
+                                       int nimpro, const int32_t *improlist,
+                                       const double *improcoeff, int nimprotypes, float box,
+                                       float ibox, float *ff_impro, double *e_improper,
+                                       double *virial3) {
+    if (!ctx) return SOFIA_EINVAL;
+    if (np <= 0 || !position || nimpro < 0 || (nimpro > 0 && !improlist) || !improcoeff ||
+        nimprotypes <= 0 || !ff_impro)
+        return sofia::fail(ctx, SOFIA_EINVAL, "bad args%s");
+    if (nimpro == 0) return SOFIA_OK;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int rc;
+    const void *dpos, *dil, *dic;
+    if ((rc = sofia::stage_in(ctx, position, sizeof(float4) * (size_t)np, 0, &dpos))) return rc;
+    if ((rc = sofia::stage_in(ctx, improlist, sizeof(int) * 5 * (size_t)nimpro, 1, &dil))) return rc;
+    if ((rc = sofia::stage_in(ctx, improcoeff, sizeof(double) * 2 * (size_t)nimprotypes, 2, &dic)))
+        return rc;
+    sofia::OutArg o_ff;
+    if ((rc = sofia::stage_out(ctx, ff_impro, sizeof(float) * 3 * (size_t)np, 5, &o_ff, true)))
+        return rc;
+    SOFIA_CUDA(ctx, ctx->acc64.ensure(sizeof(double) * 3 * (size_t)np));
+    SOFIA_CUDA(ctx, ctx->pe_atom.ensure(sizeof(double) * 4 * (size_t)nimpro));
+    SOFIA_CUDA(ctx, ctx->red_out.ensure(sizeof(double) * (16 + 8 * RED_BLOCKS)));
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->acc64.p, 0, sizeof(double) * 3 * (size_t)np, st));
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
+    k_improper_ref<<<sofia::grid_for(nimpro, 128), 128, 0, st>>>(
+        nimpro, np, (const float4 *)dpos, (const int *)dil, (const double *)dic, nimprotypes, box,
+        ibox, ctx->acc64.as<double>(), ctx->pe_atom.as<double>(), ctx->d_status);
+    reduce_cols(st, nimpro, 4, ctx->pe_atom.as<double>(), ctx->red_out.as<double>(), 1.0);
+    k_add_to_float<<<sofia::grid_for(3L * np, 256), 256, 0, st>>>(3L * np, ctx->acc64.as<double>(),
+                                                                  (float *)o_ff.dev);
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    if ((rc = sofia::finish_out(ctx, o_ff))) return rc;
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(ctx->h_red, ctx->red_out.p, sizeof(double) * 4,
+                                    cudaMemcpyDeviceToHost, st));
+    if ((rc = check_status(ctx))) return rc;
+    if (ctx->h_status[sofia::ST_BADBIN])
+        return sofia::fail(ctx, SOFIA_EINVAL, "improper atom index or type out of range%s");
+    if (e_improper) *e_improper += ctx->h_red[0];
+    if (virial3) {
+        virial3[0] += ctx->h_red[1];
+        virial3[1] += ctx->h_red[2];
+        virial3[2] += ctx->h_red[3];
+    }
     return SOFIA_OK;
 }
 

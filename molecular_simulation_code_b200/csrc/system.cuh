@@ -34,9 +34,9 @@ struct Md {
     int ready = 0;
     double dt = 2.0, temperature = 300.0, gamma = 0.0;  // fs, K, 1/fs
     unsigned long long seed = 0;
-    int nbond = 0, nangle = 0, ndihed = 0, nshake = 0;
+    int nbond = 0, nangle = 0, ndihed = 0, nshake = 0, nimpro = 0;
     int nbt = 0, nat = 0, ndt = 0;
-    DevBuf bonds, bcoef, angles, acoef, diheds, dcoef, lj14, shake, sbond;
+    DevBuf bonds, bcoef, angles, acoef, diheds, dcoef, lj14, shake, sbond, impros, icoef;
     int shake_maxiter = 25;
     double shake_tol = 1e-4;
     int terms = 15;

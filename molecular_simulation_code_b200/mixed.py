@@ -101,22 +101,27 @@ class System:
         self.ctx.check(self.ctx._lib.sofia_system_drift(self.handle, float(dt), int(nsteps)))
 
     def md_setup(self, sysdata, dt: float = 2.0, temperature: float = 300.0,
-                 gamma: float = 0.001, seed: int = 1, terms: int = 15, shake: bool = True,
+                 gamma: float = 0.001, seed: int = 1, terms: int = 31, shake: bool = True,
                  shake_maxiter: int = 0, shake_tol: float = 0.0):
-        """Bonded lists, SHAKE groups and thermostat of the device-resident MD."""
+        """Bonded lists, SHAKE groups and thermostat of the device-resident MD.
+        terms: bit 1 bonds, 2 angles, 4 torsions, 8 1-4 pairs, 16 impropers."""
         k = [np.ascontiguousarray(a) for a in (
             sysdata.bonds.astype(np.int32), sysdata.bond_coeff.astype(np.float64),
             sysdata.angles.astype(np.int32), sysdata.angle_coeff.astype(np.float64),
             sysdata.dihedrals.astype(np.int32), sysdata.dihed_coeff.astype(np.float64),
             np.ascontiguousarray(sysdata.lj14, np.float64).reshape(-1),
-            sysdata.shake.astype(np.int32), sysdata.shake_bond.astype(np.float64))]
+            sysdata.shake.astype(np.int32), sysdata.shake_bond.astype(np.float64),
+            sysdata.impropers.astype(np.int32).reshape(-1, 5),
+            sysdata.impro_coeff.astype(np.float64).reshape(-1, 2))]
         self._md_keep = k
         ns = k[7].shape[0] if shake else 0
         d = SofiaMdDesc(float(dt), float(temperature), float(gamma), int(seed), int(terms),
                         k[0].shape[0], ptr(k[0]), k[1].shape[0], ptr(k[1]),
                         k[2].shape[0], ptr(k[2]), k[3].shape[0], ptr(k[3]),
                         k[4].shape[0], ptr(k[4]), k[5].shape[0], ptr(k[5]), ptr(k[6]),
-                        ns, ptr(k[7]), ptr(k[8]), int(shake_maxiter), float(shake_tol))
+                        ns, ptr(k[7]), ptr(k[8]), int(shake_maxiter), float(shake_tol),
+                        k[9].shape[0], ptr(k[9]) if k[9].size else None, k[10].shape[0],
+                        ptr(k[10]) if k[10].size else None)
         self.ctx.check(self.ctx._lib.sofia_system_md_setup(self.handle, C.byref(d)))
 
     def md_run(self, nsteps: int, energy_every: int = 0, use_graph: bool = True) -> dict | None:

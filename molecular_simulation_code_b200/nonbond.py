@@ -246,6 +246,23 @@ def dihedral_opls_dsf(ctx: Context, position, q, ntypes: int, lj14, dihedlist, d
     return ffh, ed.value, ec.value, p14.value
 
 
+def improper_harmonic(ctx: Context, position, improlist, improcoeff, p: DsfParams,
+                      ff_impro=None):
+    """improper_harmonic_lammps14: returns (ff_impro (np,3) float32 with the forces
+    added, e_improper, virial_diag3)."""
+    n = int(position.shape[0])
+    if ff_impro is None:
+        ff_impro = np.zeros((n, 3), np.float32)
+    il = np.ascontiguousarray(improlist, np.int32)
+    ic = np.ascontiguousarray(improcoeff, np.float64)
+    e = C.c_double(0.0)
+    vir = np.zeros(3, np.float64)
+    ctx.check(ctx._lib.sofia_improper_harmonic(ctx.handle, n, ptr(position), il.shape[0], ptr(il),
+                                               ptr(ic), ic.shape[0], p.box, p.ibox, ptr(ff_impro),
+                                               C.byref(e), ptr(vir)))
+    return ff_impro, e.value, vir
+
+
 def correct_1x_bonds(ctx: Context, position, q, lst, col_a: int, col_b: int, gewald: float,
                      fudge: float, p: DsfParams, ffc=None):
     """correct_12/13/14_bonds over rows of ``lst``.  Returns (ffc, e_corr, virial3)."""

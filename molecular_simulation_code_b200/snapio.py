@@ -22,7 +22,7 @@ import math
 
 import numpy as np
 
-from .system import SofiaSystem, lj_tables_rmin
+from .system import SofiaSystem, improper_omega, lj_tables_rmin
 
 
 def _f32_times10(v):
@@ -246,7 +246,7 @@ def build_reference_system(mol: dict, top: dict, xyz: np.ndarray, box,
     n1 = np.zeros(n, np.int32)
     n2 = np.zeros(n, np.int32)
     n3 = np.zeros(n, np.int32)
-    bonds, angles, diheds, shake, sbond = [], [], [], [], []
+    bonds, angles, diheds, shake, sbond, impros = [], [], [], [], [], []
     base = 0
     for mt in range(len(counts)):
         na = int(natoms[mt])
@@ -273,6 +273,9 @@ def build_reference_system(mol: dict, top: dict, xyz: np.ndarray, box,
             for r in top["diheds"]:
                 if int(r[0]) == mt + 1:
                     diheds.append(tuple(base + int(r[c]) for c in (2, 3, 4, 5)) + (int(r[1]),))
+            for r in top["impros"]:
+                if int(r[0]) == mt + 1:
+                    impros.append(tuple(base + int(r[c]) for c in (2, 3, 4, 5)) + (int(r[1]),))
             for g in top["shake"]:
                 if int(g[1]) == mt + 1:
                     num = int(g[0])
@@ -289,6 +292,18 @@ def build_reference_system(mol: dict, top: dict, xyz: np.ndarray, box,
         angle_coeff[int(r[1]) - 1] = [r[5], r[6] * (2.0 * math.acos(-1.0) / 360.0)]
     n_gly = int(counts[0]) if natoms[0] == 10 else 0
     vel = velocity if velocity is not None else np.zeros((n, 3), np.float32)
+    # impropers: k from the topology; the reference reads no equilibrium angle
+    # (read_topol leaves theta0 unset, Source/mod_readfile.f90:433), so omega0 is the
+    # mean angle of each improper type in the given snapshot
+    impro_arr = np.array(impros, np.int32).reshape(-1, 5)
+    nit = max(int(top["nimprotypes"]), 1)
+    impro_coeff = np.zeros((nit, 2))
+    for r in top["impros"]:
+        impro_coeff[int(r[1]) - 1, 0] = r[6]
+    for t in range(nit):
+        sel = impro_arr[impro_arr[:, 4] == t + 1]
+        if len(sel):
+            impro_coeff[t, 1] = float(np.mean(improper_omega(xyz, box, sel[:, :4] - 1)))
     return SofiaSystem(
         n_gly=n_gly, n_wat=int(np.sum(counts)) - n_gly, box=np.float32(box), position=None,
         xyz=np.ascontiguousarray(xyz, np.float32), types=types, q=q, mass_type=mass_type,
@@ -299,7 +314,8 @@ def build_reference_system(mol: dict, top: dict, xyz: np.ndarray, box,
         dihedrals=np.array(diheds, np.int32).reshape(-1, 5),
         dihed_coeff=np.zeros((max(top["ndihedtypes"], 1), 4)),
         shake=np.array(shake, np.int32).reshape(-1, 5),
-        shake_bond=np.array(sbond, np.float64).reshape(-1, 3), velocity=vel, seed=0)
+        shake_bond=np.array(sbond, np.float64).reshape(-1, 3), velocity=vel, seed=0,
+        impropers=impro_arr, impro_coeff=impro_coeff)
 
 
 def load_fixture(path: str):

@@ -63,6 +63,10 @@ GLY_DIHEDRALS = [
     ((8, 1, 2, 5), 2), ((8, 1, 2, 6), 2), ((8, 1, 2, 7), 2),
     ((9, 1, 2, 5), 2), ((9, 1, 2, 6), 2), ((9, 1, 2, 7), 2),
 ]
+# the carboxylate improper (reference topol_cndo.top:72: atoms 2 4 1 5, central atom third,
+# k = 1.1 kcal/mol/rad^2); omega0 is taken from the template geometry
+GLY_IMPROPER = (1, 3, 0, 4)
+GLY_IMPROPER_K = 1.1
 # SHAKE groups (reference topol_cndo.top:78-87): CH2 (num 3), NH3 (num 4), rigid water (-3)
 WATER_OH = 1.0
 WATER_HH = 2.0 * WATER_OH * math.sin(math.radians(_TET) / 2.0)
@@ -102,6 +106,10 @@ class SofiaSystem:
     shake_bond: np.ndarray          # (ns,3) float64 bond lengths
     velocity: np.ndarray            # (np,3) float32 Angstrom/fs
     seed: int
+    impropers: np.ndarray = dataclasses.field(
+        default_factory=lambda: np.zeros((0, 5), np.int32))   # (ni,5) int32: i1..i4, type
+    impro_coeff: np.ndarray = dataclasses.field(
+        default_factory=lambda: np.zeros((1, 2), np.float64))  # (nit,2): k, omega0 (rad)
 
     @property
     def np_atoms(self) -> int:
@@ -123,6 +131,31 @@ class SofiaSystem:
         g = np.repeat(np.arange(self.n_gly, dtype=np.int32), 10)
         w = self.n_gly + np.repeat(np.arange(self.n_wat, dtype=np.int32), 3)
         return np.concatenate([g, w])
+
+
+def improper_omega(xyz: np.ndarray, box: float, quads: np.ndarray) -> np.ndarray:
+    """The improper angle omega (rad) of improper_harmonic_lammps14
+    (Source/mod_force_dihed.f90:1572-1620) for 0-based atom quadruples (m,4):
+    the angle between the planes (1,2,3) and (2,3,4), minimum image."""
+    x = np.asarray(xyz, np.float64)
+    L = float(box)
+
+    def mi(d):
+        return d - L * np.round(d / L)
+    q = np.asarray(quads)
+    v1 = mi(x[q[:, 0]] - x[q[:, 1]])
+    v2 = mi(x[q[:, 2]] - x[q[:, 1]])
+    v3 = mi(x[q[:, 3]] - x[q[:, 2]])
+    r1 = 1.0 / np.linalg.norm(v1, axis=1)
+    r2 = 1.0 / np.linalg.norm(v2, axis=1)
+    r3 = 1.0 / np.linalg.norm(v3, axis=1)
+    c0 = (v1 * v3).sum(1) * r1 * r3
+    c1 = (v1 * v2).sum(1) * r1 * r2
+    c2 = -(v3 * v2).sum(1) * r3 * r2
+    s1 = 1.0 / np.maximum(1.0 - c1 * c1, 0.001)
+    s2 = 1.0 / np.maximum(1.0 - c2 * c2, 0.001)
+    c = np.clip((c1 * c2 + c0) * np.sqrt(s1 * s2), -1.0, 1.0)
+    return np.arccos(c)
 
 
 def lj_tables_4eps(ntypes: int, sig_a: np.ndarray, eps_kcal: np.ndarray):
@@ -382,7 +415,7 @@ def _assemble(n_gly, n_wat, box, xyz32, types, q, mass_type, ntypes, tables, rng
             n2[i] = len(p12[k]) + len(p13[k])
             n3[i] = len(parts)
 
-    bonds, angles, diheds, shake, shake_bond = [], [], [], [], []
+    bonds, angles, diheds, shake, shake_bond, impros = [], [], [], [], [], []
     bond_types = {}
     bond_coeff = []
     for key in GLY_BONDS:
@@ -406,6 +439,7 @@ def _assemble(n_gly, n_wat, box, xyz32, types, q, mass_type, ntypes, tables, rng
         shake_bond.append((1.09, 1.09, 0.0))
         shake.append((4, base + 3, base + 6, base + 7, base + 8))
         shake_bond.append((1.01, 1.01, 1.01))
+        impros.append(tuple(base + i + 1 for i in GLY_IMPROPER) + (1,))
     for w in range(n_wat):
         base = 10 * n_gly + 3 * w
         fill(base, w12, w13, w14, 3)
@@ -417,6 +451,8 @@ def _assemble(n_gly, n_wat, box, xyz32, types, q, mass_type, ntypes, tables, rng
 
     # Maxwell-Boltzmann velocities in Angstrom/fs: sigma_v = sqrt(kB T / m) with
     # kB T in kcal/mol converted through kcal2amu (reference get_started.f90:32,38).
+    impro_arr = np.array(impros, np.int32).reshape(-1, 5)
+    omega0 = float(np.mean(improper_omega(xyz32, box, impro_arr[:, :4] - 1))) if n_gly else 0.0
     kboltz = 0.001987204181
     kcal2amu = 0.0004184
     m_atom = mass_type[types - 1]
@@ -435,7 +471,8 @@ def _assemble(n_gly, n_wat, box, xyz32, types, q, mass_type, ntypes, tables, rng
         dihed_coeff=np.zeros((2, 4), np.float64),
         shake=np.array(shake, np.int32).reshape(-1, 5),
         shake_bond=np.array(shake_bond, np.float64).reshape(-1, 3),
-        velocity=vel, seed=seed)
+        velocity=vel, seed=seed, impropers=impro_arr,
+        impro_coeff=np.array([[GLY_IMPROPER_K, omega0]], np.float64))
 
 
 # Named workloads (composition, seeds).  N = 10*n_gly + 3*n_wat.

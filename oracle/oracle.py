@@ -70,6 +70,8 @@ def lib(fast: bool = False) -> C.CDLL:
                                           _f32p, _f32p, _f32p, C.c_int, _i32p, _i32p, C.c_int,
                                           C.c_double, _f32p, C.POINTER(C.c_double),
                                           C.POINTER(C.c_double), _f64p, C.c_void_p, C.c_int]
+    L.orc_improper_harmonic.argtypes = [C.POINTER(OrcParams), C.c_int, _f32p, C.c_int, _i32p,
+                                        _f64p, _f32p, C.POINTER(C.c_double), _f64p]
     L.orc_force_dsf_n2.argtypes = [C.POINTER(OrcParams), C.c_int, _f32p, _f32p, _f32p, _f32p,
                                    _f32p, _f32p, C.c_int, _i32p, _i32p, _i32p, _i32p, _f64p,
                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -207,6 +209,19 @@ def force_long(p: OrcParams, pos, q, lj, ntypes, nlist, numneigh, neigh_alloc, g
                                       ff, C.byref(pot), C.byref(ec), vir,
                                       ff64.ctypes.data_as(C.c_void_p), nthreads)
     return ff.reshape(n, 3), ff64.reshape(n, 3), pot.value, ec.value, vir
+
+
+def improper_harmonic(p: OrcParams, pos, improlist, improcoeff):
+    """improper_harmonic_lammps14: ff_impro (float32, rounded per improper), e, virial3."""
+    n = pos.shape[0]
+    ff = np.zeros(n * 3, np.float32)
+    e = C.c_double(0.0)
+    vir = np.zeros(3, np.float64)
+    il = np.ascontiguousarray(improlist, np.int32)
+    lib().orc_improper_harmonic(C.byref(p), n, np.ascontiguousarray(pos, np.float32), il.shape[0],
+                                il, np.ascontiguousarray(improcoeff, np.float64), ff, C.byref(e),
+                                vir)
+    return ff.reshape(n, 3), e.value, vir
 
 
 def force_dsf_n2(p: OrcParams, pos, q, lj, ntypes, specbond, n1, n2, n3):

@@ -565,6 +565,79 @@ static inline double minimg1(double d, float box, float ibox) {
     return d - (double)s;
 }
 
+/* mod_force_dihed.f90:1546-1724 (improper_harmonic_lammps14): bond vectors from
+ * real*4 coordinate differences with the NINT minimum image, FP64 angle math,
+ * forces added to the real*4 ff_impro after every improper, energy and the
+ * diagonal virial into double accumulators.  omega0 = improcoeff(2,type). */
+void orc_improper_harmonic(const orc_params *p, int np, const orc_ainfo *pos, int nimpro,
+                           const int32_t *improlist, const double *improcoeff, float *ff_impro,
+                           double *e_improper, double *v_impro3) {
+    (void)np;
+    const float box = p->box, ibox = p->ibox;
+    const double SMALL = (double)0.001f;
+    for (int m = 0; m < nimpro; ++m) {
+        const int i1 = improlist[5 * m] - 1, i2 = improlist[5 * m + 1] - 1,
+                  i3 = improlist[5 * m + 2] - 1, i4 = improlist[5 * m + 3] - 1,
+                  t = improlist[5 * m + 4] - 1;
+        const double v1x = minimg1((double)(pos[i1].x - pos[i2].x), box, ibox);
+        const double v1y = minimg1((double)(pos[i1].y - pos[i2].y), box, ibox);
+        const double v1z = minimg1((double)(pos[i1].z - pos[i2].z), box, ibox);
+        const double v2x = minimg1((double)(pos[i3].x - pos[i2].x), box, ibox);
+        const double v2y = minimg1((double)(pos[i3].y - pos[i2].y), box, ibox);
+        const double v2z = minimg1((double)(pos[i3].z - pos[i2].z), box, ibox);
+        const double v3x = minimg1((double)(pos[i4].x - pos[i3].x), box, ibox);
+        const double v3y = minimg1((double)(pos[i4].y - pos[i3].y), box, ibox);
+        const double v3z = minimg1((double)(pos[i4].z - pos[i3].z), box, ibox);
+        const double ss1 = 1.0 / (v1x * v1x + v1y * v1y + v1z * v1z);
+        const double ss2 = 1.0 / (v2x * v2x + v2y * v2y + v2z * v2z);
+        const double ss3 = 1.0 / (v3x * v3x + v3y * v3y + v3z * v3z);
+        const double r1 = sqrt(ss1), r2 = sqrt(ss2), r3 = sqrt(ss3);
+        const double c0 = (v1x * v3x + v1y * v3y + v1z * v3z) * r1 * r3;
+        const double c1 = (v1x * v2x + v1y * v2y + v1z * v2z) * r1 * r2;
+        const double c2 = -(v3x * v2x + v3y * v2y + v3z * v2z) * r3 * r2;
+        double s1 = 1.0 - c1 * c1;
+        if (s1 < SMALL) s1 = SMALL;
+        s1 = 1.0 / s1;
+        double s2 = 1.0 - c2 * c2;
+        if (s2 < SMALL) s2 = SMALL;
+        s2 = 1.0 / s2;
+        double s12 = sqrt(s1 * s2);
+        double c = (c1 * c2 + c0) * s12;
+        if (c > 1.0) c = 1.0;
+        if (c < -1.0) c = -1.0;
+        double s = sqrt(1.0 - c * c);
+        if (s < SMALL) s = SMALL;
+        const double domega = acos(c) - improcoeff[2 * t + 1];
+        double a = improcoeff[2 * t] * domega;
+        *e_improper += a * domega;
+        a = -a * 2.0 / s;
+        c = c * a;
+        s12 = s12 * a;
+        const double a11 = c * ss1 * s1;
+        const double a22 = -ss2 * (2.0 * c0 * s12 - c * (s1 + s2));
+        const double a33 = c * ss3 * s2;
+        const double a12 = -r1 * r2 * (c1 * c * s1 + c2 * s12);
+        const double a13 = -r1 * r3 * s12;
+        const double a23 = r2 * r3 * (c2 * c * s2 + c1 * s12);
+        const double v1[3] = {v1x, v1y, v1z}, v2[3] = {v2x, v2y, v2z}, v3[3] = {v3x, v3y, v3z};
+        float *f = ff_impro;
+        for (int d = 0; d < 3; ++d) {
+            const double sx2 = a22 * v2[d] + a23 * v3[d] + a12 * v1[d];
+            const double f1 = a12 * v2[d] + a13 * v3[d] + a11 * v1[d];
+            const double f2 = -sx2 - f1;
+            const double f4 = a23 * v2[d] + a33 * v3[d] + a13 * v1[d];
+            const double f3 = sx2 - f4;
+            /* ff_impro(i)%x = f + ff_impro(i)%x : real*4 store after a double add */
+            f[3 * i1 + d] = (float)(f1 + (double)f[3 * i1 + d]);
+            f[3 * i2 + d] = (float)(f2 + (double)f[3 * i2 + d]);
+            f[3 * i3 + d] = (float)(f3 + (double)f[3 * i3 + d]);
+            f[3 * i4 + d] = (float)(f4 + (double)f[3 * i4 + d]);
+            /* v_improx = v_improx + v1x*f1 + v2x*f3 + (v3x+v2x)*f4, left to right */
+            if (v_impro3) v_impro3[d] = v_impro3[d] + v1[d] * f1 + v2[d] * f3 + (v3[d] + v2[d]) * f4;
+        }
+    }
+}
+
 /* mod_force_dihed.f90:816-1092 (dihedral_opls_DSF): OPLS torsion plus the
  * 0.5-scaled DSF Coulomb and lj14 LJ of the dihedral's 1-4 pair, into ffh. */
 void orc_dihedral_opls_dsf(const orc_params *p, int np, const orc_ainfo *pos, const float *q,

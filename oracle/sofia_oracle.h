@@ -85,6 +85,10 @@ void orc_force_long_nonewton(const orc_params *p, int np, const orc_ainfo *pos, 
                              const int32_t *numneigh, int neigh_alloc, double gewald, float *ff,
                              double *potential, double *e_coul, double *virial3,
                              double *ff64, int nthreads);
+/* improper_harmonic_lammps14 (mod_force_dihed.f90:1546-1724) */
+void orc_improper_harmonic(const orc_params *p, int np, const orc_ainfo *pos, int nimpro,
+                           const int32_t *improlist, const double *improcoeff, float *ff_impro,
+                           double *e_improper, double *v_impro3);
 void orc_force_dsf_n2(const orc_params *p, int np, const orc_ainfo *pos, const float *q,
                       const float *lj1, const float *lj2, const float *lj3, const float *lj4,
                       int ntypes, const int32_t *specbond, const int32_t *num1bond,

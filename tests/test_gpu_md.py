@@ -71,6 +71,25 @@ def test_graph_conditional_build_and_prune_equal_eager(ctx, small):
     b.close()
 
 
+def test_md_improper_term_matches_reference_entry(ctx, small):
+    """The device MD's improper energy equals sofia_improper_harmonic on the same
+    (real*4-rounded) positions, and switching the term off removes it."""
+    s = small
+    a = _system(ctx, s, dt=1.0, gamma=0.0, seed=1)
+    e = a.md_run(1, energy_every=1)
+    x, _, _ = a.get_state()
+    from molecular_simulation_code_b200.nonbond import DsfParams, improper_harmonic
+    pos = s.position_aos().copy()
+    pos[:, :3] = x.astype(np.float32)
+    p = DsfParams(alpha=0.2, box=s.box, cut_coul=8.0, rcut=8.0, neighbor_pad=2.0)
+    _, e_ref, _ = improper_harmonic(ctx, pos, s.impropers, s.impro_coeff, p)
+    assert e["improper"] == pytest.approx(e_ref, rel=1e-4, abs=1e-6)
+    b = _system(ctx, s, dt=1.0, gamma=0.0, seed=1, terms=15)
+    assert b.md_run(1, energy_every=1)["improper"] == 0.0
+    a.close()
+    b.close()
+
+
 def test_md_shake_keeps_constraints(ctx, small):
     s = small
     a = _system(ctx, s, dt=1.0, gamma=0.02, seed=3, shake_maxiter=200, shake_tol=1e-10)

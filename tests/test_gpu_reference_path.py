@@ -189,6 +189,25 @@ def test_pair14_matches_oracle(ctx):
     assert rel_err(ffh, offh) <= 1e-6
 
 
+def test_improper_matches_oracle(ctx):
+    s = small_system()
+    p = ref_params(s)
+    pos = s.position_aos().copy()
+    rng = np.random.default_rng(6)
+    pos[:100, :3] += rng.normal(0, 0.1, (100, 3)).astype(np.float32)
+    coeff = np.array([[1.1, 3.0]])
+    off, oe, ovir = O.improper_harmonic(_orc_params(p), pos, s.impropers, coeff)
+    ff, e, vir = nb.improper_harmonic(ctx, pos, s.impropers, coeff, p)
+    assert abs(e - oe) <= FP64_TOL * abs(oe)
+    assert rel_err(vir, ovir) <= 1e-9
+    # the reference rounds ff_impro to real*4 after every improper; the device once
+    assert rel_err(ff, off) <= 1e-6
+    with pytest.raises(RuntimeError):
+        bad = s.impropers.copy()
+        bad[0, 4] = 7
+        nb.improper_harmonic(ctx, pos, bad, coeff, p)
+
+
 @pytest.mark.parametrize("which", ["12", "13", "14"])
 def test_correct_1x_matches_oracle(ctx, which):
     s = small_system()

@@ -310,3 +310,33 @@ def test_product_gewald_equals_oracle():
     from molecular_simulation_code_b200.nonbond import calculate_gewald
     for c in (8.0, 9.5, 10.0, 12.0):
         assert calculate_gewald(c) == O.calculate_gewald(c)
+
+
+def test_improper_energy_gradient_and_rest_angle():
+    """improper_harmonic_lammps14 restatement: zero energy at omega0, forces equal
+    minus the finite-difference gradient of the energy, zero net force."""
+    from molecular_simulation_code_b200.system import improper_omega
+    s = small_system(4, 30, 9)
+    p = _p(s)
+    pos = s.position_aos()
+    il = s.impropers
+    om = improper_omega(pos[:, :3], float(s.box), il[:, :4] - 1)
+    coeff = np.array([[1.1, 0.0]])
+    _, e_rest, _ = O.improper_harmonic(p, pos, il[:1], np.array([[1.1, om[0]]]))
+    assert abs(e_rest) < 1e-9
+    rng = np.random.default_rng(2)
+    pos2 = pos.copy()
+    pos2[:40, :3] += rng.normal(0, 0.15, (40, 3)).astype(np.float32)
+    f, e, vir = O.improper_harmonic(p, pos2, il, coeff)
+    assert e > 0 and np.isfinite(vir).all()
+    assert np.abs(f.sum(axis=0)).max() < 1e-4
+    for i in (0, 1, 3, 4, 13):
+        for c in range(3):
+            h = 2e-3
+            ee = []
+            for sgn in (1, -1):
+                q = pos2.copy()
+                q[i, c] = np.float32(q[i, c] + sgn * h)
+                ee.append(O.improper_harmonic(p, q, il, coeff)[1])
+            hh = float(np.float32(pos2[i, c] + h)) - float(np.float32(pos2[i, c] - h))
+            assert f[i, c] == pytest.approx(-(ee[0] - ee[1]) / hh, rel=2e-2, abs=2e-3)
