@@ -106,6 +106,33 @@ int sofia_check_neighbor(sofia_nb_ctx *ctx, int np, const float *drx, const floa
                          const float *drz, double rvrc2, int32_t *nflag);
 
 /*
+ * The permutations that follow the cell sort (sofia_cell_sort returns tt and ttb):
+ *   sofia_sort_gather   -- sort_posit_charge (Source/mod_neighbor.f90:946-1005):
+ *       out[new] = in[ttb[new]-1] for rows of elem_bytes (a multiple of 4, at most
+ *       256); use it for position (16 B), v (12 B), q, mol, global_id, ...;
+ *   sofia_sort_specbond -- sort_specbond_numbond (:1011-1039), in place: row i
+ *       moves to tt[i] and its first num3bond entries are mapped through tt
+ *       (entries past num3bond come back 0; the reference leaves stale values);
+ *   sofia_remap_ids     -- sort_bondlist / anglelist / dihedlist / improlist
+ *       (:1043-1168), in place: the first ncols of each row's stride entries are
+ *       mapped through tt (0 stays 0).
+ * tt and ttb are 1-based like the reference; ids outside 1..np give SOFIA_EINVAL.
+ */
+int sofia_sort_gather(sofia_nb_ctx *ctx, int np, int elem_bytes, const int32_t *ttb,
+                      const void *in, void *out);
+int sofia_sort_specbond(sofia_nb_ctx *ctx, int np, const int32_t *tt, int32_t *specbond,
+                        int32_t *num1bond, int32_t *num2bond, int32_t *num3bond);
+int sofia_remap_ids(sofia_nb_ctx *ctx, int np, const int32_t *tt, int nrows, int stride,
+                    int ncols, int32_t *list);
+
+/*
+ * pbc (Source/mod_pbc.f90:6-39), in place: each real*4 coordinate is wrapped into
+ * (0, box] by repeated subtraction / addition of box, as the reference loops do.
+ * A coordinate that is non-finite or more than 64 boxes outside gives SOFIA_ESTATE.
+ */
+int sofia_pbc(sofia_nb_ctx *ctx, int np, sofia_ainfo *position, float box);
+
+/*
  * lj_cut_coul_dsf_nonewton_NOMIC (Source/mod_force_nonbond.f90:105-196): LJ
  * 12-6 + damped-shifted-force Coulomb over the full list, FP64 pair arithmetic
  * on the real*4 arrays.  lj1..lj4 are [ntypes*ntypes] real*4 tables indexed

@@ -87,6 +87,10 @@ SIGNATURES: dict[str, tuple] = {
                                       _F, _F, _D, _D, _D, _F, _P, C.POINTER(_D), C.POINTER(_D),
                                       _P]),
     "sofia_check_neighbor": (_I, [_P, _I, _P, _P, _P, _D, C.POINTER(C.c_int32)]),
+    "sofia_sort_gather": (_I, [_P, _I, _I, _P, _P, _P]),
+    "sofia_sort_specbond": (_I, [_P, _I, _P, _P, _P, _P, _P]),
+    "sofia_remap_ids": (_I, [_P, _I, _P, _I, _I, _I, _P]),
+    "sofia_pbc": (_I, [_P, _I, _P, _F]),
     "sofia_improper_harmonic": (_I, [_P, _I, _P, _I, _P, _P, _I, _F, _F, _P, C.POINTER(_D),
                                      _P]),
     "sofia_force_nonbond_dsf_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P,

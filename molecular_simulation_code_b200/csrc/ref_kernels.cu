@@ -1087,6 +1087,211 @@ extern "C" int sofia_improper_harmonic(sofia_nb_ctx *ctx, int np, const sofia_ai
     return SOFIA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// The permutations that follow a cell sort (sort_posit_charge,
+// sort_specbond_numbond, sort_*list; Source/mod_neighbor.f90:946-1168) and the
+// periodic wrap (pbc, Source/mod_pbc.f90:6-39).
+
+// out[new] = in[ttb[new] - 1], rows of `words` 32-bit words.
+__global__ void k_sort_gather(int np, int words, const int *__restrict__ ttb,
+                              const unsigned *__restrict__ in, unsigned *__restrict__ out,
+                              int *__restrict__ status) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)np * words) return;
+    const int i = (int)(t / words), w = (int)(t - (long)i * words);
+    const int o = ttb[i] - 1;
+    if ((unsigned)o >= (unsigned)np) {
+        atomicAdd(&status[sofia::ST_BADBIN], 1);
+        return;
+    }
+    out[t] = in[(long)o * words + w];
+}
+
+// sort_specbond_numbond: row i moves to tt(i); its first num3bond entries are
+// mapped through tt; entries past num3bond are zero.
+__global__ void k_sort_specbond(int np, const int *__restrict__ tt, const int *__restrict__ sb,
+                                const int *__restrict__ n1, const int *__restrict__ n2,
+                                const int *__restrict__ n3, int *__restrict__ sb_out,
+                                int *__restrict__ n1_out, int *__restrict__ n2_out,
+                                int *__restrict__ n3_out, int *__restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const int dst = tt[i] - 1;
+    const int k3 = n3[i];
+    if ((unsigned)dst >= (unsigned)np || k3 < 0 || k3 > 12) {
+        atomicAdd(&status[sofia::ST_BADBIN], 1);
+        return;
+    }
+    n1_out[dst] = n1[i];
+    n2_out[dst] = n2[i];
+    n3_out[dst] = k3;
+    for (int l = 0; l < 12; ++l) {
+        int v = 0;
+        if (l < k3) {
+            const int old = sb[i * 12 + l] - 1;
+            if ((unsigned)old < (unsigned)np) v = tt[old];
+            else atomicAdd(&status[sofia::ST_BADBIN], 1);
+        }
+        sb_out[dst * 12 + l] = v;
+    }
+}
+
+// sort_bondlist / sort_anglelist / ...: ids in the first ncols columns of each
+// row (1-based, 0 = unused) are mapped through tt.
+__global__ void k_remap_ids(int nrows, int stride, int ncols, int np, const int *__restrict__ tt,
+                            int *__restrict__ list, int *__restrict__ status) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nrows * ncols) return;
+    const int r = (int)(t / ncols), c = (int)(t - (long)r * ncols);
+    int *v = list + (long)r * stride + c;
+    const int id = *v;
+    if (id == 0) return;
+    if (id < 1 || id > np) {
+        atomicAdd(&status[sofia::ST_BADBIN], 1);
+        return;
+    }
+    *v = tt[id - 1];
+}
+
+// pbc: while x > box: x -= box; while x <= 0: x += box (real*4), per coordinate.
+// Each loop is bounded; a coordinate still outside after PBC_MAX_WRAPS steps
+// (a position more than that many boxes away) is flagged instead.
+constexpr int PBC_MAX_WRAPS = 64;
+__device__ __forceinline__ float pbc1(float x, float box, int *bad) {
+    int k = 0;
+    while (x > box && k < PBC_MAX_WRAPS) {
+        x = x - box;
+        ++k;
+    }
+    while (x <= 0.0f && k < PBC_MAX_WRAPS) {
+        x = x + box;
+        ++k;
+    }
+    if (!(x > 0.0f && x <= box)) *bad = 1;
+    return x;
+}
+__global__ void k_pbc(int np, float4 *__restrict__ pos, float box, int *__restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    float4 p = pos[i];
+    int bad = 0;
+    p.x = pbc1(p.x, box, &bad);
+    p.y = pbc1(p.y, box, &bad);
+    p.z = pbc1(p.z, box, &bad);
+    pos[i] = p;
+    if (bad) atomicAdd(&status[sofia::ST_NONFINITE], 1);
+}
+
+extern "C" int sofia_sort_gather(sofia_nb_ctx *ctx, int np, int elem_bytes, const int32_t *ttb,
+                                 const void *in, void *out) {
+    if (!ctx) return SOFIA_EINVAL;
+    if (np <= 0 || !ttb || !in || !out || elem_bytes <= 0 || elem_bytes % 4 || elem_bytes > 256 ||
+        in == out)
+        return sofia::fail(ctx, SOFIA_EINVAL, "bad args (elem_bytes a multiple of 4, at most 256; in != out)%s");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int rc;
+    const size_t bytes = (size_t)np * elem_bytes;
+    const void *dt, *din;
+    if ((rc = sofia::stage_in(ctx, ttb, sizeof(int) * (size_t)np, 0, &dt))) return rc;
+    if ((rc = sofia::stage_in(ctx, in, bytes, 1, &din))) return rc;
+    sofia::OutArg o;
+    if ((rc = sofia::stage_out(ctx, out, bytes, 5, &o))) return rc;
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
+    const int words = elem_bytes / 4;
+    k_sort_gather<<<sofia::grid_for((long)np * words, 256), 256, 0, st>>>(
+        np, words, (const int *)dt, (const unsigned *)din, (unsigned *)o.dev, ctx->d_status);
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    if ((rc = sofia::finish_out(ctx, o))) return rc;
+    if ((rc = check_status(ctx))) return rc;
+    if (ctx->h_status[sofia::ST_BADBIN])
+        return sofia::fail(ctx, SOFIA_EINVAL, "ttb is not a permutation of 1..np%s");
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_sort_specbond(sofia_nb_ctx *ctx, int np, const int32_t *tt, int32_t *specbond,
+                                   int32_t *num1bond, int32_t *num2bond, int32_t *num3bond) {
+    if (!ctx) return SOFIA_EINVAL;
+    if (np <= 0 || !tt || !specbond || !num1bond || !num2bond || !num3bond)
+        return sofia::fail(ctx, SOFIA_EINVAL, "bad args%s");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int rc;
+    const void *dt;
+    if ((rc = sofia::stage_in(ctx, tt, sizeof(int) * (size_t)np, 0, &dt))) return rc;
+    sofia::OutArg osb, o1, o2, o3;
+    if ((rc = sofia::stage_out(ctx, specbond, sizeof(int) * 12 * (size_t)np, 5, &osb, true))) return rc;
+    if ((rc = sofia::stage_out(ctx, num1bond, sizeof(int) * (size_t)np, 6, &o1, true))) return rc;
+    if ((rc = sofia::stage_out(ctx, num2bond, sizeof(int) * (size_t)np, 7, &o2, true))) return rc;
+    if ((rc = sofia::stage_out(ctx, num3bond, sizeof(int) * (size_t)np, 8, &o3, true))) return rc;
+    // sorted copies are built in scratch, then copied over the inputs
+    SOFIA_CUDA(ctx, ctx->acc64.ensure(sizeof(int) * 15 * (size_t)np));
+    int *scr = ctx->acc64.as<int>();
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
+    k_sort_specbond<<<sofia::grid_for(np, 256), 256, 0, st>>>(
+        np, (const int *)dt, (const int *)osb.dev, (const int *)o1.dev, (const int *)o2.dev,
+        (const int *)o3.dev, scr, scr + 12 * (size_t)np, scr + 13 * (size_t)np,
+        scr + 14 * (size_t)np, ctx->d_status);
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    if ((rc = check_status(ctx))) return rc;
+    if (ctx->h_status[sofia::ST_BADBIN])
+        return sofia::fail(ctx, SOFIA_EINVAL, "tt is not a permutation or specbond holds an id outside 1..np%s");
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(osb.dev, scr, sizeof(int) * 12 * (size_t)np, cudaMemcpyDeviceToDevice, st));
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(o1.dev, scr + 12 * (size_t)np, sizeof(int) * (size_t)np, cudaMemcpyDeviceToDevice, st));
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(o2.dev, scr + 13 * (size_t)np, sizeof(int) * (size_t)np, cudaMemcpyDeviceToDevice, st));
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(o3.dev, scr + 14 * (size_t)np, sizeof(int) * (size_t)np, cudaMemcpyDeviceToDevice, st));
+    if ((rc = sofia::finish_out(ctx, osb))) return rc;
+    if ((rc = sofia::finish_out(ctx, o1))) return rc;
+    if ((rc = sofia::finish_out(ctx, o2))) return rc;
+    if ((rc = sofia::finish_out(ctx, o3))) return rc;
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_remap_ids(sofia_nb_ctx *ctx, int np, const int32_t *tt, int nrows, int stride,
+                               int ncols, int32_t *list) {
+    if (!ctx) return SOFIA_EINVAL;
+    if (np <= 0 || !tt || nrows < 0 || (nrows > 0 && !list) || stride <= 0 || ncols < 0 ||
+        ncols > stride)
+        return sofia::fail(ctx, SOFIA_EINVAL, "bad args%s");
+    if (nrows == 0 || ncols == 0) return SOFIA_OK;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int rc;
+    const void *dt;
+    if ((rc = sofia::stage_in(ctx, tt, sizeof(int) * (size_t)np, 0, &dt))) return rc;
+    sofia::OutArg o;
+    if ((rc = sofia::stage_out(ctx, list, sizeof(int) * (size_t)nrows * stride, 5, &o, true)))
+        return rc;
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
+    k_remap_ids<<<sofia::grid_for((long)nrows * ncols, 256), 256, 0, st>>>(
+        nrows, stride, ncols, np, (const int *)dt, (int *)o.dev, ctx->d_status);
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    if ((rc = sofia::finish_out(ctx, o))) return rc;
+    if ((rc = check_status(ctx))) return rc;
+    if (ctx->h_status[sofia::ST_BADBIN])
+        return sofia::fail(ctx, SOFIA_EINVAL, "list holds an id outside 1..np%s");
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_pbc(sofia_nb_ctx *ctx, int np, sofia_ainfo *position, float box) {
+    if (!ctx) return SOFIA_EINVAL;
+    if (np <= 0 || !position || !(box > 0.0f)) return sofia::fail(ctx, SOFIA_EINVAL, "bad args%s");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int rc;
+    sofia::OutArg o;
+    if ((rc = sofia::stage_out(ctx, position, sizeof(float4) * (size_t)np, 5, &o, true))) return rc;
+    SOFIA_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS, st));
+    k_pbc<<<sofia::grid_for(np, 256), 256, 0, st>>>(np, (float4 *)o.dev, box, ctx->d_status);
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    if ((rc = sofia::finish_out(ctx, o))) return rc;
+    if ((rc = check_status(ctx))) return rc;
+    if (ctx->h_status[sofia::ST_NONFINITE])
+        return sofia::fail(ctx, SOFIA_ESTATE, "a coordinate is non-finite or more than 64 boxes outside%s");
+    return SOFIA_OK;
+}
+
 extern "C" int sofia_correct_1x(sofia_nb_ctx *ctx, int np, const sofia_ainfo *position,
                                 const float *q, int npairs, const int32_t *list, int stride,
                                 int col_a, int col_b, float box, float ibox, double cut_coulsq,

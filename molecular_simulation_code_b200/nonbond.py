@@ -167,6 +167,45 @@ def neighbor_wrapper(ctx: Context, position, specbond, num3bond, p: DsfParams,
         return nlist, numneigh, neigh_alloc
 
 
+def sort_posit(ctx: Context, ttb, arr):
+    """sort_posit_charge (Source/mod_neighbor.f90:946-1005) for one per-atom array:
+    returns arr[ttb - 1] (rows of any 4-byte-multiple size)."""
+    a = np.ascontiguousarray(arr)
+    out = np.empty_like(a)
+    n = a.shape[0]
+    ctx.check(ctx._lib.sofia_sort_gather(ctx.handle, n, a.nbytes // n, ptr(np.ascontiguousarray(
+        ttb, np.int32)), ptr(a), ptr(out)))
+    return out
+
+
+def sort_specbond_numbond(ctx: Context, tt, specbond, num1bond, num2bond, num3bond):
+    """sort_specbond_numbond (Source/mod_neighbor.f90:1011-1039): sorted copies."""
+    sb = np.array(specbond, np.int32, order="C")
+    n1 = np.array(num1bond, np.int32)
+    n2 = np.array(num2bond, np.int32)
+    n3 = np.array(num3bond, np.int32)
+    ctx.check(ctx._lib.sofia_sort_specbond(ctx.handle, sb.shape[0], ptr(np.ascontiguousarray(
+        tt, np.int32)), ptr(sb), ptr(n1), ptr(n2), ptr(n3)))
+    return sb, n1, n2, n3
+
+
+def sort_list(ctx: Context, tt, lst, ncols: int):
+    """sort_bondlist / sort_anglelist / ... (Source/mod_neighbor.f90:1043-1168): the
+    first ncols columns of each row mapped through tt (a sorted copy)."""
+    a = np.array(lst, np.int32, order="C")
+    n = int(np.asarray(tt).shape[0])
+    ctx.check(ctx._lib.sofia_remap_ids(ctx.handle, n, ptr(np.ascontiguousarray(tt, np.int32)),
+                                       a.shape[0], a.shape[1], int(ncols), ptr(a)))
+    return a
+
+
+def pbc(ctx: Context, position, box):
+    """pbc (Source/mod_pbc.f90:6-39): a wrapped copy of the (np,4) ainfo records."""
+    p = np.array(position, np.float32, order="C")
+    ctx.check(ctx._lib.sofia_pbc(ctx.handle, p.shape[0], ptr(p), np.float32(box)))
+    return p
+
+
 def check_neighbor(ctx: Context, drx, dry, drz, rvrc2: float) -> int:
     """check_neighbor (Source/mod_neighbor.f90:895-913): 1 if a rebuild is due."""
     flag = C.c_int32()

@@ -189,6 +189,54 @@ def test_pair14_matches_oracle(ctx):
     assert rel_err(ffh, offh) <= 1e-6
 
 
+def test_sort_permutations_match_reference(ctx):
+    """sort_posit_charge / sort_specbond_numbond / sort_*list on the device equal
+    their numpy restatements, with tt/ttb from the oracle's cell sort."""
+    s = small_system()
+    p = ref_params(s)
+    pos = s.position_aos()
+    tt, ttb, *_ = O.bin_sort(_orc_params(p), pos)
+    ps = nb.sort_posit(ctx, ttb, pos)
+    assert np.array_equal(ps.view(np.int32), pos[ttb - 1].view(np.int32))
+    v = s.velocity.astype(np.float32)
+    assert np.array_equal(nb.sort_posit(ctx, ttb, v), v[ttb - 1])
+    assert np.array_equal(nb.sort_posit(ctx, ttb, s.q), s.q[ttb - 1])
+    sb, n1, n2, n3 = nb.sort_specbond_numbond(ctx, tt, s.specbond, s.num1bond, s.num2bond,
+                                              s.num3bond)
+    want = np.zeros_like(s.specbond)
+    for i in range(s.np_atoms):
+        k = s.num3bond[i]
+        want[tt[i] - 1, :k] = tt[s.specbond[i, :k] - 1]
+    assert np.array_equal(sb, want)
+    assert np.array_equal(n3, s.num3bond[ttb - 1]) and np.array_equal(n1, s.num1bond[ttb - 1])
+    assert np.array_equal(n2, s.num2bond[ttb - 1])
+    bl = nb.sort_list(ctx, tt, s.bonds, 2)
+    assert np.array_equal(bl[:, :2], tt[s.bonds[:, :2] - 1]) and np.array_equal(bl[:, 2], s.bonds[:, 2])
+    dl = nb.sort_list(ctx, tt, s.dihedrals, 4)
+    assert np.array_equal(dl[:, :4], tt[s.dihedrals[:, :4] - 1])
+    bad = s.bonds.copy()
+    bad[3, 0] = s.np_atoms + 5
+    with pytest.raises(RuntimeError):
+        nb.sort_list(ctx, tt, bad, 2)
+
+
+def test_pbc_matches_reference_loops(ctx):
+    from molecular_simulation_code_b200.system import wrap_positions
+    s = small_system()
+    rng = np.random.default_rng(8)
+    pos = s.position_aos().copy()
+    L = float(s.box)
+    pos[:, :3] += rng.integers(-3, 4, size=(s.np_atoms, 3)).astype(np.float32) * np.float32(L)
+    pos[:5, 0] = [0.0, -0.0, L, -L, 2 * L]
+    out = nb.pbc(ctx, pos, s.box)
+    assert np.array_equal(out[:, :3], wrap_positions(pos[:, :3], s.box))
+    assert np.array_equal(out[:, 3].view(np.int32), pos[:, 3].view(np.int32))
+    far = pos.copy()
+    far[7, 1] = np.float32(1000 * L)
+    with pytest.raises(RuntimeError):
+        nb.pbc(ctx, far, s.box)
+
+
 def test_improper_matches_oracle(ctx):
     s = small_system()
     p = ref_params(s)
