@@ -1069,6 +1069,7 @@ extern "C" int sofia_system_set_margin(sofia_system *ss, double margin) {
     s->margin = margin;
     s->built = 0;
     sofia::md_drop_graphs(s);
+    sofia::dropin_drop(s);
     return SOFIA_OK;
 }
 

@@ -966,7 +966,16 @@ static int sys_alloc(Sys *s) {
     return SOFIA_OK;
 }
 
+void dropin_drop(Sys *s) {
+    for (auto &g : s->dropin)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
 static int sys_alloc_list(Sys *s) {
+    dropin_drop(s);  // captured drop-in graphs hold the old list pointers
     const size_t maxcl = (size_t)s->max_clusters;
     SOFIA_CUDA(s->ctx, s->jlist.ensure(sizeof(int) * maxcl * s->jcap));
     SOFIA_CUDA(s->ctx, s->jmask.ensure(sizeof(unsigned long long) * maxcl * s->jcap));
@@ -1305,6 +1314,42 @@ int sys_list_overflow(Sys *s) {
     return SOFIA_OK;
 }
 
+// The drop-in force call as one CUDA graph: AoS positions -> FP64 SoA,
+// displacement triggers, conditional rebuild and prune, pair kernel, forces ->
+// real*4 AoS.  It reads stage_pos and writes stage_ff; variant e: 0 forces,
+// 1 + energies, 2 + energies and virial.
+static int dropin_capture(Sys *s, int e) {
+    sofia_nb_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = s->n;
+    const int timing = s->timing;
+    s->timing = 0;
+    const long long l0 = s->launches;
+    cudaGraph_t g = nullptr;
+    SOFIA_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    k_aos_to_soa<<<grid_for(n, 256), 256, 0, st>>>(n, s->stage_pos.as<float4>(),
+                                                   s->x[0].as<double>(), s->x[1].as<double>(),
+                                                   s->x[2].as<double>());
+    const int rc = sys_step_forces(s, s->precision, e >= 1, e == 2, false);
+    k_fix_to_float<<<grid_for(n, 256), 256, 0, st>>>(n, s->f[0].as<long long>(),
+                                                     s->f[1].as<long long>(),
+                                                     s->f[2].as<long long>(),
+                                                     s->stage_ff.as<float>());
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    s->dropin_launches[e] = s->launches - l0 + 2;
+    s->launches = l0;
+    s->timing = timing;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture (drop-in)");
+    const cudaError_t ie = cudaGraphInstantiate(&s->dropin[e], g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return cuda_fail(ctx, ie, "cudaGraphInstantiate (drop-in)");
+    return SOFIA_OK;
+}
+
 }  // namespace sofia
 
 using sofia::Sys;
@@ -1417,6 +1462,7 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
     if (!ss) return SOFIA_OK;
     Sys *s = &ss->s;
     if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+    sofia::dropin_drop(s);
     for (auto &e : s->ev)
         if (e) cudaEventDestroy(e);
     for (int d = 0; d < 3; ++d) s->xprn[d].release();
@@ -1456,33 +1502,48 @@ extern "C" int sofia_force_nonbond_mixed(sofia_system *ss, const sofia_ainfo *po
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const int n = s->n;
-    const void *dpos = position;
-    if (!sofia::is_device_ptr(position)) {
-        SOFIA_CUDA(ctx, s->stage_pos.ensure(sizeof(float4) * (size_t)n));
-        SOFIA_CUDA(ctx, cudaMemcpyAsync(s->stage_pos.p, position, sizeof(float4) * (size_t)n,
-                                        cudaMemcpyHostToDevice, st));
-        dpos = s->stage_pos.p;
-    }
-    sofia::k_aos_to_soa<<<sofia::grid_for(n, 256), 256, 0, st>>>(
-        n, (const float4 *)dpos, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>());
+    const size_t pbytes = sizeof(float4) * (size_t)n, fbytes = sizeof(float) * 3 * (size_t)n;
+    SOFIA_CUDA(ctx, s->stage_pos.ensure(pbytes));
+    SOFIA_CUDA(ctx, s->stage_ff.ensure(fbytes));
+    // positions (host or device) into the fixed staging buffer the graph reads
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(s->stage_pos.p, position, pbytes, cudaMemcpyDefault, st));
     const bool want_e = potential || e_coul || virial_diag3;
-    int rc = sofia::sys_eval(s, s->precision, want_e, virial_diag3 != nullptr, false);
-    if (rc) return rc;
-    float *dff = ff;
-    const bool host_ff = !sofia::is_device_ptr(ff);
-    if (host_ff) {
-        SOFIA_CUDA(ctx, s->stage_ff.ensure(sizeof(float) * 3 * (size_t)n));
-        dff = s->stage_ff.as<float>();
+    const bool vir = virial_diag3 != nullptr;
+    const bool graph = s->built && !s->timing;
+    if (graph) {
+        // steady state: the whole device step is one graph launch, rebuilds and
+        // prunes decided on the device
+        const int e = vir ? 2 : (want_e ? 1 : 0);
+        if (!s->dropin[e]) {
+            const int rc = sofia::dropin_capture(s, e);
+            if (rc) return rc;
+        }
+        SOFIA_CUDA(ctx, cudaGraphLaunch(s->dropin[e], st));
+        s->launches += s->dropin_launches[e];
+    } else {
+        // first call after creation or set_state (or with timers on): host-driven
+        sofia::k_aos_to_soa<<<sofia::grid_for(n, 256), 256, 0, st>>>(
+            n, s->stage_pos.as<float4>(), s->x[0].as<double>(), s->x[1].as<double>(),
+            s->x[2].as<double>());
+        const int rc = sofia::sys_eval(s, s->precision, want_e, vir, false);
+        if (rc) return rc;
+        sofia::k_fix_to_float<<<sofia::grid_for(n, 256), 256, 0, st>>>(
+            n, s->f[0].as<long long>(), s->f[1].as<long long>(), s->f[2].as<long long>(),
+            s->stage_ff.as<float>());
+        s->launches += 2;
     }
-    sofia::k_fix_to_float<<<sofia::grid_for(n, 256), 256, 0, st>>>(
-        n, s->f[0].as<long long>(), s->f[1].as<long long>(), s->f[2].as<long long>(), dff);
-    if (host_ff)
-        SOFIA_CUDA(ctx, cudaMemcpyAsync(ff, dff, sizeof(float) * 3 * (size_t)n,
-                                        cudaMemcpyDeviceToHost, st));
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(ff, s->stage_ff.p, fbytes, cudaMemcpyDefault, st));
     double e[5] = {0, 0, 0, 0, 0};
     if (want_e)
         SOFIA_CUDA(ctx, cudaMemcpyAsync(e, s->red.p, sizeof(e), cudaMemcpyDeviceToHost, st));
     SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    if (graph) {
+        // a list row that overflowed during a device-side rebuild: grow and redo
+        const int rc = sofia::sys_list_overflow(s);
+        if (rc == SOFIA_ENEEDGROW)
+            return sofia_force_nonbond_mixed(ss, position, ff, potential, e_coul, virial_diag3);
+        if (rc) return rc;
+    }
     if (potential) *potential = e[0];
     if (e_coul) *e_coul = e[1];
     if (virial_diag3) {

@@ -91,6 +91,8 @@ struct Sys {
     long long shake_nc = 0;             // SHAKE groups that reached maxiter (warnings)
     // optional CUDA-event timing of the list build and the pair kernel
     int timing = 0;
+    cudaGraphExec_t dropin[3] = {nullptr, nullptr, nullptr};  // drop-in force call: forces / +energy / +virial
+    long long dropin_launches[3] = {0, 0, 0};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     double t_build_ms = 0.0, t_pair_ms = 0.0;
     long long n_pair = 0, n_build_timed = 0;
@@ -103,6 +105,8 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build);
 int sys_pair(Sys *s, int precision, bool energy, bool virial);
 int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build);
 int sys_list_overflow(Sys *s);
+// Frees the captured drop-in force graphs (they bake in list pointers and the margin).
+void dropin_drop(Sys *s);
 
 }  // namespace sofia
 

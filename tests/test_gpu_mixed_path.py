@@ -112,6 +112,28 @@ def test_dropin_host_buffers_equal_resident(ctx):
     sysm.close()
 
 
+def test_dropin_graph_equals_host_driven_sequence(ctx):
+    """After the first call the drop-in runs as one captured graph (rebuild and
+    prune decided on the device); with timers on it stays host-driven.  Over a
+    drifting trajectory with rebuilds both give identical forces and energies."""
+    s = small_system(20, 1200, 4)
+    a = M.System(ctx, s, cut=8.0, skin=2.0)
+    b = M.System(ctx, s, cut=8.0, skin=2.0)
+    b.timers(True)
+    pos = s.position_aos().copy()
+    v = s.velocity.astype(np.float32) * np.float32(40.0)  # ~0.5 A per call for fast atoms
+    for k in range(25):
+        fa, pa, ea, _ = a.forces_dropin(pos)
+        fb, pb, eb, _ = b.forces_dropin(pos)
+        assert np.array_equal(fa, fb) and pa == pb and ea == eb, k
+        pos[:, :3] += v
+    sa, sb = a.stats(), b.stats()
+    assert sa["builds"] == sb["builds"] and sa["builds"] >= 3
+    assert sa["prunes"] == sb["prunes"]
+    a.close()
+    b.close()
+
+
 def test_rebuild_trigger_and_wrapped_positions(ctx):
     s = small_system(20, 1200, 4)
     sysm = M.System(ctx, s, cut=8.0, skin=2.0)
