@@ -33,7 +33,13 @@ constexpr int MAX_COL = 2048;
 // launched (or captured into a CUDA graph) without a host round trip.
 #define SOFIA_COND_RETURN \
     if (cond && !(cond[0] & cmask)) return  // atoms per xy column handled by the in-column sort
-constexpr int FLUSH = 4;       // j-clusters between FP32 -> fixed-point flushes
+#ifndef SOFIA_PAIR_FLUSH
+#define SOFIA_PAIR_FLUSH 4
+#endif
+#ifndef SOFIA_PAIR_MINB
+#define SOFIA_PAIR_MINB 4
+#endif
+constexpr int FLUSH = SOFIA_PAIR_FLUSH;  // j-clusters between FP32 -> fixed-point flushes
 
 __device__ __forceinline__ double wrap_shift(double x, double L) {
     // shift s with x + s in [0, L)
@@ -567,7 +573,7 @@ __device__ __forceinline__ T reduce_scatter_j(const T (&v)[6], int lane) {
 //     order of the atomics, so results stay bit-reproducible.
 // EN adds the LJ and Coulomb energies, VIR the diagonal virial (each pair once).
 template <typename T, bool EN, bool VIR, bool SAME>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? 4 : 2) k_pair(
+__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? SOFIA_PAIR_MINB : 2) k_pair(
     int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
     const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
