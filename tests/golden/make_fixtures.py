@@ -1,14 +1,17 @@
 """Generates the reference-input fixture used by the parity tests.
 
-Reads the reference's own input files (the minimized glycine_1500 snapshot,
+Reads the reference's own input files (the minimized glycine_1500 and
+glycine_2500 snapshots,
 its topology, molecule templates and run input) from the reference checkout,
 parses them with ``molecular_simulation_code_b200.snapio`` and writes the
-parsed numbers to ``glycine_1500_solv_min.npz`` beside this script:
+parsed numbers to ``glycine_1500_solv_min.npz`` and ``glycine_2500_solv_min.npz``
+beside this script:
 
 * ``xyz_mnm`` int16 (N,3): the .gro coordinates in units of 0.001 nm (the
   file's 8.3 fields, exactly);
 * ``box_nm_1e5``: the box line's f10.5 value times 1e5;
-* ``mol_*``: molecule counts, atoms per molecule, template atom types;
+* ``mol_*``: molecule counts (from the snapshot's residues), atoms per molecule,
+  template atom types;
 * ``top_*``: topology tables as parsed by ``snapio.parse_topol``;
 * ``run_*``: cutoffs, padding, cluster radii, DSF alpha, time step and the
   1-2/1-3/1-4 factors of the run input.
@@ -44,9 +47,8 @@ def _run_input(text: str) -> dict:
             "fudge": np.array([float(v) for v in after("!---12 13 14")[:4]])}
 
 
-def main(ref_root: str):
-    d = os.path.join(ref_root, "input_files")
-    gro = open(os.path.join(d, "glycine_1500_solv_min.gro")).read()
+def fixture(d: str, gro_name: str):
+    gro = open(os.path.join(d, gro_name)).read()
     lines = gro.splitlines()
     n = int(lines[1].split()[0])
     mnm = np.empty((n, 3), np.int32)
@@ -57,15 +59,28 @@ def main(ref_root: str):
     assert np.abs(mnm).max() < 32768
     box_1e5 = int(round(float(lines[2 + n][:10]) * 1e5))
     mol = snapio.parse_mol(open(os.path.join(d, "mol_cndo_alpha.input")).read())
+    # molecule counts of this snapshot from its residues (the molecule template file
+    # holds the counts of the 1500-glycine system): 10-atom glycine, 3-atom water
+    resnames = [lines[2 + i][5:10].strip() for i in range(n)]
+    n_gly = sum(1 for r in resnames if r != "SOL") // 10
+    n_wat = sum(1 for r in resnames if r == "SOL") // 3
+    assert 10 * n_gly + 3 * n_wat == n
+    mol["counts"] = np.array([n_gly, n_wat], np.int32)
     top = snapio.parse_topol(open(os.path.join(d, "topol_cndo.top")).read(), len(mol["counts"]))
     run = _run_input(open(os.path.join(d, "input")).read())
     out = {"xyz_mnm": mnm.astype(np.int16), "box_nm_1e5": np.int64(box_1e5)}
     out.update({"mol_" + k: v for k, v in mol.items()})
     out.update({"top_" + k: np.asarray(v) for k, v in top.items()})
     out.update({"run_" + k: np.asarray(v) for k, v in run.items()})
-    path = os.path.join(HERE, "glycine_1500_solv_min.npz")
+    path = os.path.join(HERE, gro_name.replace(".gro", ".npz"))
     np.savez_compressed(path, **out)
-    print(path, os.path.getsize(path), "bytes;", n, "atoms")
+    print(path, os.path.getsize(path), "bytes;", n, "atoms;", n_gly, "glycine,", n_wat, "water")
+
+
+def main(ref_root: str):
+    d = os.path.join(ref_root, "input_files")
+    for name in ("glycine_1500_solv_min.gro", "glycine_2500_solv_min.gro"):
+        fixture(d, name)
 
 
 if __name__ == "__main__":

@@ -1,5 +1,6 @@
-"""GPU parity on the reference's own input: the minimized glycine_1500 snapshot
-(45,255 atoms, AMBER Rmin/2 force field) with the run input's cut-offs
+"""GPU parity on the reference's own input: the minimized glycine_1500 and
+glycine_2500 snapshots (45,255 and 74,524 atoms, AMBER Rmin/2 force field) with
+the run input's cut-offs
 (rcut = cut_coul = 12 A, padding 1.5 A, alpha 0.22 1/A, cluster radii 9 / 6 A,
 densmin 11), loaded from the committed fixture and wrapped into (0, box] as pbc
 does.
@@ -22,13 +23,13 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-FIX = os.path.join(os.path.dirname(__file__), "golden", "glycine_1500_solv_min.npz")
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 FP64_TOL = 1e-10
 
 
-@pytest.fixture(scope="module")
-def ref():
-    s, run = S.load_fixture(FIX)
+@pytest.fixture(scope="module", params=["glycine_1500_solv_min", "glycine_2500_solv_min"])
+def ref(request):
+    s, run = S.load_fixture(os.path.join(GOLDEN, request.param + ".npz"))
     s.xyz = wrap_positions(s.xyz, s.box)
     p = nb.DsfParams(alpha=float(run["alpha"]), box=s.box, cut_coul=float(run["cut_coul"]),
                      rcut=float(run["rcut"]), neighbor_pad=float(run["pad"]))

@@ -55,6 +55,14 @@ def test_exclusions_symmetric_and_cover_bonds(ref):
     assert all((k + 1, int(first[k])) in bonded for k in range(0, n, 97))
 
 
+def test_second_fixture_counts_from_residues():
+    s, run = S.load_fixture(os.path.join(os.path.dirname(FIX), "glycine_2500_solv_min.npz"))
+    assert s.np_atoms == 74524 and s.n_gly == 2500 and s.n_wat == 16508
+    assert s.box == np.float32(np.float64(np.float32(9.201)) * 10.0)
+    assert s.impropers.shape == (2500, 5) and s.shake.shape[0] == 2500 * 2 + 16508
+    assert run["rcut"] == 12.0
+
+
 def test_shake_groups(ref):
     s, _ = ref
     kinds, counts = np.unique(s.shake[:, 0], return_counts=True)
