@@ -66,16 +66,43 @@ __global__ void k_kick(int n, double h, const double *__restrict__ invm,
     vz[i] += c * unfix(fz[i]);
 }
 
-// nve_x: x += dt * v
-__global__ void k_stream(int n, double dt, double *__restrict__ x, double *__restrict__ y,
-                         double *__restrict__ z, const double *__restrict__ vx,
-                         const double *__restrict__ vy, const double *__restrict__ vz) {
+// First half-kick and drift of a step fused with the step counter and the
+// list triggers: v += h f / m (nve_v), x += dt v (nve_x), then bit 0 of the
+// trigger word if an atom moved more than skin/2 since the list build, bit 1
+// if more than margin/2 since the last prune (the word was cleared after the
+// previous step's list decisions).
+__global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
+                             const long long *__restrict__ fx, const long long *__restrict__ fy,
+                             const long long *__restrict__ fz, double *__restrict__ vx,
+                             double *__restrict__ vy, double *__restrict__ vz, double dt,
+                             double *__restrict__ x, double *__restrict__ y,
+                             double *__restrict__ z, const double *__restrict__ rx,
+                             const double *__restrict__ ry, const double *__restrict__ rz,
+                             const double *__restrict__ px, const double *__restrict__ py,
+                             const double *__restrict__ pz, double L, double lim2, double plim2,
+                             int *__restrict__ flag, long long *__restrict__ step) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    x[i] += dt * vx[i];
-    y[i] += dt * vy[i];
-    z[i] += dt * vz[i];
+    if (i == 0) step[0] += 1;
+    bool far = false, pfar = false;
+    if (i < n) {
+        const double c = h * invm[i];
+        const double ux = vx[i] + c * unfix(fx[i]);
+        const double uy = vy[i] + c * unfix(fy[i]);
+        const double uz = vz[i] + c * unfix(fz[i]);
+        vx[i] = ux;
+        vy[i] = uy;
+        vz[i] = uz;
+        const double xn = x[i] + dt * ux, yn = y[i] + dt * uy, zn = z[i] + dt * uz;
+        x[i] = xn;
+        y[i] = yn;
+        z[i] = zn;
+        far = disp2(xn, yn, zn, rx[i], ry[i], rz[i], L) > lim2;
+        pfar = disp2(xn, yn, zn, px[i], py[i], pz[i], L) > plim2;
+    }
+    const bool a = __any_sync(0xffffffffu, far), b = __any_sync(0xffffffffu, pfar);
+    if ((threadIdx.x & 31) == 0 && (a || b)) atomicOr(flag, (a ? 1 : 0) | (b ? 2 : 0));
 }
+
 
 // Force-form Langevin: f += -gamma m v / kcal2amu + sqrt(12 * 2 m gamma kT kcal2amu / dt) U / kcal2amu
 __global__ void k_langevin(int n, double gamma, double gsig, unsigned long long seed,
@@ -97,12 +124,11 @@ __global__ void k_langevin(int n, double gamma, double gsig, unsigned long long 
 }
 
 template <bool EN>
-__global__ void k_bond(int nb, const int *__restrict__ bl, const double *__restrict__ bc,
+__device__ __forceinline__ void bond_term(int m, int nb, const int *__restrict__ bl, const double *__restrict__ bc,
                        const double *__restrict__ x, const double *__restrict__ y,
                        const double *__restrict__ z, double L, long long *__restrict__ fx,
                        long long *__restrict__ fy, long long *__restrict__ fz,
                        double *__restrict__ e) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= nb) return;
     const int i1 = bl[3 * m] - 1, i2 = bl[3 * m + 1] - 1, t = bl[3 * m + 2] - 1;
     const double dx = mimg(x[i1] - x[i2], L), dy = mimg(y[i1] - y[i2], L), dz = mimg(z[i1] - z[i2], L);
@@ -120,12 +146,11 @@ __global__ void k_bond(int nb, const int *__restrict__ bl, const double *__restr
 }
 
 template <bool EN>
-__global__ void k_angle(int na, const int *__restrict__ al, const double *__restrict__ ac,
+__device__ __forceinline__ void angle_term(int m, int na, const int *__restrict__ al, const double *__restrict__ ac,
                         const double *__restrict__ x, const double *__restrict__ y,
                         const double *__restrict__ z, double L, long long *__restrict__ fx,
                         long long *__restrict__ fy, long long *__restrict__ fz,
                         double *__restrict__ e) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= na) return;
     const int i1 = al[4 * m] - 1, i2 = al[4 * m + 1] - 1, i3 = al[4 * m + 2] - 1,
               t = al[4 * m + 3] - 1;
@@ -161,12 +186,11 @@ __global__ void k_angle(int na, const int *__restrict__ al, const double *__rest
 
 // improper_harmonic_lammps14 (mod_force_dihed.f90:1546-1724) on the FP64 state.
 template <bool EN>
-__global__ void k_improper(int ni, const int *__restrict__ il, const double *__restrict__ ic,
+__device__ __forceinline__ void improper_term(int m, int ni, const int *__restrict__ il, const double *__restrict__ ic,
                            const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ z, double L, long long *__restrict__ fx,
                            long long *__restrict__ fy, long long *__restrict__ fz,
                            double *__restrict__ e) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= ni) return;
     const int i1 = il[5 * m] - 1, i2 = il[5 * m + 1] - 1, i3 = il[5 * m + 2] - 1,
               i4 = il[5 * m + 3] - 1, t = il[5 * m + 4] - 1;
@@ -199,8 +223,7 @@ struct DihArgs {
 
 // dihedral_opls_DSF (mod_force_dihed.f90:849-1068) on the FP64 state.
 template <bool EN>
-__global__ void k_dihedral(DihArgs a) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void dihedral_term(int n, const DihArgs &a) {
     if (n >= a.nd) return;
     const int i1 = a.dl[5 * n] - 1, i2 = a.dl[5 * n + 1] - 1, i3 = a.dl[5 * n + 2] - 1,
               i4 = a.dl[5 * n + 3] - 1, type = a.dl[5 * n + 4] - 1;
@@ -455,9 +478,6 @@ __global__ void k_ke(int n, const double *__restrict__ mass, const double *__res
     ke[i] = 0.5 * mass[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]) / KCAL2AMU;
 }
 
-__global__ void k_step_inc(long long *__restrict__ step) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) step[0] += 1;
-}
 
 // Two-stage deterministic sum of column c of in[n][w] into out[slot].
 constexpr int MRED = 64;
@@ -498,70 +518,98 @@ static void md_reduce(cudaStream_t st, int n, int w, int c, const double *in, do
 
 // energies slots in md.ered: 0 lj, 1 coul, (2..4 pair virial), 5 bond, 6 angle,
 // 7 torsion, 8 coul14, 9 lj14, 10 kinetic; partials after slot 16.
-static int md_forces(Sys *s, bool energy, bool force_build) {
+// All bonded terms of a step in one launch: threads [0, nb) take bonds, the
+// next na angles, then nd dihedrals (torsion and 1-4 pair), then ni impropers.
+// A count of 0 switches a term off.
+struct BondedArgs {
+    int nb, na, nd, ni;
+    const int *bl, *al, *il;
+    const double *bc, *ac, *ic;
+    double *eb, *ea, *ei;
+    DihArgs dih;
+};
+template <bool EN>
+__global__ void __launch_bounds__(128) k_bonded(BondedArgs b) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const DihArgs &d = b.dih;
+    if (t < b.nb) {
+        bond_term<EN>(t, b.nb, b.bl, b.bc, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.eb);
+        return;
+    }
+    t -= b.nb;
+    if (t < b.na) {
+        angle_term<EN>(t, b.na, b.al, b.ac, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.ea);
+        return;
+    }
+    t -= b.na;
+    if (t < b.nd) {
+        dihedral_term<EN>(t, d);
+        return;
+    }
+    t -= b.nd;
+    if (t < b.ni) improper_term<EN>(t, b.ni, b.il, b.ic, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.ei);
+}
+
+static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = false) {
     Md &md = s->md;
     cudaStream_t st = s->ctx->stream;
-    int rc = sys_step_forces(s, s->precision, energy, false, force_build);
+    int rc = sys_step_forces(s, s->precision, energy, false, force_build, disp_done);
     if (rc) return rc;
     long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
               *fz = s->f[2].as<long long>();
     const double *x = s->x[0].as<double>(), *y = s->x[1].as<double>(), *z = s->x[2].as<double>();
     double *et = md.eterm.as<double>();
     const int nb = md.nbond, na = md.nangle, nd = md.ndihed;
-    if ((md.terms & 1) && nb) {
+    BondedArgs b;
+    b.nb = (md.terms & 1) ? nb : 0;
+    b.na = (md.terms & 2) ? na : 0;
+    b.nd = (md.terms & 12) ? nd : 0;
+    b.ni = (md.terms & 16) ? md.nimpro : 0;
+    b.bl = md.bonds.as<int>();
+    b.bc = md.bcoef.as<double>();
+    b.al = md.angles.as<int>();
+    b.ac = md.acoef.as<double>();
+    b.il = md.impros.as<int>();
+    b.ic = md.icoef.as<double>();
+    b.eb = et;
+    b.ea = et + nb;
+    b.ei = et + nb + na + 3 * (size_t)nd;
+    DihArgs &a = b.dih;
+    a.nd = b.nd;
+    a.ntypes = s->ntypes;
+    a.terms = md.terms;
+    a.dl = md.diheds.as<int>();
+    a.dc = md.dcoef.as<double>();
+    a.lj14 = md.lj14.as<double>();
+    a.x = x;
+    a.y = y;
+    a.z = z;
+    a.type = s->type.as<int>();
+    a.q = s->q.as<float>();
+    a.L = s->L;
+    a.alpha = s->alpha;
+    a.EWALD_P = (double)0.3275911f;
+    a.A1 = (double)0.254829592f;
+    a.A2 = (double)-0.284496736f;
+    a.A3 = (double)1.421413741f;
+    a.A4 = (double)-1.453152027f;
+    a.A5 = (double)1.061405429f;
+    a.MY_PIS = (double)1.77245385090551602729f;
+    a.e_shift = s->e_shift;
+    a.f_shift = s->f_shift;
+    a.cut_coulsq = (double)(float)(s->rc * s->rc);
+    a.rcut2 = a.cut_coulsq;
+    a.coulpre = s->coulpre;
+    a.fx = fx;
+    a.fy = fy;
+    a.fz = fz;
+    a.e = et + nb + na;
+    const long nterm = (long)b.nb + b.na + b.nd + b.ni;
+    if (nterm > 0) {
         if (energy)
-            k_bond<true><<<grid_for(nb, 128), 128, 0, st>>>(nb, md.bonds.as<int>(), md.bcoef.as<double>(), x, y, z, s->L, fx, fy, fz, et);
+            k_bonded<true><<<grid_for(nterm, 128), 128, 0, st>>>(b);
         else
-            k_bond<false><<<grid_for(nb, 128), 128, 0, st>>>(nb, md.bonds.as<int>(), md.bcoef.as<double>(), x, y, z, s->L, fx, fy, fz, et);
-    }
-    if ((md.terms & 2) && na) {
-        if (energy)
-            k_angle<true><<<grid_for(na, 128), 128, 0, st>>>(na, md.angles.as<int>(), md.acoef.as<double>(), x, y, z, s->L, fx, fy, fz, et + nb);
-        else
-            k_angle<false><<<grid_for(na, 128), 128, 0, st>>>(na, md.angles.as<int>(), md.acoef.as<double>(), x, y, z, s->L, fx, fy, fz, et + nb);
-    }
-    if ((md.terms & 12) && nd) {
-        DihArgs a;
-        a.nd = nd;
-        a.ntypes = s->ntypes;
-        a.terms = md.terms;
-        a.dl = md.diheds.as<int>();
-        a.dc = md.dcoef.as<double>();
-        a.lj14 = md.lj14.as<double>();
-        a.x = x;
-        a.y = y;
-        a.z = z;
-        a.type = s->type.as<int>();
-        a.q = s->q.as<float>();
-        a.L = s->L;
-        a.alpha = s->alpha;
-        a.EWALD_P = (double)0.3275911f;
-        a.A1 = (double)0.254829592f;
-        a.A2 = (double)-0.284496736f;
-        a.A3 = (double)1.421413741f;
-        a.A4 = (double)-1.453152027f;
-        a.A5 = (double)1.061405429f;
-        a.MY_PIS = (double)1.77245385090551602729f;
-        a.e_shift = s->e_shift;
-        a.f_shift = s->f_shift;
-        a.cut_coulsq = (double)(float)(s->rc * s->rc);
-        a.rcut2 = a.cut_coulsq;
-        a.coulpre = s->coulpre;
-        a.fx = fx;
-        a.fy = fy;
-        a.fz = fz;
-        a.e = et + nb + na;
-        if (energy)
-            k_dihedral<true><<<grid_for(nd, 128), 128, 0, st>>>(a);
-        else
-            k_dihedral<false><<<grid_for(nd, 128), 128, 0, st>>>(a);
-    }
-    if ((md.terms & 16) && md.nimpro) {
-        double *ei = et + nb + na + 3 * (size_t)nd;
-        if (energy)
-            k_improper<true><<<grid_for(md.nimpro, 128), 128, 0, st>>>(md.nimpro, md.impros.as<int>(), md.icoef.as<double>(), x, y, z, s->L, fx, fy, fz, ei);
-        else
-            k_improper<false><<<grid_for(md.nimpro, 128), 128, 0, st>>>(md.nimpro, md.impros.as<int>(), md.icoef.as<double>(), x, y, z, s->L, fx, fy, fz, ei);
+            k_bonded<false><<<grid_for(nterm, 128), 128, 0, st>>>(b);
     }
     if (md.gamma > 0.0) {
         const double kT = KBOLTZ * md.temperature;
@@ -635,15 +683,18 @@ static int md_step(Sys *s, bool energy) {
     double *vx = s->v[0].as<double>(), *vy = s->v[1].as<double>(), *vz = s->v[2].as<double>();
     const long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
                     *fz = s->f[2].as<long long>();
-    k_kick<<<grid_for(n, 256), 256, 0, st>>>(n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz);
-    k_stream<<<grid_for(n, 256), 256, 0, st>>>(n, md.dt, s->x[0].as<double>(), s->x[1].as<double>(),
-                                               s->x[2].as<double>(), vx, vy, vz);
-    k_step_inc<<<1, 32, 0, st>>>(md.step_dev.as<long long>());
-    int rc = md_forces(s, energy, false);
+    const double half = 0.5 * s->skin, phalf = 0.5 * s->margin;
+    k_kick_drift<<<grid_for(n, 256), 256, 0, st>>>(
+        n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz, md.dt, s->x[0].as<double>(),
+        s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
+        s->xref[1].as<double>(), s->xref[2].as<double>(), s->xprn[0].as<double>(),
+        s->xprn[1].as<double>(), s->xprn[2].as<double>(), s->L, half * half, phalf * phalf,
+        s->flag.as<int>(), md.step_dev.as<long long>());
+    int rc = md_forces(s, energy, false, true);
     if (rc) return rc;
     k_kick<<<grid_for(n, 256), 256, 0, st>>>(n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz);
     if (energy) md_energy_reduce(s);
-    s->launches += 8;
+    s->launches += 2;
     SOFIA_CUDA(s->ctx, cudaGetLastError());
     return SOFIA_OK;
 }

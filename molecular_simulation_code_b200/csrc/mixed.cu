@@ -388,16 +388,6 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
 
 // Displacement trigger: flag a rebuild when any atom moved more than skin/2
 // (minimum image) since the last build.
-__device__ __forceinline__ double disp2(double x, double y, double z, double rx, double ry,
-                                        double rz, double L) {
-    double dx = x - rx, dy = y - ry, dz = z - rz;
-    dx -= L * rint(dx / L);
-    dy -= L * rint(dy / L);
-    dz -= L * rint(dz / L);
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    return (d2 == d2) ? d2 : 1e300;  // non-finite positions force a rebuild
-}
-
 // Displacement triggers: bit 0 = some atom moved more than skin/2 since the
 // list build, bit 1 = more than margin/2 since the last prune.
 __global__ void k_disp_check(int n, const double *__restrict__ x, const double *__restrict__ y,
@@ -852,11 +842,14 @@ __global__ void k_set_flag(int *__restrict__ flag, int v) {
     if (threadIdx.x == 0 && blockIdx.x == 0) flag[0] = v;
 }
 
-// Device-side counters of list builds and prunes (for statistics).
-__global__ void k_count_events(const int *__restrict__ flag, long long *__restrict__ cnt) {
+// Device-side counters of list builds and prunes (for statistics).  The
+// trigger word is then cleared for the next step's displacement check, which
+// only ORs bits into it.
+__global__ void k_count_events(int *__restrict__ flag, long long *__restrict__ cnt) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         if (flag[0] & 1) cnt[0] += 1;
         if (flag[0] & 3) cnt[1] += 1;
+        flag[0] = 0;
     }
 }
 
@@ -1276,14 +1269,15 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial) {
 // triggers (or a forced build), conditional rebuild, pack, conditional prune,
 // pair kernel.  Row-capacity overflow is recorded in status_local and checked
 // by the caller after the segment (sys_list_overflow).
-int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build) {
+int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build,
+                    bool disp_done) {
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     const int n = s->n;
     int *flag = s->flag.as<int>();
     if (force_build || !s->built) {
         k_set_flag<<<1, 32, 0, st>>>(flag, 3);
-    } else {
+    } else if (!disp_done) {
         const double half = 0.5 * s->skin, phalf = 0.5 * s->margin;
         k_set_flag<<<1, 32, 0, st>>>(flag, 0);
         k_disp_check<<<grid_for(n, 256), 256, 0, st>>>(
@@ -1516,6 +1510,7 @@ extern "C" int sofia_force_nonbond_mixed(sofia_system *ss, const sofia_ainfo *po
     const bool want_e = potential || e_coul || virial_diag3;
     const bool vir = virial_diag3 != nullptr;
     const bool graph = s->built && !s->timing;
+    s->md.forces_valid = 0;  // the MD's step forces are replaced
     if (graph) {
         // steady state: the whole device step is one graph launch, rebuilds and
         // prunes decided on the device
@@ -1620,6 +1615,9 @@ extern "C" int sofia_system_compute_forces(sofia_system *ss, int precision, int 
     Sys *s = &ss->s;
     sofia_nb_ctx *ctx = s->ctx;
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    // the pair-only forces replace the MD's step forces: the next MD segment
+    // recomputes them (with a fresh list decision)
+    s->md.forces_valid = 0;
     int rc = sofia::sys_eval(s, precision, energies != nullptr,
                              energies != nullptr && (flags & SOFIA_EVAL_VIRIAL),
                              (flags & SOFIA_EVAL_REBUILD) != 0);

@@ -103,11 +103,28 @@ struct Sys {
 // evaluation entry points (mixed.cu)
 int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build);
 int sys_pair(Sys *s, int precision, bool energy, bool virial);
-int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build);
+// disp_done: the caller already ORed the displacement-trigger bits into a
+// cleared trigger word (the MD step's fused kick/drift kernel does).
+int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build,
+                    bool disp_done = false);
 int sys_list_overflow(Sys *s);
 // Frees the captured drop-in force graphs (they bake in list pointers and the margin).
 void dropin_drop(Sys *s);
 
+}  // namespace sofia
+
+namespace sofia {
+// Squared minimum-image displacement since a reference position; non-finite
+// positions give a huge value so that they trigger a rebuild.
+__device__ __forceinline__ double disp2(double x, double y, double z, double rx, double ry,
+                                        double rz, double L) {
+    double dx = x - rx, dy = y - ry, dz = z - rz;
+    dx -= L * rint(dx / L);
+    dy -= L * rint(dy / L);
+    dz -= L * rint(dz / L);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    return (d2 == d2) ? d2 : 1e300;
+}
 }  // namespace sofia
 
 struct sofia_system {
