@@ -306,79 +306,117 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
     int count = 0;
     int *row = a.jlist + (size_t)icl * a.jcap;
     unsigned long long *mrow = a.jmask + (size_t)icl * a.jcap;
-    for (int dy = -a.reach; dy <= a.reach; ++dy) {
-        int cy = cyi + dy;
-        const int imy = (cy < 0) ? -1 : (cy >= a.ncx ? 1 : 0);
-        cy -= imy * a.ncx;
-        const float sy = imy * a.L;
-        const float gy = gap(ilo.y, ihi.y, cy * a.s_col + sy, (cy + 1) * a.s_col + sy);
-        if (gy * gy >= a.rl2) continue;
-        for (int dx = -a.reach; dx <= a.reach; ++dx) {
+    // Candidates: the clusters of every (column, z image) within reach, in the
+    // order column row dy, column dx, image z.  32 such segments are gathered at
+    // a time (one per lane) and their clusters are then streamed over the lanes
+    // as one flat sequence, so short segments do not leave lanes idle.
+    __shared__ int s_seg[8][3][32];  // per warp: first cluster, flat offset, image code
+    int *sj0 = s_seg[threadIdx.x >> 5][0], *scum = s_seg[threadIdx.x >> 5][1],
+        *simg = s_seg[threadIdx.x >> 5][2];
+    const int side = 2 * a.reach + 1;
+    const int ncombo = side * side * 3;
+    for (int cbase = 0; cbase < ncombo; cbase += 32) {
+        const int k = cbase + lane;
+        int len = 0, j0 = 0, imgk = 13;
+        if (k < ncombo) {
+            const int iz = k % 3, kk = k / 3;
+            const int dx = kk % side - a.reach, dy = kk / side - a.reach;
+            int cy = cyi + dy;
+            const int imy = (cy < 0) ? -1 : (cy >= a.ncx ? 1 : 0);
+            cy -= imy * a.ncx;
             int cx = cxi + dx;
             const int imx = (cx < 0) ? -1 : (cx >= a.ncx ? 1 : 0);
             cx -= imx * a.ncx;
-            const float sx = imx * a.L;
+            const int imz = iz - 1;
+            const float sx = imx * a.L, sy = imy * a.L, sz = imz * a.L;
             const float gx = gap(ilo.x, ihi.x, cx * a.s_col + sx, (cx + 1) * a.s_col + sx);
-            if (gx * gx + gy * gy >= a.rl2) continue;
-            const int jc0 = a.cl_start[cx + cy * a.ncx], jc1 = a.cl_start[cx + cy * a.ncx + 1];
-            for (int imz = -1; imz <= 1; ++imz) {
-                const float sz = imz * a.L;
-                // the column image spans z in [sz, sz + L): skip images out of reach
-                const float gz = gap(ilo.z, ihi.z, sz, sz + a.L);
-                if (gx * gx + gy * gy + gz * gz >= a.rl2) continue;
-                for (int base = jc0; base < jc1; base += 32) {
-                    const int jc = base + lane;
-                    bool acc = false, need_excl = false;
-                    unsigned long long mask = 0ull;
-                    if (jc < jc1) {
-                        const float4 jlo = a.bb[2 * jc], jhi = a.bb[2 * jc + 1];
-                        const float ex = gap(ilo.x, ihi.x, jlo.x + sx, jhi.x + sx);
-                        const float ey = gap(ilo.y, ihi.y, jlo.y + sy, jhi.y + sy);
-                        const float ez = gap(ilo.z, ihi.z, jlo.z + sz, jhi.z + sz);
-                        const float d2 = ex * ex + ey * ey + ez * ez;
-                        const int img = (imx + 1) + 3 * (imy + 1) + 9 * (imz + 1);
-                        acc = d2 < a.rl2 && half_keep(icl, jc, img);
-                        if (acc) {
-                            need_excl = d2 < a.rexcl2;
-                            const unsigned long long jreal =
-                                (unsigned long long)((unsigned)__float_as_int(jlo.w) & 0xffu);
-                            mask = (jreal * 0x0101010101010101ull) & iexp;
-                            if (jc == icl && img == 13) {
-                                // the cluster with itself: pairs ii < jj only
-#pragma unroll
-                                for (int ii = 0; ii < CL; ++ii)
-                                    mask &= ~(((2ull << ii) - 1ull) << (ii * CL));
-                            }
-                        }
-                    }
-                    const unsigned ballot = __ballot_sync(FULL, acc);
-                    // exclusions: for each nearby accepted entry the warp ORs the bits of
-                    // the i atoms' partners that sit in that j-cluster
-                    unsigned todo = __ballot_sync(FULL, need_excl);
-                    while (todo) {
-                        const int src = __ffs(todo) - 1;
-                        todo &= todo - 1;
-                        const int jsrc = __shfl_sync(FULL, jc, src);
-                        unsigned long long m = 0ull;
-#pragma unroll
-                        for (int t = 0; t < 3; ++t)
-                            if (ex_slot[t] >= 0 && (ex_slot[t] >> 3) == jsrc) m |= 1ull << ex_bit[t];
-                        const unsigned lo = __reduce_or_sync(FULL, (unsigned)m);
-                        const unsigned hi = __reduce_or_sync(FULL, (unsigned)(m >> 32));
-                        if (lane == src) mask &= ~((unsigned long long)lo | ((unsigned long long)hi << 32));
-                    }
-                    if (acc) {
-                        const int at = count + __popc(ballot & ((1u << lane) - 1u));
-                        if (at < a.jcap) {
-                            const int img = (imx + 1) + 3 * (imy + 1) + 9 * (imz + 1);
-                            row[at] = jc | (img << IMG_SHIFT);
-                            mrow[at] = mask;
-                        }
-                    }
-                    count += __popc(ballot);
-                }
+            const float gy = gap(ilo.y, ihi.y, cy * a.s_col + sy, (cy + 1) * a.s_col + sy);
+            // the column image spans z in [sz, sz + L)
+            const float gz = gap(ilo.z, ihi.z, sz, sz + a.L);
+            if (gx * gx + gy * gy + gz * gz < a.rl2) {
+                j0 = a.cl_start[cx + cy * a.ncx];
+                len = a.cl_start[cx + cy * a.ncx + 1] - j0;
+                imgk = (imx + 1) + 3 * (imy + 1) + 9 * (imz + 1);
             }
         }
+        const bool has = len > 0;
+        const unsigned hb = __ballot_sync(FULL, has);
+        if (!hb) continue;
+        const int nseg = __popc(hb);
+        int incl = len;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(FULL, incl, off);
+            if (lane >= off) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        if (has) {
+            const int at = __popc(hb & ((1u << lane) - 1u));
+            sj0[at] = j0;
+            scum[at] = incl - len;
+            simg[at] = imgk;
+        }
+        __syncwarp();
+        int seg = 0;
+        for (int base = 0; base < total; base += 32) {
+            const int t = base + lane;
+            const bool act = t < total;
+            int jc = 0, img = 13;
+            if (act) {
+                while (seg + 1 < nseg && scum[seg + 1] <= t) ++seg;
+                jc = sj0[seg] + (t - scum[seg]);
+                img = simg[seg];
+            }
+            const float sx = (float)(img % 3 - 1) * a.L, sy = (float)((img / 3) % 3 - 1) * a.L,
+                        sz = (float)(img / 9 - 1) * a.L;
+            bool acc = false, need_excl = false;
+            unsigned long long mask = 0ull;
+            if (act) {
+                const float4 jlo = a.bb[2 * jc], jhi = a.bb[2 * jc + 1];
+                const float ex = gap(ilo.x, ihi.x, jlo.x + sx, jhi.x + sx);
+                const float ey = gap(ilo.y, ihi.y, jlo.y + sy, jhi.y + sy);
+                const float ez = gap(ilo.z, ihi.z, jlo.z + sz, jhi.z + sz);
+                const float d2 = ex * ex + ey * ey + ez * ez;
+                acc = d2 < a.rl2 && half_keep(icl, jc, img);
+                if (acc) {
+                    need_excl = d2 < a.rexcl2;
+                    const unsigned long long jreal =
+                        (unsigned long long)((unsigned)__float_as_int(jlo.w) & 0xffu);
+                    mask = (jreal * 0x0101010101010101ull) & iexp;
+                    if (jc == icl && img == 13) {
+                        // the cluster with itself: pairs ii < jj only
+#pragma unroll
+                        for (int ii = 0; ii < CL; ++ii)
+                            mask &= ~(((2ull << ii) - 1ull) << (ii * CL));
+                    }
+                }
+            }
+            const unsigned ballot = __ballot_sync(FULL, acc);
+            // exclusions: for each nearby accepted entry the warp ORs the bits of
+            // the i atoms' partners that sit in that j-cluster
+            unsigned todo = __ballot_sync(FULL, need_excl);
+            while (todo) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const int jsrc = __shfl_sync(FULL, jc, src);
+                unsigned long long m = 0ull;
+#pragma unroll
+                for (int tt = 0; tt < 3; ++tt)
+                    if (ex_slot[tt] >= 0 && (ex_slot[tt] >> 3) == jsrc) m |= 1ull << ex_bit[tt];
+                const unsigned lo = __reduce_or_sync(FULL, (unsigned)m);
+                const unsigned hi = __reduce_or_sync(FULL, (unsigned)(m >> 32));
+                if (lane == src) mask &= ~((unsigned long long)lo | ((unsigned long long)hi << 32));
+            }
+            if (acc) {
+                const int at = count + __popc(ballot & ((1u << lane) - 1u));
+                if (at < a.jcap) {
+                    row[at] = jc | (img << IMG_SHIFT);
+                    mrow[at] = mask;
+                }
+            }
+            count += __popc(ballot);
+        }
+        __syncwarp();
     }
     if (lane == 0) {
         a.jcount[icl] = min(count, a.jcap);
