@@ -636,7 +636,7 @@ static void md_energy_reduce(Sys *s) {
     double *part = red + 16;
     double *et = md.eterm.as<double>();
     // nonbonded pair energies were reduced into s->red by the pair path
-    cudaMemcpyAsync(red, s->red.p, sizeof(double) * 5, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(red, s->red.p, sizeof(double) * 5, cudaMemcpyDeviceToDevice, st);  // checked with the step's launches
     if (md.nbond && (md.terms & 1)) md_reduce(st, md.nbond, 1, 0, et, part, red + 5);
     if (md.nangle && (md.terms & 2)) md_reduce(st, md.nangle, 1, 0, et + md.nbond, part, red + 6);
     if (md.ndihed && (md.terms & 12)) {
@@ -819,14 +819,13 @@ extern "C" int sofia_system_md_setup(sofia_system *ss, const sofia_md_desc *d) {
     SOFIA_CUDA(ctx, md.snap[6].ensure(sizeof(long long)));
     // DSF self energy (Source/mod_assign_types.f90:59-62) and degrees of freedom
     {
-        float *hq = new float[s->n];
-        cudaMemcpy(hq, s->q.p, sizeof(float) * s->n, cudaMemcpyDeviceToHost);
+        std::vector<float> hq(s->n);
+        SOFIA_CUDA(ctx, cudaMemcpy(hq.data(), s->q.p, sizeof(float) * s->n, cudaMemcpyDeviceToHost));
         const double my_pis = (double)1.77245385090551602729f;
         double es = 0.0;
         for (int i = 0; i < s->n; ++i)
             es -= (0.5 * s->e_shift + s->alpha / my_pis) * (double)hq[i] * (double)hq[i] *
                   (double)s->coulpre;
-        delete[] hq;
         md.e_self = es;
         int ncons = 0;
         for (int g = 0; g < md.nshake; ++g) {

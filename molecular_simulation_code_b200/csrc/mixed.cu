@@ -1439,53 +1439,56 @@ extern "C" int sofia_system_create(sofia_nb_ctx *ctx, const sofia_system_desc *d
     if (!rc) rc = sofia::sys_alloc_list(s);
     const size_t n = (size_t)s->n;
     if (!rc) {
-        cudaStream_t st = ctx->stream;
-        rc = SOFIA_OK;
-        if (s->type.ensure(sizeof(int) * n) || s->q.ensure(sizeof(float) * n) ||
+        // the system's stream is idle here: synchronous copies
+        const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+        if (se != cudaSuccess) rc = sofia::cuda_fail(ctx, se, "cudaStreamSynchronize");
+        if (!rc && (s->type.ensure(sizeof(int) * n) || s->q.ensure(sizeof(float) * n) ||
             s->specbond.ensure(sizeof(int) * 12 * n) || s->num3bond.ensure(sizeof(int) * n) ||
             s->ljtab.ensure(sizeof(float4) * (size_t)s->ntypes * s->ntypes) ||
-            s->invm.ensure(sizeof(double) * n) || s->mass.ensure(sizeof(double) * n))
+            s->invm.ensure(sizeof(double) * n) || s->mass.ensure(sizeof(double) * n)))
             rc = sofia::fail(ctx, SOFIA_ECUDA, "allocation failed%s");
         if (!rc) {
-            cudaMemcpyAsync(s->type.p, d->type, sizeof(int) * n, cudaMemcpyDefault, st);
-            cudaMemcpyAsync(s->q.p, d->q, sizeof(float) * n, cudaMemcpyDefault, st);
-            cudaMemcpyAsync(s->specbond.p, d->specbond, sizeof(int) * 12 * n, cudaMemcpyDefault, st);
-            cudaMemcpyAsync(s->num3bond.p, d->num3bond, sizeof(int) * n, cudaMemcpyDefault, st);
+            // every copy is checked; host staging lives in vectors so that an
+            // early return frees it
+            cudaError_t e = cudaSuccess;
+            auto cp = [&](void *dst, const void *src, size_t bytes) {
+                if (e == cudaSuccess) e = cudaMemcpy(dst, src, bytes, cudaMemcpyDefault);
+            };
+            cp(s->type.p, d->type, sizeof(int) * n);
+            cp(s->q.p, d->q, sizeof(float) * n);
+            cp(s->specbond.p, d->specbond, sizeof(int) * 12 * n);
+            cp(s->num3bond.p, d->num3bond, sizeof(int) * n);
             const int nt2 = s->ntypes * s->ntypes;
-            float4 *tab = new float4[nt2];
-            float *h1 = new float[4 * nt2];
-            cudaMemcpy(h1, d->lj1, sizeof(float) * nt2, cudaMemcpyDefault);
-            cudaMemcpy(h1 + nt2, d->lj2, sizeof(float) * nt2, cudaMemcpyDefault);
-            cudaMemcpy(h1 + 2 * nt2, d->lj3, sizeof(float) * nt2, cudaMemcpyDefault);
-            cudaMemcpy(h1 + 3 * nt2, d->lj4, sizeof(float) * nt2, cudaMemcpyDefault);
+            std::vector<float> h1(4 * (size_t)nt2);
+            std::vector<float4> tab(nt2);
+            cp(h1.data(), d->lj1, sizeof(float) * nt2);
+            cp(h1.data() + nt2, d->lj2, sizeof(float) * nt2);
+            cp(h1.data() + 2 * nt2, d->lj3, sizeof(float) * nt2);
+            cp(h1.data() + 3 * nt2, d->lj4, sizeof(float) * nt2);
             for (int t = 0; t < nt2; ++t)
                 tab[t] = make_float4(h1[t], h1[nt2 + t], h1[2 * nt2 + t], h1[3 * nt2 + t]);
-            cudaMemcpy(s->ljtab.p, tab, sizeof(float4) * nt2, cudaMemcpyHostToDevice);
-            delete[] tab;
-            delete[] h1;
-            int *ht = new int[n];
-            cudaMemcpy(ht, d->type, sizeof(int) * n, cudaMemcpyDefault);
-            for (size_t i = 0; i < n; ++i)
-                if (ht[i] < 1 || ht[i] > s->ntypes) rc = sofia::fail(ctx, SOFIA_EINVAL, "atom type out of range%s");
+            cp(s->ljtab.p, tab.data(), sizeof(float4) * nt2);
+            std::vector<int> ht(n);
+            cp(ht.data(), d->type, sizeof(int) * n);
+            if (e != cudaSuccess) {
+                rc = sofia::cuda_fail(ctx, e, "system upload");
+            } else {
+                for (size_t i = 0; i < n && !rc; ++i)
+                    if (ht[i] < 1 || ht[i] > s->ntypes)
+                        rc = sofia::fail(ctx, SOFIA_EINVAL, "atom type out of range%s");
+            }
             if (d->mass && !rc) {
                 // per-atom masses and inverses from the per-type table
-                double *hm = new double[n], *hi = new double[n];
-                double *mt = new double[s->ntypes];
-                cudaMemcpy(mt, d->mass, sizeof(double) * s->ntypes, cudaMemcpyDefault);
+                std::vector<double> hm(n), hi(n), mt(s->ntypes);
+                cp(mt.data(), d->mass, sizeof(double) * s->ntypes);
                 for (size_t i = 0; i < n; ++i) {
-                    const int t = ht[i] - 1;
-                    hm[i] = (t >= 0 && t < s->ntypes) ? mt[t] : 1.0;
+                    hm[i] = mt[ht[i] - 1];
                     hi[i] = 1.0 / hm[i];
                 }
-                cudaMemcpy(s->mass.p, hm, sizeof(double) * n, cudaMemcpyHostToDevice);
-                cudaMemcpy(s->invm.p, hi, sizeof(double) * n, cudaMemcpyHostToDevice);
-                delete[] hm;
-                delete[] hi;
-                delete[] mt;
+                cp(s->mass.p, hm.data(), sizeof(double) * n);
+                cp(s->invm.p, hi.data(), sizeof(double) * n);
+                if (e != cudaSuccess) rc = sofia::cuda_fail(ctx, e, "mass upload");
             }
-            delete[] ht;
-            cudaError_t e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess && !rc) rc = sofia::cuda_fail(ctx, e, "system upload");
         }
     }
     if (rc) {
