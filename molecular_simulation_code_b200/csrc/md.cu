@@ -20,13 +20,12 @@
 #include <vector>
 
 #include "improper.cuh"
+#include "langevin.cuh"
 #include "system.cuh"
 
 namespace sofia {
 namespace {
 
-constexpr double KCAL2AMU = (double)0.0004184f;  // real*4 literal (get_started.f90:32)
-constexpr double KBOLTZ = (double)0.001987204181f;  // real*4 variable (global.f90:133)
 
 __device__ __forceinline__ long long fixd(double v) { return __double2ll_rn(v * FIX_SCALE); }
 __device__ __forceinline__ double unfix(long long v) { return (double)v * FIX_INV; }
@@ -37,21 +36,6 @@ __device__ __forceinline__ void fadd(long long *f, double v) {
 
 __device__ __forceinline__ double mimg(double d, double L) { return d - L * rint(d / L); }
 
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter-based RNG.
-__device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        const unsigned lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
-        const unsigned lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-        k.x += 0x9E3779B9u;
-        k.y += 0xBB67AE85u;
-    }
-    return c;
-}
-__device__ __forceinline__ double u01m(unsigned b) {  // uniform in [-1/2, 1/2)
-    return (double)(b >> 8) * (1.0 / 16777216.0) - 0.5;
-}
 
 // nve_v: v += (dt/2) * kcal2amu * f / m
 __global__ void k_kick(int n, double h, const double *__restrict__ invm,
@@ -104,24 +88,6 @@ __global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
 }
 
 
-// Force-form Langevin: f += -gamma m v / kcal2amu + sqrt(12 * 2 m gamma kT kcal2amu / dt) U / kcal2amu
-__global__ void k_langevin(int n, double gamma, double gsig, unsigned long long seed,
-                           const long long *__restrict__ step_dev, const double *__restrict__ mass,
-                           const double *__restrict__ vx, const double *__restrict__ vy,
-                           const double *__restrict__ vz, long long *__restrict__ fx,
-                           long long *__restrict__ fy, long long *__restrict__ fz) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const long long step = step_dev[0];
-    const uint4 r = philox(make_uint4((unsigned)i, (unsigned)step, (unsigned)(step >> 32), 0x5EED5EEDu),
-                           make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
-    const double m = mass[i];
-    const double g1 = -gamma * m / KCAL2AMU;
-    const double g2 = gsig * sqrt(m);
-    fx[i] += fixd(g1 * vx[i] + g2 * u01m(r.x));
-    fy[i] += fixd(g1 * vy[i] + g2 * u01m(r.y));
-    fz[i] += fixd(g1 * vz[i] + g2 * u01m(r.z));
-}
 
 template <bool EN>
 __device__ __forceinline__ void bond_term(int m, int nb, const int *__restrict__ bl, const double *__restrict__ bc,
@@ -553,7 +519,21 @@ __global__ void __launch_bounds__(128) k_bonded(BondedArgs b) {
 static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = false) {
     Md &md = s->md;
     cudaStream_t st = s->ctx->stream;
-    int rc = sys_step_forces(s, s->precision, energy, false, force_build, disp_done);
+    // the Langevin force is added by the pair path's force unpack
+    LangevinArgs lg{};
+    if (md.gamma > 0.0) {
+        const double kT = KBOLTZ * md.temperature;
+        lg.on = 1;
+        lg.gamma = md.gamma;
+        lg.gsig = sqrt(12.0 * 2.0 * md.gamma * kT * KCAL2AMU / md.dt) / KCAL2AMU;
+        lg.seed = md.seed;
+        lg.step = md.step_dev.as<long long>();
+        lg.mass = s->mass.as<double>();
+        lg.vx = s->v[0].as<double>();
+        lg.vy = s->v[1].as<double>();
+        lg.vz = s->v[2].as<double>();
+    }
+    int rc = sys_step_forces(s, s->precision, energy, false, force_build, disp_done, &lg);
     if (rc) return rc;
     long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
               *fz = s->f[2].as<long long>();
@@ -610,13 +590,6 @@ static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = fal
             k_bonded<true><<<grid_for(nterm, 128), 128, 0, st>>>(b);
         else
             k_bonded<false><<<grid_for(nterm, 128), 128, 0, st>>>(b);
-    }
-    if (md.gamma > 0.0) {
-        const double kT = KBOLTZ * md.temperature;
-        const double gsig = sqrt(12.0 * 2.0 * md.gamma * kT * KCAL2AMU / md.dt) / KCAL2AMU;
-        k_langevin<<<grid_for(s->n, 256), 256, 0, st>>>(
-            s->n, md.gamma, gsig, md.seed, md.step_dev.as<long long>(), s->mass.as<double>(),
-            s->v[0].as<double>(), s->v[1].as<double>(), s->v[2].as<double>(), fx, fy, fz);
     }
     if (md.nshake) {
         k_shake<<<grid_for(md.nshake, 128), 128, 0, st>>>(

@@ -80,31 +80,49 @@ __global__ void k_wrap_bin(const int *__restrict__ cond, int cmask, int n,
     atomicAdd(&col_count[c], 1);
 }
 
-__global__ void k_scan1(const int *__restrict__ cond, int cmask, int n, const int *__restrict__ in,
-                        int *__restrict__ out, int round8) {
+// Column scans of a build, one block: col_start = exclusive scan of the atom
+// counts, cl_start = exclusive scan of the cluster counts (ceil(count/8)), the
+// total cluster count into ncl.  The counts are cleared for the next build.
+__global__ void k_scan_cols(const int *__restrict__ cond, int cmask, int n,
+                            int *__restrict__ col_count, int *__restrict__ col_start,
+                            int *__restrict__ cl_start, int *__restrict__ ncl) {
     SOFIA_COND_RETURN;
-    __shared__ int s[1024];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
+    __shared__ int s1[1024], s2[1024];
+    __shared__ int carry1, carry2;
+    const int t = threadIdx.x;
+    if (t == 0) carry1 = carry2 = 0;
     __syncthreads();
     for (int base = 0; base < n; base += 1024) {
-        const int t = threadIdx.x;
-        int v = (base + t < n) ? in[base + t] : 0;
-        if (round8) v = (v + CL - 1) / CL;
-        s[t] = v;
+        const int v = (base + t < n) ? col_count[base + t] : 0;
+        const int w = (v + CL - 1) / CL;
+        s1[t] = v;
+        s2[t] = w;
         __syncthreads();
         for (int off = 1; off < 1024; off <<= 1) {
-            const int a = (t >= off) ? s[t - off] : 0;
+            const int a1 = (t >= off) ? s1[t - off] : 0;
+            const int a2 = (t >= off) ? s2[t - off] : 0;
             __syncthreads();
-            s[t] += a;
+            s1[t] += a1;
+            s2[t] += a2;
             __syncthreads();
         }
-        if (base + t < n) out[base + t] = carry + s[t] - v;
+        if (base + t < n) {
+            col_start[base + t] = carry1 + s1[t] - v;
+            cl_start[base + t] = carry2 + s2[t] - w;
+            col_count[base + t] = 0;
+        }
         __syncthreads();
-        if (t == 1023) carry += s[1023];
+        if (t == 1023) {
+            carry1 += s1[1023];
+            carry2 += s2[1023];
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[n] = carry;
+    if (t == 0) {
+        col_start[n] = carry1;
+        cl_start[n] = carry2;
+        ncl[0] = carry2;
+    }
 }
 
 __global__ void k_col_scatter(const int *__restrict__ cond, int cmask, int n,
@@ -125,11 +143,13 @@ __global__ void k_col_sort_assign(const int *__restrict__ cond, int cmask, int n
                                   int *__restrict__ col_atoms, const float *__restrict__ zkey,
                                   const int *__restrict__ cl_start, int *__restrict__ slot_orig,
                                   int *__restrict__ cl_col, int *__restrict__ atom_slot,
-                                  int *__restrict__ status) {
+                                  int *__restrict__ col_fill, int *__restrict__ status) {
     SOFIA_COND_RETURN;
     __shared__ unsigned long long s[MAX_COL];
     const int c = blockIdx.x;
     if (c >= ncols) return;
+    // the scatter is done with this column's fill counter: clear it for the next build
+    if (threadIdx.x == 0) col_fill[c] = 0;
     const int b = col_start[c], nc = col_start[c + 1] - b;
     if (nc > MAX_COL) {
         if (threadIdx.x == 0) atomicAdd(&status[ST_CELLOVER], 1);
@@ -444,17 +464,6 @@ __global__ void k_disp_check(int n, const double *__restrict__ x, const double *
     if ((threadIdx.x & 31) == 0 && (a || b)) atomicOr(flag, (a ? 1 : 0) | (b ? 2 : 0));
 }
 
-__global__ void k_copy3(const int *__restrict__ cond, int cmask, int n,
-                        const double *__restrict__ x, const double *__restrict__ y,
-                        const double *__restrict__ z, double *__restrict__ ox,
-                        double *__restrict__ oy, double *__restrict__ oz) {
-    SOFIA_COND_RETURN;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    ox[i] = x[i];
-    oy[i] = y[i];
-    oz[i] = z[i];
-}
 
 struct PairConst {
     float rcut2, cut_coulsq, kexp, pa, c2a, e_shift, f_shift, coulpre;
@@ -746,15 +755,32 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? SOFIA_PAIR_MINB : 2) k
 // Slot-ordered fixed-point pair forces -> the caller's atom order (sets the
 // force arrays; bonded terms add to them afterwards).  Flags sums outside the
 // fixed-point range.
+// With flag != NULL, thread 0 also counts this step's list build and prune in
+// cnt and clears the trigger word for the next step's displacement check (only
+// bits are ORed into it).  With lg.on, each atom's Langevin force is added.
 __global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
                          const int *__restrict__ slot_orig, const long long *__restrict__ fslot,
                          long long *__restrict__ fx, long long *__restrict__ fy,
-                         long long *__restrict__ fz, int *__restrict__ status) {
+                         long long *__restrict__ fz, int *__restrict__ status,
+                         int *__restrict__ flag, long long *__restrict__ cnt, LangevinArgs lg) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (flag && s == 0) {
+        const int f = flag[0];
+        if (f & 1) cnt[0] += 1;
+        if (f & 3) cnt[1] += 1;
+        flag[0] = 0;
+    }
     if (s >= nslots || s >= ncl_dev[0] * CL) return;
     const int o = slot_orig[s];
     if (o < 0) return;
-    const long long a = fslot[s], b = fslot[nslots + s], c = fslot[2 * (size_t)nslots + s];
+    long long a = fslot[s], b = fslot[nslots + s], c = fslot[2 * (size_t)nslots + s];
+    if (lg.on) {
+        long long la, lb, lc;
+        langevin_force(lg, o, la, lb, lc);
+        a += la;
+        b += lb;
+        c += lc;
+    }
     fx[o] = a;
     fy[o] = b;
     fz[o] = c;
@@ -791,7 +817,10 @@ __global__ void __launch_bounds__(256) k_prune(
     const float4 *__restrict__ recf,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
     const int *__restrict__ jcount, int jcap, float L, float rin2, int *__restrict__ ilist,
-    unsigned long long *__restrict__ imask, int *__restrict__ icount) {
+    unsigned long long *__restrict__ imask, int *__restrict__ icount,
+    const int *__restrict__ slot_orig, const double *__restrict__ x,
+    const double *__restrict__ y, const double *__restrict__ z, double *__restrict__ px,
+    double *__restrict__ py, double *__restrict__ pz) {
     SOFIA_COND_RETURN;
     __shared__ float s_shf[27 * 3];
     if (threadIdx.x < 27) {
@@ -804,6 +833,15 @@ __global__ void __launch_bounds__(256) k_prune(
     const int lane = threadIdx.x & 31;
     const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (icl >= maxcl || icl >= ncl_dev[0]) return;
+    // the positions this prune is valid for (the prune trigger measures from them)
+    if (lane < CL) {
+        const int o = slot_orig[icl * CL + lane];
+        if (o >= 0) {
+            px[o] = x[o];
+            py[o] = y[o];
+            pz[o] = z[o];
+        }
+    }
     float xi[CL], yi[CL], zi[CL];
 #pragma unroll
     for (int ii = 0; ii < CL; ++ii) {
@@ -855,40 +893,10 @@ __global__ void __launch_bounds__(256) k_prune(
     if (lane == 0) icount[icl] = kept;
 }
 
-// Conditional list-build preparation: clear the column counters and mark
-// every slot as padding.
-__global__ void k_build_prep(const int *__restrict__ cond, int cmask, int ncols1,
-                             int *__restrict__ col_count, int *__restrict__ col_fill, int nslots,
-                             int *__restrict__ slot_orig) {
-    SOFIA_COND_RETURN;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += gridDim.x * blockDim.x) {
-        slot_orig[i] = -1;
-        if (i < ncols1) {
-            col_count[i] = 0;
-            col_fill[i] = 0;
-        }
-    }
-}
 
-__global__ void k_set_ncl(const int *__restrict__ cond, int cmask, const int *__restrict__ src,
-                          int *__restrict__ dst) {
-    SOFIA_COND_RETURN;
-    if (threadIdx.x == 0 && blockIdx.x == 0) dst[0] = src[0];
-}
 
 __global__ void k_set_flag(int *__restrict__ flag, int v) {
     if (threadIdx.x == 0 && blockIdx.x == 0) flag[0] = v;
-}
-
-// Device-side counters of list builds and prunes (for statistics).  The
-// trigger word is then cleared for the next step's displacement check, which
-// only ORs bits into it.
-__global__ void k_count_events(int *__restrict__ flag, long long *__restrict__ cnt) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        if (flag[0] & 1) cnt[0] += 1;
-        if (flag[0] & 3) cnt[1] += 1;
-        flag[0] = 0;
-    }
 }
 
 // Two-stage deterministic column sums: stage 1 = fixed grid of blocks over
@@ -978,6 +986,8 @@ static int sys_alloc(Sys *s) {
     SOFIA_CUDA(ctx, s->col_count.ensure(sizeof(int) * (s->ncols + 1)));
     SOFIA_CUDA(ctx, s->col_start.ensure(sizeof(int) * (s->ncols + 1)));
     SOFIA_CUDA(ctx, s->col_fill.ensure(sizeof(int) * (s->ncols + 1)));
+    SOFIA_CUDA(ctx, cudaMemset(s->col_count.p, 0, sizeof(int) * (s->ncols + 1)));
+    SOFIA_CUDA(ctx, cudaMemset(s->col_fill.p, 0, sizeof(int) * (s->ncols + 1)));
     SOFIA_CUDA(ctx, s->cl_start.ensure(sizeof(int) * (s->ncols + 1)));
     SOFIA_CUDA(ctx, s->col_atoms.ensure(sizeof(int) * n * 2));  // atoms + column of atom
     SOFIA_CUDA(ctx, s->col_key.ensure(sizeof(float) * n));
@@ -1044,20 +1054,16 @@ static void sys_build_bin(Sys *s, const int *cond) {
     const int cm = 1;
     int *col_of = s->col_atoms.as<int>() + n;
     int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
-    const int nslots = s->max_clusters * CL;
-    k_build_prep<<<grid_for(nslots, 256), 256, 0, st>>>(cond, cm, s->ncols + 1,
-                                                        s->col_count.as<int>(),
-                                                        s->col_fill.as<int>(), nslots,
-                                                        s->slot_orig.as<int>());
+    // col_count and col_fill start at zero (set at creation, cleared after each
+    // use); every slot of the new clusters is written by the column sort
     k_wrap_bin<<<grid_for(n, 256), 256, 0, st>>>(
         cond, cm, n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(), s->L,
         s->s_col, s->ncx, s->img[0].as<double>(), s->img[1].as<double>(), s->img[2].as<double>(),
         s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(), col_of,
         s->col_count.as<int>(), s->col_key.as<float>());
-    k_scan1<<<1, 1024, 0, st>>>(cond, cm, s->ncols, s->col_count.as<int>(),
-                                s->col_start.as<int>(), 0);
-    k_scan1<<<1, 1024, 0, st>>>(cond, cm, s->ncols, s->col_count.as<int>(),
-                                s->cl_start.as<int>(), 1);
+    k_scan_cols<<<1, 1024, 0, st>>>(cond, cm, s->ncols, s->col_count.as<int>(),
+                                    s->col_start.as<int>(), s->cl_start.as<int>(),
+                                    s->nclusters.as<int>());
     k_col_scatter<<<grid_for(n, 256), 256, 0, st>>>(cond, cm, n, col_of, s->col_start.as<int>(),
                                                     s->col_fill.as<int>(),
                                                     s->col_atoms.as<int>());
@@ -1065,10 +1071,8 @@ static void sys_build_bin(Sys *s, const int *cond) {
                                                 s->col_atoms.as<int>(), s->col_key.as<float>(),
                                                 s->cl_start.as<int>(), s->slot_orig.as<int>(),
                                                 cl_col, s->atom_slot.as<int>(),
-                                                s->status_local.as<int>());
-    k_set_ncl<<<1, 32, 0, st>>>(cond, cm, s->cl_start.as<int>() + s->ncols,
-                                s->nclusters.as<int>());
-    s->launches += 7;
+                                                s->col_fill.as<int>(), s->status_local.as<int>());
+    s->launches += 4;
 }
 
 // Part 2: cluster bounding boxes and the cluster-pair search.
@@ -1184,12 +1188,10 @@ static void sys_prune(Sys *s, const int *cond) {
         cond, 3, s->max_clusters, s->nclusters.as<int>(), s->recf.as<float4>(),
         s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,
         (float)s->L, rin2, s->ilist.as<int>(), s->imask.as<unsigned long long>(),
-        s->icount.as<int>());
-    k_copy3<<<grid_for(s->n, 256), 256, 0, st>>>(cond, 3, s->n, s->x[0].as<double>(),
-                                                 s->x[1].as<double>(), s->x[2].as<double>(),
-                                                 s->xprn[0].as<double>(), s->xprn[1].as<double>(),
-                                                 s->xprn[2].as<double>());
-    s->launches += 2;
+        s->icount.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(), s->x[1].as<double>(),
+        s->x[2].as<double>(), s->xprn[0].as<double>(), s->xprn[1].as<double>(),
+        s->xprn[2].as<double>());
+    s->launches += 1;
     if (!cond) s->n_prunes++;
 }
 
@@ -1251,7 +1253,8 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
 }
 
 // Pair kernel (+ energy reduction) on the pruned list.
-int sys_pair(Sys *s, int precision, bool energy, bool virial) {
+int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
+             const LangevinArgs *lg) {
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     PairConst k = make_pair_const(s, nullptr);
@@ -1286,10 +1289,13 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial) {
         s->pending_pair = 1;
     }
     const int nslots = s->max_clusters * CL;
+    LangevinArgs lgv{};
+    if (lg) lgv = *lg;
     k_unpack<<<grid_for(nslots, 256), 256, 0, st>>>(nslots, s->nclusters.as<int>(),
                                                     s->slot_orig.as<int>(),
                                                     s->fslot.as<long long>(), fx, fy, fz,
-                                                    ctx->d_status);
+                                                    ctx->d_status, count_flag,
+                                                    s->dcount.as<long long>(), lgv);
     s->launches += 2;
     if (energy || virial) {
         k_red_stage1<<<RED_BLOCKS, 256, 0, st>>>(s->max_clusters, 5, s->nclusters.as<int>(),
@@ -1308,7 +1314,7 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial) {
 // pair kernel.  Row-capacity overflow is recorded in status_local and checked
 // by the caller after the segment (sys_list_overflow).
 int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build,
-                    bool disp_done) {
+                    bool disp_done, const LangevinArgs *lg) {
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     const int n = s->n;
@@ -1327,9 +1333,9 @@ int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_
     int rc = sys_build(s, flag);
     if (rc) return rc;
     sys_prune(s, flag);
-    k_count_events<<<1, 32, 0, st>>>(flag, s->dcount.as<long long>());
-    s->launches += 3;
-    return sys_pair(s, precision, energy, virial);
+    s->launches += 1;
+    // the force unpack counts the build/prune events and clears the trigger word
+    return sys_pair(s, precision, energy, virial, flag, lg);
 }
 
 // After a device-only segment: SOFIA_ENEEDGROW (and a larger row capacity) if

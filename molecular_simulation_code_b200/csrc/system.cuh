@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "langevin.cuh"
 
 namespace sofia {
 
@@ -102,11 +103,15 @@ struct Sys {
 
 // evaluation entry points (mixed.cu)
 int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build);
-int sys_pair(Sys *s, int precision, bool energy, bool virial);
+// count_flag (may be NULL): the trigger word whose build/prune bits are counted
+// and then cleared; lg (may be NULL): Langevin force added to the pair forces.
+int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag = nullptr,
+             const LangevinArgs *lg = nullptr);
 // disp_done: the caller already ORed the displacement-trigger bits into a
 // cleared trigger word (the MD step's fused kick/drift kernel does).
+// lg (may be NULL): Langevin force added while the pair forces are written.
 int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build,
-                    bool disp_done = false);
+                    bool disp_done = false, const LangevinArgs *lg = nullptr);
 int sys_list_overflow(Sys *s);
 // Frees the captured drop-in force graphs (they bake in list pointers and the margin).
 void dropin_drop(Sys *s);
