@@ -39,6 +39,18 @@ constexpr int MAX_COL = 2048;
 #ifndef SOFIA_PAIR_MINB
 #define SOFIA_PAIR_MINB 4
 #endif
+#ifndef SOFIA_PAIR_MINB_EN
+#define SOFIA_PAIR_MINB_EN 4
+#endif
+#ifndef SOFIA_PAIR_HYBRID
+#define SOFIA_PAIR_HYBRID 1
+#endif
+#ifndef SOFIA_PRUNE_MINB
+#define SOFIA_PRUNE_MINB 4
+#endif
+#ifndef SOFIA_SEARCH_ZWIN
+#define SOFIA_SEARCH_ZWIN 1
+#endif
 constexpr int FLUSH = SOFIA_PAIR_FLUSH;  // j-clusters between FP32 -> fixed-point flushes
 
 __device__ __forceinline__ double wrap_shift(double x, double L) {
@@ -234,6 +246,8 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
     recf[s] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.0f);
 }
 
+// Cluster bounding boxes of the current records (FP64 bounds rounded outward
+// to float), for the cluster-pair search and the prune.
 __global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
                        const int *__restrict__ ncl_dev,
                        const AtomRec *__restrict__ rec, const int *__restrict__ slot_orig,
@@ -288,10 +302,39 @@ __device__ __forceinline__ bool half_keep(int ci, int cj, int img) {
     return img >= 13;
 }
 
+// z window of one column segment.  The clusters of a column are z-sorted, so
+// their bounding-box bounds are non-decreasing along the column (up to a few
+// ulp where float sort keys tie); the clusters whose z gap to the i box is at
+// least rw (rl plus a slack far above those ulp) form a prefix and a suffix of
+// [j0, j0 + len), found by binary search and cut off.  Each cut cluster has a
+// z gap >= rl, so the bounding-box test would reject it: the list is unchanged.
+__device__ __forceinline__ void z_window(const float4 *__restrict__ bb, float ilo_z, float ihi_z,
+                                         float sz, float rw, int &j0, int &len) {
+    int lo = 0, hi = len;
+    while (lo < hi) {  // first cluster with ilo.z - (hi.z + sz) < rw
+        const int mid = (lo + hi) >> 1;
+        if (ilo_z - (__ldg(&bb[2 * (j0 + mid) + 1].z) + sz) >= rw)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    const int first = lo;
+    hi = len;
+    while (lo < hi) {  // first cluster with (lo.z + sz) - ihi.z >= rw
+        const int mid = (lo + hi) >> 1;
+        if ((__ldg(&bb[2 * (j0 + mid)].z) + sz) - ihi_z >= rw)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    j0 += first;
+    len = lo - first;
+}
+
 // One warp per i-cluster: visit the xy columns within reach (periodic images
-// included), test every cluster's bounding box in three z images, compact the
-// accepted (cluster, image) pairs of the half list in visiting order and
-// attach the pair mask.
+// included) in three z images, cut each column image to its z window, test the
+// remaining clusters' bounding boxes, compact the accepted (cluster, image)
+// pairs of the half list in visiting order and attach the pair mask.
 __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
     if (a.cond && !(a.cond[0] & a.cmask)) return;
     const int lane = threadIdx.x & 31;
@@ -357,6 +400,7 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
                 j0 = a.cl_start[cx + cy * a.ncx];
                 len = a.cl_start[cx + cy * a.ncx + 1] - j0;
                 imgk = (imx + 1) + 3 * (imy + 1) + 9 * (imz + 1);
+                if (SOFIA_SEARCH_ZWIN) z_window(a.bb, ilo.z, ihi.z, sz, a.rl + 1e-3f, j0, len);
             }
         }
         const bool has = len > 0;
@@ -468,6 +512,8 @@ __global__ void k_disp_check(int n, const double *__restrict__ x, const double *
 struct PairConst {
     float rcut2, cut_coulsq, kexp, pa, c2a, e_shift, f_shift, coulpre;
     float A1, A2, A3, A4, A5;
+    // the same FP32 constants duplicated as {c, c} operands of packed FP32x2 math
+    float2 kexp2, pa2, c2a2, e_shift2, f_shift2, A1_2, A2_2, A3_2, A4_2, A5_2;
     double rcut2d, cut_coulsqd, alphad, e_shiftd, f_shiftd, coulpred, MY_PIS_INV;
     double A1d, A2d, A3d, A4d, A5d, EWALD_Pd;
     double L;
@@ -559,6 +605,61 @@ struct PairMath<double> {
     }
 };
 
+// Packed FP32x2 form of PairMath<float> for the two pairs a lane owns in one
+// list entry (component x: j atom lj, component y: j atom lj + 4).  sm_100
+// issues one FFMA2 / FMUL2 / FADD2 instruction for both components, so the
+// pair arithmetic takes half the issue slots; only the MUFU operations, the
+// range tests and the selects stay per component.  Each component goes
+// through the same operations, in the same order and rounding, as
+// PairMath<float>::eval.  The LJ operands arrive as {lj1, -lj2, lj3, -lj4}.
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    return __ffma2_rn(a, b, c);
+}
+
+struct PairMath2 {
+    template <bool EN, bool SAME>
+    __device__ __forceinline__ static float2 eval(float2 dx, float2 dy, float2 dz, float2 qq,
+                                                  float4 lj0, float4 lj1, bool on0, bool on1,
+                                                  const PairConst &k, float2 &elj, float2 &ec) {
+        const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+        const float2 rinv = make_float2(rsqrt_a(r2.x), rsqrt_a(r2.y));
+        const float2 r2inv = mul2(rinv, rinv);
+        const float2 r = mul2(r2, rinv);
+        const float2 dr6i = mul2(mul2(r2inv, r2inv), r2inv);
+        const bool lj0_on = on0 && r2.x <= k.rcut2, lj1_on = on1 && r2.y <= k.rcut2;
+        const bool c0_on = SAME ? lj0_on : (on0 && r2.x <= k.cut_coulsq);
+        const bool c1_on = SAME ? lj1_on : (on1 && r2.y <= k.cut_coulsq);
+        const float2 flj =
+            mul2(dr6i, fma2(make_float2(lj0.x, lj1.x), dr6i, make_float2(lj0.y, lj1.y)));
+        const float2 pref = mul2(qq, rinv);
+        const float2 kr = mul2(k.kexp2, r2);
+        const float2 ex = make_float2(ex2_a(kr.x), ex2_a(kr.y));
+        const float2 u = fma2(k.pa2, r, make_float2(1.0f, 1.0f));
+        const float2 t = make_float2(rcp_a(u.x), rcp_a(u.y));
+        const float2 poly =
+            fma2(t, fma2(t, fma2(t, fma2(t, k.A5_2, k.A4_2), k.A3_2), k.A2_2), k.A1_2);
+        const float2 erfcc = mul2(mul2(t, poly), ex);
+        const float2 fc = mul2(pref, fma2(k.f_shift2, r2, fma2(mul2(k.c2a2, ex), r, erfcc)));
+        if (EN) {
+            const float2 e6 =
+                mul2(dr6i, fma2(dr6i, make_float2(lj0.z, lj1.z), make_float2(lj0.w, lj1.w)));
+            const float2 sh = fma2(r, k.e_shift2, mul2(r2, k.f_shift2));
+            const float2 e1 = mul2(pref, fma2(sh, make_float2(-1.0f, -1.0f), erfcc));
+            elj = make_float2(lj0_on ? e6.x : 0.0f, lj1_on ? e6.y : 0.0f);
+            ec = make_float2(c0_on ? e1.x : 0.0f, c1_on ? e1.y : 0.0f);
+        }
+        if (SAME) {
+            const float2 fs = mul2(add2(fc, flj), r2inv);
+            return make_float2(lj0_on ? fs.x : 0.0f, lj1_on ? fs.y : 0.0f);
+        }
+        const float2 fcm = make_float2(c0_on ? fc.x : 0.0f, c1_on ? fc.y : 0.0f);
+        const float2 fljm = make_float2(lj0_on ? flj.x : 0.0f, lj1_on ? flj.y : 0.0f);
+        return mul2(add2(fcm, fljm), r2inv);
+    }
+};
+
 template <typename T>
 __device__ __forceinline__ long long to_fix(T v);
 template <>
@@ -610,14 +711,19 @@ __device__ __forceinline__ T reduce_scatter_j(const T (&v)[6], int lane) {
 //     order of the atomics, so results stay bit-reproducible.
 // EN adds the LJ and Coulomb energies, VIR the diagonal virial (each pair once).
 template <typename T, bool EN, bool VIR, bool SAME>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? SOFIA_PAIR_MINB : 2) k_pair(
+__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2) k_pair(
     int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
     const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
     unsigned long long *__restrict__ fslot, double *__restrict__ energy) {
     extern __shared__ float4 s_lj[];
     __shared__ double s_sh[27 * 3];
-    for (int t = threadIdx.x; t < k.ntypes * k.ntypes; t += blockDim.x) s_lj[t] = ljtab[t];
+    // FP32x2 path: lj2 and lj4 enter the packed FMAs as addends, stored negated
+    constexpr bool PACK = sizeof(T) == 4;
+    for (int t = threadIdx.x; t < k.ntypes * k.ntypes; t += blockDim.x) {
+        const float4 l = ljtab[t];
+        s_lj[t] = PACK ? make_float4(l.x, -l.y, l.z, -l.w) : l;
+    }
     if (threadIdx.x < 27) {
         const int im = threadIdx.x;
         s_sh[im * 3 + 0] = (double)(im % 3 - 1) * k.L;
@@ -642,6 +748,10 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? SOFIA_PAIR_MINB : 2) k
     const unsigned long long *mrow = jmask + (size_t)icl * jcap;
     T ax = 0, ay = 0, az = 0;
     T a_lj = 0, a_c = 0, a_xx = 0, a_yy = 0, a_zz = 0;
+    // packed accumulators of the FP32x2 path (component per j half)
+    const float2 z2 = make_float2(0.0f, 0.0f);
+    float2 ax2 = z2, ay2 = z2, az2 = z2, alj2 = z2, ac2 = z2, axx2 = z2, ayy2 = z2, azz2 = z2;
+    const float2 qiq2 = make_float2((float)qiq, (float)qiq);
     long long lx = 0, ly = 0, lz = 0;
     double e_lj = 0.0, e_c = 0.0, vxx = 0.0, vyy = 0.0, vzz = 0.0;
     for (int base = 0; base < n; base += 32) {
@@ -657,6 +767,71 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? SOFIA_PAIR_MINB : 2) k
             const double yis = ri.y - s_sh[img * 3 + 1];
             const double zis = ri.z - s_sh[img * 3 + 2];
             T v[6] = {0, 0, 0, 0, 0, 0};
+            const unsigned m0 = (unsigned)mm, m1 = (unsigned)(mm >> 32);
+            if (PACK && SOFIA_PAIR_HYBRID && (m0 == 0u || m1 == 0u)) {
+                // one j half without pairs in range: scalar evaluation of the other
+                const int h = m0 ? 0 : 1;
+                const AtomRec rj = rec[jc * CL + lj + 4 * h];
+                const float dx = (float)(xis - rj.x);
+                const float dy = (float)(yis - rj.y);
+                const float dz = (float)(zis - rj.z);
+                const float4 l = s_lj[ti + rj.type];
+                float elj = 0.0f, ec = 0.0f;
+                const float fs = PairMath<float>::template eval<EN, SAME>(
+                    dx, dy, dz, (float)qiq * rj.q, make_float4(l.x, -l.y, l.z, -l.w),
+                    ((m0 | m1) >> lane) & 1u, k, elj, ec);
+                const float px = dx * fs, py = dy * fs, pz = dz * fs;
+                ax2.x += px;
+                ay2.x += py;
+                az2.x += pz;
+                v[0] = h ? 0.0f : px;
+                v[1] = h ? 0.0f : py;
+                v[2] = h ? 0.0f : pz;
+                v[3] = h ? px : 0.0f;
+                v[4] = h ? py : 0.0f;
+                v[5] = h ? pz : 0.0f;
+                if (EN) {
+                    alj2.x += elj;
+                    ac2.x += ec;
+                }
+                if (VIR) {
+                    axx2.x += dx * px;
+                    ayy2.x += dy * py;
+                    azz2.x += dz * pz;
+                }
+            } else if constexpr (PACK) {
+                // both j halves at once; a half without pairs in range is computed
+                // and masked (the packed instructions cost the same for one or two)
+                const AtomRec r0 = rec[jc * CL + lj], r1 = rec[jc * CL + lj + 4];
+                const float2 dx = make_float2((float)(xis - r0.x), (float)(xis - r1.x));
+                const float2 dy = make_float2((float)(yis - r0.y), (float)(yis - r1.y));
+                const float2 dz = make_float2((float)(zis - r0.z), (float)(zis - r1.z));
+                const float2 qq = mul2(qiq2, make_float2(r0.q, r1.q));
+                const bool on0 = ((unsigned)mm >> lane) & 1u;
+                const bool on1 = ((unsigned)(mm >> 32) >> lane) & 1u;
+                float2 elj = z2, ec = z2;
+                const float2 fs = PairMath2::template eval<EN, SAME>(
+                    dx, dy, dz, qq, s_lj[ti + r0.type], s_lj[ti + r1.type], on0, on1, k, elj, ec);
+                const float2 px = mul2(dx, fs), py = mul2(dy, fs), pz = mul2(dz, fs);
+                ax2 = add2(ax2, px);
+                ay2 = add2(ay2, py);
+                az2 = add2(az2, pz);
+                v[0] = px.x;
+                v[1] = py.x;
+                v[2] = pz.x;
+                v[3] = px.y;
+                v[4] = py.y;
+                v[5] = pz.y;
+                if (EN) {
+                    alj2 = add2(alj2, elj);
+                    ac2 = add2(ac2, ec);
+                }
+                if (VIR) {
+                    axx2 = fma2(dx, px, axx2);
+                    ayy2 = fma2(dy, py, ayy2);
+                    azz2 = fma2(dz, pz, azz2);
+                }
+            } else
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 // pruned mask, lane layout: bit h*32 + lane; a j half with no pair in
@@ -694,6 +869,23 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? SOFIA_PAIR_MINB : 2) k
             if (jcomp < 3 && fj != (T)0)
                 atomicAdd(jdst + jc * CL + jslot, (unsigned long long)(-to_fix<T>(fj)));
             if (((base + e) & (FLUSH - 1)) == FLUSH - 1) {
+                if constexpr (PACK) {
+                    ax = ax2.x + ax2.y;
+                    ay = ay2.x + ay2.y;
+                    az = az2.x + az2.y;
+                    ax2 = ay2 = az2 = z2;
+                    if (EN) {
+                        e_lj += (double)alj2.x + (double)alj2.y;
+                        e_c += (double)ac2.x + (double)ac2.y;
+                        alj2 = ac2 = z2;
+                    }
+                    if (VIR) {
+                        vxx += (double)axx2.x + (double)axx2.y;
+                        vyy += (double)ayy2.x + (double)ayy2.y;
+                        vzz += (double)azz2.x + (double)azz2.y;
+                        axx2 = ayy2 = azz2 = z2;
+                    }
+                }
                 lx += to_fix<T>(ax);
                 ly += to_fix<T>(ay);
                 lz += to_fix<T>(az);
@@ -710,6 +902,20 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? SOFIA_PAIR_MINB : 2) k
                     a_xx = a_yy = a_zz = 0;
                 }
             }
+        }
+    }
+    if constexpr (PACK) {
+        ax = ax2.x + ax2.y;
+        ay = ay2.x + ay2.y;
+        az = az2.x + az2.y;
+        if (EN) {
+            e_lj += (double)alj2.x + (double)alj2.y;
+            e_c += (double)ac2.x + (double)ac2.y;
+        }
+        if (VIR) {
+            vxx += (double)axx2.x + (double)axx2.y;
+            vyy += (double)ayy2.x + (double)ayy2.y;
+            vzz += (double)azz2.x + (double)azz2.y;
         }
     }
     lx += to_fix<T>(ax);
@@ -809,14 +1015,16 @@ __device__ __forceinline__ unsigned long long transpose8(unsigned long long x) {
 // (checked like the rebuild trigger): a pair out of range now cannot come
 // within rc before the next prune.  One warp per i-cluster, one lane per list
 // entry: the i atoms sit in registers and every lane checks its entry's 64
-// pairs, so entries need no shuffles or ballots.  Distances here only select
+// pairs (two i atoms per packed FP32x2 operation), so entries need no shuffles
+// or ballots.  Distances here only select
 // pairs, so FP32 copies of the positions suffice (the squared radius carries a
 // 1e-3 A^2 safety margin).
-__global__ void __launch_bounds__(256) k_prune(
+__global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
     const int *__restrict__ cond, int cmask, int maxcl, const int *__restrict__ ncl_dev,
     const float4 *__restrict__ recf,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
-    const int *__restrict__ jcount, int jcap, float L, float rin2, int *__restrict__ ilist,
+    const int *__restrict__ jcount, int jcap, float L, float rin2, float rfar2,
+    const float4 *__restrict__ bb, int *__restrict__ ilist,
     unsigned long long *__restrict__ imask, int *__restrict__ icount,
     const int *__restrict__ slot_orig, const double *__restrict__ x,
     const double *__restrict__ y, const double *__restrict__ z, double *__restrict__ px,
@@ -842,14 +1050,16 @@ __global__ void __launch_bounds__(256) k_prune(
             pz[o] = z[o];
         }
     }
-    float xi[CL], yi[CL], zi[CL];
+    // i atoms 2p and 2p + 1 as the two components of packed FP32x2 operands
+    float2 xi[CL / 2], yi[CL / 2], zi[CL / 2];
 #pragma unroll
-    for (int ii = 0; ii < CL; ++ii) {
-        const float4 p = recf[icl * CL + ii];
-        xi[ii] = p.x;
-        yi[ii] = p.y;
-        zi[ii] = p.z;
+    for (int pp = 0; pp < CL / 2; ++pp) {
+        const float4 p0 = recf[icl * CL + 2 * pp], p1 = recf[icl * CL + 2 * pp + 1];
+        xi[pp] = make_float2(p0.x, p1.x);
+        yi[pp] = make_float2(p0.y, p1.y);
+        zi[pp] = make_float2(p0.z, p1.z);
     }
+    const float4 ilo = bb[2 * icl], ihi = bb[2 * icl + 1];
     const int n = jcount[icl];
     const int *row = jlist + (size_t)icl * jcap;
     const unsigned long long *mrow = jmask + (size_t)icl * jcap;
@@ -866,16 +1076,29 @@ __global__ void __launch_bounds__(256) k_prune(
             const int jc = w & ((1 << IMG_SHIFT) - 1);
             const int img = w >> IMG_SHIFT;
             const float sx = s_shf[img * 3 + 0], sy = s_shf[img * 3 + 1], sz = s_shf[img * 3 + 2];
+            // bounding boxes at the current positions: an entry whose boxes are
+            // farther apart than rfar (above r_in by far more than rounding) has
+            // no pair in range, and its atoms are not loaded
+            const float4 jlo = bb[2 * jc], jhi = bb[2 * jc + 1];
+            const float gx = gap(ilo.x, ihi.x, jlo.x + sx, jhi.x + sx);
+            const float gy = gap(ilo.y, ihi.y, jlo.y + sy, jhi.y + sy);
+            const float gz = gap(ilo.z, ihi.z, jlo.z + sz, jhi.z + sz);
+            if (gx * gx + gy * gy + gz * gz <= rfar2)
 #pragma unroll
             for (int jj = 0; jj < CL; ++jj) {
                 const float4 pj = recf[jc * CL + jj];
-                const float xs = pj.x + sx, ys = pj.y + sy, zs = pj.z + sz;
+                // -(x_j + shift): adding it rounds exactly like x_i - (x_j + shift)
+                const float nx = -(pj.x + sx), ny = -(pj.y + sy), nz = -(pj.z + sz);
+                const float2 nx2 = make_float2(nx, nx), ny2 = make_float2(ny, ny),
+                             nz2 = make_float2(nz, nz);
 #pragma unroll
-                for (int ii = 0; ii < CL; ++ii) {
-                    const float dx = xi[ii] - xs, dy = yi[ii] - ys, dz = zi[ii] - zs;
-                    const bool in = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rin2;
-                    if (jj < 4) lo |= in ? (1u << (8 * jj + ii)) : 0u;
-                    else hi |= in ? (1u << (8 * (jj - 4) + ii)) : 0u;
+                for (int pp = 0; pp < CL / 2; ++pp) {
+                    const float2 dx = add2(xi[pp], nx2), dy = add2(yi[pp], ny2),
+                                 dz = add2(zi[pp], nz2);
+                    const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+                    const unsigned in = (r2.x < rin2 ? 1u : 0u) | (r2.y < rin2 ? 2u : 0u);
+                    if (jj < 4) lo |= in << (8 * jj + 2 * pp);
+                    else hi |= in << (8 * (jj - 4) + 2 * pp);
                 }
             }
         }
@@ -1081,8 +1304,9 @@ static int sys_build_search(Sys *s, const int *cond) {
     cudaStream_t st = ctx->stream;
     const int cm = 1;
     int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
+    // the boxes serve the search (trigger bit 0) and the prune (bit 1)
     k_bbox<<<grid_for(s->max_clusters, 128), 128, 0, st>>>(
-        cond, cm, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
+        cond, 3, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
         s->slot_orig.as<int>(), s->bb.as<float4>());
     SearchArgs a;
     a.cond = cond;
@@ -1173,6 +1397,16 @@ static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
     k.A3 = 1.421413741f;
     k.A4 = -1.453152027f;
     k.A5 = 1.061405429f;
+    k.kexp2 = make_float2(k.kexp, k.kexp);
+    k.pa2 = make_float2(k.pa, k.pa);
+    k.c2a2 = make_float2(k.c2a, k.c2a);
+    k.e_shift2 = make_float2(k.e_shift, k.e_shift);
+    k.f_shift2 = make_float2(k.f_shift, k.f_shift);
+    k.A1_2 = make_float2(k.A1, k.A1);
+    k.A2_2 = make_float2(k.A2, k.A2);
+    k.A3_2 = make_float2(k.A3, k.A3);
+    k.A4_2 = make_float2(k.A4, k.A4);
+    k.A5_2 = make_float2(k.A5, k.A5);
     k.L = s->L;
     k.ntypes = s->ntypes;
     return k;
@@ -1180,14 +1414,24 @@ static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
 
 // Launches: displacement check, conditional rebuild, pack, pair kernel.
 // `force_build` rebuilds regardless of the trigger.
-static void sys_prune(Sys *s, const int *cond) {
+// bb_current: the cluster boxes were computed from the current records (by
+// the build of this evaluation, or by its conditional box kernel).
+static void sys_prune(Sys *s, const int *cond, bool bb_current) {
     cudaStream_t st = s->ctx->stream;
     const float rin = (float)(s->rc + s->margin);
     const float rin2 = rin * rin + 1e-3f;
+    const float rfar = rin + 0.01f;
+    if (!bb_current) {
+        k_bbox<<<grid_for(s->max_clusters, 128), 128, 0, st>>>(
+            cond, 3, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
+            s->slot_orig.as<int>(), s->bb.as<float4>());
+        s->launches += 1;
+    }
     k_prune<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(
         cond, 3, s->max_clusters, s->nclusters.as<int>(), s->recf.as<float4>(),
         s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,
-        (float)s->L, rin2, s->ilist.as<int>(), s->imask.as<unsigned long long>(),
+        (float)s->L, rin2, rfar * rfar, s->bb.as<float4>(), s->ilist.as<int>(),
+        s->imask.as<unsigned long long>(),
         s->icount.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(), s->x[1].as<double>(),
         s->x[2].as<double>(), s->xprn[0].as<double>(), s->xprn[1].as<double>(),
         s->xprn[2].as<double>());
@@ -1248,7 +1492,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
         }
         break;
     }
-    if (prune) sys_prune(s, nullptr);
+    if (prune) sys_prune(s, nullptr, build);
     return sys_pair(s, precision, energy, virial);
 }
 
@@ -1332,7 +1576,7 @@ int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_
     }
     int rc = sys_build(s, flag);
     if (rc) return rc;
-    sys_prune(s, flag);
+    sys_prune(s, flag, true);
     s->launches += 1;
     // the force unpack counts the build/prune events and clears the trigger word
     return sys_pair(s, precision, energy, virial, flag, lg);
