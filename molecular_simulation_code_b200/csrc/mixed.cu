@@ -2,21 +2,22 @@
 //
 // The reference evaluates LJ + damped-shifted-force Coulomb over a full
 // per-atom Verlet list in FP64 (Source/mod_force_nonbond.f90:105-196).  Here
-// atoms are grouped into clusters of 8 (xy columns, sorted by z) and the list
-// holds, for every i-cluster, the j-clusters whose bounding boxes come within
-// rlist = rc + skin, each with a 64-bit mask of the interacting atom pairs
-// (padding, self pairs and 1-2/1-3/1-4 exclusions removed).  One warp works on
-// one i-cluster: lane = (i atom, j half) covers the 8x8 pair tile in two passes,
-// the i force stays in registers and no j force is ever written, so the kernel
-// needs no atomics.  Positions are FP64 in HBM; each pair displacement is
-// formed in FP64 and rounded to FP32 (mixed) or kept in FP64 (plain FP64
-// twin); per-lane sums are flushed to 64-bit fixed point (2^-32 kcal/mol/A)
-// and combined across lanes in integers, so forces are bit-reproducible and
-// independent of summation order across lanes.
+// atoms are grouped into clusters of 8 (xy columns, sorted by z) and the half
+// list holds each cluster pair whose bounding boxes come within
+// rlist = rc + skin once, with a 64-bit mask of the interacting atom pairs
+// (padding, self pairs and 1-2/1-3/1-4 exclusions removed).  A prune keeps the
+// entries with pairs inside rc + margin and their in-range bits.  One warp
+// works on one i-cluster: lane = (i atom, j atom pair) covers the 8x8 pair
+// tile, the i force stays in registers and each entry's j forces are reduced
+// over lanes and added with 64-bit fixed-point atomics.  Positions are FP64 in
+// HBM; each pair displacement is formed in FP64 and rounded to FP32 (mixed) or
+// kept in FP64 (plain FP64 twin); FP32 partial sums are flushed to 64-bit fixed
+// point (2^-32 kcal/mol/A), so forces are bit-reproducible and independent of
+// the order of the atomics.
 //
 // The list stays valid while no atom has moved more than skin/2 since the
-// build (checked every evaluation on the device; the reference triggers at the
-// full skin, Source/mod_neighbor.f90:895-913).
+// build (checked every step on the device; the reference triggers at the full
+// skin, Source/mod_neighbor.f90:895-913).
 #include <cmath>
 #include <vector>
 
