@@ -41,6 +41,9 @@ class Batch:
         h = C.c_void_p()
         ctx.check(ctx._lib.sofia_batch_create(ctx.handle, arr, len(self.systems), C.byref(h)))
         self.handle = h
+        ctx.adopt(self)
+
+    close_rank = 0  # a batch is destroyed before the systems it steps
 
     def run(self, nsteps: int, energy_every: int = 0):
         e = np.zeros((len(self.systems), SOFIA_MD_NE))

@@ -27,7 +27,11 @@ extern "C" int sofia_nb_create(const sofia_nb_params *params, sofia_nb_ctx **out
         sofia_nb_destroy(ctx);
         return SOFIA_ECUDA;
     }
-    cudaMemset(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS);
+    if (cudaMemset(ctx->d_status, 0, sizeof(int32_t) * sofia::ST_NSLOTS) != cudaSuccess) {
+        cudaGetLastError();
+        sofia_nb_destroy(ctx);
+        return SOFIA_ECUDA;
+    }
     *out = ctx;
     return SOFIA_OK;
 }

@@ -85,17 +85,24 @@ inline int fail(sofia_nb_ctx *ctx, int code, const char *fmt, const char *a = ""
     return code;
 }
 
-inline int cuda_fail(sofia_nb_ctx *ctx, cudaError_t e, const char *where) {
+inline int cuda_fail(sofia_nb_ctx *ctx, cudaError_t e, const char *where,
+                     const char *file = nullptr, int line = 0) {
     char buf[512];
-    snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
+    if (file) {
+        const char *base = strrchr(file, '/');
+        snprintf(buf, sizeof(buf), "%s: %s (%s:%d)", where, cudaGetErrorString(e),
+                 base ? base + 1 : file, line);
+    } else {
+        snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
+    }
     if (ctx) ctx->last_error = buf;
     return SOFIA_ECUDA;
 }
 
-#define SOFIA_CUDA(ctx, call)                                              \
-    do {                                                                   \
-        cudaError_t _e = (call);                                           \
-        if (_e != cudaSuccess) return sofia::cuda_fail((ctx), _e, #call);  \
+#define SOFIA_CUDA(ctx, call)                                                                \
+    do {                                                                                     \
+        cudaError_t _e = (call);                                                             \
+        if (_e != cudaSuccess) return sofia::cuda_fail((ctx), _e, #call, __FILE__, __LINE__); \
     } while (0)
 
 // True when p is device (or managed) memory; host pointers are staged.

@@ -19,6 +19,7 @@
 // build (checked every step on the device; the reference triggers at the full
 // skin, Source/mod_neighbor.f90:895-913).
 #include <cmath>
+#include <algorithm>
 #include <vector>
 
 #include "system.cuh"
@@ -538,6 +539,17 @@ __device__ __forceinline__ float ex2_a(float x) {
     return y;
 }
 
+// Separately rounded operations.  Every product, sum and fused multiply-add of
+// the pair arithmetic is written out, so the compiler cannot fuse a product
+// into a later addition in one template instance and not in another: the
+// force-only and energy kernels then give bit-identical forces.
+__device__ __forceinline__ float mulr(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mulr(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float addr(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double addr(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fmar(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmar(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 template <typename T>
 struct PairMath;
 
@@ -552,27 +564,28 @@ struct PairMath<float> {
     __device__ __forceinline__ static float eval(float dx, float dy, float dz, float qiq,
                                                  float4 lj, bool on, const PairConst &k,
                                                  float &elj, float &ec) {
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float r2 = fmar(dx, dx, fmar(dy, dy, mulr(dz, dz)));
         const float rinv = rsqrt_a(r2);
-        const float r2inv = rinv * rinv;
-        const float r = r2 * rinv;
-        const float dr6i = r2inv * r2inv * r2inv;
+        const float r2inv = mulr(rinv, rinv);
+        const float r = mulr(r2, rinv);
+        const float dr6i = mulr(mulr(r2inv, r2inv), r2inv);
         const bool lj_on = on && r2 <= k.rcut2;
         const bool c_on = SAME ? lj_on : (on && r2 <= k.cut_coulsq);
-        const float flj = dr6i * fmaf(lj.x, dr6i, -lj.y);
-        const float pref = qiq * rinv;
-        const float ex = ex2_a(k.kexp * r2);
-        const float t = rcp_a(fmaf(k.pa, r, 1.0f));
-        const float poly = fmaf(t, fmaf(t, fmaf(t, fmaf(t, k.A5, k.A4), k.A3), k.A2), k.A1);
-        const float erfcc = t * poly * ex;
-        const float fc = pref * fmaf(k.f_shift, r2, fmaf(k.c2a * ex, r, erfcc));
+        const float flj = mulr(dr6i, fmar(lj.x, dr6i, -lj.y));
+        const float pref = mulr(qiq, rinv);
+        const float ex = ex2_a(mulr(k.kexp, r2));
+        const float t = rcp_a(fmar(k.pa, r, 1.0f));
+        const float poly = fmar(t, fmar(t, fmar(t, fmar(t, k.A5, k.A4), k.A3), k.A2), k.A1);
+        const float erfcc = mulr(mulr(t, poly), ex);
+        const float fc = mulr(pref, fmar(k.f_shift, r2, fmar(mulr(k.c2a, ex), r, erfcc)));
         if (EN) {
             // selects, not products: masked pairs may hold inf/NaN (r = 0)
-            elj = lj_on ? dr6i * fmaf(dr6i, lj.z, -lj.w) : 0.0f;
-            ec = c_on ? pref * (erfcc - fmaf(r, k.e_shift, r2 * k.f_shift)) : 0.0f;
+            elj = lj_on ? mulr(dr6i, fmar(dr6i, lj.z, -lj.w)) : 0.0f;
+            ec = c_on ? mulr(pref, fmar(fmar(r, k.e_shift, mulr(r2, k.f_shift)), -1.0f, erfcc))
+                      : 0.0f;
         }
-        if (SAME) return lj_on ? (fc + flj) * r2inv : 0.0f;
-        const float fs = ((c_on ? fc : 0.0f) + (lj_on ? flj : 0.0f)) * r2inv;
+        if (SAME) return lj_on ? mulr(addr(fc, flj), r2inv) : 0.0f;
+        const float fs = mulr(addr(c_on ? fc : 0.0f, lj_on ? flj : 0.0f), r2inv);
         return on ? fs : 0.0f;
     }
 };
@@ -583,25 +596,31 @@ struct PairMath<double> {
     __device__ __forceinline__ static double eval(double dx, double dy, double dz, double qiq,
                                                   float4 lj, bool on, const PairConst &k,
                                                   double &elj, double &ec) {
-        const double r2 = dx * dx + dy * dy + dz * dz;
+        // the reference's expressions and order, each operation rounded on its own
+        const double r2 = addr(addr(mulr(dx, dx), mulr(dy, dy)), mulr(dz, dz));
         const double r = sqrt(r2);
         const double rinv = 1.0 / r;
         const double r2inv = 1.0 / r2;
-        const double dr6i = r2inv * r2inv * r2inv;
+        const double dr6i = mulr(mulr(r2inv, r2inv), r2inv);
         const bool lj_on = on && r2 <= k.rcut2d;
         const bool c_on = on && r2 <= k.cut_coulsqd;
-        const double flj = dr6i * ((double)lj.x * dr6i - (double)lj.y);
-        const double pref = qiq * rinv;
-        const double ex = exp(-((k.alphad * k.alphad) * r) * r);
-        const double t = 1.0 / (1.0 + (k.EWALD_Pd * k.alphad) * r);
-        const double erfcc = t * (k.A1d + t * (k.A2d + t * (k.A3d + t * (k.A4d + t * k.A5d)))) * ex;
-        const double fc =
-            pref * (erfcc * rinv + ((2.0 * k.alphad) * k.MY_PIS_INV) * ex + r * k.f_shiftd) * r;
+        const double flj = mulr(dr6i, addr(mulr((double)lj.x, dr6i), -(double)lj.y));
+        const double pref = mulr(qiq, rinv);
+        const double ex = exp(-mulr(mulr(mulr(k.alphad, k.alphad), r), r));
+        const double t = 1.0 / addr(1.0, mulr(mulr(k.EWALD_Pd, k.alphad), r));
+        const double poly = addr(k.A1d, mulr(t, addr(k.A2d, mulr(t, addr(k.A3d,
+                            mulr(t, addr(k.A4d, mulr(t, k.A5d))))))));
+        const double erfcc = mulr(mulr(t, poly), ex);
+        const double c2a = mulr(mulr(2.0, k.alphad), k.MY_PIS_INV);
+        const double fc = mulr(mulr(pref, addr(addr(mulr(erfcc, rinv), mulr(c2a, ex)),
+                                               mulr(r, k.f_shiftd))), r);
         if (EN) {
-            elj = lj_on ? dr6i * (dr6i * (double)lj.z - (double)lj.w) : 0.0;
-            ec = c_on ? pref * ((erfcc - r * k.e_shiftd) - r2 * k.f_shiftd) : 0.0;
+            elj = lj_on ? mulr(dr6i, addr(mulr(dr6i, (double)lj.z), -(double)lj.w)) : 0.0;
+            ec = c_on ? mulr(pref, addr(addr(erfcc, -mulr(r, k.e_shiftd)),
+                                        -mulr(r2, k.f_shiftd)))
+                      : 0.0;
         }
-        const double fs = ((c_on ? fc : 0.0) + (lj_on ? flj : 0.0)) * r2inv;
+        const double fs = mulr(addr(c_on ? fc : 0.0, lj_on ? flj : 0.0), r2inv);
         return on ? fs : 0.0;
     }
 };
@@ -612,7 +631,8 @@ struct PairMath<double> {
 // pair arithmetic takes half the issue slots; only the MUFU operations, the
 // range tests and the selects stay per component.  Each component goes
 // through the same operations, in the same order and rounding, as
-// PairMath<float>::eval.  The LJ operands arrive as {lj1, -lj2, lj3, -lj4}.
+// PairMath<float>::eval.  The LJ operands arrive as a = {lj1, -lj2} and
+// b = {lj3, -lj4} (b read only for energies).
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
@@ -622,7 +642,8 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
 struct PairMath2 {
     template <bool EN, bool SAME>
     __device__ __forceinline__ static float2 eval(float2 dx, float2 dy, float2 dz, float2 qq,
-                                                  float4 lj0, float4 lj1, bool on0, bool on1,
+                                                  float2 a0, float2 a1, float2 b0, float2 b1,
+                                                  bool on0, bool on1,
                                                   const PairConst &k, float2 &elj, float2 &ec) {
         const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
         const float2 rinv = make_float2(rsqrt_a(r2.x), rsqrt_a(r2.y));
@@ -633,7 +654,7 @@ struct PairMath2 {
         const bool c0_on = SAME ? lj0_on : (on0 && r2.x <= k.cut_coulsq);
         const bool c1_on = SAME ? lj1_on : (on1 && r2.y <= k.cut_coulsq);
         const float2 flj =
-            mul2(dr6i, fma2(make_float2(lj0.x, lj1.x), dr6i, make_float2(lj0.y, lj1.y)));
+            mul2(dr6i, fma2(make_float2(a0.x, a1.x), dr6i, make_float2(a0.y, a1.y)));
         const float2 pref = mul2(qq, rinv);
         const float2 kr = mul2(k.kexp2, r2);
         const float2 ex = make_float2(ex2_a(kr.x), ex2_a(kr.y));
@@ -645,7 +666,7 @@ struct PairMath2 {
         const float2 fc = mul2(pref, fma2(k.f_shift2, r2, fma2(mul2(k.c2a2, ex), r, erfcc)));
         if (EN) {
             const float2 e6 =
-                mul2(dr6i, fma2(dr6i, make_float2(lj0.z, lj1.z), make_float2(lj0.w, lj1.w)));
+                mul2(dr6i, fma2(dr6i, make_float2(b0.x, b1.x), make_float2(b0.y, b1.y)));
             const float2 sh = fma2(r, k.e_shift2, mul2(r2, k.f_shift2));
             const float2 e1 = mul2(pref, fma2(sh, make_float2(-1.0f, -1.0f), erfcc));
             elj = make_float2(lj0_on ? e6.x : 0.0f, lj1_on ? e6.y : 0.0f);
@@ -718,12 +739,22 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
     const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
     unsigned long long *__restrict__ fslot, double *__restrict__ energy) {
     extern __shared__ float4 s_lj[];
+    // FP32 path: the same bytes as two float2 tables, {lj1, -lj2} and {lj3, -lj4},
+    // so a force-only lookup reads 8 bytes (fewer shared-memory wavefronts)
+    float2 *s_lja = reinterpret_cast<float2 *>(s_lj);
+    float2 *s_ljb = s_lja + k.ntypes * k.ntypes;
+
     __shared__ double s_sh[27 * 3];
     // FP32x2 path: lj2 and lj4 enter the packed FMAs as addends, stored negated
     constexpr bool PACK = sizeof(T) == 4;
     for (int t = threadIdx.x; t < k.ntypes * k.ntypes; t += blockDim.x) {
         const float4 l = ljtab[t];
-        s_lj[t] = PACK ? make_float4(l.x, -l.y, l.z, -l.w) : l;
+        if (PACK) {
+            s_lja[t] = make_float2(l.x, -l.y);
+            s_ljb[t] = make_float2(l.z, -l.w);
+        } else {
+            s_lj[t] = l;
+        }
     }
     if (threadIdx.x < 27) {
         const int im = threadIdx.x;
@@ -776,15 +807,17 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
                 const float dx = (float)(xis - rj.x);
                 const float dy = (float)(yis - rj.y);
                 const float dz = (float)(zis - rj.z);
-                const float4 l = s_lj[ti + rj.type];
+                const float2 la = s_lja[ti + rj.type];
+                const float2 lb = EN ? s_ljb[ti + rj.type] : make_float2(0.0f, 0.0f);
+                const float4 l = make_float4(la.x, la.y, lb.x, lb.y);
                 float elj = 0.0f, ec = 0.0f;
                 const float fs = PairMath<float>::template eval<EN, SAME>(
-                    dx, dy, dz, (float)qiq * rj.q, make_float4(l.x, -l.y, l.z, -l.w),
+                    dx, dy, dz, mulr((float)qiq, rj.q), make_float4(l.x, -l.y, l.z, -l.w),
                     ((m0 | m1) >> lane) & 1u, k, elj, ec);
-                const float px = dx * fs, py = dy * fs, pz = dz * fs;
-                ax2.x += px;
-                ay2.x += py;
-                az2.x += pz;
+                const float px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
+                ax2.x = addr(ax2.x, px);
+                ay2.x = addr(ay2.x, py);
+                az2.x = addr(az2.x, pz);
                 v[0] = h ? 0.0f : px;
                 v[1] = h ? 0.0f : py;
                 v[2] = h ? 0.0f : pz;
@@ -792,13 +825,13 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
                 v[4] = h ? py : 0.0f;
                 v[5] = h ? pz : 0.0f;
                 if (EN) {
-                    alj2.x += elj;
-                    ac2.x += ec;
+                    alj2.x = addr(alj2.x, elj);
+                    ac2.x = addr(ac2.x, ec);
                 }
                 if (VIR) {
-                    axx2.x += dx * px;
-                    ayy2.x += dy * py;
-                    azz2.x += dz * pz;
+                    axx2.x = fmar(dx, px, axx2.x);
+                    ayy2.x = fmar(dy, py, ayy2.x);
+                    azz2.x = fmar(dz, pz, azz2.x);
                 }
             } else if constexpr (PACK) {
                 // both j halves at once; a half without pairs in range is computed
@@ -812,7 +845,9 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
                 const bool on1 = ((unsigned)(mm >> 32) >> lane) & 1u;
                 float2 elj = z2, ec = z2;
                 const float2 fs = PairMath2::template eval<EN, SAME>(
-                    dx, dy, dz, qq, s_lj[ti + r0.type], s_lj[ti + r1.type], on0, on1, k, elj, ec);
+                    dx, dy, dz, qq, s_lja[ti + r0.type], s_lja[ti + r1.type],
+                    EN ? s_ljb[ti + r0.type] : z2, EN ? s_ljb[ti + r1.type] : z2, on0, on1, k,
+                    elj, ec);
                 const float2 px = mul2(dx, fs), py = mul2(dy, fs), pz = mul2(dz, fs);
                 ax2 = add2(ax2, px);
                 ay2 = add2(ay2, py);
@@ -847,23 +882,23 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
                 const bool on = (mh >> lane) & 1u;
                 const float4 ljp = s_lj[ti + rj.type];
                 T elj = 0, ec = 0;
-                const T fs = PairMath<T>::template eval<EN, SAME>(dx, dy, dz, qiq * (T)rj.q, ljp,
-                                                                  on, k, elj, ec);
-                const T px = dx * fs, py = dy * fs, pz = dz * fs;
-                ax += px;
-                ay += py;
-                az += pz;
+                const T fs = PairMath<T>::template eval<EN, SAME>(dx, dy, dz, mulr(qiq, (T)rj.q),
+                                                                  ljp, on, k, elj, ec);
+                const T px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
+                ax = addr(ax, px);
+                ay = addr(ay, py);
+                az = addr(az, pz);
                 v[3 * h + 0] = px;
                 v[3 * h + 1] = py;
                 v[3 * h + 2] = pz;
                 if (EN) {
-                    a_lj += elj;
-                    a_c += ec;
+                    a_lj = addr(a_lj, elj);
+                    a_c = addr(a_c, ec);
                 }
                 if (VIR) {
-                    a_xx += dx * px;
-                    a_yy += dy * py;
-                    a_zz += dz * pz;
+                    a_xx = fmar(dx, px, a_xx);
+                    a_yy = fmar(dy, py, a_yy);
+                    a_zz = fmar(dz, pz, a_zz);
                 }
             }
             const T fj = reduce_scatter_j<T>(v, lane);
@@ -1234,6 +1269,10 @@ static int sys_alloc(Sys *s) {
     SOFIA_CUDA(ctx, s->dcount.ensure(sizeof(long long) * 4));
     SOFIA_CUDA(ctx, cudaMemset(s->dcount.p, 0, sizeof(long long) * 4));
     SOFIA_CUDA(ctx, cudaMemset(s->status_local.p, 0, sizeof(int) * ST_NSLOTS));
+    // no clusters and empty rows until the first build (host queries may come first)
+    SOFIA_CUDA(ctx, cudaMemset(s->nclusters.p, 0, sizeof(int) * 4));
+    SOFIA_CUDA(ctx, cudaMemset(s->jcount.p, 0, sizeof(int) * maxcl));
+    SOFIA_CUDA(ctx, cudaMemset(s->icount.p, 0, sizeof(int) * maxcl));
     return SOFIA_OK;
 }
 
@@ -1928,23 +1967,23 @@ extern "C" int sofia_system_stats(sofia_system *ss, int64_t *stats, int nstats) 
     sofia_nb_ctx *ctx = s->ctx;
     SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     int ncl = 0;
-    SOFIA_CUDA(ctx, cudaMemcpy(&ncl, s->nclusters.p, sizeof(int), cudaMemcpyDeviceToHost));
-    long long entries = 0;
+    if (s->built)
+        SOFIA_CUDA(ctx, cudaMemcpy(&ncl, s->nclusters.p, sizeof(int), cudaMemcpyDeviceToHost));
+    ncl = std::min(std::max(ncl, 0), s->max_clusters);
+    long long entries = 0, inner = 0;
     if (ncl > 0) {
-        int *jc = new int[ncl];
-        cudaMemcpy(jc, s->jcount.p, sizeof(int) * ncl, cudaMemcpyDeviceToHost);
-        for (int i = 0; i < ncl; ++i) entries += jc[i];
-        delete[] jc;
-    }
-    long long inner = 0;
-    if (ncl > 0) {
-        int *jc = new int[ncl];
-        cudaMemcpy(jc, s->icount.p, sizeof(int) * ncl, cudaMemcpyDeviceToHost);
-        for (int i = 0; i < ncl; ++i) inner += jc[i];
-        delete[] jc;
+        std::vector<int> jc(ncl), ic(ncl);
+        SOFIA_CUDA(ctx, cudaMemcpy(jc.data(), s->jcount.p, sizeof(int) * ncl,
+                                   cudaMemcpyDeviceToHost));
+        SOFIA_CUDA(ctx, cudaMemcpy(ic.data(), s->icount.p, sizeof(int) * ncl,
+                                   cudaMemcpyDeviceToHost));
+        for (int i = 0; i < ncl; ++i) {
+            entries += jc[i];
+            inner += ic[i];
+        }
     }
     long long dc[2] = {0, 0};
-    cudaMemcpy(dc, s->dcount.p, sizeof(dc), cudaMemcpyDeviceToHost);
+    SOFIA_CUDA(ctx, cudaMemcpy(dc, s->dcount.p, sizeof(dc), cudaMemcpyDeviceToHost));
     const int64_t vals[11] = {s->n_builds + dc[0], ncl, entries, s->jcap, s->ncx,
                               s->max_clusters, s->ncol_reach, s->launches, s->n_prunes + dc[1],
                               inner, s->shake_nc};

@@ -43,6 +43,7 @@ class System:
         ctx.check(ctx._lib.sofia_system_create(ctx.handle, C.byref(d), C.byref(h)))
         self.handle = h
         self.precision = precision
+        ctx.adopt(self)
 
     def close(self):
         if getattr(self, "handle", None):

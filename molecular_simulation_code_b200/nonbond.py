@@ -17,6 +17,7 @@ reference's offload transfers) or CUDA torch tensors (used in place).
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import math
 import dataclasses
 
@@ -53,6 +54,13 @@ class Context:
         if rc != SOFIA_OK:
             raise SofiaError(rc, "sofia_nb_create failed (no usable CUDA device?)")
         self.handle = h
+        # systems and batches created on this context hold its stream: they are
+        # destroyed before it, whatever order the garbage collector picks
+        self._children = weakref.WeakSet()
+
+    def adopt(self, obj):
+        """Register an object whose ``close()`` must run before this context's."""
+        self._children.add(obj)
 
     def check(self, rc: int):
         if rc != SOFIA_OK:
@@ -68,6 +76,10 @@ class Context:
 
     def close(self):
         if self.handle:
+            # batches hold their systems: close them first
+            kids = list(getattr(self, "_children", ()))
+            for obj in sorted(kids, key=lambda o: getattr(o, "close_rank", 1)):
+                obj.close()
             self._lib.sofia_nb_destroy(self.handle)
             self.handle = None
 

@@ -51,6 +51,23 @@ def test_md_deterministic_and_graph_equals_eager(ctx, small):
         o.close()
 
 
+def test_stats_before_first_build(ctx, small):
+    """A system queried before its first list build reports no clusters, even when
+    its buffers reuse device memory full of another run's data, and the query
+    leaves no CUDA error behind for the next call."""
+    import torch
+    junk = torch.full((64 << 20,), 0x7fffffff, dtype=torch.int32, device="cuda")
+    del junk
+    torch.cuda.empty_cache()
+    a = _system(ctx, small, dt=1.0, gamma=0.01, seed=3)
+    st = a.stats()
+    assert st["clusters"] == 0 and st["entries"] == 0 and st["inner_entries"] == 0
+    a.md_run(3, use_graph=True)
+    st = a.stats()
+    assert 0 < st["clusters"] <= st["max_clusters"] and st["entries"] > 0
+    a.close()
+
+
 def test_graph_conditional_build_and_prune_equal_eager(ctx, small):
     """Long enough for several list rebuilds and prunes: the captured step (build
     and prune as conditional graph nodes) takes exactly the eager path's steps."""
