@@ -490,8 +490,9 @@ def run_ours(args, rank, ws):
         "hot_path": {"atom_steps_per_s": n * ws * args.steps / t_hot,
                      "step": "2 fs ballistic update + displacement check + rebuild/prune on "
                              "trigger + LJ/DSF forces and energies"},
+        # d2h: real*4 forces, 5 energy words and the 16 list-status words
         "e2e": {"value": n * ws * args.steps / t_e2e, "unit": "atom-steps/s",
-                "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 12 * n + 40},
+                "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 12 * n + 40 + 64},
         "gpu_launches": md_launches,
         "list": {"rebuilds": builds, "clusters": st["clusters"], "entries": st["entries"],
                  "pruned_entries": st["inner_entries"], "prunes": st["prunes"],

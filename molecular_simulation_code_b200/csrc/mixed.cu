@@ -1004,7 +1004,8 @@ __global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
                          const int *__restrict__ slot_orig, const long long *__restrict__ fslot,
                          long long *__restrict__ fx, long long *__restrict__ fy,
                          long long *__restrict__ fz, int *__restrict__ status,
-                         int *__restrict__ flag, long long *__restrict__ cnt, LangevinArgs lg) {
+                         int *__restrict__ flag, long long *__restrict__ cnt, LangevinArgs lg,
+                         float *__restrict__ ffo) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (flag && s == 0) {
         const int f = flag[0];
@@ -1026,6 +1027,11 @@ __global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
     fx[o] = a;
     fy[o] = b;
     fz[o] = c;
+    if (ffo) {
+        ffo[3 * o + 0] = (float)((double)a * FIX_INV);
+        ffo[3 * o + 1] = (float)((double)b * FIX_INV);
+        ffo[3 * o + 2] = (float)((double)c * FIX_INV);
+    }
     const long long lim = 1ll << 62;
     if (a > lim || a < -lim || b > lim || b < -lim || c > lim || c < -lim)
         atomicAdd(&status[ST_FIXED_OVF], 1);
@@ -1538,7 +1544,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
 
 // Pair kernel (+ energy reduction) on the pruned list.
 int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
-             const LangevinArgs *lg) {
+             const LangevinArgs *lg, float *ff_out) {
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     PairConst k = make_pair_const(s, nullptr);
@@ -1579,7 +1585,7 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
                                                     s->slot_orig.as<int>(),
                                                     s->fslot.as<long long>(), fx, fy, fz,
                                                     ctx->d_status, count_flag,
-                                                    s->dcount.as<long long>(), lgv);
+                                                    s->dcount.as<long long>(), lgv, ff_out);
     s->launches += 2;
     if (energy || virial) {
         k_red_stage1<<<RED_BLOCKS, 256, 0, st>>>(s->max_clusters, 5, s->nclusters.as<int>(),
@@ -1598,7 +1604,7 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
 // pair kernel.  Row-capacity overflow is recorded in status_local and checked
 // by the caller after the segment (sys_list_overflow).
 int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build,
-                    bool disp_done, const LangevinArgs *lg) {
+                    bool disp_done, const LangevinArgs *lg, float *ff_out) {
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     const int n = s->n;
@@ -1619,17 +1625,21 @@ int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_
     sys_prune(s, flag, true);
     s->launches += 1;
     // the force unpack counts the build/prune events and clears the trigger word
-    return sys_pair(s, precision, energy, virial, flag, lg);
+    return sys_pair(s, precision, energy, virial, flag, lg, ff_out);
 }
 
 // After a device-only segment: SOFIA_ENEEDGROW (and a larger row capacity) if
 // some list row overflowed; SOFIA_EINVAL if a column overflowed.
-int sys_list_overflow(Sys *s) {
+int sys_list_overflow(Sys *s, const int32_t *status) {
     sofia_nb_ctx *ctx = s->ctx;
     int hs[ST_NSLOTS];
-    SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs), cudaMemcpyDeviceToHost,
-                                    ctx->stream));
-    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (status) {
+        memcpy(hs, status, sizeof(hs));
+    } else {
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs),
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+        SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
     if (hs[ST_CELLOVER]) return fail(ctx, SOFIA_EINVAL, "an xy column holds more than 2048 atoms%s");
     if (hs[ST_NCLUSTER] > s->jcap) {
         s->jcap = (int)(hs[ST_NCLUSTER] * 1.2) + 16;
@@ -1658,13 +1668,11 @@ static int dropin_capture(Sys *s, int e) {
     k_aos_to_soa<<<grid_for(n, 256), 256, 0, st>>>(n, s->stage_pos.as<float4>(),
                                                    s->x[0].as<double>(), s->x[1].as<double>(),
                                                    s->x[2].as<double>());
-    const int rc = sys_step_forces(s, s->precision, e >= 1, e == 2, false);
-    k_fix_to_float<<<grid_for(n, 256), 256, 0, st>>>(n, s->f[0].as<long long>(),
-                                                     s->f[1].as<long long>(),
-                                                     s->f[2].as<long long>(),
-                                                     s->stage_ff.as<float>());
+    // the force unpack also writes the real*4 forces the call returns
+    const int rc = sys_step_forces(s, s->precision, e >= 1, e == 2, false, false, nullptr,
+                                   s->stage_ff.as<float>());
     const cudaError_t ce = cudaStreamEndCapture(st, &g);
-    s->dropin_launches[e] = s->launches - l0 + 2;
+    s->dropin_launches[e] = s->launches - l0 + 1;
     s->launches = l0;
     s->timing = timing;
     if (rc) {
@@ -1865,13 +1873,21 @@ extern "C" int sofia_force_nonbond_mixed(sofia_system *ss, const sofia_ainfo *po
         s->launches += 2;
     }
     SOFIA_CUDA(ctx, cudaMemcpyAsync(ff, s->stage_ff.p, fbytes, cudaMemcpyDefault, st));
+    // energies and, after a graph step, the list status words come back with the
+    // forces into the context's pinned buffers: one synchronization per call
     double e[5] = {0, 0, 0, 0, 0};
     if (want_e)
-        SOFIA_CUDA(ctx, cudaMemcpyAsync(e, s->red.p, sizeof(e), cudaMemcpyDeviceToHost, st));
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(ctx->h_red, s->red.p, sizeof(e), cudaMemcpyDeviceToHost,
+                                        st));
+    if (graph)
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, s->status_local.p,
+                                        sizeof(int32_t) * sofia::ST_NSLOTS,
+                                        cudaMemcpyDeviceToHost, st));
     SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    if (want_e) memcpy(e, ctx->h_red, sizeof(e));
     if (graph) {
         // a list row that overflowed during a device-side rebuild: grow and redo
-        const int rc = sofia::sys_list_overflow(s);
+        const int rc = sofia::sys_list_overflow(s, ctx->h_status);
         if (rc == SOFIA_ENEEDGROW)
             return sofia_force_nonbond_mixed(ss, position, ff, potential, e_coul, virial_diag3);
         if (rc) return rc;

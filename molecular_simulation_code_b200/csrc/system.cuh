@@ -104,15 +104,21 @@ struct Sys {
 // evaluation entry points (mixed.cu)
 int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build);
 // count_flag (may be NULL): the trigger word whose build/prune bits are counted
-// and then cleared; lg (may be NULL): Langevin force added to the pair forces.
+// and then cleared; lg (may be NULL): Langevin force added to the pair forces;
+// ff_out (may be NULL): the forces also written as real*4 [n][3] in atom order.
 int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag = nullptr,
-             const LangevinArgs *lg = nullptr);
+             const LangevinArgs *lg = nullptr, float *ff_out = nullptr);
 // disp_done: the caller already ORed the displacement-trigger bits into a
 // cleared trigger word (the MD step's fused kick/drift kernel does).
 // lg (may be NULL): Langevin force added while the pair forces are written.
+// ff_out (may be NULL): as for sys_pair.
 int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_build,
-                    bool disp_done = false, const LangevinArgs *lg = nullptr);
-int sys_list_overflow(Sys *s);
+                    bool disp_done = false, const LangevinArgs *lg = nullptr,
+                    float *ff_out = nullptr);
+// After a device segment: SOFIA_ENEEDGROW (and a larger row capacity) if a list
+// row overflowed.  status: the segment's status words already on the host, or
+// nullptr to copy them (one stream synchronization).
+int sys_list_overflow(Sys *s, const int32_t *status = nullptr);
 // Frees the captured drop-in force graphs (they bake in list pointers and the margin).
 void dropin_drop(Sys *s);
 

@@ -56,17 +56,22 @@ class System:
         except Exception:
             pass
 
-    def forces_dropin(self, position, ff=None, energy: bool = True):
-        """Positions (np,4) float32 AoS or device tensor; returns (ff, pot, e_coul, virial)."""
+    def forces_dropin(self, position, ff=None, energy: bool = True, virial: bool = False):
+        """Positions (np,4) float32 AoS or device tensor; returns (ff, pot, e_coul, virial).
+
+        Like lj_cut_coul_dsf_nonewton_NOMIC (mod_force_nonbond.f90:105-196), the call
+        returns the potential and Coulomb energy but no virial unless asked for
+        (virial=True selects the kernel that also accumulates it); virial is None
+        otherwise."""
         if ff is None:
             ff = np.zeros((self.n, 3), np.float32)
         pot = C.c_double()
         ec = C.c_double()
-        vir = np.zeros(3)
+        vir = np.zeros(3) if virial else None
         if energy:
-            args = (C.byref(pot), C.byref(ec), ptr(vir))
+            args = (C.byref(pot), C.byref(ec), ptr(vir) if virial else None)
         else:
-            args = (None, None, None)
+            args = (None, None, ptr(vir) if virial else None)
         self.ctx.check(self.ctx._lib.sofia_force_nonbond_mixed(self.handle, ptr(position),
                                                                ptr(ff), *args))
         return ff, pot.value, ec.value, vir
