@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 
 #include "../../include/sofia_nb.h"
 
@@ -183,4 +184,32 @@ inline void cell_grid(float box, float cut_coul, float rcut, float *rn, int *nce
     *ncellD = (int)lround(pow((double)(*ncellT), 1.0 / 3.0));
 }
 
+}  // namespace sofia
+
+// Programmatic dependent launch.  launch_pdl starts a kernel with the
+// programmatic-serialization attribute, so it may be scheduled while its
+// predecessor in the stream drains; every kernel so launched begins with
+// SOFIA_PDL_ENTRY(), which waits until the predecessor grid has completed and
+// its memory is visible (griddepcontrol.wait) before any other statement, then
+// lets its own dependents be scheduled.  Results are those of plain stream
+// order; only the launch gaps shrink.
+#define SOFIA_PDL_ENTRY() \
+    asm volatile("griddepcontrol.wait;\n\tgriddepcontrol.launch_dependents;" ::: "memory")
+
+namespace sofia {
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, A &&...args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
 }  // namespace sofia

@@ -42,6 +42,7 @@ __global__ void k_kick(int n, double h, const double *__restrict__ invm,
                        const long long *__restrict__ fx, const long long *__restrict__ fy,
                        const long long *__restrict__ fz, double *__restrict__ vx,
                        double *__restrict__ vy, double *__restrict__ vz) {
+    SOFIA_PDL_ENTRY();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double c = h * invm[i];
@@ -65,6 +66,7 @@ __global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
                              const double *__restrict__ px, const double *__restrict__ py,
                              const double *__restrict__ pz, double L, double lim2, double plim2,
                              int *__restrict__ flag, long long *__restrict__ step) {
+    SOFIA_PDL_ENTRY();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) step[0] += 1;
     bool far = false, pfar = false;
@@ -311,6 +313,7 @@ __global__ void k_shake(int ns, const int *__restrict__ sa, const double *__rest
                         int maxiter, double tol, long long *__restrict__ fx,
                         long long *__restrict__ fy, long long *__restrict__ fz,
                         int *__restrict__ status) {
+    SOFIA_PDL_ENTRY();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= ns) return;
     const int num = sa[5 * g];
@@ -439,6 +442,7 @@ __global__ void k_shake(int ns, const int *__restrict__ sa, const double *__rest
 __global__ void k_ke(int n, const double *__restrict__ mass, const double *__restrict__ vx,
                      const double *__restrict__ vy, const double *__restrict__ vz,
                      double *__restrict__ ke) {
+    SOFIA_PDL_ENTRY();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     ke[i] = 0.5 * mass[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]) / KCAL2AMU;
@@ -449,6 +453,7 @@ __global__ void k_ke(int n, const double *__restrict__ mass, const double *__res
 constexpr int MRED = 64;
 __global__ void k_mred1(int n, int w, int c, const double *__restrict__ in,
                         double *__restrict__ part) {
+    SOFIA_PDL_ENTRY();
     __shared__ double s[256];
     const int chunk = (n + gridDim.x - 1) / gridDim.x;
     const int b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
@@ -463,6 +468,7 @@ __global__ void k_mred1(int n, int w, int c, const double *__restrict__ in,
     if (threadIdx.x == 0) part[blockIdx.x] = s[0];
 }
 __global__ void k_mred2(const double *__restrict__ part, double *__restrict__ out) {
+    SOFIA_PDL_ENTRY();
     __shared__ double s[MRED];
     s[threadIdx.x] = part[threadIdx.x];
     __syncthreads();
@@ -478,8 +484,8 @@ __global__ void k_mred2(const double *__restrict__ part, double *__restrict__ ou
 static void md_reduce(cudaStream_t st, int n, int w, int c, const double *in, double *part,
                       double *out) {
     if (n <= 0) return;
-    k_mred1<<<MRED, 256, 0, st>>>(n, w, c, in, part);
-    k_mred2<<<1, MRED, 0, st>>>(part, out);
+    sofia::launch_pdl(k_mred1, MRED, 256, 0, st, n, w, c, in, part);
+    sofia::launch_pdl(k_mred2, 1, MRED, 0, st, part, out);
 }
 
 // energies slots in md.ered: 0 lj, 1 coul, (2..4 pair virial), 5 bond, 6 angle,
@@ -496,6 +502,7 @@ struct BondedArgs {
 };
 template <bool EN>
 __global__ void __launch_bounds__(128) k_bonded(BondedArgs b) {
+    SOFIA_PDL_ENTRY();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     const DihArgs &d = b.dih;
     if (t < b.nb) {
@@ -587,12 +594,12 @@ static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = fal
     const long nterm = (long)b.nb + b.na + b.nd + b.ni;
     if (nterm > 0) {
         if (energy)
-            k_bonded<true><<<grid_for(nterm, 128), 128, 0, st>>>(b);
+            sofia::launch_pdl(k_bonded<true>, grid_for(nterm, 128), 128, 0, st, b);
         else
-            k_bonded<false><<<grid_for(nterm, 128), 128, 0, st>>>(b);
+            sofia::launch_pdl(k_bonded<false>, grid_for(nterm, 128), 128, 0, st, b);
     }
     if (md.nshake) {
-        k_shake<<<grid_for(md.nshake, 128), 128, 0, st>>>(
+        sofia::launch_pdl(k_shake, grid_for(md.nshake, 128), 128, 0, st,
             md.nshake, md.shake.as<int>(), md.sbond.as<double>(), x, y, z, s->v[0].as<double>(),
             s->v[1].as<double>(), s->v[2].as<double>(), s->invm.as<double>(), s->L, md.dt,
             md.dt * md.dt * KCAL2AMU, md.shake_maxiter, md.shake_tol, fx, fy, fz,
@@ -623,7 +630,7 @@ static void md_energy_reduce(Sys *s) {
                   red + 11);
     double *ke = md.eterm.as<double>() + (md.nbond + md.nangle + 3 * (size_t)md.ndihed +
                                           (size_t)md.nimpro);
-    k_ke<<<grid_for(s->n, 256), 256, 0, st>>>(s->n, s->mass.as<double>(), s->v[0].as<double>(),
+    sofia::launch_pdl(k_ke, grid_for(s->n, 256), 256, 0, st, s->n, s->mass.as<double>(), s->v[0].as<double>(),
                                               s->v[1].as<double>(), s->v[2].as<double>(), ke);
     md_reduce(st, s->n, 1, 0, ke, part, red + 10);
 }
@@ -657,7 +664,7 @@ static int md_step(Sys *s, bool energy) {
     const long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
                     *fz = s->f[2].as<long long>();
     const double half = 0.5 * s->skin, phalf = 0.5 * s->margin;
-    k_kick_drift<<<grid_for(n, 256), 256, 0, st>>>(
+    sofia::launch_pdl(k_kick_drift, grid_for(n, 256), 256, 0, st,
         n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz, md.dt, s->x[0].as<double>(),
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->xprn[0].as<double>(),
@@ -665,7 +672,7 @@ static int md_step(Sys *s, bool energy) {
         s->flag.as<int>(), md.step_dev.as<long long>());
     int rc = md_forces(s, energy, false, true);
     if (rc) return rc;
-    k_kick<<<grid_for(n, 256), 256, 0, st>>>(n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz);
+    sofia::launch_pdl(k_kick, grid_for(n, 256), 256, 0, st, n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz);
     if (energy) md_energy_reduce(s);
     s->launches += 2;
     SOFIA_CUDA(s->ctx, cudaGetLastError());

@@ -68,6 +68,7 @@ __global__ void k_wrap_bin(const int *__restrict__ cond, int cmask, int n,
                            double *__restrict__ ry, double *__restrict__ rz,
                            int *__restrict__ col_of, int *__restrict__ col_count,
                            float *__restrict__ zkey) {
+    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -100,6 +101,7 @@ __global__ void k_wrap_bin(const int *__restrict__ cond, int cmask, int n,
 __global__ void k_scan_cols(const int *__restrict__ cond, int cmask, int n,
                             int *__restrict__ col_count, int *__restrict__ col_start,
                             int *__restrict__ cl_start, int *__restrict__ ncl) {
+    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     __shared__ int s1[1024], s2[1024];
     __shared__ int carry1, carry2;
@@ -143,6 +145,7 @@ __global__ void k_col_scatter(const int *__restrict__ cond, int cmask, int n,
                               const int *__restrict__ col_of,
                               const int *__restrict__ col_start, int *__restrict__ col_fill,
                               int *__restrict__ col_atoms) {
+    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -158,6 +161,7 @@ __global__ void k_col_sort_assign(const int *__restrict__ cond, int cmask, int n
                                   const int *__restrict__ cl_start, int *__restrict__ slot_orig,
                                   int *__restrict__ cl_col, int *__restrict__ atom_slot,
                                   int *__restrict__ col_fill, int *__restrict__ status) {
+    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     __shared__ unsigned long long s[MAX_COL];
     const int c = blockIdx.x;
@@ -218,6 +222,7 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
                        AtomRec *__restrict__ rec, float4 *__restrict__ recf,
                        long long *__restrict__ fslot) {
+    SOFIA_PDL_ENTRY();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nslots || s >= ncl_dev[0] * CL) return;
     // the pair kernel adds into the slot-ordered accumulators: start them at zero
@@ -254,6 +259,7 @@ __global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
                        const int *__restrict__ ncl_dev,
                        const AtomRec *__restrict__ rec, const int *__restrict__ slot_orig,
                        float4 *__restrict__ bb) {
+    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= maxcl || c >= ncl_dev[0]) return;
@@ -338,6 +344,7 @@ __device__ __forceinline__ void z_window(const float4 *__restrict__ bb, float il
 // remaining clusters' bounding boxes, compact the accepted (cluster, image)
 // pairs of the half list in visiting order and attach the pair mask.
 __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
+    SOFIA_PDL_ENTRY();
     if (a.cond && !(a.cond[0] & a.cmask)) return;
     const int lane = threadIdx.x & 31;
     const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -500,6 +507,7 @@ __global__ void k_disp_check(int n, const double *__restrict__ x, const double *
                              const double *__restrict__ px, const double *__restrict__ py,
                              const double *__restrict__ pz, double L, double lim2,
                              double plim2, int *__restrict__ flag) {
+    SOFIA_PDL_ENTRY();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     bool far = false, pfar = false;
     if (i < n) {
@@ -738,6 +746,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
     const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
     unsigned long long *__restrict__ fslot, double *__restrict__ energy) {
+    SOFIA_PDL_ENTRY();
     extern __shared__ float4 s_lj[];
     // FP32 path: the same bytes as two float2 tables, {lj1, -lj2} and {lj3, -lj4},
     // so a force-only lookup reads 8 bytes (fewer shared-memory wavefronts)
@@ -1006,6 +1015,7 @@ __global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
                          long long *__restrict__ fz, int *__restrict__ status,
                          int *__restrict__ flag, long long *__restrict__ cnt, LangevinArgs lg,
                          float *__restrict__ ffo) {
+    SOFIA_PDL_ENTRY();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (flag && s == 0) {
         const int f = flag[0];
@@ -1071,6 +1081,7 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
     const int *__restrict__ slot_orig, const double *__restrict__ x,
     const double *__restrict__ y, const double *__restrict__ z, double *__restrict__ px,
     double *__restrict__ py, double *__restrict__ pz) {
+    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     __shared__ float s_shf[27 * 3];
     if (threadIdx.x < 27) {
@@ -1161,6 +1172,7 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
 
 
 __global__ void k_set_flag(int *__restrict__ flag, int v) {
+    SOFIA_PDL_ENTRY();
     if (threadIdx.x == 0 && blockIdx.x == 0) flag[0] = v;
 }
 
@@ -1169,6 +1181,7 @@ __global__ void k_set_flag(int *__restrict__ flag, int v) {
 constexpr int RED_BLOCKS = 128;
 __global__ void k_red_stage1(int n, int w, const int *__restrict__ ncl_dev,
                              const double *__restrict__ in, double *__restrict__ part) {
+    SOFIA_PDL_ENTRY();
     __shared__ double s[256];
     const int nn = ncl_dev ? min(n, ncl_dev[0]) : n;
     const int chunk = (nn + gridDim.x - 1) / gridDim.x;
@@ -1188,6 +1201,7 @@ __global__ void k_red_stage1(int n, int w, const int *__restrict__ ncl_dev,
 }
 __global__ void k_red_stage2(int nblk, int w, const double *__restrict__ part,
                              double *__restrict__ out, double scale) {
+    SOFIA_PDL_ENTRY();
     __shared__ double s[256];
     for (int c = 0; c < w; ++c) {
         s[threadIdx.x] = (threadIdx.x < nblk) ? part[threadIdx.x * w + c] : 0.0;
@@ -1206,6 +1220,7 @@ __global__ void k_red_stage2(int nblk, int w, const double *__restrict__ part,
 __global__ void k_drift(int n, double dt, double *__restrict__ x, double *__restrict__ y,
                         double *__restrict__ z, const double *__restrict__ vx,
                         const double *__restrict__ vy, const double *__restrict__ vz) {
+    SOFIA_PDL_ENTRY();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     x[i] += dt * vx[i];
@@ -1215,6 +1230,7 @@ __global__ void k_drift(int n, double dt, double *__restrict__ x, double *__rest
 
 __global__ void k_aos_to_soa(int n, const float4 *__restrict__ pos, double *__restrict__ x,
                              double *__restrict__ y, double *__restrict__ z) {
+    SOFIA_PDL_ENTRY();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i];
@@ -1226,6 +1242,7 @@ __global__ void k_aos_to_soa(int n, const float4 *__restrict__ pos, double *__re
 __global__ void k_fix_to_float(int n, const long long *__restrict__ fx,
                                const long long *__restrict__ fy,
                                const long long *__restrict__ fz, float *__restrict__ ff) {
+    SOFIA_PDL_ENTRY();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     ff[3 * i + 0] = (float)((double)fx[i] * FIX_INV);
@@ -1303,7 +1320,7 @@ static int sys_alloc_list(Sys *s) {
 static void sys_pack(Sys *s) {
     cudaStream_t st = s->ctx->stream;
     const int nslots = s->max_clusters * CL;
-    k_pack<<<grid_for(nslots, 256), 256, 0, st>>>(
+    sofia::launch_pdl(k_pack, grid_for(nslots, 256), 256, 0, st,
         nslots, s->nclusters.as<int>(), s->slot_orig.as<int>(), s->x[0].as<double>(),
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
@@ -1325,18 +1342,18 @@ static void sys_build_bin(Sys *s, const int *cond) {
     int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
     // col_count and col_fill start at zero (set at creation, cleared after each
     // use); every slot of the new clusters is written by the column sort
-    k_wrap_bin<<<grid_for(n, 256), 256, 0, st>>>(
+    sofia::launch_pdl(k_wrap_bin, grid_for(n, 256), 256, 0, st,
         cond, cm, n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(), s->L,
         s->s_col, s->ncx, s->img[0].as<double>(), s->img[1].as<double>(), s->img[2].as<double>(),
         s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(), col_of,
         s->col_count.as<int>(), s->col_key.as<float>());
-    k_scan_cols<<<1, 1024, 0, st>>>(cond, cm, s->ncols, s->col_count.as<int>(),
+    sofia::launch_pdl(k_scan_cols, 1, 1024, 0, st, cond, cm, s->ncols, s->col_count.as<int>(),
                                     s->col_start.as<int>(), s->cl_start.as<int>(),
                                     s->nclusters.as<int>());
-    k_col_scatter<<<grid_for(n, 256), 256, 0, st>>>(cond, cm, n, col_of, s->col_start.as<int>(),
+    sofia::launch_pdl(k_col_scatter, grid_for(n, 256), 256, 0, st, cond, cm, n, col_of, s->col_start.as<int>(),
                                                     s->col_fill.as<int>(),
                                                     s->col_atoms.as<int>());
-    k_col_sort_assign<<<s->ncols, 256, 0, st>>>(cond, cm, s->ncols, s->col_start.as<int>(),
+    sofia::launch_pdl(k_col_sort_assign, s->ncols, 256, 0, st, cond, cm, s->ncols, s->col_start.as<int>(),
                                                 s->col_atoms.as<int>(), s->col_key.as<float>(),
                                                 s->cl_start.as<int>(), s->slot_orig.as<int>(),
                                                 cl_col, s->atom_slot.as<int>(),
@@ -1351,7 +1368,7 @@ static int sys_build_search(Sys *s, const int *cond) {
     const int cm = 1;
     int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
     // the boxes serve the search (trigger bit 0) and the prune (bit 1)
-    k_bbox<<<grid_for(s->max_clusters, 128), 128, 0, st>>>(
+    sofia::launch_pdl(k_bbox, grid_for(s->max_clusters, 128), 128, 0, st,
         cond, 3, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
         s->slot_orig.as<int>(), s->bb.as<float4>());
     SearchArgs a;
@@ -1380,7 +1397,7 @@ static int sys_build_search(Sys *s, const int *cond) {
     a.jcount = s->jcount.as<int>();
     a.jmask = s->jmask.as<unsigned long long>();
     a.status = s->status_local.as<int>();
-    k_search<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(a);
+    sofia::launch_pdl(k_search, grid_for((long)s->max_clusters * 32, 256), 256, 0, st, a);
     SOFIA_CUDA(ctx, cudaGetLastError());
     s->launches += 2;
     if (!cond) s->n_builds++;
@@ -1468,12 +1485,12 @@ static void sys_prune(Sys *s, const int *cond, bool bb_current) {
     const float rin2 = rin * rin + 1e-3f;
     const float rfar = rin + 0.01f;
     if (!bb_current) {
-        k_bbox<<<grid_for(s->max_clusters, 128), 128, 0, st>>>(
+        sofia::launch_pdl(k_bbox, grid_for(s->max_clusters, 128), 128, 0, st,
             cond, 3, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
             s->slot_orig.as<int>(), s->bb.as<float4>());
         s->launches += 1;
     }
-    k_prune<<<grid_for((long)s->max_clusters * 32, 256), 256, 0, st>>>(
+    sofia::launch_pdl(k_prune, grid_for((long)s->max_clusters * 32, 256), 256, 0, st,
         cond, 3, s->max_clusters, s->nclusters.as<int>(), s->recf.as<float4>(),
         s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,
         (float)s->L, rin2, rfar * rfar, s->bb.as<float4>(), s->ilist.as<int>(),
@@ -1497,7 +1514,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
     if (!build) {
         const double half = 0.5 * s->skin, phalf = 0.5 * s->margin;
         SOFIA_CUDA(ctx, cudaMemsetAsync(s->flag.p, 0, sizeof(int), st));
-        k_disp_check<<<grid_for(n, 256), 256, 0, st>>>(
+        sofia::launch_pdl(k_disp_check, grid_for(n, 256), 256, 0, st,
             n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
             s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(),
             s->xprn[0].as<double>(), s->xprn[1].as<double>(), s->xprn[2].as<double>(), s->L,
@@ -1560,18 +1577,18 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
     // sofia_system_create requires rcut == cut_coul: one cut-off gates both terms
     if (precision == SOFIA_PREC_FP64) {
         if (virial)
-            k_pair<double, true, true, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<double, true, true, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
         else if (energy)
-            k_pair<double, true, false, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<double, true, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
         else
-            k_pair<double, false, false, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<double, false, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
     } else {
         if (virial)
-            k_pair<float, true, true, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<float, true, true, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
         else if (energy)
-            k_pair<float, true, false, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<float, true, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
         else
-            k_pair<float, false, false, true><<<blocks, 256, smem, st>>>(SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<float, false, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
     }
 #undef SOFIA_PAIR_ARGS
     if (s->timing) {
@@ -1581,17 +1598,17 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
     const int nslots = s->max_clusters * CL;
     LangevinArgs lgv{};
     if (lg) lgv = *lg;
-    k_unpack<<<grid_for(nslots, 256), 256, 0, st>>>(nslots, s->nclusters.as<int>(),
+    sofia::launch_pdl(k_unpack, grid_for(nslots, 256), 256, 0, st, nslots, s->nclusters.as<int>(),
                                                     s->slot_orig.as<int>(),
                                                     s->fslot.as<long long>(), fx, fy, fz,
                                                     ctx->d_status, count_flag,
                                                     s->dcount.as<long long>(), lgv, ff_out);
     s->launches += 2;
     if (energy || virial) {
-        k_red_stage1<<<RED_BLOCKS, 256, 0, st>>>(s->max_clusters, 5, s->nclusters.as<int>(),
+        sofia::launch_pdl(k_red_stage1, RED_BLOCKS, 256, 0, st, s->max_clusters, 5, s->nclusters.as<int>(),
                                                  s->energy.as<double>(), s->part.as<double>());
         // the half list holds each pair once: no halving
-        k_red_stage2<<<1, 256, 0, st>>>(RED_BLOCKS, 5, s->part.as<double>(), s->red.as<double>(),
+        sofia::launch_pdl(k_red_stage2, 1, 256, 0, st, RED_BLOCKS, 5, s->part.as<double>(), s->red.as<double>(),
                                         1.0);
         s->launches += 2;
     }
@@ -1610,11 +1627,11 @@ int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_
     const int n = s->n;
     int *flag = s->flag.as<int>();
     if (force_build || !s->built) {
-        k_set_flag<<<1, 32, 0, st>>>(flag, 3);
+        sofia::launch_pdl(k_set_flag, 1, 32, 0, st, flag, 3);
     } else if (!disp_done) {
         const double half = 0.5 * s->skin, phalf = 0.5 * s->margin;
-        k_set_flag<<<1, 32, 0, st>>>(flag, 0);
-        k_disp_check<<<grid_for(n, 256), 256, 0, st>>>(
+        sofia::launch_pdl(k_set_flag, 1, 32, 0, st, flag, 0);
+        sofia::launch_pdl(k_disp_check, grid_for(n, 256), 256, 0, st,
             n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
             s->xref[0].as<double>(), s->xref[1].as<double>(), s->xref[2].as<double>(),
             s->xprn[0].as<double>(), s->xprn[1].as<double>(), s->xprn[2].as<double>(), s->L,
@@ -1665,7 +1682,7 @@ static int dropin_capture(Sys *s, int e) {
     const long long l0 = s->launches;
     cudaGraph_t g = nullptr;
     SOFIA_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    k_aos_to_soa<<<grid_for(n, 256), 256, 0, st>>>(n, s->stage_pos.as<float4>(),
+    sofia::launch_pdl(k_aos_to_soa, grid_for(n, 256), 256, 0, st, n, s->stage_pos.as<float4>(),
                                                    s->x[0].as<double>(), s->x[1].as<double>(),
                                                    s->x[2].as<double>());
     // the force unpack also writes the real*4 forces the call returns
@@ -1862,12 +1879,12 @@ extern "C" int sofia_force_nonbond_mixed(sofia_system *ss, const sofia_ainfo *po
         s->launches += s->dropin_launches[e];
     } else {
         // first call after creation or set_state (or with timers on): host-driven
-        sofia::k_aos_to_soa<<<sofia::grid_for(n, 256), 256, 0, st>>>(
+        sofia::launch_pdl(sofia::k_aos_to_soa, sofia::grid_for(n, 256), 256, 0, st,
             n, s->stage_pos.as<float4>(), s->x[0].as<double>(), s->x[1].as<double>(),
             s->x[2].as<double>());
         const int rc = sofia::sys_eval(s, s->precision, want_e, vir, false);
         if (rc) return rc;
-        sofia::k_fix_to_float<<<sofia::grid_for(n, 256), 256, 0, st>>>(
+        sofia::launch_pdl(sofia::k_fix_to_float, sofia::grid_for(n, 256), 256, 0, st,
             n, s->f[0].as<long long>(), s->f[1].as<long long>(), s->f[2].as<long long>(),
             s->stage_ff.as<float>());
         s->launches += 2;
@@ -2013,7 +2030,7 @@ extern "C" int sofia_system_drift(sofia_system *ss, double dt, int nsteps) {
     sofia_nb_ctx *ctx = s->ctx;
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
     for (int k = 0; k < nsteps; ++k) {
-        sofia::k_drift<<<sofia::grid_for(s->n, 256), 256, 0, ctx->stream>>>(
+        sofia::launch_pdl(sofia::k_drift, sofia::grid_for(s->n, 256), 256, 0, ctx->stream,
             s->n, dt, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
             s->v[0].as<double>(), s->v[1].as<double>(), s->v[2].as<double>());
         s->launches += 1;
