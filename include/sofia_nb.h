@@ -298,8 +298,12 @@ typedef struct sofia_system sofia_system;
 
 int sofia_system_create(sofia_nb_ctx *ctx, const sofia_system_desc *desc, sofia_system **out);
 int sofia_system_destroy(sofia_system *sys);
-/* Drop-in for lj_cut_coul_dsf_nonewton: reference AoS positions in (host or
- * device), real*4 forces ff[np*3] out, energies (each may be NULL). */
+/* Drop-in for lj_cut_coul_dsf_nonewton (Source/mod_force_nonbond.f90:105-196):
+ * reference AoS positions in (host or device), real*4 forces ff[np*3] out,
+ * energies (each may be NULL).  Like the reference routine, pass
+ * virial_diag3 = NULL unless the virial is wanted: a non-NULL pointer selects
+ * the kernel that also accumulates it.  Returns after one stream
+ * synchronization, with ff and the energies written. */
 int sofia_force_nonbond_mixed(sofia_system *sys, const sofia_ainfo *position, float *ff,
                               double *potential, double *e_coul, double *virial_diag3);
 /* Resident state: x, v as [np*3] doubles (host or device). */
