@@ -220,7 +220,7 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
                        const double *__restrict__ rz, const double *__restrict__ ix,
                        const double *__restrict__ iy, const double *__restrict__ iz,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
-                       AtomRec *__restrict__ rec, float4 *__restrict__ recf,
+                       AtomRec *__restrict__ rec, float *__restrict__ recf,
                        long long *__restrict__ fslot) {
     SOFIA_PDL_ENTRY();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -250,7 +250,11 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
         r.type = 0;
     }
     rec[s] = r;
-    recf[s] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.0f);
+    // FP32 copy for the prune, per cluster x[8], y[8], z[8]
+    float *rc = recf + (size_t)(s / CL) * (3 * CL) + (s % CL);
+    rc[0] = (float)r.x;
+    rc[CL] = (float)r.y;
+    rc[2 * CL] = (float)r.z;
 }
 
 // Cluster bounding boxes of the current records (FP64 bounds rounded outward
@@ -1073,7 +1077,7 @@ __device__ __forceinline__ unsigned long long transpose8(unsigned long long x) {
 // 1e-3 A^2 safety margin).
 __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
     const int *__restrict__ cond, int cmask, int maxcl, const int *__restrict__ ncl_dev,
-    const float4 *__restrict__ recf,
+    const float *__restrict__ recf,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
     const int *__restrict__ jcount, int jcap, float L, float rin2, float rfar2,
     const float4 *__restrict__ bb, int *__restrict__ ilist,
@@ -1103,14 +1107,15 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
             pz[o] = z[o];
         }
     }
-    // i atoms 2p and 2p + 1 as the two components of packed FP32x2 operands
+    // i atoms 2p and 2p + 1 as the two components of packed FP32x2 operands,
+    // read straight from the cluster's x[8], y[8], z[8]
     float2 xi[CL / 2], yi[CL / 2], zi[CL / 2];
+    const float2 *ci = reinterpret_cast<const float2 *>(recf + (size_t)icl * 3 * CL);
 #pragma unroll
     for (int pp = 0; pp < CL / 2; ++pp) {
-        const float4 p0 = recf[icl * CL + 2 * pp], p1 = recf[icl * CL + 2 * pp + 1];
-        xi[pp] = make_float2(p0.x, p1.x);
-        yi[pp] = make_float2(p0.y, p1.y);
-        zi[pp] = make_float2(p0.z, p1.z);
+        xi[pp] = ci[pp];
+        yi[pp] = ci[CL / 2 + pp];
+        zi[pp] = ci[CL + pp];
     }
     const float4 ilo = bb[2 * icl], ihi = bb[2 * icl + 1];
     const int n = jcount[icl];
@@ -1136,22 +1141,36 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
             const float gx = gap(ilo.x, ihi.x, jlo.x + sx, jhi.x + sx);
             const float gy = gap(ilo.y, ihi.y, jlo.y + sy, jhi.y + sy);
             const float gz = gap(ilo.z, ihi.z, jlo.z + sz, jhi.z + sz);
-            if (gx * gx + gy * gy + gz * gz <= rfar2)
+            if (gx * gx + gy * gy + gz * gz <= rfar2) {
+                // the j cluster's x[8], y[8], z[8]: three 16-byte loads per 4 atoms
+                // (one half at a time keeps the kernel within 64 registers)
+                const float4 *cj = reinterpret_cast<const float4 *>(recf + (size_t)jc * 3 * CL);
+#pragma unroll 1
+                for (int hh = 0; hh < 2; ++hh) {
+                    const float4 jx = __ldg(&cj[hh]), jy = __ldg(&cj[2 + hh]),
+                                 jz = __ldg(&cj[4 + hh]);
+                    unsigned acc = 0u;  // bits 8*q + ii of j atom 4*hh + q
 #pragma unroll
-            for (int jj = 0; jj < CL; ++jj) {
-                const float4 pj = recf[jc * CL + jj];
-                // -(x_j + shift): adding it rounds exactly like x_i - (x_j + shift)
-                const float nx = -(pj.x + sx), ny = -(pj.y + sy), nz = -(pj.z + sz);
-                const float2 nx2 = make_float2(nx, nx), ny2 = make_float2(ny, ny),
-                             nz2 = make_float2(nz, nz);
+                    for (int q = 0; q < 4; ++q) {
+                        // -(x_j + shift): adding it rounds exactly like x_i - (x_j + shift)
+                        const float nx = -((&jx.x)[q] + sx), ny = -((&jy.x)[q] + sy),
+                                    nz = -((&jz.x)[q] + sz);
+                        const float2 nx2 = make_float2(nx, nx), ny2 = make_float2(ny, ny),
+                                     nz2 = make_float2(nz, nz);
 #pragma unroll
-                for (int pp = 0; pp < CL / 2; ++pp) {
-                    const float2 dx = add2(xi[pp], nx2), dy = add2(yi[pp], ny2),
-                                 dz = add2(zi[pp], nz2);
-                    const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
-                    const unsigned in = (r2.x < rin2 ? 1u : 0u) | (r2.y < rin2 ? 2u : 0u);
-                    if (jj < 4) lo |= in << (8 * jj + 2 * pp);
-                    else hi |= in << (8 * (jj - 4) + 2 * pp);
+                        for (int pp = 0; pp < CL / 2; ++pp) {
+                            const float2 dx = add2(xi[pp], nx2), dy = add2(yi[pp], ny2),
+                                         dz = add2(zi[pp], nz2);
+                            const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+                            const unsigned in =
+                                (r2.x < rin2 ? 1u : 0u) | (r2.y < rin2 ? 2u : 0u);
+                            acc |= in << (8 * q + 2 * pp);
+                        }
+                    }
+                    if (hh == 0)
+                        lo = acc;
+                    else
+                        hi = acc;
                 }
             }
         }
@@ -1276,7 +1295,7 @@ static int sys_alloc(Sys *s) {
     const size_t maxcl = (size_t)s->max_clusters;
     SOFIA_CUDA(ctx, s->slot_orig.ensure(sizeof(int) * maxcl * CL + sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, s->rec.ensure(sizeof(AtomRec) * maxcl * CL));
-    SOFIA_CUDA(ctx, s->recf.ensure(sizeof(float4) * maxcl * CL));
+    SOFIA_CUDA(ctx, s->recf.ensure(sizeof(float) * 3 * maxcl * CL));
     SOFIA_CUDA(ctx, s->fslot.ensure(sizeof(long long) * 3 * maxcl * CL));
     SOFIA_CUDA(ctx, s->atom_slot.ensure(sizeof(int) * n));
     SOFIA_CUDA(ctx, s->bb.ensure(sizeof(float4) * 2 * maxcl));
@@ -1325,7 +1344,7 @@ static void sys_pack(Sys *s) {
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
         s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
-        s->rec.as<AtomRec>(), s->recf.as<float4>(), s->fslot.as<long long>());
+        s->rec.as<AtomRec>(), s->recf.as<float>(), s->fslot.as<long long>());
     s->launches += 1;
 }
 
@@ -1491,7 +1510,7 @@ static void sys_prune(Sys *s, const int *cond, bool bb_current) {
         s->launches += 1;
     }
     sofia::launch_pdl(k_prune, grid_for((long)s->max_clusters * 32, 256), 256, 0, st,
-        cond, 3, s->max_clusters, s->nclusters.as<int>(), s->recf.as<float4>(),
+        cond, 3, s->max_clusters, s->nclusters.as<int>(), s->recf.as<float>(),
         s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,
         (float)s->L, rin2, rfar * rfar, s->bb.as<float4>(), s->ilist.as<int>(),
         s->imask.as<unsigned long long>(),

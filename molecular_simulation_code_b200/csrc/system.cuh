@@ -7,7 +7,9 @@
 //   cluster order             AtomRec[slot] = {double x,y,z; float q; int type}
 //                             (32 B, two 16 B loads), slot -> global index,
 //                             8 slots per cluster, clusters grouped by xy column
-//                             and sorted by z inside a column
+//                             and sorted by z inside a column; an FP32 copy for
+//                             the prune as float x[8], y[8], z[8] per cluster
+//                             (96 B, six 16 B loads)
 //   cluster-pair list         per i-cluster a row of jcap entries:
 //                             int32 {j cluster | image << 26} + uint64 pair mask
 #pragma once
@@ -74,7 +76,8 @@ struct Sys {
     DevBuf ljtab;                      // float4 {lj1,lj2,lj3,lj4} per type pair
     // cluster structures
     DevBuf col_count, col_start, col_fill, col_atoms, col_key, cl_start;
-    DevBuf slot_orig, rec, recf, bb, jlist, jmask, jcount, nclusters;
+    DevBuf slot_orig, rec, bb, jlist, jmask, jcount, nclusters;
+    DevBuf recf;                        // FP32 positions per cluster: x[8], y[8], z[8]
     DevBuf fslot;                       // pair forces in cluster-slot order, 64-bit fixed point [3][slots]
     DevBuf atom_slot;                   // cluster slot of every atom (inverse of slot_orig)
     DevBuf status_local;
