@@ -185,26 +185,29 @@ int sofia_improper_harmonic(sofia_nb_ctx *ctx, int np, const sofia_ainfo *positi
 /*
  * Allocation-free form of sofia_force_nonbond_dsf.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot allocate device
- * memory when they need forces: work being captured into a CUDA graph (where
- * cudaMalloc is not allowed), hosts that give the library a fixed device arena
- * or enforce a memory budget from outside, and drivers that keep every device
- * array themselves.  It needs no context and allocates nothing: no cudaMalloc,
- * no cudaFree, no allocating library routine.
+ * memory when they need forces: hosts that give the library a fixed device
+ * arena or enforce a memory budget from outside, and drivers that keep every
+ * device array themselves.  It needs no context and allocates nothing: no
+ * cudaMalloc, no cudaFree, no allocating library routine.
  *   - stream: the caller's cudaStream_t (NULL = the legacy default stream).
- *   - position, q, lj1..lj4, nlist, numneigh and ff must be device memory
- *     (host pointers are rejected with SOFIA_EINVAL, because copying them would
- *     need a device buffer); potential, e_coul, virial_diag3 are host scalars
- *     and may be NULL.  Meaning of every argument as in sofia_force_nonbond_dsf.
+ *   - position, q, lj1..lj4, nlist, numneigh and ff must be device memory of
+ *     the current device (or managed memory); host pointers and buffers on
+ *     another GPU are rejected with SOFIA_EINVAL, because using them would need
+ *     a staging buffer or peer access.  potential, e_coul, virial_diag3 are host
+ *     scalars and may be NULL.  Meaning of every argument as in
+ *     sofia_force_nonbond_dsf.
  *   - np may be at most SOFIA_NOALLOC_MAX_ATOMS; larger systems get
  *     SOFIA_ETOOBIG.  The per-atom energy partials live in a fixed array of
  *     (5*SOFIA_NOALLOC_MAX_ATOMS + 1040) doubles (about 2.6 MB) compiled into
  *     the library, which every GPU that loads the library holds until exit.
  *   - The first call on a device looks up that array's device address and
- *     caches it; make this first call before any stream capture begins.
+ *     caches it for the process; after a cudaDeviceReset of that device the
+ *     cached address is stale, so do not call it across a device reset.
  *   - All calls share the one array: calls that overlap on the GPU (on
  *     different streams, threads or processes sharing the context) race and
  *     corrupt each other's energies; order them on one stream or serialise.
- *   - Returns after the energies are on the host (the stream is synchronised).
+ *   - The call copies the energies to host memory and synchronises the stream
+ *     before it returns, so it cannot be recorded into a CUDA graph.
  */
 #define SOFIA_NOALLOC_MAX_ATOMS 65536
 int sofia_force_nonbond_dsf_noalloc(void *stream, int np, const sofia_ainfo *position,
@@ -321,6 +324,17 @@ int sofia_system_compute_forces(sofia_system *sys, int precision, int flags, dou
  * entries of the pruned (rc + margin) list, SHAKE groups that reached maxiter
  * (a warning, as the reference prints, Source/mod_shake.f90:322-324). */
 int sofia_system_stats(sofia_system *sys, int64_t *stats, int nstats);
+/* The resident cluster-pair list as atom pairs (a diagnostic query; copies the
+ * list to the host).  which = 0: the outer list over rc + neighbor_pad made at
+ * the last build; 1: the pruned list over rc + margin made at the last prune.
+ * Each listed unordered pair appears once (half list): pairs[2k], pairs[2k+1]
+ * are its 0-based atom ids, *npairs the number of pairs; SOFIA_ENEEDGROW when
+ * capacity is smaller (only the first `capacity` are written).  xlist[np*3]
+ * (may be NULL) receives the positions that list was made at.  The reference's
+ * counterpart is the full list nlist/numneigh of build_neighbor_nonewton_nomic
+ * (Source/mod_neighbor.f90:622-809), which holds every pair twice. */
+int sofia_system_list_pairs(sofia_system *sys, int which, int64_t capacity, int32_t *pairs,
+                            int64_t *npairs, double *xlist);
 /* Ballistic drift x += dt*v of the resident positions, nsteps times (no forces). */
 int sofia_system_drift(sofia_system *sys, double dt, int nsteps);
 /* CUDA-event timers of the list build and the pair kernel on the system's
@@ -346,6 +360,13 @@ int sofia_system_timers(sofia_system *sys, int enable, double *timers);
 #define SOFIA_TERM_TORSION 4
 #define SOFIA_TERM_PAIR14 8
 #define SOFIA_TERM_IMPROPER 16
+/* Terms only sofia_system_md_forces selects (an MD step always has them). */
+#define SOFIA_TERM_NONBOND 32  /* LJ + DSF pair forces of the production path */
+#define SOFIA_TERM_LANGEVIN 128 /* Langevin friction + noise at the current step counter */
+#define SOFIA_TERM_SHAKE 64    /* SHAKE constraint forces for the next step, on the sum of the others */
+/* sofia_md_desc.flags */
+#define SOFIA_MD_RATTLE 1   /* RATTLE velocity stage after the second half-kick */
+#define SOFIA_MD_LJ_SHIFT 2 /* LJ pair energies shifted to zero at the cut-off (energy only) */
 #define SOFIA_MD_NE 13 /* lj, coul, self, bond, angle, torsion, coul14, lj14, kinetic, total, T(K), step, improper */
 
 typedef struct {
@@ -376,6 +397,13 @@ typedef struct {
     const int32_t *impropers;  /* [nimpro*5] i1..i4, type */
     int nimprotypes;
     const double *impro_coeff; /* [nimprotypes*2] k (kcal/mol/rad^2), omega0 (rad) */
+    /* SOFIA_MD_* options, 0 = the reference's scheme.  Neither changes positions:
+     * SOFIA_MD_RATTLE projects the full-step velocities onto the constraints
+     * (Andersen's RATTLE; the positions of SHAKE and RATTLE are the same
+     * sequence, the reference has SHAKE alone, Source/mod_shake.f90:888-913),
+     * SOFIA_MD_LJ_SHIFT subtracts E_LJ(rc) from every pair inside the cut-off
+     * (the reference truncates, Source/mod_force_nonbond.f90:155). */
+    int flags;
 } sofia_md_desc;
 
 int sofia_system_md_setup(sofia_system *sys, const sofia_md_desc *md);
@@ -385,18 +413,41 @@ int sofia_system_md_setup(sofia_system *sys, const sofia_md_desc *md);
  * (sofia_system_get_state / set_state move them). */
 int sofia_system_md_run(sofia_system *sys, int nsteps, int energy_every, int use_graph,
                         double *energies);
+/* Forces of one MD step at the resident positions and velocities, without
+ * stepping: zero, nonbonded pairs, bonded terms and 1-4 pairs, merged like
+ * force_wrapper_DSF (Source/mod_force.f90:510-554), plus the Langevin force
+ * (Source/mod_langevin.f90:15-43) and SHAKE's constraint forces for the next
+ * step (Source/mod_shake.f90:8-85, 888-913), restricted to the SOFIA_TERM_*
+ * bits in `terms` (bonded bits only act where md_setup enabled them; SHAKE acts
+ * on the sum of the other selected terms).  f[np*3] (may be NULL) receives the
+ * fixed-point sum as doubles in atom order; energies[SOFIA_MD_NE] (may be
+ * NULL; computed only when given) the selected terms' energies and the
+ * kinetic energy.  The next sofia_system_md_run recomputes its own forces. */
+int sofia_system_md_forces(sofia_system *sys, int terms, double *f, double *energies);
 
 /*
  * Batches of independent replicas (no reference counterpart: the reference
  * runs one replica per MPI rank, Source/MD.f90:26-44, with no exchange).
- * Every system must have its own context (stream) on the batch's device for
- * the replicas to overlap; one CUDA graph per step kind forks one step of
- * every replica and joins it.  energies = [n][SOFIA_MD_NE].
+ * Each kernel of an MD step runs once for all replicas (up to 256, of any
+ * sizes and boxes) over a device table of the replicas' buffers, so a batch
+ * step is one launch per kernel; steps run as captured CUDA graphs of `seg`
+ * steps (default 100).  A replica's trajectory is bit-identical to the same
+ * replica run alone.  All replicas must share precision, atom types, cut-off
+ * and DSF constants (the box may differ) and be set up for MD.
+ *   sofia_batch_md_run: nsteps steps of every replica; energies = [n][SOFIA_MD_NE]
+ *       (may be NULL) receive each replica's energies of the last step when
+ *       energy_every > 0 (only that step computes them).
+ *   sofia_batch_set_systems: new members for the next run (continuous
+ *       batching); the captured graphs are kept when the new members share the
+ *       pair constants, so membership changes need no recapture.
+ *   sofia_batch_set_segment: steps per captured graph (1..1000).
  */
 typedef struct sofia_batch sofia_batch;
 int sofia_batch_create(sofia_nb_ctx *ctx, sofia_system *const *systems, int n, sofia_batch **out);
 int sofia_batch_destroy(sofia_batch *batch);
 int sofia_batch_md_run(sofia_batch *batch, int nsteps, int energy_every, double *energies);
+int sofia_batch_set_systems(sofia_batch *batch, sofia_system *const *systems, int n);
+int sofia_batch_set_segment(sofia_batch *batch, int steps);
 /* Prune margin (A) of the pruned inner list (default 0.6): the tuning knob
  * the autotuner picks per size class. */
 int sofia_system_set_margin(sofia_system *sys, double margin);
@@ -413,6 +464,16 @@ int sofia_system_set_margin(sofia_system *sys, double margin);
  */
 int sofia_system_snapshot(sofia_system *sys);
 int sofia_system_rollback(sofia_system *sys);
+/* get_greatestCluster (Source/mod_cluster.f90:15-83) on the resident positions
+ * of a system, which never leave the device (nuc_move keeps the replica state
+ * between segments, Source/mod_nucleation.f90:396-449): the FP64 positions are
+ * wrapped into (0, box] as real*4 (x - L floor(x/L), then +box if <= 0) and
+ * analysed like sofia_greatest_cluster with global ids 1..np.  The glycine
+ * molecules are the first n_gly * atoms_per_gly atoms.  ptta_full (host or
+ * device) and *greatest_belongsto are in/out as in sofia_greatest_cluster. */
+int sofia_system_greatest_cluster(sofia_system *sys, int n_gly, int atoms_per_gly, double mrcut,
+                                  double denscut, int densmin, double *ptta_full,
+                                  int32_t *greatest_belongsto, int32_t *size_out);
 /* Thermostat step counter (counter of the Langevin noise).  Reading it with
  * the state and setting it on resume continues the same noise sequence; the
  * reference restart (read_dump_global_id_v, Source/mod_datadump.f90:216-252)

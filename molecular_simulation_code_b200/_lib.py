@@ -45,7 +45,20 @@ class SofiaMdDesc(C.Structure):
                 ("nshake", C.c_int), ("shake", C.c_void_p), ("shake_bond", C.c_void_p),
                 ("shake_maxiter", C.c_int), ("shake_tol", C.c_double),
                 ("nimpro", C.c_int), ("impropers", C.c_void_p), ("nimprotypes", C.c_int),
-                ("impro_coeff", C.c_void_p)]
+                ("impro_coeff", C.c_void_p), ("flags", C.c_int)]
+
+
+# sofia_md_desc.flags and the force terms of sofia_system_md_forces
+SOFIA_MD_RATTLE = 1
+SOFIA_MD_LJ_SHIFT = 2
+SOFIA_TERM_BOND = 1
+SOFIA_TERM_ANGLE = 2
+SOFIA_TERM_TORSION = 4
+SOFIA_TERM_PAIR14 = 8
+SOFIA_TERM_IMPROPER = 16
+SOFIA_TERM_NONBOND = 32
+SOFIA_TERM_SHAKE = 64
+SOFIA_TERM_LANGEVIN = 128
 
 
 SOFIA_MD_NE = 13
@@ -112,15 +125,21 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_system_drift": (_I, [_P, _D, _I]),
     "sofia_system_md_setup": (_I, [_P, C.POINTER(SofiaMdDesc)]),
     "sofia_system_md_run": (_I, [_P, _I, _I, _I, _P]),
+    "sofia_system_md_forces": (_I, [_P, _I, _P, _P]),
+    "sofia_system_list_pairs": (_I, [_P, _I, C.c_int64, _P, C.POINTER(C.c_int64), _P]),
     "sofia_batch_create": (_I, [_P, _P, _I, C.POINTER(_P)]),
     "sofia_batch_destroy": (_I, [_P]),
     "sofia_batch_md_run": (_I, [_P, _I, _I, _P]),
+    "sofia_batch_set_systems": (_I, [_P, _P, _I]),
+    "sofia_batch_set_segment": (_I, [_P, _I]),
     "sofia_system_set_margin": (_I, [_P, _D]),
     "sofia_system_timers": (_I, [_P, _I, _P]),
     "sofia_system_snapshot": (_I, [_P]),
     "sofia_system_rollback": (_I, [_P]),
     "sofia_system_md_get_step": (_I, [_P, _P]),
     "sofia_system_md_set_step": (_I, [_P, C.c_longlong]),
+    "sofia_system_greatest_cluster": (_I, [_P, _I, _I, _D, _D, _I, _P, C.POINTER(C.c_int32),
+                                           C.POINTER(C.c_int32)]),
 }
 
 _lib = None

@@ -1,8 +1,9 @@
 """Batches of independent replicas and the per-size-class autotuner.
 
-A ``Batch`` groups device-resident systems (each with its own context, i.e.
-its own CUDA stream) and advances all of them with one graph launch per step
-(``sofia_batch_md_run``).  Replicas never exchange data, so each replica's
+A ``Batch`` groups device-resident systems and advances all of them together
+(``sofia_batch_md_run``): each kernel of a step runs once for every replica,
+and steps run as captured graphs of ``seg`` steps.  Members can change between
+runs (``set_systems``) without a graph recapture.  Replicas never exchange data, so each replica's
 trajectory is bit-identical to the same replica run alone.
 
 ``autotune_margin`` times short MD segments of one replica per candidate
@@ -52,6 +53,16 @@ class Batch:
         if energy_every <= 0:
             return None
         return [dict(zip(MD_ENERGY_NAMES, row.tolist())) for row in e]
+
+    def set_systems(self, systems: list):
+        """New members for the next run (continuous batching, no graph recapture)."""
+        arr = (C.c_void_p * len(systems))(*[s.handle.value for s in systems])
+        self.ctx.check(self.ctx._lib.sofia_batch_set_systems(self.handle, arr, len(systems)))
+        self.systems = list(systems)
+
+    def set_segment(self, steps: int):
+        """Steps per captured graph (default 100)."""
+        self.ctx.check(self.ctx._lib.sofia_batch_set_segment(self.handle, int(steps)))
 
     def close(self):
         if getattr(self, "handle", None):

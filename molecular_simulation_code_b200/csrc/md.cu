@@ -38,17 +38,23 @@ __device__ __forceinline__ double mimg(double d, double L) { return d - L * rint
 
 
 // nve_v: v += (dt/2) * kcal2amu * f / m
-__global__ void k_kick(int n, double h, const double *__restrict__ invm,
+__device__ __forceinline__ void kick_body(int bx, int n, double h, const double *__restrict__ invm,
                        const long long *__restrict__ fx, const long long *__restrict__ fy,
                        const long long *__restrict__ fz, double *__restrict__ vx,
                        double *__restrict__ vy, double *__restrict__ vz) {
-    SOFIA_PDL_ENTRY();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bx * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double c = h * invm[i];
     vx[i] += c * unfix(fx[i]);
     vy[i] += c * unfix(fy[i]);
     vz[i] += c * unfix(fz[i]);
+}
+__global__ void k_kick(int n, double h, const double *__restrict__ invm,
+                       const long long *__restrict__ fx, const long long *__restrict__ fy,
+                       const long long *__restrict__ fz, double *__restrict__ vx,
+                       double *__restrict__ vy, double *__restrict__ vz) {
+    SOFIA_PDL_ENTRY();
+    kick_body(blockIdx.x, n, h, invm, fx, fy, fz, vx, vy, vz);
 }
 
 // First half-kick and drift of a step fused with the step counter and the
@@ -56,7 +62,7 @@ __global__ void k_kick(int n, double h, const double *__restrict__ invm,
 // trigger word if an atom moved more than skin/2 since the list build, bit 1
 // if more than margin/2 since the last prune (the word was cleared after the
 // previous step's list decisions).
-__global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
+__device__ __forceinline__ void kick_drift_body(int bx, int n, double h, const double *__restrict__ invm,
                              const long long *__restrict__ fx, const long long *__restrict__ fy,
                              const long long *__restrict__ fz, double *__restrict__ vx,
                              double *__restrict__ vy, double *__restrict__ vz, double dt,
@@ -66,8 +72,7 @@ __global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
                              const double *__restrict__ px, const double *__restrict__ py,
                              const double *__restrict__ pz, double L, double lim2, double plim2,
                              int *__restrict__ flag, long long *__restrict__ step) {
-    SOFIA_PDL_ENTRY();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bx * blockDim.x + threadIdx.x;
     if (i == 0) step[0] += 1;
     bool far = false, pfar = false;
     if (i < n) {
@@ -87,6 +92,19 @@ __global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
     }
     const bool a = __any_sync(0xffffffffu, far), b = __any_sync(0xffffffffu, pfar);
     if ((threadIdx.x & 31) == 0 && (a || b)) atomicOr(flag, (a ? 1 : 0) | (b ? 2 : 0));
+}
+__global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
+                             const long long *__restrict__ fx, const long long *__restrict__ fy,
+                             const long long *__restrict__ fz, double *__restrict__ vx,
+                             double *__restrict__ vy, double *__restrict__ vz, double dt,
+                             double *__restrict__ x, double *__restrict__ y,
+                             double *__restrict__ z, const double *__restrict__ rx,
+                             const double *__restrict__ ry, const double *__restrict__ rz,
+                             const double *__restrict__ px, const double *__restrict__ py,
+                             const double *__restrict__ pz, double L, double lim2, double plim2,
+                             int *__restrict__ flag, long long *__restrict__ step) {
+    SOFIA_PDL_ENTRY();
+    kick_drift_body(blockIdx.x, n, h, invm, fx, fy, fz, vx, vy, vz, dt, x, y, z, rx, ry, rz, px, py, pz, L, lim2, plim2, flag, step);
 }
 
 
@@ -176,18 +194,6 @@ __device__ __forceinline__ void improper_term(int m, int ni, const int *__restri
     if (EN) e[m] = r.e;
 }
 
-struct DihArgs {
-    int nd, ntypes, terms;
-    const int *dl;
-    const double *dc, *lj14;
-    const double *x, *y, *z;
-    const int *type;
-    const float *q;
-    double L, alpha, EWALD_P, A1, A2, A3, A4, A5, MY_PIS, e_shift, f_shift, cut_coulsq, rcut2;
-    float coulpre;
-    long long *fx, *fy, *fz;
-    double *e;  // [nd][3] torsion, coul14, lj14
-};
 
 // dihedral_opls_DSF (mod_force_dihed.f90:849-1068) on the FP64 state.
 template <bool EN>
@@ -265,7 +271,9 @@ __device__ __forceinline__ void dihedral_term(int n, const DihArgs &a) {
         double force = 0.0;
         if (dr2 < a.cut_coulsq) {
             const double r = sqrt(dr2), dr2i = 1.0 / dr2;
-            const double pref = (double)a.coulpre * (double)a.q[i1] * (double)a.q[i4] / r;
+            // coulpre*q(i1)*q(i4) is a real*4 product in the reference
+            // (mod_force_dihed.f90:1010), promoted by the division by r
+            const double pref = (double)__fmul_rn(__fmul_rn(a.coulpre, a.q[i1]), a.q[i4]) / r;
             const double erfcd = exp(-a.alpha * a.alpha * dr2);
             const double t = 1.0 / (1.0 + a.EWALD_P * a.alpha * r);
             const double erfcc = t * (a.A1 + t * (a.A2 + t * (a.A3 + t * (a.A4 + t * a.A5)))) * erfcd;
@@ -305,7 +313,7 @@ __device__ __forceinline__ void dihedral_term(int n, const DihArgs &a) {
 
 // SHAKE (force form) per group; each atom belongs to at most one group, so the
 // owning thread adds its constraint forces without atomics.
-__global__ void k_shake(int ns, const int *__restrict__ sa, const double *__restrict__ sb,
+__device__ __forceinline__ void shake_body(int bx, int ns, const int *__restrict__ sa, const double *__restrict__ sb,
                         const double *__restrict__ x, const double *__restrict__ y,
                         const double *__restrict__ z, const double *__restrict__ vx,
                         const double *__restrict__ vy, const double *__restrict__ vz,
@@ -313,8 +321,7 @@ __global__ void k_shake(int ns, const int *__restrict__ sa, const double *__rest
                         int maxiter, double tol, long long *__restrict__ fx,
                         long long *__restrict__ fy, long long *__restrict__ fz,
                         int *__restrict__ status) {
-    SOFIA_PDL_ENTRY();
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = bx * blockDim.x + threadIdx.x;
     if (g >= ns) return;
     const int num = sa[5 * g];
     int at[4] = {sa[5 * g + 1] - 1, sa[5 * g + 2] - 1, sa[5 * g + 3] - 1, sa[5 * g + 4] - 1};
@@ -438,25 +445,162 @@ __global__ void k_shake(int ns, const int *__restrict__ sa, const double *__rest
         }
     }
 }
+__global__ void k_shake(int ns, const int *__restrict__ sa, const double *__restrict__ sb,
+                        const double *__restrict__ x, const double *__restrict__ y,
+                        const double *__restrict__ z, const double *__restrict__ vx,
+                        const double *__restrict__ vy, const double *__restrict__ vz,
+                        const double *__restrict__ invm, double L, double dt, double dtsq,
+                        int maxiter, double tol, long long *__restrict__ fx,
+                        long long *__restrict__ fy, long long *__restrict__ fz,
+                        int *__restrict__ status) {
+    SOFIA_PDL_ENTRY();
+    shake_body(blockIdx.x, ns, sa, sb, x, y, z, vx, vy, vz, invm, L, dt, dtsq, maxiter, tol, fx, fy, fz, status);
+}
 
+// RATTLE velocity stage (Andersen, J. Comput. Phys. 52 (1983) 24; the scheme of
+// LAMMPS fix rattle) after the second half-kick: the full-step velocities of
+// each constraint group are projected so that every constrained distance has
+// zero time derivative, (v_p - v_q) . r_pq = 0, solving C_cd (r_c . r_d) mu_d =
+// -(v_p - v_q) . r_c for the impulses mu (C as in k_shake, nc <= 3, Cramer's
+// rule).  The positions of SHAKE and RATTLE are the same sequence, so the
+// impulse m dv is taken back out of the force the next step's first half-kick
+// applies (f -= m dv / h): the next half-step velocity, and with it every later
+// position, is what the plain SHAKE step gives; only the full-step velocities
+// (and the kinetic energy measured from them) change.
+__device__ __forceinline__ void rattle_body(int bx, int ns, const int *__restrict__ sa, const double *__restrict__ x,
+                         const double *__restrict__ y, const double *__restrict__ z,
+                         double *__restrict__ vx, double *__restrict__ vy,
+                         double *__restrict__ vz, const double *__restrict__ invm, double L,
+                         double h, long long *__restrict__ fx, long long *__restrict__ fy,
+                         long long *__restrict__ fz) {
+    const int g = bx * blockDim.x + threadIdx.x;
+    if (g >= ns) return;
+    const int num = sa[5 * g];
+    const int at[4] = {sa[5 * g + 1] - 1, sa[5 * g + 2] - 1, sa[5 * g + 3] - 1,
+                       sa[5 * g + 4] - 1};
+    int nc, na, cp[3], cq[3];
+    if (num == 1) {
+        nc = 1; na = 2; cp[0] = 0; cq[0] = 1;
+    } else if (num == 3) {
+        nc = 2; na = 3; cp[0] = 0; cq[0] = 1; cp[1] = 0; cq[1] = 2;
+    } else if (num == 4) {
+        nc = 3; na = 4;
+        for (int k = 0; k < 3; ++k) { cp[k] = 0; cq[k] = k + 1; }
+    } else if (num == -3) {
+        nc = 3; na = 3; cp[0] = 0; cq[0] = 1; cp[1] = 0; cq[1] = 2; cp[2] = 1; cq[2] = 2;
+    } else {
+        return;
+    }
+    double im[4], xv[4][3], vv[4][3];
+    for (int a = 0; a < na; ++a) {
+        const int i = at[a];
+        im[a] = invm[i];
+        xv[a][0] = x[i]; xv[a][1] = y[i]; xv[a][2] = z[i];
+        vv[a][0] = vx[i]; vv[a][1] = vy[i]; vv[a][2] = vz[i];
+    }
+    double r[3][3], M[3][3], rhs[3];
+    for (int c = 0; c < nc; ++c) {
+        double gdot = 0.0;
+        for (int d = 0; d < 3; ++d) {
+            r[c][d] = mimg(xv[cp[c]][d] - xv[cq[c]][d], L);
+            gdot += (vv[cp[c]][d] - vv[cq[c]][d]) * r[c][d];
+        }
+        rhs[c] = -gdot;
+    }
+    for (int c = 0; c < nc; ++c)
+        for (int d = 0; d < nc; ++d) {
+            double e = 0.0;
+            if (cp[c] == cp[d]) e += im[cp[c]];
+            if (cp[c] == cq[d]) e -= im[cp[c]];
+            if (cq[c] == cp[d]) e -= im[cq[c]];
+            if (cq[c] == cq[d]) e += im[cq[c]];
+            M[c][d] = e * (r[c][0] * r[d][0] + r[c][1] * r[d][1] + r[c][2] * r[d][2]);
+        }
+    double mu[3] = {0.0, 0.0, 0.0};
+    if (nc == 1) {
+        if (M[0][0] == 0.0) return;
+        mu[0] = rhs[0] / M[0][0];
+    } else if (nc == 2) {
+        const double det = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+        if (det == 0.0) return;
+        mu[0] = (rhs[0] * M[1][1] - M[0][1] * rhs[1]) / det;
+        mu[1] = (M[0][0] * rhs[1] - rhs[0] * M[1][0]) / det;
+    } else {
+        const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) -
+                           M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                           M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        if (det == 0.0) return;
+        for (int c = 0; c < 3; ++c) {
+            double A[3][3];
+            for (int u = 0; u < 3; ++u)
+                for (int w = 0; w < 3; ++w) A[u][w] = (w == c) ? rhs[u] : M[u][w];
+            mu[c] = (A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                     A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                     A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0])) / det;
+        }
+    }
+    double dv[4][3] = {};
+    for (int c = 0; c < nc; ++c)
+        for (int d = 0; d < 3; ++d) {
+            dv[cp[c]][d] += mu[c] * im[cp[c]] * r[c][d];
+            dv[cq[c]][d] -= mu[c] * im[cq[c]] * r[c][d];
+        }
+    double *V[3] = {vx, vy, vz};
+    long long *F[3] = {fx, fy, fz};
+    for (int a = 0; a < na; ++a) {
+        const double mh = 1.0 / (im[a] * h);
+        for (int d = 0; d < 3; ++d) {
+            V[d][at[a]] = vv[a][d] + dv[a][d];
+            F[d][at[a]] -= fixd(dv[a][d] * mh);
+        }
+    }
+}
+__global__ void k_rattle(int ns, const int *__restrict__ sa, const double *__restrict__ x,
+                         const double *__restrict__ y, const double *__restrict__ z,
+                         double *__restrict__ vx, double *__restrict__ vy,
+                         double *__restrict__ vz, const double *__restrict__ invm, double L,
+                         double h, long long *__restrict__ fx, long long *__restrict__ fy,
+                         long long *__restrict__ fz) {
+    SOFIA_PDL_ENTRY();
+    rattle_body(blockIdx.x, ns, sa, x, y, z, vx, vy, vz, invm, L, h, fx, fy, fz);
+}
+
+// Langevin force alone (friction + noise of the current step counter) as the
+// whole force: the forces-only query's way to the thermostat term.
+__global__ void k_langevin_only(int n, LangevinArgs lg, long long *__restrict__ fx,
+                                long long *__restrict__ fy, long long *__restrict__ fz) {
+    SOFIA_PDL_ENTRY();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long a, b, c;
+    langevin_force(lg, i, a, b, c);
+    fx[i] = a;
+    fy[i] = b;
+    fz[i] = c;
+}
+
+__device__ __forceinline__ void ke_body(int bx, int n, const double *__restrict__ mass, const double *__restrict__ vx,
+                     const double *__restrict__ vy, const double *__restrict__ vz,
+                     double *__restrict__ ke) {
+    const int i = bx * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ke[i] = 0.5 * mass[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]) / KCAL2AMU;
+}
 __global__ void k_ke(int n, const double *__restrict__ mass, const double *__restrict__ vx,
                      const double *__restrict__ vy, const double *__restrict__ vz,
                      double *__restrict__ ke) {
     SOFIA_PDL_ENTRY();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    ke[i] = 0.5 * mass[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]) / KCAL2AMU;
+    ke_body(blockIdx.x, n, mass, vx, vy, vz, ke);
 }
 
 
 // Two-stage deterministic sum of column c of in[n][w] into out[slot].
 constexpr int MRED = 64;
-__global__ void k_mred1(int n, int w, int c, const double *__restrict__ in,
-                        double *__restrict__ part) {
-    SOFIA_PDL_ENTRY();
+__device__ __forceinline__ void mred1_body(int bx, int n, int w, int c, const double *__restrict__ in,
+                        double *__restrict__ part, int nblk) {
     __shared__ double s[256];
-    const int chunk = (n + gridDim.x - 1) / gridDim.x;
-    const int b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+    const int chunk = (n + nblk - 1) / nblk;
+    const int b0 = bx * chunk, b1 = min(n, b0 + chunk);
     double acc = 0.0;
     for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) acc += in[(size_t)i * w + c];
     s[threadIdx.x] = acc;
@@ -465,10 +609,14 @@ __global__ void k_mred1(int n, int w, int c, const double *__restrict__ in,
         if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
         __syncthreads();
     }
-    if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+    if (threadIdx.x == 0) part[bx] = s[0];
 }
-__global__ void k_mred2(const double *__restrict__ part, double *__restrict__ out) {
+__global__ void k_mred1(int n, int w, int c, const double *__restrict__ in,
+                        double *__restrict__ part) {
     SOFIA_PDL_ENTRY();
+    mred1_body(blockIdx.x, n, w, c, in, part, (int)gridDim.x);
+}
+__device__ __forceinline__ void mred2_body(int bx, const double *__restrict__ part, double *__restrict__ out) {
     __shared__ double s[MRED];
     s[threadIdx.x] = part[threadIdx.x];
     __syncthreads();
@@ -477,6 +625,10 @@ __global__ void k_mred2(const double *__restrict__ part, double *__restrict__ ou
         __syncthreads();
     }
     if (threadIdx.x == 0) out[0] = s[0];
+}
+__global__ void k_mred2(const double *__restrict__ part, double *__restrict__ out) {
+    SOFIA_PDL_ENTRY();
+    mred2_body(blockIdx.x, part, out);
 }
 
 }  // namespace
@@ -493,17 +645,9 @@ static void md_reduce(cudaStream_t st, int n, int w, int c, const double *in, do
 // All bonded terms of a step in one launch: threads [0, nb) take bonds, the
 // next na angles, then nd dihedrals (torsion and 1-4 pair), then ni impropers.
 // A count of 0 switches a term off.
-struct BondedArgs {
-    int nb, na, nd, ni;
-    const int *bl, *al, *il;
-    const double *bc, *ac, *ic;
-    double *eb, *ea, *ei;
-    DihArgs dih;
-};
 template <bool EN>
-__global__ void __launch_bounds__(128) k_bonded(BondedArgs b) {
-    SOFIA_PDL_ENTRY();
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bonded_body(int bx, const BondedArgs &b) {
+    int t = bx * blockDim.x + threadIdx.x;
     const DihArgs &d = b.dih;
     if (t < b.nb) {
         bond_term<EN>(t, b.nb, b.bl, b.bc, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.eb);
@@ -522,13 +666,57 @@ __global__ void __launch_bounds__(128) k_bonded(BondedArgs b) {
     t -= b.nd;
     if (t < b.ni) improper_term<EN>(t, b.ni, b.il, b.ic, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.ei);
 }
+template <bool EN>
+__global__ void __launch_bounds__(128) k_bonded(BondedArgs b) {
+    SOFIA_PDL_ENTRY();
+    bonded_body<EN>(blockIdx.x, b);
+}
 
-static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = false) {
+// Arguments of the torsion / 1-4 term (everything but the dihedral count).
+static void md_dih_args(Sys *s, double *et, DihArgs *ap) {
+    Md &md = s->md;
+    DihArgs &a = *ap;
+    a.ntypes = s->ntypes;
+    a.terms = md.terms;
+    a.dl = md.diheds.as<int>();
+    a.dc = md.dcoef.as<double>();
+    a.lj14 = md.lj14.as<double>();
+    a.x = s->x[0].as<double>();
+    a.y = s->x[1].as<double>();
+    a.z = s->x[2].as<double>();
+    a.type = s->type.as<int>();
+    a.q = s->q.as<float>();
+    a.L = s->L;
+    a.alpha = s->alpha;
+    a.EWALD_P = (double)0.3275911f;
+    a.A1 = (double)0.254829592f;
+    a.A2 = (double)-0.284496736f;
+    a.A3 = (double)1.421413741f;
+    a.A4 = (double)-1.453152027f;
+    a.A5 = (double)1.061405429f;
+    a.MY_PIS = (double)1.77245385090551602729f;
+    a.e_shift = s->e_shift;
+    a.f_shift = s->f_shift;
+    a.cut_coulsq = (double)(float)(s->rc * s->rc);
+    a.rcut2 = a.cut_coulsq;
+    a.coulpre = s->coulpre;
+    a.fx = s->f[0].as<long long>();
+    a.fy = s->f[1].as<long long>();
+    a.fz = s->f[2].as<long long>();
+    a.e = et + md.nbond + md.nangle;
+}
+
+// Parts of a step's force evaluation (all of them in an MD step; the
+// forces-only query selects).
+constexpr int MDF_PAIR = 1, MDF_LANGEVIN = 2, MDF_SHAKE = 4, MDF_ALL = 7;
+
+static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = false,
+                     int sel = MDF_ALL) {
     Md &md = s->md;
     cudaStream_t st = s->ctx->stream;
     // the Langevin force is added by the pair path's force unpack
     LangevinArgs lg{};
-    if (md.gamma > 0.0) {
+    if (md.gamma > 0.0 && (sel & MDF_LANGEVIN)) {
         const double kT = KBOLTZ * md.temperature;
         lg.on = 1;
         lg.gamma = md.gamma;
@@ -540,10 +728,23 @@ static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = fal
         lg.vy = s->v[1].as<double>();
         lg.vz = s->v[2].as<double>();
     }
-    int rc = sys_step_forces(s, s->precision, energy, false, force_build, disp_done, &lg);
-    if (rc) return rc;
     long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
               *fz = s->f[2].as<long long>();
+    if (sel & MDF_PAIR) {
+        int rc = sys_step_forces(s, s->precision, energy, false, force_build, disp_done, &lg);
+        if (rc) return rc;
+    } else {
+        const size_t nb = sizeof(long long) * (size_t)s->n;
+        SOFIA_CUDA(s->ctx, cudaMemsetAsync(fx, 0, nb, st));
+        SOFIA_CUDA(s->ctx, cudaMemsetAsync(fy, 0, nb, st));
+        SOFIA_CUDA(s->ctx, cudaMemsetAsync(fz, 0, nb, st));
+        SOFIA_CUDA(s->ctx, cudaMemsetAsync(s->red.p, 0, sizeof(double) * 5, st));
+        if (lg.on) {
+            sofia::launch_pdl(k_langevin_only, grid_for(s->n, 256), 256, 0, st, s->n, lg, fx, fy,
+                              fz);
+            s->launches += 1;
+        }
+    }
     const double *x = s->x[0].as<double>(), *y = s->x[1].as<double>(), *z = s->x[2].as<double>();
     double *et = md.eterm.as<double>();
     const int nb = md.nbond, na = md.nangle, nd = md.ndihed;
@@ -562,35 +763,8 @@ static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = fal
     b.ea = et + nb;
     b.ei = et + nb + na + 3 * (size_t)nd;
     DihArgs &a = b.dih;
+    md_dih_args(s, et, &a);
     a.nd = b.nd;
-    a.ntypes = s->ntypes;
-    a.terms = md.terms;
-    a.dl = md.diheds.as<int>();
-    a.dc = md.dcoef.as<double>();
-    a.lj14 = md.lj14.as<double>();
-    a.x = x;
-    a.y = y;
-    a.z = z;
-    a.type = s->type.as<int>();
-    a.q = s->q.as<float>();
-    a.L = s->L;
-    a.alpha = s->alpha;
-    a.EWALD_P = (double)0.3275911f;
-    a.A1 = (double)0.254829592f;
-    a.A2 = (double)-0.284496736f;
-    a.A3 = (double)1.421413741f;
-    a.A4 = (double)-1.453152027f;
-    a.A5 = (double)1.061405429f;
-    a.MY_PIS = (double)1.77245385090551602729f;
-    a.e_shift = s->e_shift;
-    a.f_shift = s->f_shift;
-    a.cut_coulsq = (double)(float)(s->rc * s->rc);
-    a.rcut2 = a.cut_coulsq;
-    a.coulpre = s->coulpre;
-    a.fx = fx;
-    a.fy = fy;
-    a.fz = fz;
-    a.e = et + nb + na;
     const long nterm = (long)b.nb + b.na + b.nd + b.ni;
     if (nterm > 0) {
         if (energy)
@@ -598,7 +772,7 @@ static int md_forces(Sys *s, bool energy, bool force_build, bool disp_done = fal
         else
             sofia::launch_pdl(k_bonded<false>, grid_for(nterm, 128), 128, 0, st, b);
     }
-    if (md.nshake) {
+    if (md.nshake && (sel & MDF_SHAKE)) {
         sofia::launch_pdl(k_shake, grid_for(md.nshake, 128), 128, 0, st,
             md.nshake, md.shake.as<int>(), md.sbond.as<double>(), x, y, z, s->v[0].as<double>(),
             s->v[1].as<double>(), s->v[2].as<double>(), s->invm.as<double>(), s->L, md.dt,
@@ -673,6 +847,14 @@ static int md_step(Sys *s, bool energy) {
     int rc = md_forces(s, energy, false, true);
     if (rc) return rc;
     sofia::launch_pdl(k_kick, grid_for(n, 256), 256, 0, st, n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz);
+    if (md.rattle && md.nshake) {
+        sofia::launch_pdl(k_rattle, grid_for(md.nshake, 128), 128, 0, st, md.nshake,
+                          md.shake.as<int>(), s->x[0].as<double>(), s->x[1].as<double>(),
+                          s->x[2].as<double>(), vx, vy, vz, s->invm.as<double>(), s->L, h,
+                          s->f[0].as<long long>(), s->f[1].as<long long>(),
+                          s->f[2].as<long long>());
+        s->launches += 1;
+    }
     if (energy) md_energy_reduce(s);
     s->launches += 2;
     SOFIA_CUDA(s->ctx, cudaGetLastError());
@@ -746,6 +928,11 @@ extern "C" int sofia_system_md_setup(sofia_system *ss, const sofia_md_desc *d) {
     md.nshake = d->shake ? d->nshake : 0;
     md.nimpro = d->impropers ? d->nimpro : 0;
     md.terms = d->terms;
+    if (d->flags & ~(SOFIA_MD_RATTLE | SOFIA_MD_LJ_SHIFT))
+        return sofia::fail(ctx, SOFIA_EINVAL, "unknown sofia_md_desc flags%s");
+    md.rattle = (d->flags & SOFIA_MD_RATTLE) ? 1 : 0;
+    s->lj_shift = (d->flags & SOFIA_MD_LJ_SHIFT) ? 1 : 0;
+    sofia::dropin_drop(s);  // the captured drop-in graphs hold the pair constants
     md.shake_maxiter = d->shake_maxiter > 0 ? d->shake_maxiter : 25;
     md.shake_tol = d->shake_tol > 0.0 ? d->shake_tol : (double)0.0001f;
     int rc;
@@ -792,6 +979,7 @@ extern "C" int sofia_system_md_setup(sofia_system *ss, const sofia_md_desc *d) {
                          (size_t)md.nimpro + (size_t)s->n;
     SOFIA_CUDA(ctx, md.eterm.ensure(sizeof(double) * nterm));
     SOFIA_CUDA(ctx, md.ered.ensure(sizeof(double) * (16 + sofia::MRED)));
+    SOFIA_CUDA(ctx, md.bpart.ensure(sizeof(double) * sofia::MD_NJOB * sofia::MRED));
     SOFIA_CUDA(ctx, cudaMemset(md.ered.p, 0, sizeof(double) * 16));
     SOFIA_CUDA(ctx, md.step_dev.ensure(sizeof(long long)));
     SOFIA_CUDA(ctx, cudaMemset(md.step_dev.p, 0, sizeof(long long)));
@@ -892,21 +1080,279 @@ extern "C" int sofia_system_md_run(sofia_system *ss, int nsteps, int energy_ever
     return sofia::fail(ctx, SOFIA_ENEEDGROW, "list capacity kept overflowing%s");
 }
 
+// Forces of one MD step at the resident positions and velocities, without
+// stepping: the step's force evaluation (force_wrapper_DSF's zero / nonbond /
+// bonded / 1-4 merge, Source/mod_force.f90:510-554, plus the Langevin force
+// and SHAKE's constraint forces for the next step) restricted to the selected
+// terms, all summed in 64-bit fixed point as in the step.
+extern "C" int sofia_system_md_forces(sofia_system *ss, int terms, double *f, double *energies) {
+    if (!ss) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    Md &md = s->md;
+    if (!md.ready) return sofia::fail(ctx, SOFIA_EINVAL, "sofia_system_md_setup first%s");
+    if (!s->mass.p) return sofia::fail(ctx, SOFIA_EINVAL, "system created without masses%s");
+    if (terms & ~(SOFIA_TERM_BOND | SOFIA_TERM_ANGLE | SOFIA_TERM_TORSION | SOFIA_TERM_PAIR14 |
+                  SOFIA_TERM_IMPROPER | SOFIA_TERM_NONBOND | SOFIA_TERM_LANGEVIN |
+                  SOFIA_TERM_SHAKE))
+        return sofia::fail(ctx, SOFIA_EINVAL, "unknown force term bits%s");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int sel = 0;
+    if (terms & SOFIA_TERM_NONBOND) sel |= sofia::MDF_PAIR;
+    if (terms & SOFIA_TERM_LANGEVIN) sel |= sofia::MDF_LANGEVIN;
+    if (terms & SOFIA_TERM_SHAKE) sel |= sofia::MDF_SHAKE;
+    const int saved = md.terms;
+    md.terms = saved & terms & 31;
+    SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * sofia::ST_NSLOTS, st));
+    // terms left out keep no energy from an earlier step
+    SOFIA_CUDA(ctx, cudaMemsetAsync(md.ered.p, 0, sizeof(double) * 16, st));
+    int rc = sofia::md_forces(s, energies != nullptr, false, false, sel);
+    if (!rc && energies) sofia::md_energy_reduce(s);
+    md.terms = saved;
+    if (rc) return rc;
+    // the step's forces are replaced: the next MD run recomputes its own
+    md.forces_valid = 0;
+    rc = sofia::sys_list_overflow(s);
+    if (rc == SOFIA_ENEEDGROW) {
+        // the row capacity grew: evaluate again on the rebuilt list
+        md.terms = saved & terms & 31;
+        rc = sofia::md_forces(s, energies != nullptr, true, false, sel);
+        if (!rc && energies) sofia::md_energy_reduce(s);
+        md.terms = saved;
+        if (!rc) rc = sofia::sys_list_overflow(s);
+    }
+    if (rc) return rc;
+    int hs[sofia::ST_NSLOTS];
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(hs, s->status_local.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
+    if (hs[sofia::ST_SHAKE])
+        return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE determinant <= 0 (mod_shake.f90:146-153, :267)%s");
+    if (f) {
+        const size_t n = (size_t)s->n;
+        std::vector<long long> h(3 * n);
+        for (int d = 0; d < 3; ++d)
+            SOFIA_CUDA(ctx, cudaMemcpy(h.data() + d * n, s->f[d].p, sizeof(long long) * n,
+                                       cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) f[3 * i + d] = (double)h[d * n + i] * sofia::FIX_INV;
+    }
+    if (energies) {
+        double e[16];
+        SOFIA_CUDA(ctx, cudaMemcpy(e, md.ered.p, sizeof(double) * 16, cudaMemcpyDeviceToHost));
+        sofia::md_fill_energies(md, e, energies);
+    }
+    return SOFIA_OK;
+}
+
 // ---------------------------------------------------------------------------
-// Batches of independent replicas.  Every replica keeps its own resident state
-// and list on its own context stream; one CUDA graph per step kind forks from
-// the batch stream into every replica stream, records each replica's MD step
-// there, and joins back, so a whole multi-replica step is one graph launch and
-// replicas of different sizes overlap on the GPU.  Replicas never exchange
-// data: each result is bit-identical to the same replica run alone.
+// Batches of independent replicas.  Every kernel of an MD step runs once for all
+// replicas of the batch (BatchDev in system.cuh): a launch walks its virtual
+// blocks in a grid-stride loop over the replicas' own buffers, with the block
+// size and body of the single-system kernel, so a replica's trajectory is
+// bit-identical to the same replica run alone.  Steps are captured as CUDA
+// graphs of `seg` steps (100 by default); the graphs hold only the address of
+// the device table, which the host rewrites when membership changes or a list
+// grows, so neither needs a recapture.  Replicas never exchange data (the
+// reference runs one replica per MPI rank, Source/MD.f90:26-44).
+namespace sofia {
+namespace {
+
+#define SOFIA_BATCH_LOOP(KIND)                                                   \
+    const int nrep_ = tab->nrep;                                                 \
+    const int *pre_ = tab->pre[KIND];                                            \
+    const int tot_ = pre_[nrep_];                                                \
+    for (int vb = blockIdx.x; vb < tot_; vb += gridDim.x) {                      \
+        const int r_ = batch_rep(pre_, nrep_, vb);                               \
+        const RepDev &d = tab->rep[r_];                                          \
+        const int lb = vb - pre_[r_];
+#define SOFIA_BATCH_END }
+
+__global__ void k_kick_drift_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_A256)
+    kick_drift_body(lb, d.n, d.h, d.invm, d.fx, d.fy, d.fz, d.vx, d.vy, d.vz, d.dt, d.x, d.y,
+                    d.z, d.rx, d.ry, d.rz, d.px, d.py, d.pz, d.L, d.lim2, d.plim2, d.flag,
+                    d.step);
+    SOFIA_BATCH_END
+}
+
+template <bool EN>
+__global__ void __launch_bounds__(128) k_bonded_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_B128)
+    bonded_body<EN>(lb, d.b);
+    SOFIA_BATCH_END
+}
+
+__global__ void k_shake_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_G128)
+    shake_body(lb, d.nshake, d.shake, d.sbond, d.x, d.y, d.z, d.vx, d.vy, d.vz, d.invm, d.L,
+               d.dt, d.dtsq, d.shake_maxiter, d.shake_tol, d.fx, d.fy, d.fz, d.status);
+    SOFIA_BATCH_END
+}
+
+__global__ void k_kick_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_A256)
+    kick_body(lb, d.n, d.h, d.invm, d.fx, d.fy, d.fz, d.vx, d.vy, d.vz);
+    SOFIA_BATCH_END
+}
+
+__global__ void k_rattle_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_G128)
+    if (d.rattle)
+        rattle_body(lb, d.nshake, d.shake, d.x, d.y, d.z, d.vx, d.vy, d.vz, d.invm, d.L, d.h,
+                    d.fx, d.fy, d.fz);
+    SOFIA_BATCH_END
+}
+
+// Energy steps: pair sums to their slots, kinetic energy, then the per-term sums
+// with the same two-stage trees (MRED blocks, then one block) as md_reduce.
+__global__ void k_copyred_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_REP)
+    if (threadIdx.x < 5) d.ered[threadIdx.x] = d.red[threadIdx.x];
+    SOFIA_BATCH_END
+}
+
+__global__ void k_ke_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_A256)
+    ke_body(lb, d.n, d.mass, d.vx, d.vy, d.vz, d.ke);
+    SOFIA_BATCH_END
+}
+
+__global__ void k_mred1_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_MRED)
+    const int job = lb / MRED, blk = lb - job * MRED;
+    if (d.job_n[job] > 0)
+        mred1_body(blk, d.job_n[job], d.job_w[job], d.job_c[job], d.job_in[job],
+                   d.ebpart + job * MRED, MRED);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+__global__ void k_mred2_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_MJOB)
+    if (d.job_n[lb] > 0) mred2_body(0, d.ebpart + lb * MRED, d.ered + d.job_slot[lb]);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+#undef SOFIA_BATCH_LOOP
+#undef SOFIA_BATCH_END
+
+}  // namespace
+
+// The MD part of a replica's table entry (step constants, thermostat, bonded
+// terms, SHAKE, energy-sum jobs); the argument values of md_forces / md_step.
+static void repdev_fill_md(Sys *s, RepDev *d) {
+    Md &md = s->md;
+    d->h = 0.5 * md.dt * KCAL2AMU;
+    d->dt = md.dt;
+    d->dtsq = md.dt * md.dt * KCAL2AMU;
+    d->shake_maxiter = md.shake_maxiter;
+    d->shake_tol = md.shake_tol;
+    d->nshake = md.nshake;
+    d->rattle = md.rattle;
+    d->shake = md.shake.as<int>();
+    d->sbond = md.sbond.as<double>();
+    d->step = md.step_dev.as<long long>();
+    LangevinArgs lg{};
+    if (md.gamma > 0.0) {
+        const double kT = KBOLTZ * md.temperature;
+        lg.on = 1;
+        lg.gamma = md.gamma;
+        lg.gsig = sqrt(12.0 * 2.0 * md.gamma * kT * KCAL2AMU / md.dt) / KCAL2AMU;
+        lg.seed = md.seed;
+        lg.step = md.step_dev.as<long long>();
+        lg.mass = s->mass.as<double>();
+        lg.vx = s->v[0].as<double>();
+        lg.vy = s->v[1].as<double>();
+        lg.vz = s->v[2].as<double>();
+    }
+    d->lg = lg;
+    double *et = md.eterm.as<double>();
+    const int nb = md.nbond, na = md.nangle, nd = md.ndihed;
+    BondedArgs &b = d->b;
+    b.nb = (md.terms & 1) ? nb : 0;
+    b.na = (md.terms & 2) ? na : 0;
+    b.nd = (md.terms & 12) ? nd : 0;
+    b.ni = (md.terms & 16) ? md.nimpro : 0;
+    b.bl = md.bonds.as<int>();
+    b.bc = md.bcoef.as<double>();
+    b.al = md.angles.as<int>();
+    b.ac = md.acoef.as<double>();
+    b.il = md.impros.as<int>();
+    b.ic = md.icoef.as<double>();
+    b.eb = et;
+    b.ea = et + nb;
+    b.ei = et + nb + na + 3 * (size_t)nd;
+    DihArgs &a = b.dih;
+    md_dih_args(s, et, &a);
+    a.nd = b.nd;
+    d->ered = md.ered.as<double>();
+    d->ebpart = md.bpart.as<double>();
+    d->ke = et + (nb + na + 3 * (size_t)nd + (size_t)md.nimpro);
+    const int jn[MD_NJOB] = {(nb && (md.terms & 1)) ? nb : 0, (na && (md.terms & 2)) ? na : 0,
+                             (nd && (md.terms & 12)) ? nd : 0, (nd && (md.terms & 12)) ? nd : 0,
+                             (nd && (md.terms & 12)) ? nd : 0,
+                             (md.nimpro && (md.terms & 16)) ? md.nimpro : 0, s->n};
+    const int jw[MD_NJOB] = {1, 1, 3, 3, 3, 1, 1}, jc[MD_NJOB] = {0, 0, 0, 1, 2, 0, 0};
+    const int js[MD_NJOB] = {5, 6, 7, 8, 9, 11, 10};
+    const double *jin[MD_NJOB] = {et, et + nb, et + nb + na, et + nb + na, et + nb + na,
+                                  et + nb + na + 3 * (size_t)nd, d->ke};
+    for (int k = 0; k < MD_NJOB; ++k) {
+        d->job_n[k] = jn[k];
+        d->job_w[k] = jw[k];
+        d->job_c[k] = jc[k];
+        d->job_slot[k] = js[k];
+        d->job_in[k] = jin[k];
+    }
+}
+
+// One batched MD step: the same kernels, in the same order, as md_step.
+static void batch_step(const BatchDev *tab, Sys *s0, bool energy, bool rattle, cudaStream_t st,
+                       int nsm) {
+    const int g256 = nsm * 8, g128 = nsm * 16;
+    launch_pdl(k_kick_drift_b, g256, 256, 0, st, tab);
+    batch_pair_path(tab, s0, s0->precision, energy, st, nsm);
+    if (energy)
+        launch_pdl(k_bonded_b<true>, g128, 128, 0, st, tab);
+    else
+        launch_pdl(k_bonded_b<false>, g128, 128, 0, st, tab);
+    launch_pdl(k_shake_b, g128, 128, 0, st, tab);
+    launch_pdl(k_kick_b, g256, 256, 0, st, tab);
+    if (rattle) launch_pdl(k_rattle_b, g128, 128, 0, st, tab);
+    if (energy) {
+        launch_pdl(k_copyred_b, nsm, 32, 0, st, tab);
+        launch_pdl(k_ke_b, g256, 256, 0, st, tab);
+        launch_pdl(k_mred1_b, g256, 256, 0, st, tab);
+        launch_pdl(k_mred2_b, nsm * 8, MRED, 0, st, tab);
+    }
+}
+
+}  // namespace sofia
+
 struct sofia_batch {
     sofia_nb_ctx *ctx = nullptr;
     std::vector<sofia_system *> sys;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    long long graph_launches[2] = {0, 0};
+    sofia::DevBuf tab;                  // BatchDev on the device
+    std::vector<unsigned char> htab;    // its host image
+    int seg = 100;                      // steps per captured segment graph
+    int nsm = 148;
+    // captured graphs: [0] one step, [1] one step with energies, [2] seg steps,
+    // [3] seg steps with energies on the last
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
     int graph_ok = 0;
-    cudaEvent_t fork = nullptr;
-    std::vector<cudaEvent_t> join;
+    int graph_rattle = 0;               // the graphs hold the RATTLE launch
+    sofia::PairKey graph_key{};         // the pair constants the graphs hold
+    long long step_launches[2] = {0, 0};
 };
 
 static void batch_drop_graphs(sofia_batch *b) {
@@ -918,31 +1364,66 @@ static void batch_drop_graphs(sofia_batch *b) {
     b->graph_ok = 0;
 }
 
-extern "C" int sofia_batch_create(sofia_nb_ctx *ctx, sofia_system *const *systems, int n,
-                                  sofia_batch **out) {
-    if (!ctx || !systems || n <= 0 || !out) return SOFIA_EINVAL;
-    *out = nullptr;
-    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+static int batch_check_members(sofia_nb_ctx *ctx, sofia_system *const *systems, int n) {
+    if (n <= 0 || n > sofia::MAXREP)
+        return sofia::fail(ctx, SOFIA_EINVAL, "a batch holds 1 to 256 replicas%s");
     for (int i = 0; i < n; ++i) {
         if (!systems[i]) return sofia::fail(ctx, SOFIA_EINVAL, "null system in batch%s");
         if (systems[i]->s.ctx->device != ctx->device)
             return sofia::fail(ctx, SOFIA_EINVAL, "batch systems must share the device%s");
         if (!systems[i]->s.md.ready)
             return sofia::fail(ctx, SOFIA_EINVAL, "sofia_system_md_setup every system first%s");
+        if (!systems[i]->s.mass.p)
+            return sofia::fail(ctx, SOFIA_EINVAL, "system created without masses%s");
+        if (!sofia::pair_const_compatible(&systems[0]->s, &systems[i]->s))
+            return sofia::fail(ctx, SOFIA_EINVAL,
+                               "batch systems must share precision, types, cut-off and DSF "
+                               "constants%s");
         for (int j = 0; j < i; ++j)
             if (systems[j] == systems[i]) return sofia::fail(ctx, SOFIA_EINVAL, "system listed twice%s");
     }
+    return SOFIA_OK;
+}
+
+// Rewrites the device table from the members' current buffers and sizes.
+static int batch_upload(sofia_batch *b) {
+    sofia_nb_ctx *ctx = b->ctx;
+    const int n = (int)b->sys.size();
+    if (b->htab.size() != sizeof(sofia::BatchDev)) b->htab.assign(sizeof(sofia::BatchDev), 0);
+    auto *h = reinterpret_cast<sofia::BatchDev *>(b->htab.data());
+    h->nrep = n;
+    for (int k = 0; k < sofia::BK_N; ++k) h->pre[k][0] = 0;
+    for (int r = 0; r < n; ++r) {
+        Sys *s = &b->sys[r]->s;
+        sofia::RepDev &d = h->rep[r];
+        sofia::repdev_fill_pair(s, &d);
+        sofia::repdev_fill_md(s, &d);
+        const long nterm = (long)d.b.nb + d.b.na + d.b.nd + d.b.ni;
+        const int cnt[sofia::BK_N] = {
+            sofia::grid_for(s->n, 256), 1, s->ncols, sofia::grid_for((long)s->max_clusters * 8, 256),
+            sofia::grid_for(s->max_clusters, 128), sofia::grid_for((long)s->max_clusters * 32, 256),
+            sofia::grid_for(nterm, 128), sofia::grid_for(s->md.nshake, 128), sofia::RED_BLOCKS,
+            1, sofia::MD_NJOB * sofia::MRED, sofia::MD_NJOB};
+        for (int k = 0; k < sofia::BK_N; ++k) h->pre[k][r + 1] = h->pre[k][r] + cnt[k];
+    }
+    SOFIA_CUDA(ctx, b->tab.ensure(sizeof(sofia::BatchDev)));
+    const size_t used = offsetof(sofia::BatchDev, rep) + sizeof(sofia::RepDev) * (size_t)n;
+    SOFIA_CUDA(ctx, cudaMemcpyAsync(b->tab.p, h, used, cudaMemcpyHostToDevice, ctx->stream));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_batch_create(sofia_nb_ctx *ctx, sofia_system *const *systems, int n,
+                                  sofia_batch **out) {
+    if (!ctx || !systems || !out) return SOFIA_EINVAL;
+    *out = nullptr;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    int rc = batch_check_members(ctx, systems, n);
+    if (rc) return rc;
     sofia_batch *b = new sofia_batch();
     b->ctx = ctx;
     b->sys.assign(systems, systems + n);
-    b->join.resize(n, nullptr);
-    cudaError_t e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
-    for (int i = 0; i < n && e == cudaSuccess; ++i)
-        e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
-    if (e != cudaSuccess) {
-        sofia_batch_destroy(b);
-        return sofia::cuda_fail(ctx, e, "batch events");
-    }
+    cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
     *out = b;
     return SOFIA_OK;
 }
@@ -951,10 +1432,39 @@ extern "C" int sofia_batch_destroy(sofia_batch *b) {
     if (!b) return SOFIA_OK;
     if (b->ctx) cudaStreamSynchronize(b->ctx->stream);
     batch_drop_graphs(b);
-    if (b->fork) cudaEventDestroy(b->fork);
-    for (auto e : b->join)
-        if (e) cudaEventDestroy(e);
+    b->tab.release();
     delete b;
+    return SOFIA_OK;
+}
+
+// Replaces the batch's members (continuous batching).  The captured graphs stay
+// valid when the new members share the first member's pair constants and need
+// no RATTLE launch the graphs lack.
+extern "C" int sofia_batch_set_systems(sofia_batch *b, sofia_system *const *systems, int n) {
+    if (!b || !systems) return SOFIA_EINVAL;
+    sofia_nb_ctx *ctx = b->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    int rc = batch_check_members(ctx, systems, n);
+    if (rc) return rc;
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    b->sys.assign(systems, systems + n);
+    if (b->graph_ok) {
+        bool rat = false;
+        for (auto *s : b->sys) rat = rat || (s->s.md.rattle && s->s.md.nshake);
+        const bool keep = (!rat || b->graph_rattle) && b->graph_key == sofia::pair_key(&b->sys[0]->s);
+        if (!keep) batch_drop_graphs(b);
+    }
+    return SOFIA_OK;
+}
+
+extern "C" int sofia_batch_set_segment(sofia_batch *b, int steps) {
+    if (!b || steps < 1 || steps > 1000) return SOFIA_EINVAL;
+    if (steps != b->seg) {
+        sofia_nb_ctx *ctx = b->ctx;
+        SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        batch_drop_graphs(b);
+        b->seg = steps;
+    }
     return SOFIA_OK;
 }
 
@@ -962,50 +1472,34 @@ static int batch_capture(sofia_batch *b) {
     batch_drop_graphs(b);
     sofia_nb_ctx *ctx = b->ctx;
     cudaStream_t ms = ctx->stream;
-    for (int e = 0; e < 2; ++e) {
-        cudaGraph_t g = nullptr;
-        long long launches = 0;
-        SOFIA_CUDA(ctx, cudaStreamBeginCapture(ms, cudaStreamCaptureModeRelaxed));
-        int rc = SOFIA_OK;
-        if (cudaEventRecord(b->fork, ms) != cudaSuccess) rc = SOFIA_ECUDA;
-        for (size_t i = 0; i < b->sys.size() && !rc; ++i) {
-            Sys *s = &b->sys[i]->s;
-            cudaStream_t st = s->ctx->stream;
-            if (st != ms && cudaStreamWaitEvent(st, b->fork, 0) != cudaSuccess) {
-                rc = SOFIA_ECUDA;
-                break;
-            }
-            const int timing = s->timing;
-            s->timing = 0;
-            const long long l0 = s->launches;
-            rc = sofia::md_step(s, e == 1);
-            launches += s->launches - l0;
-            s->launches = l0;
-            s->timing = timing;
-            if (!rc && st != ms) {
-                if (cudaEventRecord(b->join[i], st) != cudaSuccess ||
-                    cudaStreamWaitEvent(ms, b->join[i], 0) != cudaSuccess)
-                    rc = SOFIA_ECUDA;
-            }
-        }
-        cudaError_t ce = cudaStreamEndCapture(ms, &g);
-        if (rc) {
-            if (g) cudaGraphDestroy(g);
-            cudaGetLastError();
-            return rc == SOFIA_ECUDA ? sofia::fail(ctx, rc, "batch capture failed%s") : rc;
-        }
+    const auto *tab = b->tab.as<sofia::BatchDev>();
+    Sys *s0 = &b->sys[0]->s;
+    bool rat = false;
+    for (auto *s : b->sys) rat = rat || (s->s.md.rattle && s->s.md.nshake);
+    const int nsteps[4] = {1, 1, b->seg, b->seg};
+    for (int g = 0; g < 4; ++g) {
+        cudaGraph_t graph = nullptr;
+        SOFIA_CUDA(ctx, cudaStreamBeginCapture(ms, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < nsteps[g]; ++k)
+            sofia::batch_step(tab, s0, (g & 1) && k == nsteps[g] - 1, rat, ms, b->nsm);
+        cudaError_t ce = cudaStreamEndCapture(ms, &graph);
         if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaStreamEndCapture (batch)");
-        ce = cudaGraphInstantiate(&b->graph[e], g, 0);
-        cudaGraphDestroy(g);
+        ce = cudaGraphInstantiate(&b->graph[g], graph, 0);
+        cudaGraphDestroy(graph);
         if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaGraphInstantiate (batch)");
-        b->graph_launches[e] = launches;
     }
+    b->step_launches[0] = 12 + 1 + 5 + (rat ? 1 : 0);
+    b->step_launches[1] = b->step_launches[0] + 2 + 4;
+    b->graph_rattle = rat;
+    b->graph_key = sofia::pair_key(s0);
     b->graph_ok = 1;
     return SOFIA_OK;
 }
 
-// Runs nsteps steps of every replica.  energies[n*SOFIA_MD_NE] (may be NULL)
-// receive each replica's last-step energies when energy_every > 0.
+// Runs nsteps steps of every replica: segments of `seg` steps as one graph
+// launch each, the rest one step per launch.  energies[n*SOFIA_MD_NE] (may be
+// NULL) receive each replica's energies of the last step when energy_every > 0
+// (only that step computes them).
 extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
                                   double *energies) {
     if (!b || nsteps < 0) return SOFIA_EINVAL;
@@ -1013,6 +1507,7 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t ms = ctx->stream;
     const int n = (int)b->sys.size();
+    const bool want_e = energy_every > 0 && nsteps > 0;
     for (int attempt = 0; attempt < 4; ++attempt) {
         for (int i = 0; i < n; ++i) {
             Sys *s = &b->sys[i]->s;
@@ -1030,30 +1525,39 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
                 if (rc) return rc;
                 md.forces_valid = 1;
             }
-            SOFIA_CUDA(ctx, cudaStreamSynchronize(st));
         }
+        for (int i = 0; i < n; ++i) SOFIA_CUDA(ctx, cudaStreamSynchronize(b->sys[i]->s.ctx->stream));
+        int rc = batch_upload(b);
+        if (rc) return rc;
         if (!b->graph_ok) {
-            int rc = batch_capture(b);
+            rc = batch_capture(b);
             if (rc) return rc;
         }
-        for (int k = 0; k < nsteps; ++k) {
-            const bool en = energy_every > 0 && ((k + 1) % energy_every == 0 || k + 1 == nsteps);
-            SOFIA_CUDA(ctx, cudaGraphLaunch(b->graph[en ? 1 : 0], ms));
+        int left = nsteps;
+        long long launched = 0;
+        while (left > 0) {
+            const bool full = left >= b->seg;
+            const int k = full ? b->seg : 1;
+            const bool en = want_e && left == k;
+            SOFIA_CUDA(ctx, cudaGraphLaunch(b->graph[(full ? 2 : 0) + (en ? 1 : 0)], ms));
+            launched += (long long)k * b->step_launches[0] + (en ? 6 : 0);
+            left -= k;
         }
         SOFIA_CUDA(ctx, cudaStreamSynchronize(ms));
         bool regrow = false;
         for (int i = 0; i < n; ++i) {
             Sys *s = &b->sys[i]->s;
-            s->launches += (long long)nsteps * (b->graph_launches[0]) / (n > 0 ? n : 1);
-            const int rc = sofia::sys_list_overflow(s);
-            if (rc == SOFIA_ENEEDGROW) {
+            s->launches += launched / (n > 0 ? n : 1);
+            const int r2 = sofia::sys_list_overflow(s);
+            if (r2 == SOFIA_ENEEDGROW) {
                 regrow = true;
                 continue;
             }
-            if (rc) return rc;
+            if (r2) return r2;
         }
         if (regrow) {
-            batch_drop_graphs(b);
+            // a list row overflowed: every replica restarts the segment from its
+            // snapshot (the table is rewritten with the grown lists)
             for (int i = 0; i < n; ++i) {
                 Sys *s = &b->sys[i]->s;
                 Md &md = s->md;
@@ -1080,7 +1584,7 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
                 return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE determinant <= 0 in a batch replica%s");
             s->shake_nc += hs[sofia::ST_SHAKE_NC];
             md.step += nsteps;
-            if (energies && energy_every > 0) {
+            if (energies && want_e) {
                 double e[16];
                 SOFIA_CUDA(ctx, cudaMemcpy(e, md.ered.p, sizeof(double) * 16, cudaMemcpyDeviceToHost));
                 double *o = energies + (size_t)i * SOFIA_MD_NE;
@@ -1161,6 +1665,57 @@ extern "C" int sofia_system_rollback(sofia_system *ss) {
     s->built = 0;
     md.forces_valid = 0;
     return SOFIA_OK;
+}
+
+namespace sofia {
+namespace {
+// Resident FP64 positions -> real*4 ainfo records wrapped into (0, box] (the
+// state the reference's pbc leaves, Source/mod_pbc.f90:6-39, from the
+// double-precision wrap x - L floor(x / L)), and global ids 1..n.
+__global__ void k_resident_ainfo(int n, const double *__restrict__ x,
+                                 const double *__restrict__ y, const double *__restrict__ z,
+                                 const int *__restrict__ type, double L, float box,
+                                 float4 *__restrict__ out, int *__restrict__ gid) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float w[3];
+    const double p[3] = {x[i], y[i], z[i]};
+    for (int d = 0; d < 3; ++d) {
+        float f = (float)(p[d] - L * floor(p[d] / L));
+        if (f <= 0.0f) f += box;
+        w[d] = f;
+    }
+    out[i] = make_float4(w[0], w[1], w[2], __int_as_float(type[i]));
+    gid[i] = i + 1;
+}
+}  // namespace
+}  // namespace sofia
+
+// Largest-cluster analysis (get_greatestCluster, Source/mod_cluster.f90:15-83)
+// on a resident system's current positions: the positions never leave the
+// device, as nuc_move keeps them between segments
+// (Source/mod_nucleation.f90:396-449).  Glycine molecules are the first
+// n_gly * atoms_per_gly atoms; ptta_full (host or device) and
+// *greatest_belongsto are in/out as in sofia_greatest_cluster.
+extern "C" int sofia_system_greatest_cluster(sofia_system *ss, int n_gly, int atoms_per_gly,
+                                             double mrcut, double denscut, int densmin,
+                                             double *ptta_full, int32_t *greatest_belongsto,
+                                             int32_t *size_out) {
+    if (!ss || !size_out) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    if (n_gly < 0 || atoms_per_gly <= 0 || (size_t)n_gly * atoms_per_gly > (size_t)s->n)
+        return sofia::fail(ctx, SOFIA_EINVAL, "glycine atoms beyond the system%s");
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    SOFIA_CUDA(ctx, s->cl_pos.ensure(sizeof(float4) * (size_t)s->n));
+    SOFIA_CUDA(ctx, s->cl_gid.ensure(sizeof(int) * (size_t)s->n));
+    sofia::k_resident_ainfo<<<sofia::grid_for(s->n, 256), 256, 0, ctx->stream>>>(
+        s->n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
+        s->type.as<int>(), s->L, s->box, s->cl_pos.as<float4>(), s->cl_gid.as<int>());
+    SOFIA_CUDA(ctx, cudaGetLastError());
+    return sofia_greatest_cluster(ctx, s->n, s->cl_pos.as<sofia_ainfo>(), s->cl_gid.as<int32_t>(),
+                                  n_gly, atoms_per_gly, s->box, mrcut, denscut, densmin,
+                                  ptta_full, greatest_belongsto, size_out, nullptr, nullptr);
 }
 
 // Thermostat step counter (the Philox counter of the Langevin noise): read it

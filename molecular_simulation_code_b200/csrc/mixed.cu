@@ -60,7 +60,7 @@ __device__ __forceinline__ double wrap_shift(double x, double L) {
     return -L * floor(x / L);
 }
 
-__global__ void k_wrap_bin(const int *__restrict__ cond, int cmask, int n,
+__device__ __forceinline__ void wrap_bin_body(int bx, const int *__restrict__ cond, int cmask, int n,
                            const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ z, double L, double s_col, int ncx,
                            double *__restrict__ ix, double *__restrict__ iy,
@@ -68,9 +68,8 @@ __global__ void k_wrap_bin(const int *__restrict__ cond, int cmask, int n,
                            double *__restrict__ ry, double *__restrict__ rz,
                            int *__restrict__ col_of, int *__restrict__ col_count,
                            float *__restrict__ zkey) {
-    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = bx * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double px = x[i], py = y[i], pz = z[i];
     double sx = wrap_shift(px, L), sy = wrap_shift(py, L), sz = wrap_shift(pz, L);
@@ -94,14 +93,24 @@ __global__ void k_wrap_bin(const int *__restrict__ cond, int cmask, int n,
     zkey[i] = (float)wz;
     atomicAdd(&col_count[c], 1);
 }
+__global__ void k_wrap_bin(const int *__restrict__ cond, int cmask, int n,
+                           const double *__restrict__ x, const double *__restrict__ y,
+                           const double *__restrict__ z, double L, double s_col, int ncx,
+                           double *__restrict__ ix, double *__restrict__ iy,
+                           double *__restrict__ iz, double *__restrict__ rx,
+                           double *__restrict__ ry, double *__restrict__ rz,
+                           int *__restrict__ col_of, int *__restrict__ col_count,
+                           float *__restrict__ zkey) {
+    SOFIA_PDL_ENTRY();
+    wrap_bin_body(blockIdx.x, cond, cmask, n, x, y, z, L, s_col, ncx, ix, iy, iz, rx, ry, rz, col_of, col_count, zkey);
+}
 
 // Column scans of a build, one block: col_start = exclusive scan of the atom
 // counts, cl_start = exclusive scan of the cluster counts (ceil(count/8)), the
 // total cluster count into ncl.  The counts are cleared for the next build.
-__global__ void k_scan_cols(const int *__restrict__ cond, int cmask, int n,
+__device__ __forceinline__ void scan_cols_body(int bx, const int *__restrict__ cond, int cmask, int n,
                             int *__restrict__ col_count, int *__restrict__ col_start,
                             int *__restrict__ cl_start, int *__restrict__ ncl) {
-    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     __shared__ int s1[1024], s2[1024];
     __shared__ int carry1, carry2;
@@ -140,31 +149,42 @@ __global__ void k_scan_cols(const int *__restrict__ cond, int cmask, int n,
         ncl[0] = carry2;
     }
 }
+__global__ void k_scan_cols(const int *__restrict__ cond, int cmask, int n,
+                            int *__restrict__ col_count, int *__restrict__ col_start,
+                            int *__restrict__ cl_start, int *__restrict__ ncl) {
+    SOFIA_PDL_ENTRY();
+    scan_cols_body(blockIdx.x, cond, cmask, n, col_count, col_start, cl_start, ncl);
+}
 
-__global__ void k_col_scatter(const int *__restrict__ cond, int cmask, int n,
+__device__ __forceinline__ void col_scatter_body(int bx, const int *__restrict__ cond, int cmask, int n,
                               const int *__restrict__ col_of,
                               const int *__restrict__ col_start, int *__restrict__ col_fill,
                               int *__restrict__ col_atoms) {
-    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = bx * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int c = col_of[i];
     const int s = atomicAdd(&col_fill[c], 1);
     col_atoms[col_start[c] + s] = i;
 }
+__global__ void k_col_scatter(const int *__restrict__ cond, int cmask, int n,
+                              const int *__restrict__ col_of,
+                              const int *__restrict__ col_start, int *__restrict__ col_fill,
+                              int *__restrict__ col_atoms) {
+    SOFIA_PDL_ENTRY();
+    col_scatter_body(blockIdx.x, cond, cmask, n, col_of, col_start, col_fill, col_atoms);
+}
 
 // Sort each column by (z, index); then lay the column out as clusters of 8.
-__global__ void k_col_sort_assign(const int *__restrict__ cond, int cmask, int ncols,
+__device__ __forceinline__ void col_sort_assign_body(int bx, const int *__restrict__ cond, int cmask, int ncols,
                                   const int *__restrict__ col_start,
                                   int *__restrict__ col_atoms, const float *__restrict__ zkey,
                                   const int *__restrict__ cl_start, int *__restrict__ slot_orig,
                                   int *__restrict__ cl_col, int *__restrict__ atom_slot,
                                   int *__restrict__ col_fill, int *__restrict__ status) {
-    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     __shared__ unsigned long long s[MAX_COL];
-    const int c = blockIdx.x;
+    const int c = bx;
     if (c >= ncols) return;
     // the scatter is done with this column's fill counter: clear it for the next build
     if (threadIdx.x == 0) col_fill[c] = 0;
@@ -209,11 +229,20 @@ __global__ void k_col_sort_assign(const int *__restrict__ cond, int cmask, int n
         if ((t & (CL - 1)) == 0) cl_col[c0 + t / CL] = c;
     }
 }
+__global__ void k_col_sort_assign(const int *__restrict__ cond, int cmask, int ncols,
+                                  const int *__restrict__ col_start,
+                                  int *__restrict__ col_atoms, const float *__restrict__ zkey,
+                                  const int *__restrict__ cl_start, int *__restrict__ slot_orig,
+                                  int *__restrict__ cl_col, int *__restrict__ atom_slot,
+                                  int *__restrict__ col_fill, int *__restrict__ status) {
+    SOFIA_PDL_ENTRY();
+    col_sort_assign_body(blockIdx.x, cond, cmask, ncols, col_start, col_atoms, zkey, cl_start, slot_orig, cl_col, atom_slot, col_fill, status);
+}
 
 // Gather the cluster-ordered records.  The position used is the build-time
 // wrapped image plus the minimum-image displacement since the build, so a
 // caller that wraps atoms back into the box between builds stays consistent.
-__global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
+__device__ __forceinline__ void pack_body(int bx, int nslots, const int *__restrict__ ncl_dev,
                        const int *__restrict__ slot_orig, const double *__restrict__ x,
                        const double *__restrict__ y, const double *__restrict__ z,
                        const double *__restrict__ rx, const double *__restrict__ ry,
@@ -222,8 +251,7 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
                        AtomRec *__restrict__ rec, float *__restrict__ recf,
                        long long *__restrict__ fslot) {
-    SOFIA_PDL_ENTRY();
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = bx * blockDim.x + threadIdx.x;
     if (s >= nslots || s >= ncl_dev[0] * CL) return;
     // the pair kernel adds into the slot-ordered accumulators: start them at zero
     fslot[s] = 0;
@@ -256,16 +284,27 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
     rc[CL] = (float)r.y;
     rc[2 * CL] = (float)r.z;
 }
+__global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
+                       const int *__restrict__ slot_orig, const double *__restrict__ x,
+                       const double *__restrict__ y, const double *__restrict__ z,
+                       const double *__restrict__ rx, const double *__restrict__ ry,
+                       const double *__restrict__ rz, const double *__restrict__ ix,
+                       const double *__restrict__ iy, const double *__restrict__ iz,
+                       const float *__restrict__ q, const int *__restrict__ type, double L,
+                       AtomRec *__restrict__ rec, float *__restrict__ recf,
+                       long long *__restrict__ fslot) {
+    SOFIA_PDL_ENTRY();
+    pack_body(blockIdx.x, nslots, ncl_dev, slot_orig, x, y, z, rx, ry, rz, ix, iy, iz, q, type, L, rec, recf, fslot);
+}
 
 // Cluster bounding boxes of the current records (FP64 bounds rounded outward
 // to float), for the cluster-pair search and the prune.
-__global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
+__device__ __forceinline__ void bbox_body(int bx, const int *__restrict__ cond, int cmask, int maxcl,
                        const int *__restrict__ ncl_dev,
                        const AtomRec *__restrict__ rec, const int *__restrict__ slot_orig,
                        float4 *__restrict__ bb) {
-    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = bx * blockDim.x + threadIdx.x;
     if (c >= maxcl || c >= ncl_dev[0]) return;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     int real = 0;
@@ -285,6 +324,13 @@ __global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
                             __double2float_rd(lo[2]), __int_as_float(real));
     bb[2 * c + 1] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
                                 __double2float_ru(hi[2]), 0.0f);
+}
+__global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
+                       const int *__restrict__ ncl_dev,
+                       const AtomRec *__restrict__ rec, const int *__restrict__ slot_orig,
+                       float4 *__restrict__ bb) {
+    SOFIA_PDL_ENTRY();
+    bbox_body(blockIdx.x, cond, cmask, maxcl, ncl_dev, rec, slot_orig, bb);
 }
 
 __device__ __forceinline__ float gap(float alo, float ahi, float blo, float bhi) {
@@ -347,11 +393,10 @@ __device__ __forceinline__ void z_window(const float4 *__restrict__ bb, float il
 // included) in three z images, cut each column image to its z window, test the
 // remaining clusters' bounding boxes, compact the accepted (cluster, image)
 // pairs of the half list in visiting order and attach the pair mask.
-__global__ void __launch_bounds__(256) k_search(SearchArgs a) {
-    SOFIA_PDL_ENTRY();
+__device__ __forceinline__ void search_body(int bx, const SearchArgs &a) {
     if (a.cond && !(a.cond[0] & a.cmask)) return;
     const int lane = threadIdx.x & 31;
-    const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int icl = (bx * blockDim.x + threadIdx.x) >> 5;
     if (icl >= a.maxcl || icl >= a.ncl_dev[0]) return;
     const float4 ilo = a.bb[2 * icl], ihi = a.bb[2 * icl + 1];
     const int col = a.cl_col[icl];
@@ -500,6 +545,10 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs a) {
         atomicMax(&a.status[ST_NCLUSTER], count);
     }
 }
+__global__ void __launch_bounds__(256) k_search(SearchArgs a) {
+    SOFIA_PDL_ENTRY();
+    search_body(blockIdx.x, a);
+}
 
 // Displacement trigger: flag a rebuild when any atom moved more than skin/2
 // (minimum image) since the last build.
@@ -528,6 +577,11 @@ struct PairConst {
     float A1, A2, A3, A4, A5;
     // the same FP32 constants duplicated as {c, c} operands of packed FP32x2 math
     float2 kexp2, pa2, c2a2, e_shift2, f_shift2, A1_2, A2_2, A3_2, A4_2, A5_2;
+    // optional LJ energy shift: each in-range pair's energy minus its value at
+    // the cut-off, ljs6 = rc^-6 (0 = no shift: the energies are unchanged bit for bit)
+    float ljs6;
+    float2 ljs6_2;
+    double ljs6d;
     double rcut2d, cut_coulsqd, alphad, e_shiftd, f_shiftd, coulpred, MY_PIS_INV;
     double A1d, A2d, A3d, A4d, A5d, EWALD_Pd;
     double L;
@@ -592,7 +646,8 @@ struct PairMath<float> {
         const float fc = mulr(pref, fmar(k.f_shift, r2, fmar(mulr(k.c2a, ex), r, erfcc)));
         if (EN) {
             // selects, not products: masked pairs may hold inf/NaN (r = 0)
-            elj = lj_on ? mulr(dr6i, fmar(dr6i, lj.z, -lj.w)) : 0.0f;
+            const float esh = mulr(k.ljs6, fmar(k.ljs6, lj.z, -lj.w));
+            elj = lj_on ? addr(mulr(dr6i, fmar(dr6i, lj.z, -lj.w)), -esh) : 0.0f;
             ec = c_on ? mulr(pref, fmar(fmar(r, k.e_shift, mulr(r2, k.f_shift)), -1.0f, erfcc))
                       : 0.0f;
         }
@@ -627,7 +682,9 @@ struct PairMath<double> {
         const double fc = mulr(mulr(pref, addr(addr(mulr(erfcc, rinv), mulr(c2a, ex)),
                                                mulr(r, k.f_shiftd))), r);
         if (EN) {
-            elj = lj_on ? mulr(dr6i, addr(mulr(dr6i, (double)lj.z), -(double)lj.w)) : 0.0;
+            const double esh = mulr(k.ljs6d, addr(mulr(k.ljs6d, (double)lj.z), -(double)lj.w));
+            elj = lj_on ? addr(mulr(dr6i, addr(mulr(dr6i, (double)lj.z), -(double)lj.w)), -esh)
+                        : 0.0;
             ec = c_on ? mulr(pref, addr(addr(erfcc, -mulr(r, k.e_shiftd)),
                                         -mulr(r2, k.f_shiftd)))
                       : 0.0;
@@ -677,8 +734,9 @@ struct PairMath2 {
         const float2 erfcc = mul2(mul2(t, poly), ex);
         const float2 fc = mul2(pref, fma2(k.f_shift2, r2, fma2(mul2(k.c2a2, ex), r, erfcc)));
         if (EN) {
-            const float2 e6 =
-                mul2(dr6i, fma2(dr6i, make_float2(b0.x, b1.x), make_float2(b0.y, b1.y)));
+            const float2 b3 = make_float2(b0.x, b1.x), b4 = make_float2(b0.y, b1.y);
+            const float2 esh = mul2(k.ljs6_2, fma2(k.ljs6_2, b3, b4));
+            const float2 e6 = fma2(esh, make_float2(-1.0f, -1.0f), mul2(dr6i, fma2(dr6i, b3, b4)));
             const float2 sh = fma2(r, k.e_shift2, mul2(r2, k.f_shift2));
             const float2 e1 = mul2(pref, fma2(sh, make_float2(-1.0f, -1.0f), erfcc));
             elj = make_float2(lj0_on ? e6.x : 0.0f, lj1_on ? e6.y : 0.0f);
@@ -745,12 +803,12 @@ __device__ __forceinline__ T reduce_scatter_j(const T (&v)[6], int lane) {
 //     order of the atomics, so results stay bit-reproducible.
 // EN adds the LJ and Coulomb energies, VIR the diagonal virial (each pair once).
 template <typename T, bool EN, bool VIR, bool SAME>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2) k_pair(
-    int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
+__device__ __forceinline__ void pair_body(
+    int bx, int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
-    const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
-    unsigned long long *__restrict__ fslot, double *__restrict__ energy) {
-    SOFIA_PDL_ENTRY();
+    const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab,
+    const PairConst &k, double L, unsigned long long *__restrict__ fslot,
+    double *__restrict__ energy) {
     extern __shared__ float4 s_lj[];
     // FP32 path: the same bytes as two float2 tables, {lj1, -lj2} and {lj3, -lj4},
     // so a force-only lookup reads 8 bytes (fewer shared-memory wavefronts)
@@ -771,14 +829,14 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
     }
     if (threadIdx.x < 27) {
         const int im = threadIdx.x;
-        s_sh[im * 3 + 0] = (double)(im % 3 - 1) * k.L;
-        s_sh[im * 3 + 1] = (double)((im / 3) % 3 - 1) * k.L;
-        s_sh[im * 3 + 2] = (double)(im / 9 - 1) * k.L;
+        s_sh[im * 3 + 0] = (double)(im % 3 - 1) * L;
+        s_sh[im * 3 + 1] = (double)((im / 3) % 3 - 1) * L;
+        s_sh[im * 3 + 2] = (double)(im / 9 - 1) * L;
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int li = lane & 7, lj = lane >> 3;
-    const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int icl = (bx * blockDim.x + threadIdx.x) >> 5;
     if (icl >= maxcl || icl >= ncl_dev[0]) return;
     const size_t stride = (size_t)maxcl * CL;
     // this lane's share of the reduced j force: component jcomp of j atom jslot
@@ -1006,6 +1064,16 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
         }
     }
 }
+template <typename T, bool EN, bool VIR, bool SAME>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2) k_pair(
+    int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
+    const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
+    const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
+    unsigned long long *__restrict__ fslot, double *__restrict__ energy) {
+    SOFIA_PDL_ENTRY();
+    pair_body<T, EN, VIR, SAME>(blockIdx.x, maxcl, ncl_dev, rec, jlist, jmask, jcount, jcap,
+                                ljtab, k, k.L, fslot, energy);
+}
 
 // Slot-ordered fixed-point pair forces -> the caller's atom order (sets the
 // force arrays; bonded terms add to them afterwards).  Flags sums outside the
@@ -1013,14 +1081,13 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
 // With flag != NULL, thread 0 also counts this step's list build and prune in
 // cnt and clears the trigger word for the next step's displacement check (only
 // bits are ORed into it).  With lg.on, each atom's Langevin force is added.
-__global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
+__device__ __forceinline__ void unpack_body(int bx, int nslots, const int *__restrict__ ncl_dev,
                          const int *__restrict__ slot_orig, const long long *__restrict__ fslot,
                          long long *__restrict__ fx, long long *__restrict__ fy,
                          long long *__restrict__ fz, int *__restrict__ status,
                          int *__restrict__ flag, long long *__restrict__ cnt, LangevinArgs lg,
                          float *__restrict__ ffo) {
-    SOFIA_PDL_ENTRY();
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = bx * blockDim.x + threadIdx.x;
     if (flag && s == 0) {
         const int f = flag[0];
         if (f & 1) cnt[0] += 1;
@@ -1050,6 +1117,15 @@ __global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
     if (a > lim || a < -lim || b > lim || b < -lim || c > lim || c < -lim)
         atomicAdd(&status[ST_FIXED_OVF], 1);
 }
+__global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
+                         const int *__restrict__ slot_orig, const long long *__restrict__ fslot,
+                         long long *__restrict__ fx, long long *__restrict__ fy,
+                         long long *__restrict__ fz, int *__restrict__ status,
+                         int *__restrict__ flag, long long *__restrict__ cnt, LangevinArgs lg,
+                         float *__restrict__ ffo) {
+    SOFIA_PDL_ENTRY();
+    unpack_body(blockIdx.x, nslots, ncl_dev, slot_orig, fslot, fx, fy, fz, status, flag, cnt, lg, ffo);
+}
 
 // 8x8 bit-matrix transpose: bit (r*8 + c) -> bit (c*8 + r)  (three swap rounds).
 __device__ __forceinline__ unsigned long long transpose8(unsigned long long x) {
@@ -1075,7 +1151,7 @@ __device__ __forceinline__ unsigned long long transpose8(unsigned long long x) {
 // or ballots.  Distances here only select
 // pairs, so FP32 copies of the positions suffice (the squared radius carries a
 // 1e-3 A^2 safety margin).
-__global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
+__device__ __forceinline__ void prune_body(int bx, 
     const int *__restrict__ cond, int cmask, int maxcl, const int *__restrict__ ncl_dev,
     const float *__restrict__ recf,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
@@ -1085,7 +1161,6 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
     const int *__restrict__ slot_orig, const double *__restrict__ x,
     const double *__restrict__ y, const double *__restrict__ z, double *__restrict__ px,
     double *__restrict__ py, double *__restrict__ pz) {
-    SOFIA_PDL_ENTRY();
     SOFIA_COND_RETURN;
     __shared__ float s_shf[27 * 3];
     if (threadIdx.x < 27) {
@@ -1096,7 +1171,7 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int icl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int icl = (bx * blockDim.x + threadIdx.x) >> 5;
     if (icl >= maxcl || icl >= ncl_dev[0]) return;
     // the positions this prune is valid for (the prune trigger measures from them)
     if (lane < CL) {
@@ -1187,6 +1262,19 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
     }
     if (lane == 0) icount[icl] = kept;
 }
+__global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune(
+    const int *__restrict__ cond, int cmask, int maxcl, const int *__restrict__ ncl_dev,
+    const float *__restrict__ recf,
+    const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
+    const int *__restrict__ jcount, int jcap, float L, float rin2, float rfar2,
+    const float4 *__restrict__ bb, int *__restrict__ ilist,
+    unsigned long long *__restrict__ imask, int *__restrict__ icount,
+    const int *__restrict__ slot_orig, const double *__restrict__ x,
+    const double *__restrict__ y, const double *__restrict__ z, double *__restrict__ px,
+    double *__restrict__ py, double *__restrict__ pz) {
+    SOFIA_PDL_ENTRY();
+    prune_body(blockIdx.x, cond, cmask, maxcl, ncl_dev, recf, jlist, jmask, jcount, jcap, L, rin2, rfar2, bb, ilist, imask, icount, slot_orig, x, y, z, px, py, pz);
+}
 
 
 
@@ -1197,14 +1285,12 @@ __global__ void k_set_flag(int *__restrict__ flag, int v) {
 
 // Two-stage deterministic column sums: stage 1 = fixed grid of blocks over
 // contiguous ranges (coalesced), stage 2 = one block over the partials.
-constexpr int RED_BLOCKS = 128;
-__global__ void k_red_stage1(int n, int w, const int *__restrict__ ncl_dev,
-                             const double *__restrict__ in, double *__restrict__ part) {
-    SOFIA_PDL_ENTRY();
+__device__ __forceinline__ void red_stage1_body(int bx, int n, int w, const int *__restrict__ ncl_dev,
+                             const double *__restrict__ in, double *__restrict__ part, int nblk) {
     __shared__ double s[256];
     const int nn = ncl_dev ? min(n, ncl_dev[0]) : n;
-    const int chunk = (nn + gridDim.x - 1) / gridDim.x;
-    const int b0 = blockIdx.x * chunk, b1 = min(nn, b0 + chunk);
+    const int chunk = (nn + nblk - 1) / nblk;
+    const int b0 = bx * chunk, b1 = min(nn, b0 + chunk);
     for (int c = 0; c < w; ++c) {
         double acc = 0.0;
         for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) acc += in[(size_t)i * w + c];
@@ -1214,13 +1300,17 @@ __global__ void k_red_stage1(int n, int w, const int *__restrict__ ncl_dev,
             if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
             __syncthreads();
         }
-        if (threadIdx.x == 0) part[blockIdx.x * w + c] = s[0];
+        if (threadIdx.x == 0) part[bx * w + c] = s[0];
         __syncthreads();
     }
 }
-__global__ void k_red_stage2(int nblk, int w, const double *__restrict__ part,
-                             double *__restrict__ out, double scale) {
+__global__ void k_red_stage1(int n, int w, const int *__restrict__ ncl_dev,
+                             const double *__restrict__ in, double *__restrict__ part) {
     SOFIA_PDL_ENTRY();
+    red_stage1_body(blockIdx.x, n, w, ncl_dev, in, part, (int)gridDim.x);
+}
+__device__ __forceinline__ void red_stage2_body(int bx, int nblk, int w, const double *__restrict__ part,
+                             double *__restrict__ out, double scale) {
     __shared__ double s[256];
     for (int c = 0; c < w; ++c) {
         s[threadIdx.x] = (threadIdx.x < nblk) ? part[threadIdx.x * w + c] : 0.0;
@@ -1232,6 +1322,11 @@ __global__ void k_red_stage2(int nblk, int w, const double *__restrict__ part,
         if (threadIdx.x == 0) out[c] = scale * s[0];
         __syncthreads();
     }
+}
+__global__ void k_red_stage2(int nblk, int w, const double *__restrict__ part,
+                             double *__restrict__ out, double scale) {
+    SOFIA_PDL_ENTRY();
+    red_stage2_body(blockIdx.x, nblk, w, part, out, scale);
 }
 
 // Ballistic drift x += dt*v (FP64), used to move a system between
@@ -1489,6 +1584,9 @@ static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
     k.A3_2 = make_float2(k.A3, k.A3);
     k.A4_2 = make_float2(k.A4, k.A4);
     k.A5_2 = make_float2(k.A5, k.A5);
+    k.ljs6d = s->lj_shift ? 1.0 / (rcut2 * rcut2 * rcut2) : 0.0;
+    k.ljs6 = (float)k.ljs6d;
+    k.ljs6_2 = make_float2(k.ljs6, k.ljs6);
     k.L = s->L;
     k.ntypes = s->ntypes;
     return k;
@@ -2079,3 +2177,343 @@ extern "C" int sofia_system_timers(sofia_system *ss, int enable, double *timers)
     s->timing = enable ? 1 : 0;
     return SOFIA_OK;
 }
+
+// The cluster-pair list expanded into atom pairs on the host (a diagnostic
+// query, not a hot path): which = 0 the outer list (rc + skin, made at the
+// last build, masks bit 8*ii + jj), 1 the pruned list (rc + margin, made at the
+// last prune, masks in the pair kernel's lane layout: bit 32*h + lane is i atom
+// lane & 7 with j atom (lane >> 3) + 4*h).
+extern "C" int sofia_system_list_pairs(sofia_system *ss, int which, int64_t capacity,
+                                       int32_t *pairs, int64_t *npairs, double *xlist) {
+    if (!ss || !npairs || (which != 0 && which != 1) || capacity < 0 || (capacity > 0 && !pairs))
+        return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *npairs = 0;
+    if (!s->built) return sofia::fail(ctx, SOFIA_ESTATE, "list_pairs: no list built yet%s");
+    int ncl = 0;
+    SOFIA_CUDA(ctx, cudaMemcpy(&ncl, s->nclusters.p, sizeof(int), cudaMemcpyDeviceToHost));
+    ncl = std::min(std::max(ncl, 0), s->max_clusters);
+    const size_t cap = (size_t)s->jcap;
+    std::vector<int> cnt(ncl), lst((size_t)ncl * cap), orig((size_t)ncl * sofia::CL);
+    std::vector<unsigned long long> msk((size_t)ncl * cap);
+    const sofia::DevBuf &L = which ? s->ilist : s->jlist;
+    const sofia::DevBuf &Mk = which ? s->imask : s->jmask;
+    const sofia::DevBuf &Cn = which ? s->icount : s->jcount;
+    if (ncl > 0) {
+        SOFIA_CUDA(ctx, cudaMemcpy(cnt.data(), Cn.p, sizeof(int) * ncl, cudaMemcpyDeviceToHost));
+        SOFIA_CUDA(ctx, cudaMemcpy(lst.data(), L.p, sizeof(int) * ncl * cap,
+                                   cudaMemcpyDeviceToHost));
+        SOFIA_CUDA(ctx, cudaMemcpy(msk.data(), Mk.p, sizeof(unsigned long long) * ncl * cap,
+                                   cudaMemcpyDeviceToHost));
+        SOFIA_CUDA(ctx, cudaMemcpy(orig.data(), s->slot_orig.p, sizeof(int) * ncl * sofia::CL,
+                                   cudaMemcpyDeviceToHost));
+    }
+    int64_t k = 0;
+    for (int ic = 0; ic < ncl; ++ic) {
+        const int c = std::min(std::max(cnt[ic], 0), (int)cap);
+        for (int e = 0; e < c; ++e) {
+            const int w = lst[(size_t)ic * cap + e];
+            const int jc = w & ((1 << sofia::IMG_SHIFT) - 1);
+            if (jc < 0 || jc >= ncl)
+                return sofia::fail(ctx, SOFIA_ESTATE, "list_pairs: j cluster out of range%s");
+            unsigned long long m = msk[(size_t)ic * cap + e];
+            while (m) {
+                const int b = __builtin_ctzll(m);
+                m &= m - 1;
+                int ii, jj;
+                if (which == 0) {
+                    ii = b >> 3;
+                    jj = b & 7;
+                } else {
+                    const int lane = b & 31;
+                    ii = lane & 7;
+                    jj = (lane >> 3) + 4 * (b >> 5);
+                }
+                const int a = orig[(size_t)ic * sofia::CL + ii];
+                const int o = orig[(size_t)jc * sofia::CL + jj];
+                if (a < 0 || o < 0)
+                    return sofia::fail(ctx, SOFIA_ESTATE, "list_pairs: a padding slot is listed%s");
+                if (k < capacity) {
+                    pairs[2 * k] = a;
+                    pairs[2 * k + 1] = o;
+                }
+                ++k;
+            }
+        }
+    }
+    *npairs = k;
+    if (xlist) {
+        const size_t n = (size_t)s->n;
+        std::vector<double> h(n);
+        const sofia::DevBuf *src = which ? s->xprn : s->xref;
+        for (int d = 0; d < 3; ++d) {
+            SOFIA_CUDA(ctx, cudaMemcpy(h.data(), src[d].p, sizeof(double) * n,
+                                       cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; ++i) xlist[3 * i + d] = h[i];
+        }
+    }
+    if (k > capacity) return SOFIA_ENEEDGROW;
+    return SOFIA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched replicas (see BatchDev in system.cuh): the nonbonded part of an MD
+// step for every replica of a batch, one launch per kernel.  Each launch walks
+// its virtual blocks in a grid-stride loop and runs the single-system kernel
+// body on the owning replica's buffers, so a replica's results are bit-identical
+// to the same replica stepped alone.
+namespace sofia {
+namespace {
+
+#define SOFIA_BATCH_LOOP(KIND)                                                   \
+    const int nrep_ = tab->nrep;                                                 \
+    const int *pre_ = tab->pre[KIND];                                            \
+    const int tot_ = pre_[nrep_];                                                \
+    for (int vb = blockIdx.x; vb < tot_; vb += gridDim.x) {                      \
+        const int r_ = batch_rep(pre_, nrep_, vb);                               \
+        const RepDev &d = tab->rep[r_];                                          \
+        const int lb = vb - pre_[r_];
+#define SOFIA_BATCH_END }
+
+__global__ void k_wrap_bin_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_A256)
+    wrap_bin_body(lb, d.flag, 1, d.n, d.x, d.y, d.z, d.L, d.s_col, d.ncx, d.ix, d.iy, d.iz, d.rx,
+                  d.ry, d.rz, d.col_of, d.col_count, d.col_key);
+    SOFIA_BATCH_END
+}
+
+__global__ void __launch_bounds__(1024) k_scan_cols_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_SCAN)
+    scan_cols_body(lb, d.flag, 1, d.ncols, d.col_count, d.col_start, d.cl_start, d.ncl);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+__global__ void k_col_scatter_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_A256)
+    col_scatter_body(lb, d.flag, 1, d.n, d.col_of, d.col_start, d.col_fill, d.col_atoms);
+    SOFIA_BATCH_END
+}
+
+__global__ void k_col_sort_assign_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_COLS)
+    col_sort_assign_body(lb, d.flag, 1, d.ncols, d.col_start, d.col_atoms, d.col_key, d.cl_start,
+                         d.slot_orig, d.cl_col, d.atom_slot, d.col_fill, d.status);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+__global__ void k_pack_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_S256)
+    pack_body(lb, d.nslots, d.ncl, d.slot_orig, d.x, d.y, d.z, d.rx, d.ry, d.rz, d.ix, d.iy, d.iz,
+              d.q, d.type, d.L, d.rec, d.recf, reinterpret_cast<long long *>(d.fslot));
+    SOFIA_BATCH_END
+}
+
+__global__ void k_bbox_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_C128)
+    bbox_body(lb, d.flag, 3, d.maxcl, d.ncl, d.rec, d.slot_orig, d.bb);
+    SOFIA_BATCH_END
+}
+
+__global__ void __launch_bounds__(256) k_search_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_W256)
+    SearchArgs a;
+    a.cond = d.flag;
+    a.cmask = 1;
+    a.maxcl = d.maxcl;
+    a.ncx = d.ncx;
+    a.reach = d.reach;
+    a.jcap = d.jcap;
+    a.n = d.n;
+    a.L = (float)d.L;
+    a.s_col = (float)d.s_col;
+    a.rl = d.rl;
+    a.rl2 = d.rl2;
+    a.rexcl2 = d.rexcl2;
+    a.ncl_dev = d.ncl;
+    a.cl_start = d.cl_start;
+    a.cl_col = d.cl_col;
+    a.slot_orig = d.slot_orig;
+    a.specbond = d.specbond;
+    a.num3bond = d.num3bond;
+    a.atom_slot = d.atom_slot;
+    a.bb = d.bb;
+    a.jlist = d.jlist;
+    a.jcount = d.jcount;
+    a.jmask = d.jmask;
+    a.status = d.status;
+    search_body(lb, a);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+__global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_W256)
+    prune_body(lb, d.flag, 3, d.maxcl, d.ncl, d.recf, d.jlist, d.jmask, d.jcount, d.jcap,
+               (float)d.L, d.rin2, d.rfar2, d.bb, d.ilist, d.imask, d.icount, d.slot_orig, d.x,
+               d.y, d.z, d.px, d.py, d.pz);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+template <typename T, bool EN, bool VIR, bool SAME>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2)
+    k_pair_b(const BatchDev *__restrict__ tab, PairConst k) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_W256)
+    pair_body<T, EN, VIR, SAME>(lb, d.maxcl, d.ncl, d.rec, d.ilist, d.imask, d.icount, d.jcap,
+                                d.ljtab, k, d.L, d.fslot, d.energy);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+__global__ void k_unpack_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_S256)
+    unpack_body(lb, d.nslots, d.ncl, d.slot_orig, reinterpret_cast<const long long *>(d.fslot),
+                d.fx, d.fy, d.fz, d.ctx_status, d.flag, d.dcount, d.lg, nullptr);
+    SOFIA_BATCH_END
+}
+
+__global__ void k_red_stage1_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_RED)
+    red_stage1_body(lb, d.maxcl, 5, d.ncl, d.energy, d.part, RED_BLOCKS);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+__global__ void k_red_stage2_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_REP)
+    red_stage2_body(lb, RED_BLOCKS, 5, d.part, d.red, 1.0);
+    __syncthreads();
+    SOFIA_BATCH_END
+}
+
+#undef SOFIA_BATCH_LOOP
+#undef SOFIA_BATCH_END
+
+}  // namespace
+
+void repdev_fill_pair(const Sys *s, RepDev *d) {
+    d->n = s->n;
+    d->ncols = s->ncols;
+    d->ncx = s->ncx;
+    d->maxcl = s->max_clusters;
+    d->jcap = s->jcap;
+    d->reach = s->ncol_reach;
+    d->nslots = s->max_clusters * CL;
+    d->L = s->L;
+    d->s_col = s->s_col;
+    const float rl = (float)s->rlist + 1e-3f;
+    d->rl = rl;
+    d->rl2 = rl * rl;
+    d->rexcl2 = (float)(s->r_excl * s->r_excl);
+    const float rin = (float)(s->rc + s->margin);
+    d->rin2 = rin * rin + 1e-3f;
+    const float rfar = rin + 0.01f;
+    d->rfar2 = rfar * rfar;
+    d->lim2 = (0.5 * s->skin) * (0.5 * s->skin);
+    d->plim2 = (0.5 * s->margin) * (0.5 * s->margin);
+    d->x = s->x[0].as<double>();
+    d->y = s->x[1].as<double>();
+    d->z = s->x[2].as<double>();
+    d->vx = s->v[0].as<double>();
+    d->vy = s->v[1].as<double>();
+    d->vz = s->v[2].as<double>();
+    d->fx = s->f[0].as<long long>();
+    d->fy = s->f[1].as<long long>();
+    d->fz = s->f[2].as<long long>();
+    d->rx = s->xref[0].as<double>();
+    d->ry = s->xref[1].as<double>();
+    d->rz = s->xref[2].as<double>();
+    d->ix = s->img[0].as<double>();
+    d->iy = s->img[1].as<double>();
+    d->iz = s->img[2].as<double>();
+    d->px = s->xprn[0].as<double>();
+    d->py = s->xprn[1].as<double>();
+    d->pz = s->xprn[2].as<double>();
+    d->invm = s->invm.as<double>();
+    d->mass = s->mass.as<double>();
+    d->q = s->q.as<float>();
+    d->type = s->type.as<int>();
+    d->specbond = s->specbond.as<int>();
+    d->num3bond = s->num3bond.as<int>();
+    d->col_count = s->col_count.as<int>();
+    d->col_start = s->col_start.as<int>();
+    d->col_fill = s->col_fill.as<int>();
+    d->col_atoms = s->col_atoms.as<int>();
+    d->col_of = s->col_atoms.as<int>() + s->n;
+    d->cl_start = s->cl_start.as<int>();
+    d->slot_orig = s->slot_orig.as<int>();
+    d->cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
+    d->atom_slot = s->atom_slot.as<int>();
+    d->col_key = s->col_key.as<float>();
+    d->rec = s->rec.as<AtomRec>();
+    d->recf = s->recf.as<float>();
+    d->bb = s->bb.as<float4>();
+    d->jlist = s->jlist.as<int>();
+    d->jcount = s->jcount.as<int>();
+    d->ilist = s->ilist.as<int>();
+    d->icount = s->icount.as<int>();
+    d->jmask = s->jmask.as<unsigned long long>();
+    d->imask = s->imask.as<unsigned long long>();
+    d->fslot = s->fslot.as<unsigned long long>();
+    d->ncl = s->nclusters.as<int>();
+    d->flag = s->flag.as<int>();
+    d->status = s->status_local.as<int>();
+    d->ctx_status = s->ctx->d_status;
+    d->dcount = s->dcount.as<long long>();
+    d->ljtab = s->ljtab.as<float4>();
+    d->energy = s->energy.as<double>();
+    d->part = s->part.as<double>();
+    d->red = s->red.as<double>();
+}
+
+void batch_pair_path(const BatchDev *tab, const Sys *s0, int precision, bool energy,
+                     cudaStream_t st, int nsm) {
+    const int g256 = nsm * 8, g128 = nsm * 16;
+    launch_pdl(k_wrap_bin_b, g256, 256, 0, st, tab);
+    launch_pdl(k_scan_cols_b, nsm * 2, 1024, 0, st, tab);
+    launch_pdl(k_col_scatter_b, g256, 256, 0, st, tab);
+    launch_pdl(k_col_sort_assign_b, nsm * 4, 256, 0, st, tab);
+    launch_pdl(k_pack_b, g256, 256, 0, st, tab);
+    launch_pdl(k_bbox_b, g128, 128, 0, st, tab);
+    launch_pdl(k_search_b, g256, 256, 0, st, tab);
+    launch_pdl(k_prune_b, nsm * SOFIA_PRUNE_MINB, 256, 0, st, tab);
+    const PairConst k = make_pair_const(s0, nullptr);
+    const size_t smem = sizeof(float4) * (size_t)s0->ntypes * s0->ntypes;
+    if (precision == SOFIA_PREC_FP64) {
+        if (energy)
+            launch_pdl(k_pair_b<double, true, false, true>, nsm * 2, 256, smem, st, tab, k);
+        else
+            launch_pdl(k_pair_b<double, false, false, true>, nsm * 2, 256, smem, st, tab, k);
+    } else {
+        if (energy)
+            launch_pdl(k_pair_b<float, true, false, true>, nsm * SOFIA_PAIR_MINB_EN, 256, smem, st,
+                       tab, k);
+        else
+            launch_pdl(k_pair_b<float, false, false, true>, nsm * SOFIA_PAIR_MINB, 256, smem, st,
+                       tab, k);
+    }
+    launch_pdl(k_unpack_b, g256, 256, 0, st, tab);
+    if (energy) {
+        launch_pdl(k_red_stage1_b, g256, 256, 0, st, tab);
+        launch_pdl(k_red_stage2_b, nsm * 2, 256, 0, st, tab);
+    }
+}
+
+}  // namespace sofia

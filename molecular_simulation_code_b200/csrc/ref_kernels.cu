@@ -1388,6 +1388,21 @@ int noalloc_scratch(double **out) {
     return SOFIA_OK;
 }
 
+// Device memory on the current device (the one the scratch address and the
+// launches belong to), or managed memory.  A buffer on another GPU would be
+// read without peer access: rejected here instead of faulting in the kernel.
+bool noalloc_buffer_ok(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    int dev = -1;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 }  // namespace
 
 extern "C" int sofia_force_nonbond_dsf_noalloc(
@@ -1400,10 +1415,11 @@ extern "C" int sofia_force_nonbond_dsf_noalloc(
         !lj4 || !nlist || !numneigh || !ff)
         return SOFIA_EINVAL;
     if (np > SOFIA_NOALLOC_MAX_ATOMS) return SOFIA_ETOOBIG;
-    // every array must already be in device memory: staging would need an allocation
+    // every array must already be in the current device's memory: staging would
+    // need an allocation
     const void *ptrs[] = {position, q, lj1, lj2, lj3, lj4, nlist, numneigh, ff};
     for (const void *p : ptrs)
-        if (!sofia::is_device_ptr(p)) return SOFIA_EINVAL;
+        if (!noalloc_buffer_ok(p)) return SOFIA_EINVAL;
     double *scratch = nullptr;
     int rc = noalloc_scratch(&scratch);
     if (rc) return rc;

@@ -43,8 +43,10 @@ struct Md {
     int shake_maxiter = 25;
     double shake_tol = 1e-4;
     int terms = 15;
+    int rattle = 0;        // RATTLE velocity stage after the second half-kick (SOFIA_MD_RATTLE)
     DevBuf eterm;          // per-term energy partials
     DevBuf ered;           // reduced energies
+    DevBuf bpart;          // stage-1 partials of the batched energy sums
     DevBuf step_dev;       // device step counter (RNG counter inside graphs)
     DevBuf snap[7];        // x, v (3 each) and the step counter at segment start
     DevBuf keep[7];        // caller-requested snapshot (same layout), for rollback
@@ -85,9 +87,13 @@ struct Sys {
     DevBuf red;                         // reduced energies
     DevBuf flag;                        // rebuild flag (int)
     DevBuf stage_pos, stage_ff;
+    DevBuf cl_pos, cl_gid;              // resident positions as real*4 ainfo records, ids 1..n (cluster analysis)
     // pruned inner list (rc + margin) and the positions it was pruned at
     DevBuf ilist, imask, icount, xprn[3], part, dcount;
     double margin = 0.6;
+    // LJ energy of every pair inside the cut-off shifted by -E_LJ(rc) (SOFIA_MD_LJ_SHIFT);
+    // forces are unchanged, so only the energy bookkeeping differs
+    int lj_shift = 0;
     long long n_prunes = 0;
     int built = 0;
     long long n_builds = 0;
@@ -103,6 +109,141 @@ struct Sys {
     int pending_build = 0, pending_pair = 0;
     Md md;
 };
+
+
+// Arguments of the bonded-term kernel (md.cu): torsions with their 1-4 pairs.
+struct DihArgs {
+    int nd, ntypes, terms;
+    const int *dl;
+    const double *dc, *lj14;
+    const double *x, *y, *z;
+    const int *type;
+    const float *q;
+    double L, alpha, EWALD_P, A1, A2, A3, A4, A5, MY_PIS, e_shift, f_shift, cut_coulsq, rcut2;
+    float coulpre;
+    long long *fx, *fy, *fz;
+    double *e;  // [nd][3] torsion, coul14, lj14
+};
+
+// All bonded terms of a step in one launch: threads [0, nb) take bonds, the
+// next na angles, then nd dihedrals (torsion and 1-4 pair), then ni impropers.
+// A count of 0 switches a term off.
+struct BondedArgs {
+    int nb, na, nd, ni;
+    const int *bl, *al, *il;
+    const double *bc, *ac, *ic;
+    double *eb, *ea, *ei;
+    DihArgs dih;
+};
+
+// ---------------------------------------------------------------------------
+// Batched replicas: every kernel of an MD step runs once for all replicas of a
+// batch.  The launch walks "virtual blocks" in a grid-stride loop; the blocks of
+// kernel kind K for replica r are [pre[K][r], pre[K][r+1]), each with the block
+// size of the single-system kernel, so a block never spans two replicas and the
+// single-system kernel bodies run unchanged on replica r's buffers.  Replica
+// data live in a device table that the host rewrites when membership or a
+// buffer changes; the captured graphs only hold the table's address.
+enum BatchKind {
+    BK_A256 = 0,  // ceil(n / 256): per-atom kernels
+    BK_SCAN,      // 1: the column scans (1024 threads)
+    BK_COLS,      // ncols: the column sort
+    BK_S256,      // ceil(max_clusters * 8 / 256): per-slot kernels
+    BK_C128,      // ceil(max_clusters / 128): cluster boxes
+    BK_W256,      // ceil(max_clusters * 32 / 256): warp-per-cluster kernels
+    BK_B128,      // ceil(bonded terms / 128)
+    BK_G128,      // ceil(SHAKE groups / 128)
+    BK_RED,       // RED_BLOCKS: stage 1 of the pair-energy sums
+    BK_REP,       // 1 per replica
+    BK_MRED,      // MD_NJOB * MRED: stage 1 of the MD energy sums
+    BK_MJOB,      // MD_NJOB: stage 2 of the MD energy sums
+    BK_N
+};
+constexpr int MAXREP = 256;
+constexpr int RED_BLOCKS = 128;  // blocks of stage 1 of the pair-energy sums
+constexpr int MD_NJOB = 7;  // bonds, angles, torsion, coul14, lj14, impropers, kinetic
+
+struct RepDev {
+    int n, ncols, ncx, maxcl, jcap, reach, nslots, nshake, rattle, shake_maxiter;
+    double L, s_col, lim2, plim2, h, dt, dtsq, shake_tol;
+    float rl, rl2, rexcl2, rin2, rfar2;
+    // global-order atom state
+    double *x, *y, *z, *vx, *vy, *vz;
+    long long *fx, *fy, *fz;
+    double *rx, *ry, *rz, *ix, *iy, *iz, *px, *py, *pz;
+    const double *invm, *mass;
+    const float *q;
+    const int *type, *specbond, *num3bond;
+    // list build and cluster order
+    int *col_count, *col_start, *col_fill, *col_atoms, *col_of, *cl_start, *slot_orig, *cl_col,
+        *atom_slot;
+    float *col_key;
+    AtomRec *rec;
+    float *recf;
+    float4 *bb;
+    int *jlist, *jcount, *ilist, *icount;
+    unsigned long long *jmask, *imask, *fslot;
+    int *ncl, *flag, *status, *ctx_status;
+    long long *dcount;
+    const float4 *ljtab;
+    double *energy, *part, *red;
+    // MD
+    long long *step;
+    LangevinArgs lg;
+    BondedArgs b;
+    const int *shake;
+    const double *sbond;
+    double *ered, *ebpart, *ke;
+    // energy-sum jobs: column count n (0 = off), width, column, input, output slot of ered
+    int job_n[MD_NJOB], job_w[MD_NJOB], job_c[MD_NJOB], job_slot[MD_NJOB];
+    const double *job_in[MD_NJOB];
+};
+
+struct BatchDev {
+    int nrep;
+    int pre[BK_N][MAXREP + 1];
+    RepDev rep[MAXREP];
+};
+
+// Replica of virtual block vb: the last r with pre[r] <= vb.
+__device__ __forceinline__ int batch_rep(const int *__restrict__ pre, int nrep, int vb) {
+    int lo = 0, hi = nrep - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= vb)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Fills the nonbonded-path part of a replica's table entry (mixed.cu).
+void repdev_fill_pair(const Sys *s, RepDev *d);
+// The nonbonded part of one batched MD step (mixed.cu): list build and prune on
+// each replica's trigger, record pack, pair kernel, force unpack with the
+// Langevin force, and (energy) the pair-energy sums.  All replicas share the
+// pair constants k (all but the box) and the precision.
+// nsm: multiprocessors of the device (the grid-stride launches are sized from it).
+void batch_pair_path(const BatchDev *tab, const Sys *s0, int precision, bool energy,
+                     cudaStream_t st, int nsm);
+// The pair constants a captured batch graph holds (everything but the box).
+struct PairKey {
+    int precision, ntypes, lj_shift;
+    double rc, alpha, e_shift, f_shift;
+    float coulpre;
+};
+inline PairKey pair_key(const Sys *s) {
+    return PairKey{s->precision, s->ntypes, s->lj_shift, s->rc, s->alpha, s->e_shift,
+                   s->f_shift, s->coulpre};
+}
+inline bool operator==(const PairKey &a, const PairKey &b) {
+    return a.precision == b.precision && a.ntypes == b.ntypes && a.lj_shift == b.lj_shift &&
+           a.rc == b.rc && a.alpha == b.alpha && a.e_shift == b.e_shift &&
+           a.f_shift == b.f_shift && a.coulpre == b.coulpre;
+}
+// True when two systems' pair constants agree in everything but the box.
+inline bool pair_const_compatible(const Sys *a, const Sys *b) { return pair_key(a) == pair_key(b); }
 
 // evaluation entry points (mixed.cu)
 int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build);

@@ -12,8 +12,9 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (MD_ENERGY_NAMES, SOFIA_MD_NE, SOFIA_OK, SOFIA_PREC_FP64, SOFIA_PREC_MIXED,
-                   SofiaError, SofiaMdDesc, SofiaSystemDesc)
+from ._lib import (MD_ENERGY_NAMES, SOFIA_ENEEDGROW, SOFIA_MD_LJ_SHIFT, SOFIA_MD_NE,
+                   SOFIA_MD_RATTLE, SOFIA_OK, SOFIA_PREC_FP64, SOFIA_PREC_MIXED, SofiaError,
+                   SofiaMdDesc, SofiaSystemDesc)
 from .nonbond import Context, ptr
 
 MIXED = SOFIA_PREC_MIXED
@@ -108,9 +109,13 @@ class System:
 
     def md_setup(self, sysdata, dt: float = 2.0, temperature: float = 300.0,
                  gamma: float = 0.001, seed: int = 1, terms: int = 31, shake: bool = True,
-                 shake_maxiter: int = 0, shake_tol: float = 0.0):
+                 shake_maxiter: int = 0, shake_tol: float = 0.0, rattle: bool = False,
+                 lj_shift: bool = False):
         """Bonded lists, SHAKE groups and thermostat of the device-resident MD.
-        terms: bit 1 bonds, 2 angles, 4 torsions, 8 1-4 pairs, 16 impropers."""
+        terms: bit 1 bonds, 2 angles, 4 torsions, 8 1-4 pairs, 16 impropers.
+        rattle: RATTLE velocity stage (full-step velocities on the constraints);
+        lj_shift: LJ pair energies shifted to zero at the cut-off.  Both default to
+        the reference's scheme and neither changes the positions."""
         k = [np.ascontiguousarray(a) for a in (
             sysdata.bonds.astype(np.int32), sysdata.bond_coeff.astype(np.float64),
             sysdata.angles.astype(np.int32), sysdata.angle_coeff.astype(np.float64),
@@ -127,7 +132,8 @@ class System:
                         k[4].shape[0], ptr(k[4]), k[5].shape[0], ptr(k[5]), ptr(k[6]),
                         ns, ptr(k[7]), ptr(k[8]), int(shake_maxiter), float(shake_tol),
                         k[9].shape[0], ptr(k[9]) if k[9].size else None, k[10].shape[0],
-                        ptr(k[10]) if k[10].size else None)
+                        ptr(k[10]) if k[10].size else None,
+                        (SOFIA_MD_RATTLE if rattle else 0) | (SOFIA_MD_LJ_SHIFT if lj_shift else 0))
         self.ctx.check(self.ctx._lib.sofia_system_md_setup(self.handle, C.byref(d)))
 
     def md_run(self, nsteps: int, energy_every: int = 0, use_graph: bool = True) -> dict | None:
@@ -138,6 +144,32 @@ class System:
         if energy_every <= 0:
             return None
         return dict(zip(MD_ENERGY_NAMES, e.tolist()))
+
+    def md_forces(self, terms: int, energy: bool = True):
+        """Forces of one MD step at the resident state without stepping, restricted to
+        the SOFIA_TERM_* bits in ``terms`` (see ``_lib``).  Returns (f (n,3) float64,
+        energies dict or None)."""
+        f = np.zeros((self.n, 3))
+        e = np.zeros(SOFIA_MD_NE) if energy else None
+        self.ctx.check(self.ctx._lib.sofia_system_md_forces(self.handle, int(terms), ptr(f),
+                                                            ptr(e)))
+        return f, (dict(zip(MD_ENERGY_NAMES, e.tolist())) if energy else None)
+
+    def list_pairs(self, which: int = 1):
+        """The resident list as (npairs, 2) int32 0-based atom pairs (each pair once)
+        and the (n, 3) positions it was made at; which = 0 outer, 1 pruned."""
+        cap = 1 << 20
+        while True:
+            pairs = np.zeros((cap, 2), np.int32)
+            xl = np.zeros((self.n, 3))
+            cnt = C.c_int64()
+            rc = self.ctx._lib.sofia_system_list_pairs(self.handle, int(which), cap,
+                                                       ptr(pairs), C.byref(cnt), ptr(xl))
+            if rc == SOFIA_ENEEDGROW:
+                cap = int(cnt.value) + 1
+                continue
+            self.ctx.check(rc)
+            return pairs[:cnt.value], xl
 
     def snapshot(self):
         """Device copy of x, v and the thermostat step (nuc_move's save)."""

@@ -78,7 +78,7 @@ def lib(fast: bool = False) -> C.CDLL:
     L.orc_dihedral_opls_dsf.argtypes = [C.POINTER(OrcParams), C.c_int, _f32p, _f32p, C.c_int,
                                         _f64p, C.c_int, _i32p, _f64p, _f32p,
                                         C.POINTER(C.c_double), C.POINTER(C.c_double),
-                                        C.POINTER(C.c_double)]
+                                        C.POINTER(C.c_double), C.c_void_p]
     L.orc_correct_pairs.argtypes = [C.POINTER(OrcParams), _f32p, _f32p, C.c_int, C.c_void_p,
                                     C.c_void_p, C.c_int, C.c_double, C.c_double, _f32p,
                                     C.POINTER(C.c_double), _f64p]
@@ -237,9 +237,13 @@ def force_dsf_n2(p: OrcParams, pos, q, lj, ntypes, specbond, n1, n2, n3):
     return ff64.reshape(n, 3), pot.value, ec.value
 
 
-def dihedral_opls_dsf(p: OrcParams, pos, q, ntypes, lj14, dihedlist, dihedcoeff):
+def dihedral_opls_dsf(p: OrcParams, pos, q, ntypes, lj14, dihedlist, dihedcoeff,
+                      want_f64: bool = False):
+    """Returns (ffh real*4 (n,3), e_dihedral, e_coul_14, pot_14), plus the same forces
+    summed in double as a fifth item when ``want_f64``."""
     n = pos.shape[0]
     ffh = np.zeros(n * 3, np.float32)
+    f64 = np.zeros(n * 3) if want_f64 else None
     ed = C.c_double(0.0)
     ec = C.c_double(0.0)
     p14 = C.c_double(0.0)
@@ -248,7 +252,10 @@ def dihedral_opls_dsf(p: OrcParams, pos, q, ntypes, lj14, dihedlist, dihedcoeff)
                                 np.ascontiguousarray(lj14, np.float64), dihedlist.shape[0],
                                 np.ascontiguousarray(dihedlist, np.int32),
                                 np.ascontiguousarray(dihedcoeff, np.float64), ffh, C.byref(ed),
-                                C.byref(ec), C.byref(p14))
+                                C.byref(ec), C.byref(p14),
+                                None if f64 is None else f64.ctypes.data_as(C.c_void_p))
+    if want_f64:
+        return ffh.reshape(n, 3), ed.value, ec.value, p14.value, f64.reshape(n, 3)
     return ffh.reshape(n, 3), ed.value, ec.value, p14.value
 
 

@@ -643,7 +643,8 @@ void orc_improper_harmonic(const orc_params *p, int np, const orc_ainfo *pos, in
 void orc_dihedral_opls_dsf(const orc_params *p, int np, const orc_ainfo *pos, const float *q,
                            int ntypes, const double *lj14, int ndihed,
                            const int32_t *dihedlist, const double *dihedcoeff, float *ffh,
-                           double *e_dihedral, double *e_coul_14, double *pot_14) {
+                           double *e_dihedral, double *e_coul_14, double *pot_14,
+                           double *ffh64) {
     (void)np;
     const float box = p->box, ibox = p->ibox;
     const double alpha = p->alpha;
@@ -771,6 +772,13 @@ void orc_dihedral_opls_dsf(const orc_params *p, int np, const orc_ainfo *pos, co
             ffh[(size_t)i2 * 3 + c3] = (float)((double)ffh[(size_t)i2 * 3 + c3] + f2[c3]);
             ffh[(size_t)i3 * 3 + c3] = (float)((double)ffh[(size_t)i3 * 3 + c3] + f3[c3]);
             ffh[(size_t)i4 * 3 + c3] = (float)((double)ffh[(size_t)i4 * 3 + c3] + f4[c3]);
+            if (ffh64) {
+                /* the same per-dihedral terms summed in double (for FP64 comparisons) */
+                ffh64[(size_t)i1 * 3 + c3] += f1[c3];
+                ffh64[(size_t)i2 * 3 + c3] += f2[c3];
+                ffh64[(size_t)i3 * 3 + c3] += f3[c3];
+                ffh64[(size_t)i4 * 3 + c3] += f4[c3];
+            }
         }
     }
     *e_dihedral += edih;

@@ -100,7 +100,8 @@ void orc_dihedral_opls_dsf(const orc_params *p, int np, const orc_ainfo *pos, co
                            int ntypes, const double *lj14 /* [4][ntypes][ntypes] */,
                            int ndihed, const int32_t *dihedlist /* [n][5] */,
                            const double *dihedcoeff /* [ntype][4] */, float *ffh,
-                           double *e_dihedral, double *e_coul_14, double *pot_14);
+                           double *e_dihedral, double *e_coul_14, double *pot_14,
+                           double *ffh64 /* optional (np,3) double sums, may be NULL */);
 
 /* ---- PME exclusion corrections (Source/mod_force_correction.f90) ---- */
 void orc_correct_pairs(const orc_params *p, const orc_ainfo *pos, const float *q, int npairs,

@@ -16,7 +16,8 @@ beside this script:
 * ``run_*``: cutoffs, padding, cluster radii, DSF alpha, time step and the
   1-2/1-3/1-4 factors of the run input.
 
-Run it from the repository root:  python tests/golden/make_fixtures.py [reference_root]
+Run it from the repository root:  python tests/golden/make_fixtures.py REFERENCE_ROOT
+(REFERENCE_ROOT = the checkout holding input_files/).
 The tests only read the .npz; the reference checkout is not needed to run them.
 """
 import os
@@ -84,4 +85,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py REFERENCE_ROOT")
+    main(sys.argv[1])

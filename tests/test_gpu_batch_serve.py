@@ -52,6 +52,62 @@ def test_batch_equals_alone(ctx, replicas):
         c.close()
 
 
+def _alone(s, seed, nsteps, **md):
+    c = nb.Context(0)
+    m = M.System(c, s, cut=8.0, skin=2.0)
+    m.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
+    m.md_setup(s, dt=1.0, gamma=0.01, seed=seed, **md)
+    e = m.md_run(nsteps, energy_every=nsteps)
+    x, v, _ = m.get_state()
+    m.close()
+    c.close()
+    return x, v, e
+
+
+def test_batch_segment_graphs_equal_alone(ctx, replicas):
+    """Captured multi-step segments (10 steps per graph) and single-step launches
+    give each replica exactly its lone trajectory and last-step energies."""
+    ref = [_alone(s, 300 + k, 37) for k, s in enumerate(replicas)]
+    ctxs = [nb.Context(0) for _ in replicas]
+    systems = [_prep(c, s, 300 + k) for k, (c, s) in enumerate(zip(ctxs, replicas))]
+    b = Batch(ctx, systems)
+    b.set_segment(10)
+    e = b.run(37, energy_every=37)  # 3 segment graphs + 7 single steps
+    for k, m in enumerate(systems):
+        x, v, _ = m.get_state()
+        assert np.array_equal(x, ref[k][0]) and np.array_equal(v, ref[k][1]), k
+        assert e[k] == ref[k][2], k
+    b.close()
+    for m in systems:
+        m.close()
+    for c in ctxs:
+        c.close()
+
+
+def test_batch_membership_change_keeps_trajectories(ctx, replicas):
+    """Continuous batching: members leave and join between runs (no recapture);
+    every replica still follows its lone trajectory."""
+    ref = [_alone(s, 400 + k, 30) for k, s in enumerate(replicas)]
+    ctxs = [nb.Context(0) for _ in replicas]
+    systems = [_prep(c, s, 400 + k) for k, (c, s) in enumerate(zip(ctxs, replicas))]
+    b = Batch(ctx, systems[:2])
+    b.set_segment(5)
+    b.run(10)                       # replicas 0, 1: 10 steps
+    b.set_systems(systems[1:])      # 0 leaves, 2 joins
+    b.run(20)                       # replica 1: 30 steps, replica 2: 20
+    b.set_systems([systems[0], systems[2]])
+    b.run(10)                       # replica 0: 20, replica 2: 30
+    b.set_systems([systems[0]])
+    b.run(10)                       # replica 0: 30
+    for k, m in enumerate(systems):
+        assert np.array_equal(m.get_state()[0], ref[k][0]), k
+    b.close()
+    for m in systems:
+        m.close()
+    for c in ctxs:
+        c.close()
+
+
 def test_segments_compose(ctx, replicas):
     s = replicas[0]
     a = _prep(ctx, s, 5)

@@ -152,3 +152,37 @@ def test_md_fp64_and_mixed_trajectories_stay_close(ctx, small):
     assert np.abs(xa - xb).max() < 1e-3
     a.close()
     b.close()
+
+
+def _velocity_constraint_residual(s, x, v):
+    """max |(v_p - v_q) . r_pq| / |r_pq| over all SHAKE constraints, relative to rms |v|."""
+    L = float(s.box)
+    worst = 0.0
+    for g in s.shake:
+        num, a = int(g[0]), g[1:] - 1
+        pairs = {1: [(0, 1)], 3: [(0, 1), (0, 2)], 4: [(0, 1), (0, 2), (0, 3)],
+                 -3: [(0, 1), (0, 2), (1, 2)]}[num]
+        for u, w in pairs:
+            d = x[a[u]] - x[a[w]]
+            d -= L * np.round(d / L)
+            worst = max(worst, abs(np.dot(v[a[u]] - v[a[w]], d)) / np.linalg.norm(d))
+    return worst / np.sqrt((v * v).sum(axis=1).mean())
+
+
+def test_md_rattle_changes_only_full_step_velocities(ctx, small):
+    """The RATTLE stage projects the full-step velocities onto the constraints
+    and leaves the positions of the SHAKE step unchanged (to rounding of the
+    fixed-point force it compensates)."""
+    s = small
+    kw = dict(dt=2.0, gamma=0.0, seed=1, shake_maxiter=200, shake_tol=1e-12)
+    a = _system(ctx, s, **kw)
+    b = _system(ctx, s, rattle=True, **kw)
+    a.md_run(10)
+    b.md_run(10)
+    xa, va, _ = a.get_state()
+    xb, vb, _ = b.get_state()
+    assert np.abs(xa - xb).max() < 1e-8, np.abs(xa - xb).max()
+    assert _velocity_constraint_residual(s, xb, vb) < 1e-9
+    assert _velocity_constraint_residual(s, xa, va) > 1e-6
+    a.close()
+    b.close()

@@ -180,12 +180,68 @@ def test_small_box_images(ctx):
     sysm.close()
 
 
+def _pairs_within(x, box, r):
+    """All unordered atom pairs within r (minimum image) as sorted int64 keys i*N + j, i < j."""
+    from scipy.spatial import cKDTree
+    L = float(box)
+    xw = np.mod(np.asarray(x, np.float64), L)
+    xw[xw >= L] = 0.0
+    pr = cKDTree(xw, boxsize=L).query_pairs(r, output_type="ndarray").astype(np.int64)
+    n = x.shape[0]
+    return np.unique(pr.min(axis=1) * n + pr.max(axis=1))
+
+
+def _list_keys(pairs, n):
+    a, b = pairs[:, 0].astype(np.int64), pairs[:, 1].astype(np.int64)
+    return np.minimum(a, b) * n + np.maximum(a, b)
+
+
+def _excluded_keys(s):
+    n = s.np_atoms
+    ks = []
+    for i in range(n):
+        for l in range(int(s.num3bond[i])):
+            j = int(s.specbond[i, l]) - 1
+            if j >= 0:
+                ks.append(min(i, j) * n + max(i, j))
+    return np.unique(np.array(ks, np.int64))
+
+
 def test_list_covers_every_pair_within_rlist(ctx):
-    """The cluster list reaches every atom pair within rc + skin (minimum image)."""
-    s = small_system(10, 700, 6)
-    sysm = M.System(ctx, s, cut=7.0, skin=2.0, precision=M.FP64)
-    sysm.set_state(s.xyz.astype(np.float64))
-    sysm.compute(M.FP64, rebuild=True)
+    """The cluster lists, expanded into atom pairs, hold every non-excluded pair
+    once: the outer list every pair within rc + skin at its build positions, the
+    pruned list every pair within rc + margin at its prune positions and every
+    pair within rc at the current positions, after a rebuild and along a
+    drifting trajectory with several prunes and rebuilds."""
+    s = make_system(150, 2500, 1)
+    n = s.np_atoms
+    cut, skin, margin = 10.0, 2.0, 0.6
+    sysm = M.System(ctx, s, cut=cut, skin=skin, precision=M.MIXED)
+    sysm.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
+    sysm.md_setup(s, dt=2.0, temperature=300.0, gamma=0.01, seed=4)
+    sysm.compute(M.MIXED, rebuild=True, energy=False, virial=False)
+    excl = _excluded_keys(s)
+    st0 = sysm.stats()
+    checks = 0
+    for seg in range(6):
+        x, _, _ = sysm.get_state()
+        outer, xo = sysm.list_pairs(0)
+        inner, xi = sysm.list_pairs(1)
+        ko, ki = _list_keys(outer, n), _list_keys(inner, n)
+        # each pair at most once, never an excluded (1-2, 1-3, 1-4) or self pair
+        assert np.unique(ko).size == ko.size and np.unique(ki).size == ki.size
+        assert not np.isin(ko, excl).any() and not np.isin(ki, excl).any()
+        assert (outer[:, 0] != outer[:, 1]).all()
+        assert np.isin(ki, ko).all()  # the pruned list is a subset of the outer list
+        need_o = np.setdiff1d(_pairs_within(xo, s.box, cut + skin), excl)
+        need_i = np.setdiff1d(_pairs_within(xi, s.box, cut + margin), excl)
+        need_c = np.setdiff1d(_pairs_within(x, s.box, cut), excl)
+        assert np.isin(need_o, ko).all(), np.setdiff1d(need_o, ko)[:5]
+        assert np.isin(need_i, ki).all(), np.setdiff1d(need_i, ki)[:5]
+        assert np.isin(need_c, ki).all(), np.setdiff1d(need_c, ki)[:5]
+        checks += 1
+        sysm.md_run(40)
     st = sysm.stats()
-    assert st["entries"] > 0 and st["clusters"] * 8 >= s.np_atoms
+    assert checks == 6
+    assert st["prunes"] - st0["prunes"] >= 3 and st["builds"] - st0["builds"] >= 1, (st0, st)
     sysm.close()

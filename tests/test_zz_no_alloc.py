@@ -1,13 +1,15 @@
 """The allocation-free force entry point agrees with the regular one.
 
 ``sofia_force_nonbond_dsf_noalloc`` serves callers that cannot allocate device
-memory when they need forces (for example while a stream is being captured into
-a CUDA graph, or under a device-memory budget enforced outside the library).
-It takes only caller-owned device buffers and keeps its scratch in a fixed
-array inside the library.  This test calls it through the C ABI twice in a row
-and checks both results against ``sofia_force_nonbond_dsf`` on the same inputs,
-with the FP64 tolerance used by the other parity tests.  It lives in its own
-file so that pytest collects it last.
+memory when they need forces (for example under a device-memory budget or arena
+enforced outside the library, or drivers that own every device array).  It
+takes only caller-owned device buffers and keeps its scratch in a fixed array
+inside the library.  This test calls it through the C ABI twice in a row and
+checks both results against ``sofia_force_nonbond_dsf`` on the same inputs,
+with the FP64 tolerance used by the other parity tests, and checks that the
+device's free memory does not change across the two calls (after a warm-up
+call, which may load the kernels' code).  It lives in its own file so that
+pytest collects it last.
 """
 import ctypes as C
 
@@ -59,10 +61,19 @@ def test_noalloc_matches_regular_entry_point(ctx, n_gly, n_wat, cut):
                                                               na, p, ff=ff_ref)
     L = _lib.lib()
     stream = torch.cuda.current_stream().cuda_stream
+    ffs = [torch.full((n, 3), float("nan"), dtype=torch.float32, device=dev) for _ in range(3)]
+    torch.cuda.synchronize()
+    rc, *_ = _noalloc(L, stream, n, pos, q, lj, s.ntypes, nl, nn, na, p, ffs[2])  # warm-up
+    assert rc == _lib.SOFIA_OK
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    results = []
     for call in range(2):
-        ff = torch.full((n, 3), float("nan"), dtype=torch.float32, device=dev)
-        torch.cuda.synchronize()
-        rc, pot, ec, vir = _noalloc(L, stream, n, pos, q, lj, s.ntypes, nl, nn, na, p, ff)
+        results.append(_noalloc(L, stream, n, pos, q, lj, s.ntypes, nl, nn, na, p, ffs[call]))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(dev)[0] == free0, "the calls changed the device's free memory"
+    for call, (rc, pot, ec, vir) in enumerate(results):
+        ff = ffs[call]
         assert rc == _lib.SOFIA_OK, f"call {call}: rc {rc}"
         assert abs(pot - pot_ref) <= FP64_TOL * abs(pot_ref)
         assert abs(ec - ec_ref) <= FP64_TOL * abs(ec_ref)
