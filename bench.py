@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--only-hot", action="store_true",
                     help="time only the nonbonded hot path (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the rows of the other configurations (9k, 90k, batch, serving)")
+    ap.add_argument("--serve-requests", type=int, default=48)
     return ap.parse_args()
 
 
@@ -187,6 +190,16 @@ def measure_fp32_peak() -> float:
     return 2.0 * n ** 3 / best / 1e12
 
 
+def measured_hbm():
+    """HBM copy bandwidth of this pool's B200s (GB/s) and where it came from."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured copy)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
+
+
 def read_profile_traffic():
     """Per-launch DRAM bytes of the pair kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "k_pair_mixed_275k.md")
@@ -295,6 +308,178 @@ def run_reference(args, rank, ws):
            "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+def md_rate(ctx, M, s, precision, nsteps, seed=11):
+    """Device-resident MD atom-steps/s of one system: damped relaxation and 300 K
+    equilibration (untimed), then nsteps in captured graphs with CUDA events."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctx._lib.sofia_stream(ctx.handle))
+    m = M.System(ctx, s, alpha=ALPHA, cut=CUT, skin=SKIN, precision=precision)
+    m.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
+    m.md_setup(s, dt=1.0, temperature=300.0, gamma=0.02, seed=seed)
+    m.md_run(RELAX_STEPS)
+    m.md_setup(s, dt=DT, temperature=300.0, gamma=0.02, seed=seed + 1)
+    m.md_run(EQUIL_STEPS)
+    m.md_setup(s, dt=DT, temperature=300.0, gamma=0.001, seed=seed + 2)
+    m.md_run(10)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    en = m.md_run(nsteps, energy_every=nsteps, use_graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    x, v, _ = m.get_state()
+    m.close()
+    return {"atom_steps_per_s": s.np_atoms * nsteps / t, "ms_per_step": 1e3 * t / nsteps,
+            "ns_per_day": DT * 1e-6 * nsteps / t * 86400.0, "steps": nsteps,
+            "temperature_K": en["temperature"]}, x, v
+
+
+def cpu_md_sample(s, nsteps):
+    """Oracle port (OpenMP, all host threads) on a ballistic trajectory: neighbour
+    rebuild on the half-skin trigger plus the FP64 force every step."""
+    import ctypes as C
+    from oracle import oracle as O
+    p = O.params(ALPHA, s.box, CUT, CUT, SKIN)
+    lj = (s.lj1, s.lj2, s.lj3, s.lj4)
+    x0 = s.xyz.astype(np.float64)
+    v = s.velocity.astype(np.float64)
+    pos = s.position_aos()
+    Lb = float(s.box)
+    L = O.lib(fast=True)
+    xref = None
+    nl = nn = None
+    na = 1024
+    half2 = (0.5 * SKIN) ** 2
+    builds = 0
+    t0 = time.perf_counter()
+    for k in range(nsteps):
+        x = x0 + v * DT * (k + 1)
+        posk = pos.copy()
+        posk[:, :3] = np.mod(x, Lb).astype(np.float32)
+        posk[:, :3][posk[:, :3] <= 0] += np.float32(Lb)
+        if xref is None:
+            rebuild = True
+        else:
+            d = x - xref
+            d -= Lb * np.round(d / Lb)
+            rebuild = bool((np.einsum("ij,ij->i", d, d) > half2).any())
+        if rebuild:
+            nl, nn, na = O.neighbor_wrapper(p, posk, s.specbond, s.num3bond, na, fast=True)
+            xref = x.copy()
+            builds += 1
+        ff = np.zeros(s.np_atoms * 3, np.float32)
+        pot = C.c_double()
+        ec = C.c_double()
+        L.orc_force_dsf_nonewton(C.byref(p), s.np_atoms, posk, np.ascontiguousarray(s.q), lj[0],
+                                 lj[1], lj[2], lj[3], s.ntypes, nl, nn, na, ff, C.byref(pot),
+                                 C.byref(ec), np.zeros(3), None, 0)
+    t = time.perf_counter() - t0
+    return {"value": s.np_atoms * nsteps / t, "unit": "atom-steps/s", "cores": os.cpu_count(),
+            "kind": "port", "steps": nsteps, "list_rebuilds": builds,
+            "sample": f"{s.np_atoms} atoms, {nsteps} steps: reference list build on the half-skin "
+                      "trigger + FP64 force every step, ballistic trajectory"}
+
+
+def row_hash(nl, nn, na):
+    """Order-independent hash of each neighbour row (sum of a 64-bit mix of its ids)."""
+    n = nn.shape[0]
+    m = nl.reshape(n, na).astype(np.uint64)
+    valid = np.arange(na)[None, :] < nn[:, None]
+    h = m * np.uint64(0x9E3779B97F4A7C15)
+    h ^= h >> np.uint64(29)
+    h *= np.uint64(0xBF58476D1CE4E5B9)
+    return np.where(valid, h, np.uint64(0)).sum(axis=1, dtype=np.uint64)
+
+
+def extra_rows(args, ctx, budget_s=420.0):
+    """The other configurations' rows (9k, 90k, 64-replica batch, serving), each
+    bounded in time; the MD rows use the same step and timing as ``value``."""
+    import torch
+
+    from molecular_simulation_code_b200 import mixed as M
+    from molecular_simulation_code_b200 import nonbond as nb
+    from molecular_simulation_code_b200.system import make_workload
+    t_start = time.time()
+    out = {}
+    # config 1: 9,000 atoms
+    s9 = make_workload("gly150_wat2500_9k", seed=1000)
+    r_mixed, _, _ = md_rate(ctx, M, s9, M.MIXED, 1000)
+    r_fp64, _, _ = md_rate(ctx, M, s9, M.FP64, 1000)
+    cpu = cpu_md_sample(s9, 1000)
+    out["cfg1_9k"] = {"atoms": s9.np_atoms, "mixed": r_mixed, "fp64": r_fp64,
+                      "mixed_over_fp64": r_mixed["atom_steps_per_s"] / r_fp64["atom_steps_per_s"],
+                      "cpu_reference_1000_steps": cpu,
+                      "gpu_mixed_over_cpu": r_mixed["atom_steps_per_s"] / cpu["value"]}
+    # config 2: 90,000 atoms
+    s90 = make_workload("gly1500_wat25000_90k", seed=2000)
+    r_mixed, x, v = md_rate(ctx, M, s90, M.MIXED, 500)
+    r_fp64, _, _ = md_rate(ctx, M, s90, M.FP64, 500)
+    row = {"atoms": s90.np_atoms, "mixed": r_mixed, "fp64": r_fp64,
+           "mixed_over_fp64": r_mixed["atom_steps_per_s"] / r_fp64["atom_steps_per_s"]}
+    # force error on snapshots of a Langevin trajectory
+    run = M.System(ctx, s90, alpha=ALPHA, cut=CUT, skin=SKIN)
+    run.set_state(x, v)
+    run.md_setup(s90, dt=DT, temperature=300.0, gamma=0.001, seed=31)
+    probe = M.System(ctx, s90, alpha=ALPHA, cut=CUT, skin=SKIN)
+    rms, mx = [], []
+    for _ in range(5):
+        run.md_run(200)
+        xs, _, _ = run.get_state()
+        probe.set_state(xs)
+        probe.compute(M.FP64, rebuild=True, energy=False, virial=False)
+        f64 = probe.get_state()[2]
+        probe.compute(M.MIXED, rebuild=True, energy=False, virial=False)
+        f32 = probe.get_state()[2]
+        rms.append(M.force_rms_rel(f32, f64))
+        mx.append(M.force_max_rel(f32, f64))
+    row["force_error_vs_fp64"] = {"snapshots": 5, "rms_rel_max": max(rms),
+                                  "max_rel_max": max(mx), "bar_rms": 1e-6}
+    # neighbour rows of the reference-semantics GPU build vs the oracle, as sets
+    from oracle import oracle as O
+    xs, vs, _ = run.get_state()
+    pos = s90.position_aos().copy()
+    Lb = float(s90.box)
+    w = np.mod(xs, Lb).astype(np.float32)
+    w[w <= 0] += np.float32(Lb)
+    pos[:, :3] = w
+    p = nb.DsfParams(alpha=ALPHA, box=s90.box, cut_coul=CUT, rcut=CUT, neighbor_pad=SKIN)
+    gnl, gnn, gna = nb.neighbor_wrapper(ctx, pos, s90.specbond, s90.num3bond, p, 1024)
+    op = O.params(ALPHA, s90.box, CUT, CUT, SKIN)
+    onl, onn, ona = O.neighbor_wrapper(op, pos, s90.specbond, s90.num3bond, 1024, fast=True)
+    same = bool(np.array_equal(gnn, onn) and
+                np.array_equal(row_hash(gnl, gnn, gna), row_hash(onl, onn, ona)))
+    row["neighbor_sets_bit_exact"] = {"equal": same, "entries": int(onn.sum())}
+    run.close()
+    probe.close()
+    # NVE drift: the reference scheme and the RATTLE + LJ-shift variant
+    from molecular_simulation_code_b200.validate import nve_drift
+    drift = {}
+    for name, rattle, shift in (("reference_scheme", False, False),
+                                ("rattle_ljshift", True, True)):
+        drift[name] = nve_drift(M, ctx, s90, xs, vs, dt=DT, precision=M.MIXED, rattle=rattle,
+                                lj_shift=shift, shake_tol=1e-10, ps=20.0, cut=CUT, skin=SKIN)
+    row["nve_drift_20ps"] = drift
+    out["cfg2_90k"] = row
+    # config 4: 64 replicas in one batch
+    if time.time() - t_start < budget_s:
+        from molecular_simulation_code_b200.replica_bench import bench_batch
+        a = argparse.Namespace(replicas=64, seed=5000, procs=min(16, os.cpu_count() or 1),
+                               tune=False, segment=100, segments=3)
+        out["cfg4_batch64"] = bench_batch(a)
+        out["cfg4_batch64"]["pair_launches_per_batch_step"] = 1
+    # config 5: serving
+    if time.time() - t_start < budget_s:
+        from molecular_simulation_code_b200.replica_bench import bench_serve
+        a = argparse.Namespace(requests=args.serve_requests, rate=200.0, steps_scale=1.0,
+                               chunk=100, max_active=64, budget_gb=96.0, seed=7000,
+                               procs=min(16, os.cpu_count() or 1), nucleus_every=4)
+        out["cfg5_serve"] = bench_serve(a)
+    out["wall_s"] = time.time() - t_start
+    return out
 
 
 def run_ours(args, rank, ws):
@@ -467,6 +652,17 @@ def run_ours(args, rank, ws):
     rebuild_interval = args.steps / max(md_builds, 1)
     cpu = None if args.no_cpu_baseline else cpu_baseline(s, rebuild_interval)
     clocks = clk.summary()
+    # the list build: algorithmic bytes per rebuild (positions and types read, sorted
+    # records written, cell ids, 4 B list index per pair within rc + skin) over the
+    # measured build time, against the measured HBM copy bandwidth
+    build_ms = tm["build_ms"] / max(tm["builds"], 1)
+    b_nb = n * (24 + 4) + n * 28 + n * 4 + 4 * P_rv
+    hbm_peak, peak_src = measured_hbm()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    fp32_spec = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    extras = None
+    if not args.no_extras and ws == 1:
+        extras = extra_rows(args, ctx)
     out = {
         "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
@@ -504,9 +700,19 @@ def run_ours(args, rank, ws):
                      "pair_ms": pair_ms, "pairs_P_rv": P_rv,
                      "flop_per_pair": FLOP_PER_PAIR,
                      "peak_source": "measured cuBLAS SGEMM 8192^3, TF32 off, on this GPU"},
+        "roofline_build": {"bound": "hbm", "kernels": "k_wrap_bin .. k_search (one rebuild)",
+                           "build_ms": build_ms, "algorithmic_bytes": b_nb,
+                           "achieved": b_nb / (build_ms / 1e3) / 1e9 if build_ms else None,
+                           "peak": hbm_peak, "unit": "GB/s",
+                           "frac": (b_nb / (build_ms / 1e3) / 1e9 / hbm_peak) if build_ms else None,
+                           "peak_source": peak_src,
+                           "list_bytes_written": st["entries"] * 12},
         "cpu_baseline": cpu,
         "clocks": clocks,
+        "configs": extras,
     }
+    out["roofline"]["peak_fp32_spec"] = fp32_spec
+    out["roofline"]["frac_of_fp32_spec"] = achieved / fp32_spec
     print(json.dumps(out), flush=True)
 
 

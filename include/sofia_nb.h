@@ -470,10 +470,14 @@ int sofia_system_rollback(sofia_system *sys);
  * wrapped into (0, box] as real*4 (x - L floor(x/L), then +box if <= 0) and
  * analysed like sofia_greatest_cluster with global ids 1..np.  The glycine
  * molecules are the first n_gly * atoms_per_gly atoms.  ptta_full (host or
- * device) and *greatest_belongsto are in/out as in sofia_greatest_cluster. */
+ * device) and *greatest_belongsto are in/out as in sofia_greatest_cluster;
+ * ptta_full == NULL uses the system's own device copy, set from its current
+ * positions by the first such call. */
 int sofia_system_greatest_cluster(sofia_system *sys, int n_gly, int atoms_per_gly, double mrcut,
                                   double denscut, int densmin, double *ptta_full,
                                   int32_t *greatest_belongsto, int32_t *size_out);
+/* Device memory the system holds now (buffers grow with the list capacity). */
+int sofia_system_device_bytes(sofia_system *sys, int64_t *bytes);
 /* Thermostat step counter (counter of the Langevin noise).  Reading it with
  * the state and setting it on resume continues the same noise sequence; the
  * reference restart (read_dump_global_id_v, Source/mod_datadump.f90:216-252)

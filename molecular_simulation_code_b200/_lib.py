@@ -140,6 +140,7 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_system_md_set_step": (_I, [_P, C.c_longlong]),
     "sofia_system_greatest_cluster": (_I, [_P, _I, _I, _D, _D, _I, _P, C.POINTER(C.c_int32),
                                            C.POINTER(C.c_int32)]),
+    "sofia_system_device_bytes": (_I, [_P, C.POINTER(C.c_int64)]),
 }
 
 _lib = None

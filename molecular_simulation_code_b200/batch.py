@@ -124,15 +124,18 @@ class Tuner:
 
 
 def _gen(args):
-    seed, n_min, n_max = args
+    seed, n_min, n_max, nucleus = args
     rng = np.random.default_rng(seed)
-    return random_replica(rng, n_min, n_max, seed=seed)
+    return random_replica(rng, n_min, n_max, seed=seed, nucleus=nucleus)
 
 
 def make_replicas(n: int, seed: int = 4000, n_min: int = 3000, n_max: int = 30000,
-                  processes: int = 8):
-    """Seeded replicas of N ~ U[n_min, n_max] atoms (generated in a spawn pool)."""
-    args = [(seed + k, n_min, n_max) for k in range(n)]
+                  processes: int = 8, nucleus_every: int = 0, nucleus: int = 60):
+    """Seeded replicas of N ~ U[n_min, n_max] atoms (generated in a spawn pool).
+    Every ``nucleus_every``-th replica (0 = none) starts with a compact crystalline
+    glycine nucleus of up to ``nucleus`` molecules (5.5 A fcc)."""
+    args = [(seed + k, n_min, n_max,
+             nucleus if nucleus_every and k % nucleus_every == 0 else 0) for k in range(n)]
     if processes <= 1 or n <= 2:
         return [_gen(a) for a in args]
     with mp.get_context("spawn").Pool(processes) as pool:

@@ -1,9 +1,13 @@
 """Builds ``libsofia_nb.so`` (all CUDA kernels + the C ABI) for sm_100a, in tree.
 
 Each ``csrc/*.cu`` translation unit is compiled with
-``-gencode arch=compute_100a,code=sm_100a``; the reference-semantics units
-(``ref_kernels.cu``, ``cluster.cu``) additionally with ``-fmad=false`` so that
-every real*4 / real*8 operation is rounded separately, in source order.
+``-gencode arch=compute_100a,code=sm_100a -fmad=false``: the compiler contracts
+no product into a later sum, so every real*4 / real*8 operation is rounded
+separately, in source order, and the fused multiply-adds that the kernels want
+are written out (``__fma_rn``, ``__fmaf_rn``, ``__ffma2_rn``).  A kernel body
+then gives the same bits whichever kernel inlines it: the single-system
+kernels and the batched ones that run the same bodies for many replicas
+produce identical trajectories.
 """
 from __future__ import annotations
 
@@ -21,7 +25,6 @@ NVCC = os.environ.get("SOFIA_NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-ccbin", "g++"]
-STRICT_UNITS = {"ref_kernels.cu", "cluster.cu"}
 
 
 def _units():
@@ -54,9 +57,7 @@ def build(verbose: bool = False, extra_flags: list[str] | None = None) -> str:
         objs.append(obj)
         if not _stale(obj, [src] + headers + [__file__]):
             continue
-        flags = list(COMMON) + ARCH + (extra_flags or [])
-        if u in STRICT_UNITS:
-            flags += ["-fmad=false"]
+        flags = list(COMMON) + ARCH + ["-fmad=false"] + (extra_flags or [])
         cmd = [NVCC] + flags + ["-I", INCLUDE, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)

@@ -1168,8 +1168,11 @@ namespace {
         const int lb = vb - pre_[r_];
 #define SOFIA_BATCH_END }
 
-__global__ void k_kick_drift_b(const BatchDev *__restrict__ tab) {
+__global__ void k_kick_drift_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
+    // the step's first kernel: clear the work-queue counters of the later ones
+    // (each of them starts after this grid has completed)
+    if (blockIdx.x == 0 && threadIdx.x < BC_N) tab->ctr[threadIdx.x] = 0;
     SOFIA_BATCH_LOOP(BK_A256)
     kick_drift_body(lb, d.n, d.h, d.invm, d.fx, d.fy, d.fz, d.vx, d.vy, d.vz, d.dt, d.x, d.y,
                     d.z, d.rx, d.ry, d.rz, d.px, d.py, d.pz, d.L, d.lim2, d.plim2, d.flag,
@@ -1178,16 +1181,16 @@ __global__ void k_kick_drift_b(const BatchDev *__restrict__ tab) {
 }
 
 template <bool EN>
-__global__ void __launch_bounds__(128) k_bonded_b(const BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(128) k_bonded_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_B128)
+    SOFIA_BATCH_QUEUE_LOOP(BK_B128, BC_BONDED)
     bonded_body<EN>(lb, d.b);
     SOFIA_BATCH_END
 }
 
-__global__ void k_shake_b(const BatchDev *__restrict__ tab) {
+__global__ void k_shake_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_G128)
+    SOFIA_BATCH_QUEUE_LOOP(BK_G128, BC_SHAKE)
     shake_body(lb, d.nshake, d.shake, d.sbond, d.x, d.y, d.z, d.vx, d.vy, d.vz, d.invm, d.L,
                d.dt, d.dtsq, d.shake_maxiter, d.shake_tol, d.fx, d.fy, d.fz, d.status);
     SOFIA_BATCH_END
@@ -1317,7 +1320,7 @@ static void repdev_fill_md(Sys *s, RepDev *d) {
 }
 
 // One batched MD step: the same kernels, in the same order, as md_step.
-static void batch_step(const BatchDev *tab, Sys *s0, bool energy, bool rattle, cudaStream_t st,
+static void batch_step(BatchDev *tab, Sys *s0, bool energy, bool rattle, cudaStream_t st,
                        int nsm) {
     const int g256 = nsm * 8, g128 = nsm * 16;
     launch_pdl(k_kick_drift_b, g256, 256, 0, st, tab);
@@ -1472,7 +1475,7 @@ static int batch_capture(sofia_batch *b) {
     batch_drop_graphs(b);
     sofia_nb_ctx *ctx = b->ctx;
     cudaStream_t ms = ctx->stream;
-    const auto *tab = b->tab.as<sofia::BatchDev>();
+    auto *tab = b->tab.as<sofia::BatchDev>();
     Sys *s0 = &b->sys[0]->s;
     bool rat = false;
     for (auto *s : b->sys) rat = rat || (s->s.md.rattle && s->s.md.nshake);
@@ -1688,6 +1691,16 @@ __global__ void k_resident_ainfo(int n, const double *__restrict__ x,
     out[i] = make_float4(w[0], w[1], w[2], __int_as_float(type[i]));
     gid[i] = i + 1;
 }
+
+// ptta_full[i*3 + d] = the current FP64 position of glycine atom i (first call).
+__global__ void k_ptta_init(int na, const double *__restrict__ x, const double *__restrict__ y,
+                            const double *__restrict__ z, double *__restrict__ ptta) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= na) return;
+    ptta[3 * i + 0] = x[i];
+    ptta[3 * i + 1] = y[i];
+    ptta[3 * i + 2] = z[i];
+}
 }  // namespace
 }  // namespace sofia
 
@@ -1713,9 +1726,48 @@ extern "C" int sofia_system_greatest_cluster(sofia_system *ss, int n_gly, int at
         s->n, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
         s->type.as<int>(), s->L, s->box, s->cl_pos.as<float4>(), s->cl_gid.as<int>());
     SOFIA_CUDA(ctx, cudaGetLastError());
+    if (!ptta_full) {
+        // the system keeps its own ptta_full on the device, set from the current
+        // positions by the first call
+        const int na = n_gly * atoms_per_gly;
+        if (s->ptta_atoms != na) {
+            SOFIA_CUDA(ctx, s->ptta.ensure(sizeof(double) * 3 * (size_t)(na > 0 ? na : 1)));
+            if (na > 0)
+                sofia::k_ptta_init<<<sofia::grid_for(na, 256), 256, 0, ctx->stream>>>(
+                    na, s->x[0].as<double>(), s->x[1].as<double>(), s->x[2].as<double>(),
+                    s->ptta.as<double>());
+            SOFIA_CUDA(ctx, cudaGetLastError());
+            s->ptta_atoms = na;
+        }
+        ptta_full = s->ptta.as<double>();
+    }
     return sofia_greatest_cluster(ctx, s->n, s->cl_pos.as<sofia_ainfo>(), s->cl_gid.as<int32_t>(),
                                   n_gly, atoms_per_gly, s->box, mrcut, denscut, densmin,
                                   ptta_full, greatest_belongsto, size_out, nullptr, nullptr);
+}
+
+// Device memory a system holds (all its buffers, lists and MD state).
+extern "C" int sofia_system_device_bytes(sofia_system *ss, int64_t *bytes) {
+    if (!ss || !bytes) return SOFIA_EINVAL;
+    const Sys *s = &ss->s;
+    const Md &md = s->md;
+    const sofia::DevBuf *bufs[] = {
+        &s->x[0], &s->x[1], &s->x[2], &s->v[0], &s->v[1], &s->v[2], &s->f[0], &s->f[1], &s->f[2],
+        &s->xref[0], &s->xref[1], &s->xref[2], &s->img[0], &s->img[1], &s->img[2], &s->type,
+        &s->q, &s->invm, &s->mass, &s->specbond, &s->num3bond, &s->ljtab, &s->col_count,
+        &s->col_start, &s->col_fill, &s->col_atoms, &s->col_key, &s->cl_start, &s->slot_orig,
+        &s->rec, &s->bb, &s->jlist, &s->jmask, &s->jcount, &s->nclusters, &s->recf, &s->fslot,
+        &s->atom_slot, &s->status_local, &s->energy, &s->red, &s->flag, &s->stage_pos,
+        &s->stage_ff, &s->cl_pos, &s->cl_gid, &s->ptta, &s->ilist, &s->imask, &s->icount,
+        &s->xprn[0], &s->xprn[1], &s->xprn[2], &s->part, &s->dcount, &md.bonds, &md.bcoef,
+        &md.angles, &md.acoef, &md.diheds, &md.dcoef, &md.lj14, &md.shake, &md.sbond, &md.impros,
+        &md.icoef, &md.eterm, &md.ered, &md.bpart, &md.step_dev, &md.snap[0], &md.snap[1],
+        &md.snap[2], &md.snap[3], &md.snap[4], &md.snap[5], &md.snap[6], &md.keep[0], &md.keep[1],
+        &md.keep[2], &md.keep[3], &md.keep[4], &md.keep[5], &md.keep[6]};
+    int64_t total = 0;
+    for (const sofia::DevBuf *b : bufs) total += (int64_t)b->bytes;
+    *bytes = total;
+    return SOFIA_OK;
 }
 
 // Thermostat step counter (the Philox counter of the Langevin noise): read it

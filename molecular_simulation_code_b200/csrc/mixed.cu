@@ -36,7 +36,7 @@ constexpr int MAX_COL = 2048;
 #define SOFIA_COND_RETURN \
     if (cond && !(cond[0] & cmask)) return  // atoms per xy column handled by the in-column sort
 #ifndef SOFIA_PAIR_FLUSH
-#define SOFIA_PAIR_FLUSH 4
+#define SOFIA_PAIR_FLUSH 8
 #endif
 #ifndef SOFIA_PAIR_MINB
 #define SOFIA_PAIR_MINB 4
@@ -53,7 +53,7 @@ constexpr int MAX_COL = 2048;
 #ifndef SOFIA_SEARCH_ZWIN
 #define SOFIA_SEARCH_ZWIN 1
 #endif
-constexpr int FLUSH = SOFIA_PAIR_FLUSH;  // j-clusters between FP32 -> fixed-point flushes
+constexpr int FLUSH = SOFIA_PAIR_FLUSH;  // list entries between FP32 -> fixed-point flushes of the i forces
 
 __device__ __forceinline__ double wrap_shift(double x, double L) {
     // shift s with x + s in [0, L)
@@ -763,45 +763,54 @@ __device__ __forceinline__ long long to_fix<double>(double v) {
     return __double2ll_rn(v * FIX_SCALE);
 }
 
-// The j-force values of one entry, v[3h + c] (component c of j atom lj + 4h),
-// summed over the 8 lanes that share lj (lane bits 0..2) by reduce-scatter:
-// each butterfly level keeps half of the values and trades the other half.
-// Afterwards lane (b2 b1 b0) holds component 2*b1 + b0 (3 = none) of j atom
-// lj + 4*b2.  6 shuffles instead of 18 for a full butterfly of 6 values.
+// The j force of one entry, (v0, v1, v2) on each of the 4 lanes that share a j
+// atom (lane bits 3 and 4), summed over those lanes by reduce-scatter: afterwards
+// lane bits (4, 3) = (0, 0) hold component x, (0, 1) y, (1, 0) z, (1, 1) none.
+// Three shuffles.
 template <typename T>
-__device__ __forceinline__ T reduce_scatter_j(const T (&v)[6], int lane) {
-    const bool u2 = lane & 4, u1 = lane & 2, u0 = lane & 1;
-    T s0, s1, s2;
-    {
-        const T k0 = u2 ? v[3] : v[0], k1 = u2 ? v[4] : v[1], k2 = u2 ? v[5] : v[2];
-        const T o0 = u2 ? v[0] : v[3], o1 = u2 ? v[1] : v[4], o2 = u2 ? v[2] : v[5];
-        s0 = k0 + __shfl_xor_sync(FULL, o0, 4);
-        s1 = k1 + __shfl_xor_sync(FULL, o1, 4);
-        s2 = k2 + __shfl_xor_sync(FULL, o2, 4);
-    }
-    T t0, t1;
-    {
-        const T k0 = u1 ? s2 : s0, k1 = u1 ? (T)0 : s1;
-        const T o0 = u1 ? s0 : s2, o1 = u1 ? s1 : (T)0;
-        t0 = k0 + __shfl_xor_sync(FULL, o0, 2);
-        t1 = k1 + __shfl_xor_sync(FULL, o1, 2);
-    }
-    const T k0 = u0 ? t1 : t0, o0 = u0 ? t0 : t1;
-    return k0 + __shfl_xor_sync(FULL, o0, 1);
+__device__ __forceinline__ T reduce_j4(T v0, T v1, T v2, int lane) {
+    const bool u4 = lane & 16, u3 = lane & 8;
+    const T k0 = u4 ? v2 : v0, k1 = u4 ? (T)0 : v1;
+    const T o0 = u4 ? v0 : v2, o1 = u4 ? v1 : (T)0;
+    const T s0 = k0 + __shfl_xor_sync(FULL, o0, 16);
+    const T s1 = k1 + __shfl_xor_sync(FULL, o1, 16);
+    const T k = u3 ? s1 : s0, o = u3 ? s0 : s1;
+    return k + __shfl_xor_sync(FULL, o, 8);
+}
+
+// i-force partial sums of one lane (i atoms q and q + 4) -> the warp's 64-bit
+// fixed-point sums in shared memory (integer adds: order-independent).
+template <typename T>
+__device__ __forceinline__ void flush_i(long long *__restrict__ fi, int q, T x0, T y0, T z0,
+                                        T x1, T y1, T z1) {
+    unsigned long long *u = reinterpret_cast<unsigned long long *>(fi);
+    if (x0 != (T)0) atomicAdd(u + 0 * CL + q, (unsigned long long)to_fix<T>(x0));
+    if (y0 != (T)0) atomicAdd(u + 1 * CL + q, (unsigned long long)to_fix<T>(y0));
+    if (z0 != (T)0) atomicAdd(u + 2 * CL + q, (unsigned long long)to_fix<T>(z0));
+    if (x1 != (T)0) atomicAdd(u + 0 * CL + q + 4, (unsigned long long)to_fix<T>(x1));
+    if (y1 != (T)0) atomicAdd(u + 1 * CL + q + 4, (unsigned long long)to_fix<T>(y1));
+    if (z1 != (T)0) atomicAdd(u + 2 * CL + q + 4, (unsigned long long)to_fix<T>(z1));
 }
 
 // Pair kernel on the half cluster-pair list (each atom pair once, Newton's
-// third law).  One warp per i-cluster; lane = li (i atom, 0..7) + 8*lj (each
-// lane takes j atoms lj and lj+4 of every j-cluster).  List rows are read 32
-// entries at a time with coalesced loads and broadcast by shuffles.
-//   * i forces stay in registers (flushed from FP32 to 64-bit fixed point every
-//     FLUSH entries) and are added once at the end;
-//   * the j forces of each entry are reduced over the 8 lanes of a j atom
-//     (reduce_scatter_j) and added to the slot-ordered fixed-point
-//     accumulators, 24 lanes x one 64-bit atomic add into one j-cluster's
-//     contiguous slots.  Integer addition makes the sums independent of the
-//     order of the atomics, so results stay bit-reproducible.
-// EN adds the LJ and Coulomb energies, VIR the diagonal virial (each pair once).
+// third law).  One warp per i-cluster; lane = jj + 8 q (jj = j atom 0..7,
+// q = 0..3): for every listed j-cluster the lane evaluates the pairs of j atom
+// jj with i atoms q and q + 4, both in one stream of packed FP32x2
+// instructions (component x: i atom q, y: i atom q + 4).  List rows are read 32
+// entries at a time with coalesced loads and broadcast by shuffles.  Pruned
+// mask bit 8 ii + jj (i atom ii, j atom jj) is bit 32 h + lane of the lane that
+// evaluates it (ii = q + 4 h).
+//   * a lane loads one j record per entry;
+//   * the j force of an entry (the sum of the lane's two pairs) is reduced over
+//     the 4 lanes of its j atom (reduce_j4) and added to the slot-ordered
+//     fixed-point accumulators, 24 lanes x one 64-bit atomic add into one
+//     j-cluster's contiguous slots;
+//   * i forces are summed per lane in FP32 and flushed every FLUSH entries into
+//     the warp's 64-bit fixed-point sums in shared memory, which are added to
+//     the slot accumulators once at the end.
+// Integer addition makes every sum independent of the order of the atomics, so
+// results stay bit-reproducible.  EN adds the LJ and Coulomb energies, VIR the
+// diagonal virial (each pair once).
 template <typename T, bool EN, bool VIR, bool SAME>
 __device__ __forceinline__ void pair_body(
     int bx, int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
@@ -816,6 +825,7 @@ __device__ __forceinline__ void pair_body(
     float2 *s_ljb = s_lja + k.ntypes * k.ntypes;
 
     __shared__ double s_sh[27 * 3];
+    __shared__ long long s_fi[8][3 * CL];  // per warp: i-force sums [component][i atom]
     // FP32x2 path: lj2 and lj4 enter the packed FMAs as addends, stored negated
     constexpr bool PACK = sizeof(T) == 4;
     for (int t = threadIdx.x; t < k.ntypes * k.ntypes; t += blockDim.x) {
@@ -833,29 +843,29 @@ __device__ __forceinline__ void pair_body(
         s_sh[im * 3 + 1] = (double)((im / 3) % 3 - 1) * L;
         s_sh[im * 3 + 2] = (double)(im / 9 - 1) * L;
     }
-    __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int li = lane & 7, lj = lane >> 3;
+    long long *fi = s_fi[threadIdx.x >> 5];
+    if (lane < 3 * CL) fi[lane] = 0;
+    __syncthreads();
+    const int jj = lane & 7, q = lane >> 3;
     const int icl = (bx * blockDim.x + threadIdx.x) >> 5;
     if (icl >= maxcl || icl >= ncl_dev[0]) return;
     const size_t stride = (size_t)maxcl * CL;
-    // this lane's share of the reduced j force: component jcomp of j atom jslot
-    const int jcomp = 2 * ((lane >> 1) & 1) + (lane & 1);
-    const int jslot = lj + 4 * ((lane >> 2) & 1);
-    unsigned long long *jdst = fslot + (size_t)(jcomp < 3 ? jcomp : 0) * stride;
-    const AtomRec ri = rec[icl * CL + li];
-    const T qiq = (T)k.coulpre * (T)ri.q;
-    const int ti = ri.type * k.ntypes;
+    // this lane's share of the reduced j force: component q (3 = none) of j atom jj
+    unsigned long long *jdst = fslot + (size_t)(q < 3 ? q : 0) * stride;
+    const AtomRec ri0 = rec[icl * CL + q], ri1 = rec[icl * CL + q + 4];
+    const T qiq0 = (T)k.coulpre * (T)ri0.q, qiq1 = (T)k.coulpre * (T)ri1.q;
+    const int ti0 = ri0.type * k.ntypes, ti1 = ri1.type * k.ntypes;
     const int n = jcount[icl];
     const int *row = jlist + (size_t)icl * jcap;
     const unsigned long long *mrow = jmask + (size_t)icl * jcap;
-    T ax = 0, ay = 0, az = 0;
+    // i-force partial sums: i atom q (x0..) and q + 4 (x1..)
+    T ax0 = 0, ay0 = 0, az0 = 0, ax1 = 0, ay1 = 0, az1 = 0;
     T a_lj = 0, a_c = 0, a_xx = 0, a_yy = 0, a_zz = 0;
-    // packed accumulators of the FP32x2 path (component per j half)
+    // packed accumulators of the FP32x2 path (component per i atom)
     const float2 z2 = make_float2(0.0f, 0.0f);
     float2 ax2 = z2, ay2 = z2, az2 = z2, alj2 = z2, ac2 = z2, axx2 = z2, ayy2 = z2, azz2 = z2;
-    const float2 qiq2 = make_float2((float)qiq, (float)qiq);
-    long long lx = 0, ly = 0, lz = 0;
+    const float2 qiq2 = make_float2((float)qiq0, (float)qiq1);
     double e_lj = 0.0, e_c = 0.0, vxx = 0.0, vyy = 0.0, vzz = 0.0;
     for (int base = 0; base < n; base += 32) {
         const int cnt = min(32, n - base);
@@ -866,35 +876,42 @@ __device__ __forceinline__ void pair_body(
             const unsigned long long mm = __shfl_sync(FULL, mym, e);
             const int jc = w & ((1 << IMG_SHIFT) - 1);
             const int img = w >> IMG_SHIFT;
-            const double xis = ri.x - s_sh[img * 3 + 0];
-            const double yis = ri.y - s_sh[img * 3 + 1];
-            const double zis = ri.z - s_sh[img * 3 + 2];
-            T v[6] = {0, 0, 0, 0, 0, 0};
+            const AtomRec rj = rec[jc * CL + jj];
+            // j position in the image the entry pairs with
+            const double xj = rj.x + s_sh[img * 3 + 0];
+            const double yj = rj.y + s_sh[img * 3 + 1];
+            const double zj = rj.z + s_sh[img * 3 + 2];
+            T v0 = 0, v1 = 0, v2 = 0;  // the entry's force on j atom jj (negated)
             const unsigned m0 = (unsigned)mm, m1 = (unsigned)(mm >> 32);
             if (PACK && SOFIA_PAIR_HYBRID && (m0 == 0u || m1 == 0u)) {
-                // one j half without pairs in range: scalar evaluation of the other
-                const int h = m0 ? 0 : 1;
-                const AtomRec rj = rec[jc * CL + lj + 4 * h];
-                const float dx = (float)(xis - rj.x);
-                const float dy = (float)(yis - rj.y);
-                const float dz = (float)(zis - rj.z);
+                // one i half without pairs in range: scalar evaluation of the other
+                // (a warp-uniform branch per half, so no selects of i data)
+                const bool h1 = m0 == 0u;
+                const double xi = h1 ? ri1.x : ri0.x, yi = h1 ? ri1.y : ri0.y,
+                             zi = h1 ? ri1.z : ri0.z;
+                const float dx = (float)(xi - xj);
+                const float dy = (float)(yi - yj);
+                const float dz = (float)(zi - zj);
+                const int ti = h1 ? ti1 : ti0;
                 const float2 la = s_lja[ti + rj.type];
                 const float2 lb = EN ? s_ljb[ti + rj.type] : make_float2(0.0f, 0.0f);
-                const float4 l = make_float4(la.x, la.y, lb.x, lb.y);
                 float elj = 0.0f, ec = 0.0f;
                 const float fs = PairMath<float>::template eval<EN, SAME>(
-                    dx, dy, dz, mulr((float)qiq, rj.q), make_float4(l.x, -l.y, l.z, -l.w),
-                    ((m0 | m1) >> lane) & 1u, k, elj, ec);
+                    dx, dy, dz, mulr(h1 ? qiq2.y : qiq2.x, rj.q),
+                    make_float4(la.x, -la.y, lb.x, -lb.y), ((m0 | m1) >> lane) & 1u, k, elj, ec);
                 const float px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
-                ax2.x = addr(ax2.x, px);
-                ay2.x = addr(ay2.x, py);
-                az2.x = addr(az2.x, pz);
-                v[0] = h ? 0.0f : px;
-                v[1] = h ? 0.0f : py;
-                v[2] = h ? 0.0f : pz;
-                v[3] = h ? px : 0.0f;
-                v[4] = h ? py : 0.0f;
-                v[5] = h ? pz : 0.0f;
+                if (h1) {
+                    ax2.y = addr(ax2.y, px);
+                    ay2.y = addr(ay2.y, py);
+                    az2.y = addr(az2.y, pz);
+                } else {
+                    ax2.x = addr(ax2.x, px);
+                    ay2.x = addr(ay2.x, py);
+                    az2.x = addr(az2.x, pz);
+                }
+                v0 = px;
+                v1 = py;
+                v2 = pz;
                 if (EN) {
                     alj2.x = addr(alj2.x, elj);
                     ac2.x = addr(ac2.x, ec);
@@ -905,30 +922,26 @@ __device__ __forceinline__ void pair_body(
                     azz2.x = fmar(dz, pz, azz2.x);
                 }
             } else if constexpr (PACK) {
-                // both j halves at once; a half without pairs in range is computed
+                // both i halves at once; a half without pairs in range is computed
                 // and masked (the packed instructions cost the same for one or two)
-                const AtomRec r0 = rec[jc * CL + lj], r1 = rec[jc * CL + lj + 4];
-                const float2 dx = make_float2((float)(xis - r0.x), (float)(xis - r1.x));
-                const float2 dy = make_float2((float)(yis - r0.y), (float)(yis - r1.y));
-                const float2 dz = make_float2((float)(zis - r0.z), (float)(zis - r1.z));
-                const float2 qq = mul2(qiq2, make_float2(r0.q, r1.q));
-                const bool on0 = ((unsigned)mm >> lane) & 1u;
-                const bool on1 = ((unsigned)(mm >> 32) >> lane) & 1u;
+                const float2 dx = make_float2((float)(ri0.x - xj), (float)(ri1.x - xj));
+                const float2 dy = make_float2((float)(ri0.y - yj), (float)(ri1.y - yj));
+                const float2 dz = make_float2((float)(ri0.z - zj), (float)(ri1.z - zj));
+                const float2 qq = mul2(qiq2, make_float2(rj.q, rj.q));
+                const bool on0 = (m0 >> lane) & 1u;
+                const bool on1 = (m1 >> lane) & 1u;
                 float2 elj = z2, ec = z2;
                 const float2 fs = PairMath2::template eval<EN, SAME>(
-                    dx, dy, dz, qq, s_lja[ti + r0.type], s_lja[ti + r1.type],
-                    EN ? s_ljb[ti + r0.type] : z2, EN ? s_ljb[ti + r1.type] : z2, on0, on1, k,
+                    dx, dy, dz, qq, s_lja[ti0 + rj.type], s_lja[ti1 + rj.type],
+                    EN ? s_ljb[ti0 + rj.type] : z2, EN ? s_ljb[ti1 + rj.type] : z2, on0, on1, k,
                     elj, ec);
                 const float2 px = mul2(dx, fs), py = mul2(dy, fs), pz = mul2(dz, fs);
                 ax2 = add2(ax2, px);
                 ay2 = add2(ay2, py);
                 az2 = add2(az2, pz);
-                v[0] = px.x;
-                v[1] = py.x;
-                v[2] = pz.x;
-                v[3] = px.y;
-                v[4] = py.y;
-                v[5] = pz.y;
+                v0 = addr(px.x, px.y);
+                v1 = addr(py.x, py.y);
+                v2 = addr(pz.x, pz.y);
                 if (EN) {
                     alj2 = add2(alj2, elj);
                     ac2 = add2(ac2, ec);
@@ -938,48 +951,52 @@ __device__ __forceinline__ void pair_body(
                     ayy2 = fma2(dy, py, ayy2);
                     azz2 = fma2(dz, pz, azz2);
                 }
-            } else
+            } else {
+                // FP64 twin: the two i halves one after the other; a half with no
+                // pair in range is skipped by the whole warp
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                // pruned mask, lane layout: bit h*32 + lane; a j half with no pair in
-                // range is skipped by the whole warp
-                const unsigned mh = (unsigned)(mm >> (32 * h));
-                if (mh == 0u) continue;
-                const int jj = lj + 4 * h;
-                const AtomRec rj = rec[jc * CL + jj];
-                const T dx = (T)(xis - rj.x);
-                const T dy = (T)(yis - rj.y);
-                const T dz = (T)(zis - rj.z);
-                const bool on = (mh >> lane) & 1u;
-                const float4 ljp = s_lj[ti + rj.type];
-                T elj = 0, ec = 0;
-                const T fs = PairMath<T>::template eval<EN, SAME>(dx, dy, dz, mulr(qiq, (T)rj.q),
-                                                                  ljp, on, k, elj, ec);
-                const T px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
-                ax = addr(ax, px);
-                ay = addr(ay, py);
-                az = addr(az, pz);
-                v[3 * h + 0] = px;
-                v[3 * h + 1] = py;
-                v[3 * h + 2] = pz;
-                if (EN) {
-                    a_lj = addr(a_lj, elj);
-                    a_c = addr(a_c, ec);
-                }
-                if (VIR) {
-                    a_xx = fmar(dx, px, a_xx);
-                    a_yy = fmar(dy, py, a_yy);
-                    a_zz = fmar(dz, pz, a_zz);
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned mh = h ? m1 : m0;
+                    if (mh == 0u) continue;
+                    const AtomRec &ri = h ? ri1 : ri0;
+                    const T dx = (T)(ri.x - xj);
+                    const T dy = (T)(ri.y - yj);
+                    const T dz = (T)(ri.z - zj);
+                    const bool on = (mh >> lane) & 1u;
+                    const float4 ljp = s_lj[(h ? ti1 : ti0) + rj.type];
+                    T elj = 0, ec = 0;
+                    const T fs = PairMath<T>::template eval<EN, SAME>(
+                        dx, dy, dz, mulr(h ? qiq1 : qiq0, (T)rj.q), ljp, on, k, elj, ec);
+                    const T px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
+                    if (h) {
+                        ax1 = addr(ax1, px);
+                        ay1 = addr(ay1, py);
+                        az1 = addr(az1, pz);
+                    } else {
+                        ax0 = addr(ax0, px);
+                        ay0 = addr(ay0, py);
+                        az0 = addr(az0, pz);
+                    }
+                    v0 = addr(v0, px);
+                    v1 = addr(v1, py);
+                    v2 = addr(v2, pz);
+                    if (EN) {
+                        a_lj = addr(a_lj, elj);
+                        a_c = addr(a_c, ec);
+                    }
+                    if (VIR) {
+                        a_xx = fmar(dx, px, a_xx);
+                        a_yy = fmar(dy, py, a_yy);
+                        a_zz = fmar(dz, pz, a_zz);
+                    }
                 }
             }
-            const T fj = reduce_scatter_j<T>(v, lane);
-            if (jcomp < 3 && fj != (T)0)
-                atomicAdd(jdst + jc * CL + jslot, (unsigned long long)(-to_fix<T>(fj)));
+            const T fj = reduce_j4<T>(v0, v1, v2, lane);
+            if (q < 3 && fj != (T)0)
+                atomicAdd(jdst + jc * CL + jj, (unsigned long long)(-to_fix<T>(fj)));
             if (((base + e) & (FLUSH - 1)) == FLUSH - 1) {
                 if constexpr (PACK) {
-                    ax = ax2.x + ax2.y;
-                    ay = ay2.x + ay2.y;
-                    az = az2.x + az2.y;
+                    flush_i<float>(fi, q, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
                     ax2 = ay2 = az2 = z2;
                     if (EN) {
                         e_lj += (double)alj2.x + (double)alj2.y;
@@ -992,29 +1009,26 @@ __device__ __forceinline__ void pair_body(
                         vzz += (double)azz2.x + (double)azz2.y;
                         axx2 = ayy2 = azz2 = z2;
                     }
-                }
-                lx += to_fix<T>(ax);
-                ly += to_fix<T>(ay);
-                lz += to_fix<T>(az);
-                ax = ay = az = 0;
-                if (EN) {
-                    e_lj += (double)a_lj;
-                    e_c += (double)a_c;
-                    a_lj = a_c = 0;
-                }
-                if (VIR) {
-                    vxx += (double)a_xx;
-                    vyy += (double)a_yy;
-                    vzz += (double)a_zz;
-                    a_xx = a_yy = a_zz = 0;
+                } else {
+                    flush_i<T>(fi, q, ax0, ay0, az0, ax1, ay1, az1);
+                    ax0 = ay0 = az0 = ax1 = ay1 = az1 = 0;
+                    if (EN) {
+                        e_lj += (double)a_lj;
+                        e_c += (double)a_c;
+                        a_lj = a_c = 0;
+                    }
+                    if (VIR) {
+                        vxx += (double)a_xx;
+                        vyy += (double)a_yy;
+                        vzz += (double)a_zz;
+                        a_xx = a_yy = a_zz = 0;
+                    }
                 }
             }
         }
     }
     if constexpr (PACK) {
-        ax = ax2.x + ax2.y;
-        ay = ay2.x + ay2.y;
-        az = az2.x + az2.y;
+        flush_i<float>(fi, q, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
         if (EN) {
             e_lj += (double)alj2.x + (double)alj2.y;
             e_c += (double)ac2.x + (double)ac2.y;
@@ -1024,21 +1038,14 @@ __device__ __forceinline__ void pair_body(
             vyy += (double)ayy2.x + (double)ayy2.y;
             vzz += (double)azz2.x + (double)azz2.y;
         }
+    } else {
+        flush_i<T>(fi, q, ax0, ay0, az0, ax1, ay1, az1);
     }
-    lx += to_fix<T>(ax);
-    ly += to_fix<T>(ay);
-    lz += to_fix<T>(az);
-#pragma unroll
-    for (int off = 8; off <= 16; off <<= 1) {
-        lx += __shfl_xor_sync(FULL, lx, off);
-        ly += __shfl_xor_sync(FULL, ly, off);
-        lz += __shfl_xor_sync(FULL, lz, off);
-    }
-    if (lj == 0) {
-        const size_t si = (size_t)icl * CL + li;
-        if (lx) atomicAdd(fslot + si, (unsigned long long)lx);
-        if (ly) atomicAdd(fslot + stride + si, (unsigned long long)ly);
-        if (lz) atomicAdd(fslot + 2 * stride + si, (unsigned long long)lz);
+    __syncwarp();
+    if (lane < 3 * CL) {
+        const long long v = fi[lane];
+        if (v) atomicAdd(fslot + (size_t)(lane >> 3) * stride + (size_t)icl * CL + (lane & 7),
+                         (unsigned long long)v);
     }
     if (EN || VIR) {
         e_lj += (double)a_lj;
@@ -1127,23 +1134,12 @@ __global__ void k_unpack(int nslots, const int *__restrict__ ncl_dev,
     unpack_body(blockIdx.x, nslots, ncl_dev, slot_orig, fslot, fx, fy, fz, status, flag, cnt, lg, ffo);
 }
 
-// 8x8 bit-matrix transpose: bit (r*8 + c) -> bit (c*8 + r)  (three swap rounds).
-__device__ __forceinline__ unsigned long long transpose8(unsigned long long x) {
-    unsigned long long t;
-    t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
-    x = x ^ t ^ (t << 7);
-    t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
-    x = x ^ t ^ (t << 14);
-    t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
-    x = x ^ t ^ (t << 28);
-    return x;
-}
 
 // Dynamic pruning: keep the outer-list entries that have at least one unmasked
 // atom pair within r_in = rc + margin at the current positions, and replace
-// their pair mask by the in-range bits in the pair kernel's lane layout (bit
-// 8*jj + ii = pair (i atom ii, j atom jj), i.e. bit h*32 + lane for pair
-// (lane & 7, (lane >> 3) + 4h)).  Valid until an atom moves more than margin/2
+// their pair mask by the in-range bits (bit 8*ii + jj = pair (i atom ii, j atom
+// jj), the outer list's layout, which is also the pair kernel's lane layout:
+// bit h*32 + lane is the pair (i atom (lane >> 3) + 4h, j atom lane & 7)).  Valid until an atom moves more than margin/2
 // (checked like the rebuild trigger): a pair out of range now cannot come
 // within rc before the next prune.  One warp per i-cluster, one lane per list
 // entry: the i atoms sit in registers and every lane checks its entry's 64
@@ -1204,7 +1200,7 @@ __device__ __forceinline__ void prune_body(int bx,
         const bool active = e < n;
         const int w = active ? row[e] : 0;
         const unsigned long long m = active ? mrow[e] : 0ull;
-        unsigned lo = 0u, hi = 0u;  // in-range bits 8*jj + ii, jj < 4 and jj >= 4
+        unsigned lo = 0u, hi = 0u;  // in-range bits 8*ii + jj: i atoms 0-3 in lo, 4-7 in hi
         if (active) {
             const int jc = w & ((1 << IMG_SHIFT) - 1);
             const int img = w >> IMG_SHIFT;
@@ -1224,7 +1220,9 @@ __device__ __forceinline__ void prune_body(int bx,
                 for (int hh = 0; hh < 2; ++hh) {
                     const float4 jx = __ldg(&cj[hh]), jy = __ldg(&cj[2 + hh]),
                                  jz = __ldg(&cj[4 + hh]);
-                    unsigned acc = 0u;  // bits 8*q + ii of j atom 4*hh + q
+                    // j atom jj = 4*hh + q: bit 8*(ii & 3) + jj of lo (i atoms 0-3)
+                    // or hi (4-7)
+                    const int sh = 4 * hh;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         // -(x_j + shift): adding it rounds exactly like x_i - (x_j + shift)
@@ -1234,23 +1232,22 @@ __device__ __forceinline__ void prune_body(int bx,
                                      nz2 = make_float2(nz, nz);
 #pragma unroll
                         for (int pp = 0; pp < CL / 2; ++pp) {
+                            // i atoms 2pp (component x) and 2pp + 1 (component y)
                             const float2 dx = add2(xi[pp], nx2), dy = add2(yi[pp], ny2),
                                          dz = add2(zi[pp], nz2);
                             const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
-                            const unsigned in =
-                                (r2.x < rin2 ? 1u : 0u) | (r2.y < rin2 ? 2u : 0u);
-                            acc |= in << (8 * q + 2 * pp);
+                            const unsigned in = ((r2.x < rin2 ? 1u : 0u) |
+                                                 (r2.y < rin2 ? (1u << 8) : 0u)) << sh;
+                            if (pp < 2)
+                                lo |= in << (16 * pp + q);
+                            else
+                                hi |= in << (16 * (pp - 2) + q);
                         }
                     }
-                    if (hh == 0)
-                        lo = acc;
-                    else
-                        hi = acc;
                 }
             }
         }
-        const unsigned long long newm =
-            (((unsigned long long)hi << 32) | lo) & transpose8(m);
+        const unsigned long long newm = (((unsigned long long)hi << 32) | lo) & m;
         const bool keep = newm != 0ull;
         const unsigned kb = __ballot_sync(FULL, keep);
         if (keep) {
@@ -1951,8 +1948,19 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
                              &s->ljtab, &s->col_count, &s->col_start, &s->col_fill, &s->col_atoms,
                              &s->col_key, &s->cl_start, &s->slot_orig, &s->rec, &s->bb, &s->jlist,
                              &s->jmask, &s->jcount, &s->nclusters, &s->status_local, &s->energy,
-                             &s->red, &s->flag, &s->stage_pos, &s->stage_ff};
+                             &s->red, &s->flag, &s->stage_pos, &s->stage_ff, &s->cl_pos,
+                             &s->cl_gid, &s->ptta};
     for (auto *b : bufs) b->release();
+    // MD state (md_setup)
+    sofia::Md &md = s->md;
+    for (auto &g : md.graph)
+        if (g) cudaGraphExecDestroy(g);
+    sofia::DevBuf *mbufs[] = {&md.bonds, &md.bcoef, &md.angles, &md.acoef, &md.diheds,
+                              &md.dcoef, &md.lj14, &md.shake, &md.sbond, &md.impros,
+                              &md.icoef, &md.eterm, &md.ered, &md.bpart, &md.step_dev};
+    for (auto *b : mbufs) b->release();
+    for (auto &b : md.snap) b.release();
+    for (auto &b : md.keep) b.release();
     for (int d = 0; d < 3; ++d) {
         s->x[d].release();
         s->v[d].release();
@@ -2180,9 +2188,8 @@ extern "C" int sofia_system_timers(sofia_system *ss, int enable, double *timers)
 
 // The cluster-pair list expanded into atom pairs on the host (a diagnostic
 // query, not a hot path): which = 0 the outer list (rc + skin, made at the
-// last build, masks bit 8*ii + jj), 1 the pruned list (rc + margin, made at the
-// last prune, masks in the pair kernel's lane layout: bit 32*h + lane is i atom
-// lane & 7 with j atom (lane >> 3) + 4*h).
+// last build), 1 the pruned list (rc + margin, made at the last prune); both
+// masks hold pair (i atom ii, j atom jj) at bit 8*ii + jj.
 extern "C" int sofia_system_list_pairs(sofia_system *ss, int which, int64_t capacity,
                                        int32_t *pairs, int64_t *npairs, double *xlist) {
     if (!ss || !npairs || (which != 0 && which != 1) || capacity < 0 || (capacity > 0 && !pairs))
@@ -2223,15 +2230,7 @@ extern "C" int sofia_system_list_pairs(sofia_system *ss, int which, int64_t capa
             while (m) {
                 const int b = __builtin_ctzll(m);
                 m &= m - 1;
-                int ii, jj;
-                if (which == 0) {
-                    ii = b >> 3;
-                    jj = b & 7;
-                } else {
-                    const int lane = b & 31;
-                    ii = lane & 7;
-                    jj = (lane >> 3) + 4 * (b >> 5);
-                }
+                const int ii = b >> 3, jj = b & 7;
                 const int a = orig[(size_t)ic * sofia::CL + ii];
                 const int o = orig[(size_t)jc * sofia::CL + jj];
                 if (a < 0 || o < 0)
@@ -2325,9 +2324,9 @@ __global__ void k_bbox_b(const BatchDev *__restrict__ tab) {
     SOFIA_BATCH_END
 }
 
-__global__ void __launch_bounds__(256) k_search_b(const BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(256) k_search_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_W256)
+    SOFIA_BATCH_QUEUE_LOOP(BK_W256, BC_SEARCH)
     SearchArgs a;
     a.cond = d.flag;
     a.cmask = 1;
@@ -2358,9 +2357,9 @@ __global__ void __launch_bounds__(256) k_search_b(const BatchDev *__restrict__ t
     SOFIA_BATCH_END
 }
 
-__global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune_b(const BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_W256)
+    SOFIA_BATCH_QUEUE_LOOP(BK_W256, BC_PRUNE)
     prune_body(lb, d.flag, 3, d.maxcl, d.ncl, d.recf, d.jlist, d.jmask, d.jcount, d.jcap,
                (float)d.L, d.rin2, d.rfar2, d.bb, d.ilist, d.imask, d.icount, d.slot_orig, d.x,
                d.y, d.z, d.px, d.py, d.pz);
@@ -2370,9 +2369,9 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune_b(const BatchDe
 
 template <typename T, bool EN, bool VIR, bool SAME>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2)
-    k_pair_b(const BatchDev *__restrict__ tab, PairConst k) {
+    k_pair_b(BatchDev *__restrict__ tab, PairConst k) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_W256)
+    SOFIA_BATCH_QUEUE_LOOP(BK_W256, BC_PAIR)
     pair_body<T, EN, VIR, SAME>(lb, d.maxcl, d.ncl, d.rec, d.ilist, d.imask, d.icount, d.jcap,
                                 d.ljtab, k, d.L, d.fslot, d.energy);
     __syncthreads();
@@ -2483,7 +2482,7 @@ void repdev_fill_pair(const Sys *s, RepDev *d) {
     d->red = s->red.as<double>();
 }
 
-void batch_pair_path(const BatchDev *tab, const Sys *s0, int precision, bool energy,
+void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
                      cudaStream_t st, int nsm) {
     const int g256 = nsm * 8, g128 = nsm * 16;
     launch_pdl(k_wrap_bin_b, g256, 256, 0, st, tab);

@@ -88,6 +88,8 @@ struct Sys {
     DevBuf flag;                        // rebuild flag (int)
     DevBuf stage_pos, stage_ff;
     DevBuf cl_pos, cl_gid;              // resident positions as real*4 ainfo records, ids 1..n (cluster analysis)
+    DevBuf ptta;                        // resident ptta_full of the cluster analysis
+    int ptta_atoms = 0;                 // glycine atoms ptta holds (0 = not yet set)
     // pruned inner list (rc + margin) and the positions it was pruned at
     DevBuf ilist, imask, icount, xprn[3], part, dcount;
     double margin = 0.6;
@@ -199,11 +201,49 @@ struct RepDev {
     const double *job_in[MD_NJOB];
 };
 
+// Work-queue counters of the dynamically scheduled batched kernels (one per
+// launch of a step; the step's first kernel clears them).
+enum BatchCounter { BC_SEARCH = 1, BC_PRUNE, BC_PAIR, BC_BONDED, BC_SHAKE, BC_N = 8 };
+
 struct BatchDev {
     int nrep;
+    int ctr[BC_N];
     int pre[BK_N][MAXREP + 1];
     RepDev rep[MAXREP];
 };
+
+// Dynamically scheduled loop over the virtual blocks of kind KIND: each block
+// takes the next virtual block from the work-queue counter CTR (an atomic add
+// by thread 0), so blocks that finish early take more work.  Inside, d is the
+// owning replica's entry and lb the block index within that replica.
+#ifndef SOFIA_BATCH_DYNAMIC
+#define SOFIA_BATCH_DYNAMIC 1
+#endif
+#if SOFIA_BATCH_DYNAMIC
+#define SOFIA_BATCH_QUEUE_LOOP(KIND, CTR)                                        \
+    __shared__ int s_vb_;                                                        \
+    for (;;) {                                                                   \
+        if (threadIdx.x == 0) s_vb_ = atomicAdd(&tab->ctr[CTR], 1);              \
+        __syncthreads();                                                         \
+        const int vb = s_vb_;                                                    \
+        __syncthreads();                                                         \
+        /* re-read each round: nothing of the loop stays live across the body */ \
+        const int nrep_ = *reinterpret_cast<const volatile int *>(&tab->nrep);   \
+        const int *pre_ = tab->pre[KIND];                                        \
+        if (vb >= pre_[nrep_]) break;                                            \
+        const int r_ = batch_rep(pre_, nrep_, vb);                               \
+        const RepDev &d = tab->rep[r_];                                          \
+        const int lb = vb - pre_[r_];
+#else
+#define SOFIA_BATCH_QUEUE_LOOP(KIND, CTR)                                        \
+    for (int vb = blockIdx.x;; vb += gridDim.x) {                                \
+        const int nrep_ = tab->nrep;                                             \
+        const int *pre_ = tab->pre[KIND];                                        \
+        if (vb >= pre_[nrep_]) break;                                            \
+        const int r_ = batch_rep(pre_, nrep_, vb);                               \
+        const RepDev &d = tab->rep[r_];                                          \
+        const int lb = vb - pre_[r_];
+#endif
 
 // Replica of virtual block vb: the last r with pre[r] <= vb.
 __device__ __forceinline__ int batch_rep(const int *__restrict__ pre, int nrep, int vb) {
@@ -225,7 +265,7 @@ void repdev_fill_pair(const Sys *s, RepDev *d);
 // Langevin force, and (energy) the pair-energy sums.  All replicas share the
 // pair constants k (all but the box) and the precision.
 // nsm: multiprocessors of the device (the grid-stride launches are sized from it).
-void batch_pair_path(const BatchDev *tab, const Sys *s0, int precision, bool energy,
+void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
                      cudaStream_t st, int nsm);
 // The pair constants a captured batch graph holds (everything but the box).
 struct PairKey {

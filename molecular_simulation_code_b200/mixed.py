@@ -171,6 +171,24 @@ class System:
             self.ctx.check(rc)
             return pairs[:cnt.value], xl
 
+    def greatest_cluster(self, n_gly: int, mrcut: float, denscut: float, densmin: int,
+                         greatest: int = 0, ptta=None, atoms_per_gly: int = 10):
+        """get_greatestCluster on the resident positions (no host copy of them).
+        ptta (n_gly*atoms_per_gly, 3) float64 is in/out like the module array; None
+        uses the system's device copy.  Returns (size, greatest_belongsto)."""
+        g = C.c_int32(greatest)
+        size = C.c_int32(0)
+        self.ctx.check(self.ctx._lib.sofia_system_greatest_cluster(
+            self.handle, int(n_gly), int(atoms_per_gly), float(mrcut), float(denscut),
+            int(densmin), ptr(ptta), C.byref(g), C.byref(size)))
+        return int(size.value), int(g.value)
+
+    def device_bytes(self) -> int:
+        """Device memory this system holds now."""
+        b = C.c_int64()
+        self.ctx.check(self.ctx._lib.sofia_system_device_bytes(self.handle, C.byref(b)))
+        return int(b.value)
+
     def snapshot(self):
         """Device copy of x, v and the thermostat step (nuc_move's save)."""
         self.ctx.check(self.ctx._lib.sofia_system_snapshot(self.handle))

@@ -16,6 +16,7 @@ reference's offload transfers) or CUDA torch tensors (used in place).
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import weakref
 import math
@@ -43,6 +44,22 @@ def ptr(a):
     raise TypeError(f"unsupported array type {type(a)}")
 
 
+_LIVE = weakref.WeakSet()
+
+
+def _close_all():
+    """At interpreter exit, close every live context (its systems and batches first)
+    while the CUDA runtime is still up, whatever the caller left open."""
+    for c in list(_LIVE):
+        try:
+            c.close()
+        except Exception:
+            pass
+
+
+atexit.register(_close_all)
+
+
 class Context:
     """One ``sofia_nb_ctx`` (CUDA stream + device buffers) on one GPU."""
 
@@ -57,6 +74,7 @@ class Context:
         # systems and batches created on this context hold its stream: they are
         # destroyed before it, whatever order the garbage collector picks
         self._children = weakref.WeakSet()
+        _LIVE.add(self)
 
     def adopt(self, obj):
         """Register an object whose ``close()`` must run before this context's."""

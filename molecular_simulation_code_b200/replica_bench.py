@@ -5,9 +5,10 @@ batch:  64 seeded replicas, N ~ U[3,000, 30,000] atoms, glycine 5-20 % of
         launch per step for all replicas); prune margin autotuned per size
         class; mixed and FP64 atom-steps/s.
 serve:  Poisson request stream (default 200 requests/s), systems of
-        N ~ U[2,000, 60,000] atoms, U[500, 5,000] steps times --steps-scale,
-        up to 64 concurrent replicas, largest-cluster analysis at the end of
-        every segment; p50/p99 latency and replica-steps/s, mixed and FP64.
+        N ~ U[2,000, 60,000] atoms, U[500, 5,000] steps (times --steps-scale),
+        every 4th with a crystalline glycine nucleus, up to 64 concurrent
+        replicas, largest-cluster analysis on the device at the end of every
+        segment; p50/p99 segment latency and replica-steps/s, mixed and FP64.
 
 Prints one JSON line per mode:
     python -m molecular_simulation_code_b200.replica_bench --mode batch|serve
@@ -89,7 +90,7 @@ def bench_serve(args):
 
     rng = np.random.default_rng(args.seed)
     systems = make_replicas(args.requests, seed=args.seed + 1, n_min=2000, n_max=60000,
-                            processes=args.procs)
+                            processes=args.procs, nucleus_every=args.nucleus_every)
     arrivals = poisson_arrivals(args.rate, args.requests, seed=args.seed + 2)
     steps = (rng.integers(500, 5001, size=args.requests) * args.steps_scale).astype(int)
     steps = np.maximum(steps // args.chunk, 1) * args.chunk
@@ -106,7 +107,15 @@ def bench_serve(args):
         per_step = np.array([r.service / r.nsteps for r in srv.results])
         stats["per_step_service_p50_ms"] = float(np.percentile(per_step, 50) * 1e3)
         stats["per_step_service_p99_ms"] = float(np.percentile(per_step, 99) * 1e3)
-        stats["cluster_sizes"] = sorted(int(r.cluster_size) for r in srv.results)[-5:]
+        stats["segment_latency_p99_over_p50"] = (stats["segment_latency_p99_s"] /
+                                                 stats["segment_latency_p50_s"])
+        seeded = [r for r in srv.results if args.nucleus_every and r.rid % args.nucleus_every == 0]
+        stats["cluster_sizes_seeded"] = sorted(int(r.cluster_size) for r in seeded)
+        stats["cluster_sizes_top5_other"] = sorted(int(r.cluster_size) for r in srv.results
+                                                   if r not in seeded)[-5:]
+        stats["batch_graph_captures"] = srv.recaptures
+        stats["cluster_criterion"] = {"mrcut_A": srv.mrcut, "denscut_A": srv.denscut,
+                                      "densmin": srv.densmin}
         out[name] = stats
         srv.close()
     out["mixed_over_fp64_replica_steps"] = (out["mixed"]["replica_steps_per_s"] /
@@ -123,8 +132,10 @@ def main(argv=None):
     ap.add_argument("--tune", action="store_true")
     ap.add_argument("--requests", type=int, default=128)
     ap.add_argument("--rate", type=float, default=200.0)
-    ap.add_argument("--steps-scale", type=float, default=0.2)
-    ap.add_argument("--chunk", type=int, default=50)
+    ap.add_argument("--steps-scale", type=float, default=1.0)
+    ap.add_argument("--nucleus-every", type=int, default=4,
+                    help="every k-th request starts with a crystalline glycine nucleus")
+    ap.add_argument("--chunk", type=int, default=100)
     ap.add_argument("--max-active", type=int, default=64)
     ap.add_argument("--budget-gb", type=float, default=64.0)
     ap.add_argument("--seed", type=int, default=5000)

@@ -8,15 +8,22 @@ runs many such segments at once on one GPU:
 * requests (a seeded glycine/water system, a step count, optionally the id
   of an earlier request to continue) queue FIFO;
 * admission: up to ``max_active`` replicas run at once, and a request is
-  admitted only while the estimated device memory of everything resident
-  (running + parked) stays within ``hbm_budget`` bytes; parked states are
-  evicted least-recently-used when room is needed;
-* every chunk of ``chunk_steps`` steps advances all running replicas with one
-  graph launch per step (``Batch``); requests that arrived meanwhile are
-  admitted at the next chunk boundary (continuous batching);
-* a finished segment ends with the largest-cluster analysis on the device;
-  its state (positions, velocities, neighbour list, RNG step counter) stays
-  resident so a continuation request resumes it without a host round trip.
+  admitted only while the device memory of everything resident (running +
+  parked) stays within ``hbm_budget`` bytes.  Resident systems count what they
+  actually hold (``System.device_bytes``, which grows with their lists); a new
+  request is charged the largest bytes-per-atom seen so far until it exists.
+  Parked states are evicted least-recently-used when room is needed;
+* all running replicas advance together in one ``Batch`` (every kernel of a
+  step once for all of them, captured segment graphs); requests that arrive
+  meanwhile join at the next chunk boundary and finished ones leave, by
+  changing the batch's members without a graph recapture (continuous
+  batching);
+* a new replica's damped warm-in from its lattice start runs inside the batch
+  (1 fs steps, strong friction) instead of blocking the running replicas;
+* a finished segment ends with the largest-cluster analysis on the device-
+  resident positions (no host copy of them); its state (positions,
+  velocities, neighbour list, RNG step counter, the analysis's reference
+  positions) stays resident so a continuation request resumes it.
 
 Results do not depend on what else is in the batch (replicas never exchange
 data and every force sum is in fixed point), which ``tests`` check.
@@ -31,10 +38,13 @@ import numpy as np
 
 from . import mixed as M
 from .batch import Batch, Tuner, set_margin
-from .nonbond import Context, get_greatest_cluster
+from .nonbond import Context
 
-BYTES_PER_ATOM = 1200      # resident state + lists + records, measured order of magnitude
-FIXED_BYTES = 8 << 20      # per-replica constant overhead (contexts, staging, reductions)
+BYTES_PER_ATOM = 1200      # charge per atom of a request before any system exists
+FIXED_BYTES = 8 << 20      # per-replica constant overhead (context, staging, reductions)
+# largest-cluster criterion of the reference's run input (mrcut, denscut, densmin):
+# input_files/input:41
+REFERENCE_CLUSTER = (9.0, 6.0, 11)
 
 
 @dataclasses.dataclass
@@ -59,6 +69,7 @@ class Result:
 
     @property
     def latency(self) -> float:
+        """Segment latency: arrival to the end of the segment's cluster analysis."""
         return self.finished - self.arrival
 
     @property
@@ -67,20 +78,23 @@ class Result:
 
 
 class _Replica:
-    def __init__(self, req: Request, ctx: Context, system: M.System, now: float):
+    def __init__(self, req: Request, ctx: Context, system: M.System, now: float, warm: int):
         self.req = req
         self.ctx = ctx
         self.system = system
+        self.warm = warm            # warm-in steps left (run before the segment's steps)
         self.remaining = req.nsteps
         self.admitted = now
-        s = req.sysdata
-        self.ptta = s.xyz[:10 * s.n_gly].astype(np.float64).copy()
         self.greatest = 0
         self.last_used = now
+        self.bytes = system.device_bytes()
+
+    def to_event(self) -> int:
+        return self.warm if self.warm > 0 else self.remaining
 
 
-def estimate_bytes(n_atoms: int) -> int:
-    return FIXED_BYTES + BYTES_PER_ATOM * int(n_atoms)
+def estimate_bytes(n_atoms: int, bytes_per_atom: float = BYTES_PER_ATOM) -> int:
+    return FIXED_BYTES + int(bytes_per_atom * int(n_atoms))
 
 
 class Server:
@@ -88,7 +102,7 @@ class Server:
                  chunk_steps: int = 100, precision: int = M.MIXED, tune: bool = False,
                  cut: float = 10.0, skin: float = 2.0, dt: float = 2.0,
                  temperature: float = 300.0, gamma: float = 0.001,
-                 cluster=(9.0, 5.0, 11), warm_in: int = 50):
+                 cluster=REFERENCE_CLUSTER, warm_in: int = 50, segment_graph: int = 50):
         self.device = device
         self.ctx = Context(device)
         self.max_active = max_active
@@ -99,6 +113,7 @@ class Server:
         self.temperature, self.gamma = temperature, gamma
         self.mrcut, self.denscut, self.densmin = cluster
         self.warm_in = warm_in
+        self.segment_graph = segment_graph
         self.tuner = Tuner() if tune else None
         self.queue: collections.deque[Request] = collections.deque()
         self.active: list[_Replica] = []
@@ -109,14 +124,16 @@ class Server:
         self.t0 = time.perf_counter()
         self.atom_steps = 0
         self.replica_steps = 0
+        self.bytes_per_atom = float(BYTES_PER_ATOM)
+        self.recaptures = 0
 
     # -- clock and memory -------------------------------------------------
     def now(self) -> float:
         return time.perf_counter() - self.t0
 
     def resident_bytes(self) -> int:
-        return sum(estimate_bytes(r.req.sysdata.np_atoms) for r in self.active) + \
-            sum(estimate_bytes(r.req.sysdata.np_atoms) for r in self.parked.values())
+        return sum(FIXED_BYTES + r.bytes for r in self.active) + \
+            sum(FIXED_BYTES + r.bytes for r in self.parked.values())
 
     # -- admission ----------------------------------------------------------
     def submit(self, req: Request):
@@ -131,13 +148,19 @@ class Server:
                                                 precision=self.precision))
         m.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
         if self.warm_in:
-            # damped warm-in from a lattice start (part of the request's service time)
+            # damped warm-in from a lattice start, run inside the batch (part of the
+            # request's service time)
             m.md_setup(s, dt=1.0, temperature=self.temperature, gamma=0.02,
                        seed=7 * (req.rid + 1))
-            m.md_run(self.warm_in)
-        m.md_setup(s, dt=self.dt, temperature=self.temperature, gamma=self.gamma,
+        else:
+            self._production(m, req)
+        rep = _Replica(req, ctx, m, self.now(), self.warm_in)
+        self.bytes_per_atom = max(self.bytes_per_atom, rep.bytes / s.np_atoms)
+        return rep
+
+    def _production(self, m: M.System, req: Request):
+        m.md_setup(req.sysdata, dt=self.dt, temperature=self.temperature, gamma=self.gamma,
                    seed=1000003 * (req.rid + 1))
-        return _Replica(req, ctx, m, self.now())
 
     def _admit(self):
         while self.queue and len(self.active) < self.max_active:
@@ -146,40 +169,58 @@ class Server:
                 rep = self.parked.pop(req.continues)
                 rep.req = dataclasses.replace(req, sysdata=rep.req.sysdata)
                 rep.remaining = req.nsteps
+                rep.warm = 0
                 rep.admitted = self.now()
                 self.queue.popleft()
                 self.active.append(rep)
                 continue
-            need = estimate_bytes(req.sysdata.np_atoms)
+            need = estimate_bytes(req.sysdata.np_atoms, self.bytes_per_atom)
             while self.resident_bytes() + need > self.hbm_budget and self.parked:
                 _, old = self.parked.popitem(last=False)  # evict least recently used
                 old.system.close()
                 old.ctx.close()
-            if self.resident_bytes() + need > self.hbm_budget:
-                break  # wait for running replicas to finish
+            if self.resident_bytes() + need > self.hbm_budget and self.active:
+                break  # wait for running replicas to finish (a lone request always runs)
             self.queue.popleft()
             self.active.append(self._new_replica(req))
 
     # -- one chunk ----------------------------------------------------------
+    def _sync_batch(self):
+        members = tuple(id(r) for r in self.active)
+        if members == self.batch_members:
+            return
+        systems = [r.system for r in self.active]
+        if self.batch is None:
+            self.batch = Batch(self.ctx, systems)
+            self.batch.set_segment(self.segment_graph)
+            self.recaptures += 1
+        else:
+            self.batch.set_systems(systems)
+        self.batch_members = members
+
     def step_chunk(self) -> int:
         self._admit()
         if not self.active:
             return 0
-        members = tuple(id(r) for r in self.active)
-        if members != self.batch_members:
-            if self.batch is not None:
-                self.batch.close()
-            self.batch = Batch(self.ctx, [r.system for r in self.active])
-            self.batch_members = members
-        k = min(self.chunk_steps, min(r.remaining for r in self.active))
-        want_e = any(r.remaining == k for r in self.active)
+        self._sync_batch()
+        k = min(self.chunk_steps, min(r.to_event() for r in self.active))
+        want_e = any(r.warm == 0 and r.remaining == k for r in self.active)
         energies = self.batch.run(k, energy_every=k if want_e else 0)
-        for r in self.active:
-            r.remaining -= k
+        finished = []
+        for i, r in enumerate(self.active):
+            r.bytes = r.system.device_bytes()  # lists may have grown
+            self.bytes_per_atom = max(self.bytes_per_atom, r.bytes / r.req.sysdata.np_atoms)
             self.atom_steps += k * r.req.sysdata.np_atoms
             self.replica_steps += k
-        done = [i for i, r in enumerate(self.active) if r.remaining == 0]
-        for i in reversed(done):
+            if r.warm > 0:
+                r.warm -= k
+                if r.warm == 0:
+                    self._production(r.system, r.req)
+                continue
+            r.remaining -= k
+            if r.remaining == 0:
+                finished.append(i)
+        for i in reversed(finished):
             r = self.active.pop(i)
             size = self._cluster(r)
             now = self.now()
@@ -187,6 +228,7 @@ class Server:
                                        r.req.sysdata.np_atoms, size,
                                        energies[i] if energies else None))
             r.last_used = now
+            r.bytes = r.system.device_bytes()
             self.parked[r.req.rid] = r
         return k
 
@@ -194,15 +236,8 @@ class Server:
         s = r.req.sysdata
         if s.n_gly == 0:
             return 0
-        x, _, _ = r.system.get_state()
-        L = float(s.box)
-        xw = np.mod(x, L).astype(np.float32)
-        xw[xw <= 0] += np.float32(L)
-        pos = s.position_aos()
-        pos[:, :3] = xw
-        gid = np.arange(1, s.np_atoms + 1, dtype=np.int32)
-        size, g, _, _ = get_greatest_cluster(r.ctx, pos, gid, s.n_gly, 10, s.box, self.mrcut,
-                                             self.denscut, self.densmin, r.ptta, r.greatest)
+        size, g = r.system.greatest_cluster(s.n_gly, self.mrcut, self.denscut, self.densmin,
+                                            greatest=r.greatest)
         r.greatest = g
         return size
 
@@ -242,6 +277,8 @@ def run_stream(server: Server, requests: list[Request]) -> dict:
     lat = np.array([r.latency for r in server.results])
     svc = np.array([r.service for r in server.results])
     return {"requests": len(server.results), "wall_s": wall,
+            "segment_latency_p50_s": float(np.percentile(lat, 50)),
+            "segment_latency_p99_s": float(np.percentile(lat, 99)),
             "latency_p50_s": float(np.percentile(lat, 50)),
             "latency_p99_s": float(np.percentile(lat, 99)),
             "service_p50_s": float(np.percentile(svc, 50)),

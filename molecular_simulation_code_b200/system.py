@@ -352,24 +352,60 @@ def _partner_lists(n_atoms: int, bonds: list[tuple[int, int]]):
     return p12, p13, p14
 
 
+def _nucleus_centres(k: int, spacing: float, L: float) -> np.ndarray:
+    """k points of an fcc lattice (nearest-neighbour distance ``spacing``) closest to
+    the box centre: a compact, crystal-like glycine nucleus."""
+    a = spacing * math.sqrt(2.0)
+    n = int(math.ceil((4.0 * k) ** (1.0 / 3.0))) + 2
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    g = np.arange(-n, n + 1)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pts = (cells[:, None, :] + basis[None, :, :]).reshape(-1, 3) * a
+    order = np.argsort(np.einsum("ij,ij->i", pts, pts), kind="stable")
+    return pts[order[:k]] + 0.5 * L
+
+
 def make_system(n_gly: int, n_wat: int, seed: int, *, jitter_a: float = 0.2,
-                density_gcc: float = 1.0, temperature: float = 300.0) -> SofiaSystem:
-    """Build a seeded glycine/water system: cubic lattice, random orientation, jitter."""
+                density_gcc: float = 1.0, temperature: float = 300.0, nucleus: int = 0,
+                nucleus_spacing: float = 5.5) -> SofiaSystem:
+    """Build a seeded glycine/water system: cubic lattice, random orientation, jitter.
+
+    ``nucleus`` > 0 places that many glycine molecules (the first ones) as a
+    compact fcc cluster with one common orientation at the box centre, centres
+    ``nucleus_spacing`` A apart, so that the largest-cluster analysis finds a
+    solid nucleus; the other molecules fill the lattice sites away from it."""
     rng = np.random.default_rng(seed)
     L = box_length(n_gly, n_wat, density_gcc)
     box = np.float32(L)
     n_mol = n_gly + n_wat
+    nuc = min(max(int(nucleus), 0), n_gly)
+    centres_nuc = _nucleus_centres(nuc, nucleus_spacing, L) if nuc else np.zeros((0, 3))
     m = int(math.ceil(n_mol ** (1.0 / 3.0) - 1e-9))
-    a = L / m
-    sites = rng.permutation(m ** 3)[:n_mol]
+    while True:
+        a = L / m
+        grid = np.arange(m ** 3)
+        cen = (np.stack([grid % m, (grid // m) % m, grid // (m * m)], -1) + 0.5) * a
+        if nuc:
+            d = cen[:, None, :] - centres_nuc[None, :, :]
+            d -= L * np.round(d / L)
+            free = (np.einsum("ijk,ijk->ij", d, d) > (0.75 * nucleus_spacing) ** 2).all(axis=1)
+        else:
+            free = np.ones(m ** 3, bool)
+        if free.sum() >= n_mol - nuc:
+            break
+        m += 1
+    sites = rng.permutation(np.nonzero(free)[0])[:n_mol - nuc]
     # glycine molecules take the first n_gly of the permuted sites
     gt = glycine_template()
     wt = water_template()
     coords = []
+    rot_nuc = _rotation(rng)
     for mol in range(n_mol):
-        s = int(sites[mol])
-        ix, iy, iz = s % m, (s // m) % m, s // (m * m)
-        centre = (np.array([ix, iy, iz], dtype=np.float64) + 0.5) * a
+        if mol < nuc:
+            coords.append(gt @ rot_nuc.T + centres_nuc[mol])
+            continue
+        s = int(sites[mol - nuc])
+        centre = cen[s]
         rot = _rotation(rng)
         tmpl = gt if mol < n_gly else wt
         pts = tmpl @ rot.T + centre
@@ -489,11 +525,11 @@ def make_workload(name: str, seed: int = 0) -> SofiaSystem:
 
 
 def random_replica(rng: np.random.Generator, n_min: int, n_max: int, gly_frac=(0.05, 0.20),
-                   seed: int = 0) -> SofiaSystem:
+                   seed: int = 0, nucleus: int = 0) -> SofiaSystem:
     """A replica of N ~ U[n_min, n_max] atoms with glycine a seeded fraction of molecules."""
     n_target = int(rng.integers(n_min, n_max + 1))
     f = float(rng.uniform(*gly_frac))
     # N = 10 g + 3 w, g = f (g + w)  =>  g = f N / (10 f + 3 (1 - f))
     n_gly = max(1, int(round(f * n_target / (10 * f + 3 * (1 - f)))))
     n_wat = max(1, int(round((n_target - 10 * n_gly) / 3)))
-    return make_system(n_gly, n_wat, seed)
+    return make_system(n_gly, n_wat, seed, nucleus=min(nucleus, n_gly))

@@ -138,15 +138,18 @@ def nve_drift(M, ctx, s, x, v, *, dt, precision, rattle, lj_shift, shake_tol, ps
                   rattle=rattle, lj_shift=lj_shift)
     chunk = max(1, int(round(sample_fs / dt)))
     nsteps = int(round(ps * 1000.0 / dt))
-    ts, es = [], []
+    ts, es, comps = [], [], []
+    names = ("lj", "coul", "kinetic", "bond", "angle", "coul14", "lj14", "improper")
     e = None
     t0 = time.time()
     for k in range(nsteps // chunk):
         e = sysn.md_run(chunk, energy_every=chunk)
         ts.append((k + 1) * chunk * dt * 1e-6)  # ns
         es.append(e["total"])
+        comps.append([e[c] for c in names])
     wall = time.time() - t0
     ts, es = np.array(ts), np.array(es)
+    comps = np.array(comps)
     coef = np.polyfit(ts, es, 1)
     resid = es - np.polyval(coef, ts)
     se = float(np.sqrt((resid ** 2).sum() / max(len(ts) - 2, 1) / ((ts - ts.mean()) ** 2).sum()))
@@ -155,7 +158,9 @@ def nve_drift(M, ctx, s, x, v, *, dt, precision, rattle, lj_shift, shake_tol, ps
     st = sysn.stats()
     sysn.close()
     scale = 1.0 / kT / n
+    parts = {c: float(np.polyfit(ts, comps[:, i], 1)[0]) * scale for i, c in enumerate(names)}
     return {"kT_per_ns_per_atom": float(coef[0]) * scale,
+            "component_slopes_kT_per_ns_per_atom": parts,
             "stderr_lsq": se * scale,
             "stderr_blocks": float(np.std(blocks, ddof=1) / np.sqrt(len(blocks))) * scale,
             "energy_rms_fluct_kcal": float(np.std(resid)),

@@ -130,7 +130,7 @@ def test_autotune_returns_a_candidate(ctx, replicas):
 
 
 def test_server_serves_and_continues(replicas):
-    srv = Server(max_active=2, hbm_budget=2 * estimate_bytes(6000), chunk_steps=20, cut=8.0,
+    srv = Server(max_active=2, hbm_budget=1 << 30, chunk_steps=20, cut=8.0,
                  dt=1.0, gamma=0.01, warm_in=0)
     reqs = [Request(k, 0.0, s, 40) for k, s in enumerate(replicas)]
     reqs.append(Request(10, 0.0, replicas[0], 20, continues=0))
@@ -151,3 +151,53 @@ def test_server_serves_and_continues(replicas):
     assert np.array_equal(m.get_state()[0], x_served)
     m.close()
     c.close()
+
+
+def test_resident_cluster_analysis_equals_host_path(ctx):
+    """get_greatestCluster on the device-resident positions equals the host-fed
+    call on the same (wrapped real*4) positions; a seeded crystalline nucleus
+    takes the analysis's real branch (solid molecules, greatest label > 0)."""
+    from molecular_simulation_code_b200.nonbond import get_greatest_cluster
+    s = make_system(60, 1500, 5, nucleus=40)
+    m = M.System(ctx, s, cut=8.0, skin=2.0)
+    m.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
+    m.md_setup(s, dt=1.0, gamma=0.02, seed=9)
+    m.md_run(20)
+    x, _, _ = m.get_state()
+    L = float(s.box)
+    w = (x - L * np.floor(x / L)).astype(np.float32)
+    w[w <= 0] += np.float32(L)
+    pos = s.position_aos().copy()
+    pos[:, :3] = w
+    gid = np.arange(1, s.np_atoms + 1, dtype=np.int32)
+    mrcut, denscut, densmin = 9.0, 6.0, 11
+    ptta_h = s.xyz[:10 * s.n_gly].astype(np.float64).copy()
+    ptta_d = ptta_h.copy()
+    size_h, g_h, dens, _ = get_greatest_cluster(ctx, pos, gid, s.n_gly, 10, s.box, mrcut, denscut,
+                                                densmin, ptta_h, 0)
+    size_d, g_d = m.greatest_cluster(s.n_gly, mrcut, denscut, densmin, greatest=0, ptta=ptta_d)
+    assert (size_d, g_d) == (size_h, g_h)
+    assert np.array_equal(ptta_d, ptta_h)
+    assert (np.asarray(dens) >= densmin).sum() > 0 and g_h > 0 and size_h > 0
+    # the system's own device copy of ptta (set from the current positions)
+    size_r, g_r = m.greatest_cluster(s.n_gly, mrcut, denscut, densmin, greatest=0)
+    assert size_r > 0 and g_r > 0
+    assert m.device_bytes() > 0
+    m.close()
+
+
+def test_server_warm_in_inside_batch_and_nucleus(replicas):
+    """Warm-in runs inside the batch (admission does not step the replica), every
+    request finishes with the device cluster analysis, and a nucleus-seeded request
+    reports a non-trivial cluster; the batch graphs are captured once."""
+    nuc = make_system(60, 1500, 5, nucleus=40)
+    srv = Server(max_active=3, hbm_budget=1 << 30, chunk_steps=20, cut=8.0, dt=1.0,
+                 gamma=0.01, warm_in=10, segment_graph=10)
+    reqs = [Request(0, 0.0, nuc, 40), Request(1, 0.0, replicas[1], 60),
+            Request(2, 0.01, replicas[2], 20)]
+    stats = run_stream(srv, reqs)
+    assert stats["requests"] == 3 and srv.recaptures == 1
+    got = {r.rid: r for r in srv.results}
+    assert got[0].cluster_size > 0
+    assert all(r.latency >= r.service > 0 for r in srv.results)
+    srv.close()

@@ -186,3 +186,32 @@ def test_md_rattle_changes_only_full_step_velocities(ctx, small):
     assert _velocity_constraint_residual(s, xa, va) > 1e-6
     a.close()
     b.close()
+
+
+def test_md_nve_drift_slope_bounded(ctx):
+    """NVE energy drift of the 9,000-atom system over 4 ps after a Langevin
+    warm-up (0.5 fs steps, RATTLE velocity stage, LJ energy shift, SHAKE to
+    1e-10): the least-squares slope of the total energy stays within
+    0.02 kT/ns/atom (the 90k-atom 100 ps runs give |slope| <= 3e-4 at 2 fs with
+    the same options), which a broken force or integrator exceeds by orders of
+    magnitude."""
+    s = make_system(150, 2500, 1)
+    m = M.System(ctx, s, cut=10.0, skin=2.0)
+    m.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
+    m.md_setup(s, dt=1.0, gamma=0.02, seed=3)
+    m.md_run(500)
+    m.md_setup(s, dt=2.0, gamma=0.01, seed=4)
+    m.md_run(1000)
+    m.md_setup(s, dt=0.5, gamma=0.0, seed=5, shake_maxiter=200, shake_tol=1e-10, rattle=True,
+               lj_shift=True)
+    ts, es = [], []
+    for k in range(40):
+        e = m.md_run(200, energy_every=200)
+        ts.append((k + 1) * 200 * 0.5e-6)  # ns
+        es.append(e["total"])
+    kT = 0.001987204181 * 300.0
+    slope = np.polyfit(np.array(ts), np.array(es), 1)[0] / kT / s.np_atoms
+    print("9k NVE drift (kT/ns/atom):", slope, "T:", e["temperature"])
+    assert abs(slope) < 0.02, slope
+    assert 250.0 < e["temperature"] < 360.0
+    m.close()
