@@ -384,15 +384,21 @@ def cpu_md_sample(s, nsteps):
                       "trigger + FP64 force every step, ballistic trajectory"}
 
 
-def row_hash(nl, nn, na):
-    """Order-independent hash of each neighbour row (sum of a 64-bit mix of its ids)."""
+def row_hash(nl, nn, na, chunk=4096):
+    """Order-independent hash of each neighbour row (sum of a 64-bit mix of its ids),
+    computed over blocks of rows to bound the host memory."""
     n = nn.shape[0]
-    m = nl.reshape(n, na).astype(np.uint64)
-    valid = np.arange(na)[None, :] < nn[:, None]
-    h = m * np.uint64(0x9E3779B97F4A7C15)
-    h ^= h >> np.uint64(29)
-    h *= np.uint64(0xBF58476D1CE4E5B9)
-    return np.where(valid, h, np.uint64(0)).sum(axis=1, dtype=np.uint64)
+    rows = nl.reshape(n, na)
+    out = np.zeros(n, np.uint64)
+    cols = np.arange(na)[None, :]
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        h = rows[a:b].astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+        h ^= h >> np.uint64(29)
+        h *= np.uint64(0xBF58476D1CE4E5B9)
+        h[cols >= nn[a:b, None]] = 0
+        out[a:b] = h.sum(axis=1, dtype=np.uint64)
+    return out
 
 
 def extra_rows(args, ctx, budget_s=420.0):

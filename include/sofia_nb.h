@@ -451,6 +451,11 @@ int sofia_batch_set_segment(sofia_batch *batch, int steps);
 /* Prune margin (A) of the pruned inner list (default 0.6): the tuning knob
  * the autotuner picks per size class. */
 int sofia_system_set_margin(sofia_system *sys, double margin);
+/* Cluster shape: the xy column width as a multiple (0.5..2) of the cube side of
+ * 8 atoms (1 = default; < 1 taller, > 1 flatter clusters).  Reallocates the
+ * column and list buffers; the next evaluation rebuilds the lists.  The
+ * autotuner's geometry knob, chosen per size class with the prune margin. */
+int sofia_system_set_cluster_shape(sofia_system *sys, double aspect);
 
 /*
  * Snapshot / rollback of the resident replica state, replacing the in-memory

@@ -133,6 +133,7 @@ SIGNATURES: dict[str, tuple] = {
     "sofia_batch_set_systems": (_I, [_P, _P, _I]),
     "sofia_batch_set_segment": (_I, [_P, _I]),
     "sofia_system_set_margin": (_I, [_P, _D]),
+    "sofia_system_set_cluster_shape": (_I, [_P, _D]),
     "sofia_system_timers": (_I, [_P, _I, _P]),
     "sofia_system_snapshot": (_I, [_P]),
     "sofia_system_rollback": (_I, [_P]),

@@ -6,9 +6,13 @@ and steps run as captured graphs of ``seg`` steps.  Members can change between
 runs (``set_systems``) without a graph recapture.  Replicas never exchange data, so each replica's
 trajectory is bit-identical to the same replica run alone.
 
-``autotune_margin`` times short MD segments of one replica per candidate
-prune margin and keeps the fastest for the replica's size class; ``Tuner``
-caches the choice per class, so every replica of that class uses it.
+``autotune`` times short MD segments of one replica per candidate shape --
+the cluster geometry (the xy column width relative to the cube side of 8
+atoms, i.e. how tall the 8-atom clusters are) and the prune margin of the
+inner list -- and keeps the fastest for the replica's size class; ``Tuner``
+caches the choice per class, so every replica of that class uses it (in a
+batch every replica keeps its own shape: the batched kernels read each
+replica's geometry from the device table).
 """
 from __future__ import annotations
 
@@ -25,6 +29,7 @@ from .system import random_replica
 
 SIZE_CLASSES = [(0, 6000), (6000, 12000), (12000, 24000), (24000, 48000), (48000, 1 << 30)]
 MARGINS = (0.3, 0.5, 0.8, 1.2)
+ASPECTS = (0.8, 1.0, 1.25)
 
 
 def size_class(n: int) -> int:
@@ -80,6 +85,55 @@ def set_margin(system: M.System, margin: float):
     system.ctx.check(system.ctx._lib.sofia_system_set_margin(system.handle, float(margin)))
 
 
+def set_cluster_shape(system: M.System, aspect: float):
+    system.ctx.check(system.ctx._lib.sofia_system_set_cluster_shape(system.handle,
+                                                                   float(aspect)))
+
+
+def apply_shape(system: M.System, shape):
+    """shape = (aspect, margin) as chosen by the tuner."""
+    set_cluster_shape(system, shape[0])
+    set_margin(system, shape[1])
+
+
+def autotune(ctx: Context, sysdata, aspects=ASPECTS, margins=(0.4, 0.6, 0.8), steps: int = 40,
+             cut: float = 10.0, skin: float = 2.0, precision: int = M.MIXED):
+    """Fastest (cluster aspect, prune margin) for this replica: short Langevin
+    segments timed with CUDA events, every candidate from the same state."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctx._lib.sofia_stream(ctx.handle))
+    base = M.System(ctx, sysdata, cut=cut, skin=skin, precision=precision)
+    base.set_state(sysdata.xyz.astype(np.float64), sysdata.velocity.astype(np.float64))
+    base.md_setup(sysdata, dt=1.0, gamma=0.02, seed=1)
+    base.md_run(30)
+    x, v, _ = base.get_state()
+    base.close()
+    times = {}
+    for a in aspects:
+        for mg in margins:
+            m = M.System(ctx, sysdata, cut=cut, skin=skin, precision=precision)
+            try:
+                set_cluster_shape(m, a)
+            except Exception:
+                m.close()
+                continue  # the box is too small for that column grid
+            set_margin(m, mg)
+            m.set_state(x, v)
+            m.md_setup(sysdata, dt=2.0, gamma=0.001, seed=2)
+            m.md_run(10)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            m.md_run(steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times[(a, mg)] = e0.elapsed_time(e1) / steps
+            m.close()
+    best = min(times, key=times.get)
+    return best, times
+
+
 def autotune_margin(ctx: Context, sysdata, margins=MARGINS, steps: int = 60, cut: float = 10.0,
                     skin: float = 2.0, precision: int = M.MIXED) -> tuple[float, dict]:
     """Fastest prune margin for this replica (short Langevin segments, CUDA events)."""
@@ -108,19 +162,23 @@ def autotune_margin(ctx: Context, sysdata, margins=MARGINS, steps: int = 60, cut
 
 
 class Tuner:
-    """Per-size-class margin choices (filled lazily by autotune_margin)."""
+    """Per-size-class (cluster aspect, prune margin) choices, filled lazily by
+    ``autotune`` on the first replica of each class."""
 
     def __init__(self):
-        self.choice: dict[int, float] = {}
+        self.choice: dict[int, tuple] = {}
         self.timings: dict[int, dict] = {}
 
-    def margin_for(self, ctx: Context, sysdata, **kw) -> float:
+    def shape_for(self, ctx: Context, sysdata, **kw) -> tuple:
         k = size_class(sysdata.np_atoms)
         if k not in self.choice:
-            best, t = autotune_margin(ctx, sysdata, **kw)
+            best, t = autotune(ctx, sysdata, **kw)
             self.choice[k] = best
             self.timings[k] = t
         return self.choice[k]
+
+    def margin_for(self, ctx: Context, sysdata, **kw) -> float:
+        return self.shape_for(ctx, sysdata, **kw)[1]
 
 
 def _gen(args):

@@ -1600,13 +1600,21 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
 }
 
 // Prune margin (A) of the pruned inner list: the per-size-class tuning knob.
+namespace sofia {
+void md_invalidate(Sys *s) {
+    s->built = 0;
+    s->md.forces_valid = 0;  // the next run rebuilds and recomputes before any capture
+    md_drop_graphs(s);
+    dropin_drop(s);
+}
+}  // namespace sofia
+
 extern "C" int sofia_system_set_margin(sofia_system *ss, double margin) {
     if (!ss || !(margin >= 0.05) || !(margin <= ss->s.skin)) return SOFIA_EINVAL;
     Sys *s = &ss->s;
+    SOFIA_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
     s->margin = margin;
-    s->built = 0;
-    sofia::md_drop_graphs(s);
-    sofia::dropin_drop(s);
+    sofia::md_invalidate(s);
     return SOFIA_OK;
 }
 

@@ -778,18 +778,18 @@ __device__ __forceinline__ T reduce_j4(T v0, T v1, T v2, int lane) {
     return k + __shfl_xor_sync(FULL, o, 8);
 }
 
-// i-force partial sums of one lane (i atoms q and q + 4) -> the warp's 64-bit
-// fixed-point sums in shared memory (integer adds: order-independent).
+// i-force partial sums of one lane (i atoms q and q + 4) -> the lane's own 64-bit
+// fixed-point sums in shared memory, fi[c * 32 + lane] for component c of i atom
+// q (c = 0..2) and q + 4 (c = 3..5): no atomics, no bank conflicts.
 template <typename T>
-__device__ __forceinline__ void flush_i(long long *__restrict__ fi, int q, T x0, T y0, T z0,
+__device__ __forceinline__ void flush_i(long long *__restrict__ fi, int lane, T x0, T y0, T z0,
                                         T x1, T y1, T z1) {
-    unsigned long long *u = reinterpret_cast<unsigned long long *>(fi);
-    if (x0 != (T)0) atomicAdd(u + 0 * CL + q, (unsigned long long)to_fix<T>(x0));
-    if (y0 != (T)0) atomicAdd(u + 1 * CL + q, (unsigned long long)to_fix<T>(y0));
-    if (z0 != (T)0) atomicAdd(u + 2 * CL + q, (unsigned long long)to_fix<T>(z0));
-    if (x1 != (T)0) atomicAdd(u + 0 * CL + q + 4, (unsigned long long)to_fix<T>(x1));
-    if (y1 != (T)0) atomicAdd(u + 1 * CL + q + 4, (unsigned long long)to_fix<T>(y1));
-    if (z1 != (T)0) atomicAdd(u + 2 * CL + q + 4, (unsigned long long)to_fix<T>(z1));
+    fi[0 * 32 + lane] += to_fix<T>(x0);
+    fi[1 * 32 + lane] += to_fix<T>(y0);
+    fi[2 * 32 + lane] += to_fix<T>(z0);
+    fi[3 * 32 + lane] += to_fix<T>(x1);
+    fi[4 * 32 + lane] += to_fix<T>(y1);
+    fi[5 * 32 + lane] += to_fix<T>(z1);
 }
 
 // Pair kernel on the half cluster-pair list (each atom pair once, Newton's
@@ -806,8 +806,9 @@ __device__ __forceinline__ void flush_i(long long *__restrict__ fi, int q, T x0,
 //     fixed-point accumulators, 24 lanes x one 64-bit atomic add into one
 //     j-cluster's contiguous slots;
 //   * i forces are summed per lane in FP32 and flushed every FLUSH entries into
-//     the warp's 64-bit fixed-point sums in shared memory, which are added to
-//     the slot accumulators once at the end.
+//     the lane's 64-bit fixed-point sums in shared memory; at the end of the row
+//     they are summed over the 8 lanes of an i atom and added to the slot
+//     accumulators.
 // Integer addition makes every sum independent of the order of the atomics, so
 // results stay bit-reproducible.  EN adds the LJ and Coulomb energies, VIR the
 // diagonal virial (each pair once).
@@ -825,7 +826,7 @@ __device__ __forceinline__ void pair_body(
     float2 *s_ljb = s_lja + k.ntypes * k.ntypes;
 
     __shared__ double s_sh[27 * 3];
-    __shared__ long long s_fi[8][3 * CL];  // per warp: i-force sums [component][i atom]
+    __shared__ long long s_fi[8][6 * 32];  // per warp and lane: i-force sums (see flush_i)
     // FP32x2 path: lj2 and lj4 enter the packed FMAs as addends, stored negated
     constexpr bool PACK = sizeof(T) == 4;
     for (int t = threadIdx.x; t < k.ntypes * k.ntypes; t += blockDim.x) {
@@ -845,7 +846,8 @@ __device__ __forceinline__ void pair_body(
     }
     const int lane = threadIdx.x & 31;
     long long *fi = s_fi[threadIdx.x >> 5];
-    if (lane < 3 * CL) fi[lane] = 0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) fi[c * 32 + lane] = 0;
     __syncthreads();
     const int jj = lane & 7, q = lane >> 3;
     const int icl = (bx * blockDim.x + threadIdx.x) >> 5;
@@ -996,7 +998,7 @@ __device__ __forceinline__ void pair_body(
                 atomicAdd(jdst + jc * CL + jj, (unsigned long long)(-to_fix<T>(fj)));
             if (((base + e) & (FLUSH - 1)) == FLUSH - 1) {
                 if constexpr (PACK) {
-                    flush_i<float>(fi, q, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
+                    flush_i<float>(fi, lane, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
                     ax2 = ay2 = az2 = z2;
                     if (EN) {
                         e_lj += (double)alj2.x + (double)alj2.y;
@@ -1010,7 +1012,7 @@ __device__ __forceinline__ void pair_body(
                         axx2 = ayy2 = azz2 = z2;
                     }
                 } else {
-                    flush_i<T>(fi, q, ax0, ay0, az0, ax1, ay1, az1);
+                    flush_i<T>(fi, lane, ax0, ay0, az0, ax1, ay1, az1);
                     ax0 = ay0 = az0 = ax1 = ay1 = az1 = 0;
                     if (EN) {
                         e_lj += (double)a_lj;
@@ -1028,7 +1030,7 @@ __device__ __forceinline__ void pair_body(
         }
     }
     if constexpr (PACK) {
-        flush_i<float>(fi, q, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
+        flush_i<float>(fi, lane, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
         if (EN) {
             e_lj += (double)alj2.x + (double)alj2.y;
             e_c += (double)ac2.x + (double)ac2.y;
@@ -1039,13 +1041,26 @@ __device__ __forceinline__ void pair_body(
             vzz += (double)azz2.x + (double)azz2.y;
         }
     } else {
-        flush_i<T>(fi, q, ax0, ay0, az0, ax1, ay1, az1);
+        flush_i<T>(fi, lane, ax0, ay0, az0, ax1, ay1, az1);
     }
-    __syncwarp();
-    if (lane < 3 * CL) {
-        const long long v = fi[lane];
-        if (v) atomicAdd(fslot + (size_t)(lane >> 3) * stride + (size_t)icl * CL + (lane & 7),
-                         (unsigned long long)v);
+    // sum each i atom's partials over its 8 lanes (lane bits 0-2), then lane
+    // jj = 0 of each quarter adds the totals of i atoms q and q + 4
+    long long fsum[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        long long v = fi[c * 32 + lane];
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) v += __shfl_xor_sync(FULL, v, off);
+        fsum[c] = v;
+    }
+    if (jj == 0) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const int atom = q + 4 * (c / 3);
+            if (fsum[c])
+                atomicAdd(fslot + (size_t)(c % 3) * stride + (size_t)icl * CL + atom,
+                          (unsigned long long)fsum[c]);
+        }
     }
     if (EN || VIR) {
         e_lj += (double)a_lj;
@@ -1408,6 +1423,30 @@ static int sys_alloc(Sys *s) {
     SOFIA_CUDA(ctx, cudaMemset(s->jcount.p, 0, sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, cudaMemset(s->icount.p, 0, sizeof(int) * maxcl));
     return SOFIA_OK;
+}
+
+// Column grid and list capacities.  aspect scales the xy column width from the
+// cube side of 8 atoms (aspect 1: clusters about as tall as wide; < 1: narrower
+// columns and taller clusters; > 1: wider and flatter ones).  False if the box is
+// too small for the grid.
+bool sys_geometry(Sys *s, double aspect) {
+    const double rho = (double)s->n / (s->L * s->L * s->L);
+    const double s_target = aspect * cbrt((double)CL / rho);
+    const int ncx = (int)fmax(1.0, floor(s->L / s_target));
+    const double s_col = s->L / ncx;
+    const int reach = (int)ceil(s->rlist / s_col);
+    if (reach >= ncx) return false;
+    s->ncx = ncx;
+    s->s_col = s_col;
+    s->ncols = ncx * ncx;
+    s->ncol_reach = reach;
+    s->aspect = aspect;
+    s->max_clusters = s->n / CL + s->ncols + 1;
+    // expected j-clusters per row: bounding-box volume around rlist, plus headroom
+    const double zext = (double)CL / (rho * s_col * s_col);  // cluster height
+    const double reach_d = s->rlist + 1.5 * fmax(s_col, zext);
+    s->jcap = (int)(4.19 * reach_d * reach_d * reach_d * rho / CL * 1.3) + 32;
+    return true;
 }
 
 void dropin_drop(Sys *s) {
@@ -1850,20 +1889,10 @@ extern "C" int sofia_system_create(sofia_nb_ctx *ctx, const sofia_system_desc *d
         delete ss;
         return sofia::fail(ctx, SOFIA_EINVAL, "box too small for rc + skin%s");
     }
-    const double rho = (double)s->n / (s->L * s->L * s->L);
-    const double s_target = cbrt((double)sofia::CL / rho);
-    s->ncx = (int)fmax(1.0, floor(s->L / s_target));
-    s->s_col = s->L / s->ncx;
-    s->ncols = s->ncx * s->ncx;
-    s->ncol_reach = (int)ceil(s->rlist / s->s_col);
-    if (s->ncol_reach >= s->ncx) {
+    if (!sofia::sys_geometry(s, 1.0)) {
         delete ss;
         return sofia::fail(ctx, SOFIA_EINVAL, "box too small for the column grid%s");
     }
-    s->max_clusters = s->n / sofia::CL + s->ncols + 1;
-    // expected j-clusters per row: bounding-box volume around rlist, plus headroom
-    const double reach = s->rlist + 1.5 * s_target;
-    s->jcap = (int)(4.19 * reach * reach * reach * rho / sofia::CL * 1.3) + 32;
     int rc = sofia::sys_alloc(s);
     if (!rc) rc = sofia::sys_alloc_list(s);
     const size_t n = (size_t)s->n;
@@ -2516,3 +2545,31 @@ void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
 }
 
 }  // namespace sofia
+
+// Cluster shape (the autotuner's geometry knob): the xy column width as a
+// multiple of the cube side of 8 atoms.  Reallocates the column and list
+// buffers; the next evaluation rebuilds the lists.
+extern "C" int sofia_system_set_cluster_shape(sofia_system *ss, double aspect) {
+    if (!ss || !(aspect >= 0.5) || !(aspect <= 2.0)) return SOFIA_EINVAL;
+    Sys *s = &ss->s;
+    sofia_nb_ctx *ctx = s->ctx;
+    SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    SOFIA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const Sys keep_geom = *s;
+    if (!sofia::sys_geometry(s, aspect)) {
+        s->ncx = keep_geom.ncx;
+        s->s_col = keep_geom.s_col;
+        s->ncols = keep_geom.ncols;
+        s->ncol_reach = keep_geom.ncol_reach;
+        s->max_clusters = keep_geom.max_clusters;
+        s->jcap = keep_geom.jcap;
+        s->aspect = keep_geom.aspect;
+        return sofia::fail(ctx, SOFIA_EINVAL, "box too small for that column grid%s");
+    }
+    if (s->jcap < keep_geom.jcap) s->jcap = keep_geom.jcap;
+    int rc = sofia::sys_alloc(s);
+    if (!rc) rc = sofia::sys_alloc_list(s);
+    if (rc) return rc;
+    sofia::md_invalidate(s);
+    return SOFIA_OK;
+}

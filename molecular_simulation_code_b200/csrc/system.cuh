@@ -72,6 +72,7 @@ struct Sys {
     // column grid
     int ncx = 0, ncols = 0, max_clusters = 0, jcap = 0, ncol_reach = 0;
     double s_col = 0.0;
+    double aspect = 1.0;              // column width / cube side of 8 atoms (cluster shape)
     // global-order state
     DevBuf x[3], v[3], f[3], xref[3], img[3];
     DevBuf type, q, invm, mass, specbond, num3bond;
@@ -305,6 +306,11 @@ int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_
 int sys_list_overflow(Sys *s, const int32_t *status = nullptr);
 // Frees the captured drop-in force graphs (they bake in list pointers and the margin).
 void dropin_drop(Sys *s);
+// Column grid and list capacities for a cluster shape (mixed.cu).
+bool sys_geometry(Sys *s, double aspect);
+// After a change of list geometry or margin (md.cu): drops the system's captured
+// graphs and makes the next MD run start with a fresh build and force evaluation.
+void md_invalidate(Sys *s);
 
 }  // namespace sofia
 

@@ -2,8 +2,8 @@
 
 batch:  64 seeded replicas, N ~ U[3,000, 30,000] atoms, glycine 5-20 % of
         molecules, own cubic box at 1.0 g/cm^3; 100-step segments (one graph
-        launch per step for all replicas); prune margin autotuned per size
-        class; mixed and FP64 atom-steps/s.
+        launch per kernel and step for all replicas); cluster shape and prune
+        margin autotuned per size class (--tune); mixed and FP64 atom-steps/s.
 serve:  Poisson request stream (default 200 requests/s), systems of
         N ~ U[2,000, 60,000] atoms, U[500, 5,000] steps (times --steps-scale),
         every 4th with a crystalline glycine nucleus, up to 64 concurrent
@@ -28,7 +28,7 @@ def bench_batch(args):
     import torch
 
     from . import mixed as M
-    from .batch import Batch, Tuner, make_replicas, set_margin, size_class
+    from .batch import Batch, Tuner, apply_shape, make_replicas, size_class
     from .nonbond import Context
 
     reps = make_replicas(args.replicas, seed=args.seed, n_min=3000, n_max=30000,
@@ -41,8 +41,9 @@ def bench_batch(args):
     tuner = Tuner()
     if args.tune:
         for r in reps:
-            tuner.margin_for(master, r, steps=20)
-        out["tuned_margin_per_class"] = {str(k): v for k, v in tuner.choice.items()}
+            tuner.shape_for(master, r, steps=30)
+        out["tuned_shape_per_class"] = {str(k): {"aspect": v[0], "margin": v[1]}
+                                        for k, v in tuner.choice.items()}
     stream = torch.cuda.ExternalStream(master._lib.sofia_stream(master.handle))
     for name, prec in (("mixed", M.MIXED), ("fp64", M.FP64)):
         ctxs = [Context(0) for _ in reps]
@@ -50,7 +51,7 @@ def bench_batch(args):
         for c, r in zip(ctxs, reps):
             m = M.System(c, r, precision=prec)
             if args.tune:
-                set_margin(m, tuner.choice[size_class(r.np_atoms)])
+                apply_shape(m, tuner.choice[size_class(r.np_atoms)])
             m.set_state(r.xyz.astype(np.float64), r.velocity.astype(np.float64))
             m.md_setup(r, dt=1.0, gamma=0.02, seed=7)
             systems.append(m)

@@ -37,7 +37,7 @@ import time
 import numpy as np
 
 from . import mixed as M
-from .batch import Batch, Tuner, set_margin
+from .batch import Batch, Tuner, apply_shape
 from .nonbond import Context
 
 BYTES_PER_ATOM = 1200      # charge per atom of a request before any system exists
@@ -144,7 +144,7 @@ class Server:
         ctx = Context(self.device)
         m = M.System(ctx, s, cut=self.cut, skin=self.skin, precision=self.precision)
         if self.tuner is not None:
-            set_margin(m, self.tuner.margin_for(ctx, s, cut=self.cut, skin=self.skin,
+            apply_shape(m, self.tuner.shape_for(ctx, s, cut=self.cut, skin=self.skin,
                                                 precision=self.precision))
         m.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
         if self.warm_in:

@@ -9,7 +9,8 @@ import pytest
 
 from molecular_simulation_code_b200 import mixed as M
 from molecular_simulation_code_b200 import nonbond as nb
-from molecular_simulation_code_b200.batch import Batch, autotune_margin, set_margin
+from molecular_simulation_code_b200.batch import (Batch, autotune, autotune_margin,
+                                                  set_cluster_shape, set_margin)
 from molecular_simulation_code_b200.serve import Request, Server, estimate_bytes, run_stream
 from molecular_simulation_code_b200.system import make_system
 
@@ -123,6 +124,9 @@ def test_segments_compose(ctx, replicas):
 def test_autotune_returns_a_candidate(ctx, replicas):
     best, times = autotune_margin(ctx, replicas[1], margins=(0.4, 0.8), steps=10, cut=8.0)
     assert best in (0.4, 0.8) and all(t > 0 for t in times.values())
+    best, times = autotune(ctx, replicas[1], aspects=(0.8, 1.0), margins=(0.5,), steps=10,
+                           cut=8.0)
+    assert best in times and best[1] == 0.5 and all(t > 0 for t in times.values())
     m = M.System(ctx, replicas[1], cut=8.0, skin=2.0)
     with pytest.raises(Exception):
         set_margin(m, 5.0)  # larger than the skin
@@ -201,3 +205,38 @@ def test_server_warm_in_inside_batch_and_nucleus(replicas):
     assert got[0].cluster_size > 0
     assert all(r.latency >= r.service > 0 for r in srv.results)
     srv.close()
+
+
+def test_cluster_shape_keeps_forces_and_coverage(ctx):
+    """Taller or flatter clusters (the tuner's geometry knob) change the list, not the
+    physics: FP64 forces and energies agree within 1e-10 relative, and the pruned list
+    still holds every pair within rc."""
+    from scipy.spatial import cKDTree
+    s = make_system(150, 2500, 1)
+    ref = None
+    for aspect in (1.0, 0.8, 1.25):
+        m = M.System(ctx, s, cut=10.0, skin=2.0, precision=M.FP64)
+        if aspect != 1.0:
+            set_cluster_shape(m, aspect)
+        m.set_state(s.xyz.astype(np.float64))
+        e = m.compute(M.FP64, rebuild=True)
+        f = m.get_state()[2]
+        pairs, _ = m.list_pairs(1)
+        n = s.np_atoms
+        keys = np.unique(np.minimum(pairs[:, 0], pairs[:, 1]).astype(np.int64) * n +
+                         np.maximum(pairs[:, 0], pairs[:, 1]))
+        L = float(s.box)
+        xw = np.mod(s.xyz.astype(np.float64), L)
+        pr = cKDTree(xw, boxsize=L).query_pairs(10.0, output_type="ndarray").astype(np.int64)
+        need = pr.min(axis=1) * n + pr.max(axis=1)
+        excl = {min(i, int(j) - 1) * n + max(i, int(j) - 1)
+                for i in range(n) for j in s.specbond[i, :s.num3bond[i]] if j > 0}
+        need = np.setdiff1d(need, np.array(sorted(excl), np.int64))
+        assert np.isin(need, keys).all(), aspect
+        if ref is None:
+            ref = (e, f)
+        else:
+            assert M.force_max_rel(f, ref[1]) <= 1e-10, aspect
+            assert abs(e[0] - ref[0][0]) <= 1e-10 * abs(ref[0][0])
+            assert abs(e[1] - ref[0][1]) <= 1e-10 * abs(ref[0][1])
+        m.close()
