@@ -455,7 +455,8 @@ def extra_rows(args, ctx, budget_s=420.0):
     p = nb.DsfParams(alpha=ALPHA, box=s90.box, cut_coul=CUT, rcut=CUT, neighbor_pad=SKIN)
     gnl, gnn, gna = nb.neighbor_wrapper(ctx, pos, s90.specbond, s90.num3bond, p, 1024)
     op = O.params(ALPHA, s90.box, CUT, CUT, SKIN)
-    onl, onn, ona = O.neighbor_wrapper(op, pos, s90.specbond, s90.num3bond, 1024, fast=True)
+    # the strict-IEEE oracle (the parity checker), not the contracting timing build
+    onl, onn, ona = O.neighbor_wrapper(op, pos, s90.specbond, s90.num3bond, 1024)
     same = bool(np.array_equal(gnn, onn) and
                 np.array_equal(row_hash(gnl, gnn, gna), row_hash(onl, onn, ona)))
     row["neighbor_sets_bit_exact"] = {"equal": same, "entries": int(onn.sum())}

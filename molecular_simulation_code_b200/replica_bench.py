@@ -65,10 +65,12 @@ def bench_batch(args):
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push(f"batch_timed_{name}")  # lets ncu select the timed steps
         e0.record(stream)
         for _ in range(args.segments):
             b.run(args.segment, energy_every=args.segment)
         e1.record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         t = e0.elapsed_time(e1) / 1e3
         steps = args.segments * args.segment
