@@ -1491,7 +1491,9 @@ static int batch_capture(sofia_batch *b) {
         cudaGraphDestroy(graph);
         if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaGraphInstantiate (batch)");
     }
-    b->step_launches[0] = 12 + 1 + 5 + (rat ? 1 : 0);
+    // kick+drift, the pair path (active-replica compaction, bin, scan, scatter,
+    // sort, pack, bbox, search, prune, pair, unpack), bonded, SHAKE, kick
+    b->step_launches[0] = 1 + 11 + 3 + (rat ? 1 : 0);
     b->step_launches[1] = b->step_launches[0] + 2 + 4;
     b->graph_rattle = rat;
     b->graph_key = sofia::pair_key(s0);

@@ -36,7 +36,7 @@ constexpr int MAX_COL = 2048;
 #define SOFIA_COND_RETURN \
     if (cond && !(cond[0] & cmask)) return  // atoms per xy column handled by the in-column sort
 #ifndef SOFIA_PAIR_FLUSH
-#define SOFIA_PAIR_FLUSH 8
+#define SOFIA_PAIR_FLUSH 16
 #endif
 #ifndef SOFIA_PAIR_MINB
 #define SOFIA_PAIR_MINB 4
@@ -50,10 +50,19 @@ constexpr int MAX_COL = 2048;
 #ifndef SOFIA_PRUNE_MINB
 #define SOFIA_PRUNE_MINB 4
 #endif
+// resident blocks per SM of the batched pair and prune kernels (their replica
+// arguments come from the device table, not the constant bank)
+#ifndef SOFIA_BATCH_PAIR_MINB
+#define SOFIA_BATCH_PAIR_MINB SOFIA_PAIR_MINB
+#endif
+#ifndef SOFIA_BATCH_PRUNE_MINB
+#define SOFIA_BATCH_PRUNE_MINB SOFIA_PRUNE_MINB
+#endif
 #ifndef SOFIA_SEARCH_ZWIN
 #define SOFIA_SEARCH_ZWIN 1
 #endif
 constexpr int FLUSH = SOFIA_PAIR_FLUSH;  // list entries between FP32 -> fixed-point flushes of the i forces
+static_assert(FLUSH >= 1 && FLUSH <= 32 && (32 % FLUSH) == 0, "FLUSH must divide 32");
 
 __device__ __forceinline__ double wrap_shift(double x, double L) {
     // shift s with x + s in [0, L)
@@ -873,175 +882,164 @@ __device__ __forceinline__ void pair_body(
         const int cnt = min(32, n - base);
         const int myw = (lane < cnt) ? row[base + lane] : 0;
         const unsigned long long mym = (lane < cnt) ? mrow[base + lane] : 0ull;
-        for (int e = 0; e < cnt; ++e) {
-            const int w = __shfl_sync(FULL, myw, e);
-            const unsigned long long mm = __shfl_sync(FULL, mym, e);
-            const int jc = w & ((1 << IMG_SHIFT) - 1);
-            const int img = w >> IMG_SHIFT;
-            const AtomRec rj = rec[jc * CL + jj];
-            // j position in the image the entry pairs with
-            const double xj = rj.x + s_sh[img * 3 + 0];
-            const double yj = rj.y + s_sh[img * 3 + 1];
-            const double zj = rj.z + s_sh[img * 3 + 2];
-            T v0 = 0, v1 = 0, v2 = 0;  // the entry's force on j atom jj (negated)
-            const unsigned m0 = (unsigned)mm, m1 = (unsigned)(mm >> 32);
-            if (PACK && SOFIA_PAIR_HYBRID && (m0 == 0u || m1 == 0u)) {
-                // one i half without pairs in range: scalar evaluation of the other
-                // (a warp-uniform branch per half, so no selects of i data)
-                const bool h1 = m0 == 0u;
-                const double xi = h1 ? ri1.x : ri0.x, yi = h1 ? ri1.y : ri0.y,
-                             zi = h1 ? ri1.z : ri0.z;
-                const float dx = (float)(xi - xj);
-                const float dy = (float)(yi - yj);
-                const float dz = (float)(zi - zj);
-                const int ti = h1 ? ti1 : ti0;
-                const float2 la = s_lja[ti + rj.type];
-                const float2 lb = EN ? s_ljb[ti + rj.type] : make_float2(0.0f, 0.0f);
-                float elj = 0.0f, ec = 0.0f;
-                const float fs = PairMath<float>::template eval<EN, SAME>(
-                    dx, dy, dz, mulr(h1 ? qiq2.y : qiq2.x, rj.q),
-                    make_float4(la.x, -la.y, lb.x, -lb.y), ((m0 | m1) >> lane) & 1u, k, elj, ec);
-                const float px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
-                if (h1) {
-                    ax2.y = addr(ax2.y, px);
-                    ay2.y = addr(ay2.y, py);
-                    az2.y = addr(az2.y, pz);
+        // chunks of FLUSH entries (FLUSH divides 32), each followed by a flush of
+        // the lane's FP32 i-force partials
+        for (int e0 = 0; e0 < cnt; e0 += FLUSH) {
+            const int e1 = min(e0 + FLUSH, cnt);
+            for (int e = e0; e < e1; ++e) {
+                const int w = __shfl_sync(FULL, myw, e);
+                const unsigned long long mm = __shfl_sync(FULL, mym, e);
+                const int jc = w & ((1 << IMG_SHIFT) - 1);
+                const int img = w >> IMG_SHIFT;
+                const AtomRec rj = rec[jc * CL + jj];
+                // j position in the image the entry pairs with
+                const double xj = rj.x + s_sh[img * 3 + 0];
+                const double yj = rj.y + s_sh[img * 3 + 1];
+                const double zj = rj.z + s_sh[img * 3 + 2];
+                T v0 = 0, v1 = 0, v2 = 0;  // the entry's force on j atom jj (negated)
+                const unsigned m0 = (unsigned)mm, m1 = (unsigned)(mm >> 32);
+                if (PACK && SOFIA_PAIR_HYBRID && (m0 == 0u || m1 == 0u)) {
+                    // one i half without pairs in range: scalar evaluation of the other
+                    // (a warp-uniform branch per half, so no selects of i data)
+                    const bool h1 = m0 == 0u;
+                    const double xi = h1 ? ri1.x : ri0.x, yi = h1 ? ri1.y : ri0.y,
+                                 zi = h1 ? ri1.z : ri0.z;
+                    const float dx = (float)(xi - xj);
+                    const float dy = (float)(yi - yj);
+                    const float dz = (float)(zi - zj);
+                    const int ti = h1 ? ti1 : ti0;
+                    const float2 la = s_lja[ti + rj.type];
+                    const float2 lb = EN ? s_ljb[ti + rj.type] : make_float2(0.0f, 0.0f);
+                    float elj = 0.0f, ec = 0.0f;
+                    const float fs = PairMath<float>::template eval<EN, SAME>(
+                        dx, dy, dz, mulr(h1 ? qiq2.y : qiq2.x, rj.q),
+                        make_float4(la.x, -la.y, lb.x, -lb.y), ((m0 | m1) >> lane) & 1u, k, elj, ec);
+                    const float px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
+                    if (h1) {
+                        ax2.y = addr(ax2.y, px);
+                        ay2.y = addr(ay2.y, py);
+                        az2.y = addr(az2.y, pz);
+                    } else {
+                        ax2.x = addr(ax2.x, px);
+                        ay2.x = addr(ay2.x, py);
+                        az2.x = addr(az2.x, pz);
+                    }
+                    v0 = px;
+                    v1 = py;
+                    v2 = pz;
+                    if (EN) {
+                        alj2.x = addr(alj2.x, elj);
+                        ac2.x = addr(ac2.x, ec);
+                    }
+                    if (VIR) {
+                        axx2.x = fmar(dx, px, axx2.x);
+                        ayy2.x = fmar(dy, py, ayy2.x);
+                        azz2.x = fmar(dz, pz, azz2.x);
+                    }
+                } else if constexpr (PACK) {
+                    // both i halves at once; a half without pairs in range is computed
+                    // and masked (the packed instructions cost the same for one or two)
+                    const float2 dx = make_float2((float)(ri0.x - xj), (float)(ri1.x - xj));
+                    const float2 dy = make_float2((float)(ri0.y - yj), (float)(ri1.y - yj));
+                    const float2 dz = make_float2((float)(ri0.z - zj), (float)(ri1.z - zj));
+                    const float2 qq = mul2(qiq2, make_float2(rj.q, rj.q));
+                    const bool on0 = (m0 >> lane) & 1u;
+                    const bool on1 = (m1 >> lane) & 1u;
+                    float2 elj = z2, ec = z2;
+                    const float2 fs = PairMath2::template eval<EN, SAME>(
+                        dx, dy, dz, qq, s_lja[ti0 + rj.type], s_lja[ti1 + rj.type],
+                        EN ? s_ljb[ti0 + rj.type] : z2, EN ? s_ljb[ti1 + rj.type] : z2, on0, on1, k,
+                        elj, ec);
+                    const float2 px = mul2(dx, fs), py = mul2(dy, fs), pz = mul2(dz, fs);
+                    ax2 = add2(ax2, px);
+                    ay2 = add2(ay2, py);
+                    az2 = add2(az2, pz);
+                    v0 = addr(px.x, px.y);
+                    v1 = addr(py.x, py.y);
+                    v2 = addr(pz.x, pz.y);
+                    if (EN) {
+                        alj2 = add2(alj2, elj);
+                        ac2 = add2(ac2, ec);
+                    }
+                    if (VIR) {
+                        axx2 = fma2(dx, px, axx2);
+                        ayy2 = fma2(dy, py, ayy2);
+                        azz2 = fma2(dz, pz, azz2);
+                    }
                 } else {
-                    ax2.x = addr(ax2.x, px);
-                    ay2.x = addr(ay2.x, py);
-                    az2.x = addr(az2.x, pz);
+                    // FP64 twin: the two i halves one after the other; a half with no
+                    // pair in range is skipped by the whole warp
+    #pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const unsigned mh = h ? m1 : m0;
+                        if (mh == 0u) continue;
+                        const AtomRec &ri = h ? ri1 : ri0;
+                        const T dx = (T)(ri.x - xj);
+                        const T dy = (T)(ri.y - yj);
+                        const T dz = (T)(ri.z - zj);
+                        const bool on = (mh >> lane) & 1u;
+                        const float4 ljp = s_lj[(h ? ti1 : ti0) + rj.type];
+                        T elj = 0, ec = 0;
+                        const T fs = PairMath<T>::template eval<EN, SAME>(
+                            dx, dy, dz, mulr(h ? qiq1 : qiq0, (T)rj.q), ljp, on, k, elj, ec);
+                        const T px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
+                        if (h) {
+                            ax1 = addr(ax1, px);
+                            ay1 = addr(ay1, py);
+                            az1 = addr(az1, pz);
+                        } else {
+                            ax0 = addr(ax0, px);
+                            ay0 = addr(ay0, py);
+                            az0 = addr(az0, pz);
+                        }
+                        v0 = addr(v0, px);
+                        v1 = addr(v1, py);
+                        v2 = addr(v2, pz);
+                        if (EN) {
+                            a_lj = addr(a_lj, elj);
+                            a_c = addr(a_c, ec);
+                        }
+                        if (VIR) {
+                            a_xx = fmar(dx, px, a_xx);
+                            a_yy = fmar(dy, py, a_yy);
+                            a_zz = fmar(dz, pz, a_zz);
+                        }
+                    }
                 }
-                v0 = px;
-                v1 = py;
-                v2 = pz;
+                const T fj = reduce_j4<T>(v0, v1, v2, lane);
+                if (q < 3 && fj != (T)0)
+                    atomicAdd(jdst + jc * CL + jj, (unsigned long long)(-to_fix<T>(fj)));
+            }
+            if constexpr (PACK) {
+                flush_i<float>(fi, lane, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
+                ax2 = ay2 = az2 = z2;
                 if (EN) {
-                    alj2.x = addr(alj2.x, elj);
-                    ac2.x = addr(ac2.x, ec);
+                    e_lj += (double)alj2.x + (double)alj2.y;
+                    e_c += (double)ac2.x + (double)ac2.y;
+                    alj2 = ac2 = z2;
                 }
                 if (VIR) {
-                    axx2.x = fmar(dx, px, axx2.x);
-                    ayy2.x = fmar(dy, py, ayy2.x);
-                    azz2.x = fmar(dz, pz, azz2.x);
-                }
-            } else if constexpr (PACK) {
-                // both i halves at once; a half without pairs in range is computed
-                // and masked (the packed instructions cost the same for one or two)
-                const float2 dx = make_float2((float)(ri0.x - xj), (float)(ri1.x - xj));
-                const float2 dy = make_float2((float)(ri0.y - yj), (float)(ri1.y - yj));
-                const float2 dz = make_float2((float)(ri0.z - zj), (float)(ri1.z - zj));
-                const float2 qq = mul2(qiq2, make_float2(rj.q, rj.q));
-                const bool on0 = (m0 >> lane) & 1u;
-                const bool on1 = (m1 >> lane) & 1u;
-                float2 elj = z2, ec = z2;
-                const float2 fs = PairMath2::template eval<EN, SAME>(
-                    dx, dy, dz, qq, s_lja[ti0 + rj.type], s_lja[ti1 + rj.type],
-                    EN ? s_ljb[ti0 + rj.type] : z2, EN ? s_ljb[ti1 + rj.type] : z2, on0, on1, k,
-                    elj, ec);
-                const float2 px = mul2(dx, fs), py = mul2(dy, fs), pz = mul2(dz, fs);
-                ax2 = add2(ax2, px);
-                ay2 = add2(ay2, py);
-                az2 = add2(az2, pz);
-                v0 = addr(px.x, px.y);
-                v1 = addr(py.x, py.y);
-                v2 = addr(pz.x, pz.y);
-                if (EN) {
-                    alj2 = add2(alj2, elj);
-                    ac2 = add2(ac2, ec);
-                }
-                if (VIR) {
-                    axx2 = fma2(dx, px, axx2);
-                    ayy2 = fma2(dy, py, ayy2);
-                    azz2 = fma2(dz, pz, azz2);
+                    vxx += (double)axx2.x + (double)axx2.y;
+                    vyy += (double)ayy2.x + (double)ayy2.y;
+                    vzz += (double)azz2.x + (double)azz2.y;
+                    axx2 = ayy2 = azz2 = z2;
                 }
             } else {
-                // FP64 twin: the two i halves one after the other; a half with no
-                // pair in range is skipped by the whole warp
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const unsigned mh = h ? m1 : m0;
-                    if (mh == 0u) continue;
-                    const AtomRec &ri = h ? ri1 : ri0;
-                    const T dx = (T)(ri.x - xj);
-                    const T dy = (T)(ri.y - yj);
-                    const T dz = (T)(ri.z - zj);
-                    const bool on = (mh >> lane) & 1u;
-                    const float4 ljp = s_lj[(h ? ti1 : ti0) + rj.type];
-                    T elj = 0, ec = 0;
-                    const T fs = PairMath<T>::template eval<EN, SAME>(
-                        dx, dy, dz, mulr(h ? qiq1 : qiq0, (T)rj.q), ljp, on, k, elj, ec);
-                    const T px = mulr(dx, fs), py = mulr(dy, fs), pz = mulr(dz, fs);
-                    if (h) {
-                        ax1 = addr(ax1, px);
-                        ay1 = addr(ay1, py);
-                        az1 = addr(az1, pz);
-                    } else {
-                        ax0 = addr(ax0, px);
-                        ay0 = addr(ay0, py);
-                        az0 = addr(az0, pz);
-                    }
-                    v0 = addr(v0, px);
-                    v1 = addr(v1, py);
-                    v2 = addr(v2, pz);
-                    if (EN) {
-                        a_lj = addr(a_lj, elj);
-                        a_c = addr(a_c, ec);
-                    }
-                    if (VIR) {
-                        a_xx = fmar(dx, px, a_xx);
-                        a_yy = fmar(dy, py, a_yy);
-                        a_zz = fmar(dz, pz, a_zz);
-                    }
+                flush_i<T>(fi, lane, ax0, ay0, az0, ax1, ay1, az1);
+                ax0 = ay0 = az0 = ax1 = ay1 = az1 = 0;
+                if (EN) {
+                    e_lj += (double)a_lj;
+                    e_c += (double)a_c;
+                    a_lj = a_c = 0;
                 }
-            }
-            const T fj = reduce_j4<T>(v0, v1, v2, lane);
-            if (q < 3 && fj != (T)0)
-                atomicAdd(jdst + jc * CL + jj, (unsigned long long)(-to_fix<T>(fj)));
-            if (((base + e) & (FLUSH - 1)) == FLUSH - 1) {
-                if constexpr (PACK) {
-                    flush_i<float>(fi, lane, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
-                    ax2 = ay2 = az2 = z2;
-                    if (EN) {
-                        e_lj += (double)alj2.x + (double)alj2.y;
-                        e_c += (double)ac2.x + (double)ac2.y;
-                        alj2 = ac2 = z2;
-                    }
-                    if (VIR) {
-                        vxx += (double)axx2.x + (double)axx2.y;
-                        vyy += (double)ayy2.x + (double)ayy2.y;
-                        vzz += (double)azz2.x + (double)azz2.y;
-                        axx2 = ayy2 = azz2 = z2;
-                    }
-                } else {
-                    flush_i<T>(fi, lane, ax0, ay0, az0, ax1, ay1, az1);
-                    ax0 = ay0 = az0 = ax1 = ay1 = az1 = 0;
-                    if (EN) {
-                        e_lj += (double)a_lj;
-                        e_c += (double)a_c;
-                        a_lj = a_c = 0;
-                    }
-                    if (VIR) {
-                        vxx += (double)a_xx;
-                        vyy += (double)a_yy;
-                        vzz += (double)a_zz;
-                        a_xx = a_yy = a_zz = 0;
-                    }
+                if (VIR) {
+                    vxx += (double)a_xx;
+                    vyy += (double)a_yy;
+                    vzz += (double)a_zz;
+                    a_xx = a_yy = a_zz = 0;
                 }
             }
         }
-    }
-    if constexpr (PACK) {
-        flush_i<float>(fi, lane, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
-        if (EN) {
-            e_lj += (double)alj2.x + (double)alj2.y;
-            e_c += (double)ac2.x + (double)ac2.y;
-        }
-        if (VIR) {
-            vxx += (double)axx2.x + (double)axx2.y;
-            vyy += (double)ayy2.x + (double)ayy2.y;
-            vzz += (double)azz2.x + (double)azz2.y;
-        }
-    } else {
-        flush_i<T>(fi, lane, ax0, ay0, az0, ax1, ay1, az1);
     }
     // sum each i atom's partials over its 8 lanes (lane bits 0-2), then lane
     // jj = 0 of each quarter adds the totals of i atoms q and q + 4
@@ -2308,7 +2306,7 @@ namespace {
 
 __global__ void k_wrap_bin_b(const BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_A256)
+    SOFIA_BATCH_ACTIVE_LOOP(BK_A256, BA_BUILD)
     wrap_bin_body(lb, d.flag, 1, d.n, d.x, d.y, d.z, d.L, d.s_col, d.ncx, d.ix, d.iy, d.iz, d.rx,
                   d.ry, d.rz, d.col_of, d.col_count, d.col_key);
     SOFIA_BATCH_END
@@ -2316,7 +2314,7 @@ __global__ void k_wrap_bin_b(const BatchDev *__restrict__ tab) {
 
 __global__ void __launch_bounds__(1024) k_scan_cols_b(const BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_SCAN)
+    SOFIA_BATCH_ACTIVE_LOOP(BK_SCAN, BA_BUILD)
     scan_cols_body(lb, d.flag, 1, d.ncols, d.col_count, d.col_start, d.cl_start, d.ncl);
     __syncthreads();
     SOFIA_BATCH_END
@@ -2324,14 +2322,14 @@ __global__ void __launch_bounds__(1024) k_scan_cols_b(const BatchDev *__restrict
 
 __global__ void k_col_scatter_b(const BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_A256)
+    SOFIA_BATCH_ACTIVE_LOOP(BK_A256, BA_BUILD)
     col_scatter_body(lb, d.flag, 1, d.n, d.col_of, d.col_start, d.col_fill, d.col_atoms);
     SOFIA_BATCH_END
 }
 
 __global__ void k_col_sort_assign_b(const BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_COLS)
+    SOFIA_BATCH_ACTIVE_LOOP(BK_COLS, BA_BUILD)
     col_sort_assign_body(lb, d.flag, 1, d.ncols, d.col_start, d.col_atoms, d.col_key, d.cl_start,
                          d.slot_orig, d.cl_col, d.atom_slot, d.col_fill, d.status);
     __syncthreads();
@@ -2348,14 +2346,14 @@ __global__ void k_pack_b(const BatchDev *__restrict__ tab) {
 
 __global__ void k_bbox_b(const BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_LOOP(BK_C128)
+    SOFIA_BATCH_ACTIVE_LOOP(BK_C128, BA_PRUNE)
     bbox_body(lb, d.flag, 3, d.maxcl, d.ncl, d.rec, d.slot_orig, d.bb);
     SOFIA_BATCH_END
 }
 
 __global__ void __launch_bounds__(256) k_search_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_QUEUE_LOOP(BK_W256, BC_SEARCH)
+    SOFIA_BATCH_ACTIVE_QUEUE_LOOP(BK_W256, BA_BUILD, BC_SEARCH)
     SearchArgs a;
     a.cond = d.flag;
     a.cmask = 1;
@@ -2386,9 +2384,9 @@ __global__ void __launch_bounds__(256) k_search_b(BatchDev *__restrict__ tab) {
     SOFIA_BATCH_END
 }
 
-__global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune_b(BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(256, SOFIA_BATCH_PRUNE_MINB) k_prune_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_QUEUE_LOOP(BK_W256, BC_PRUNE)
+    SOFIA_BATCH_ACTIVE_QUEUE_LOOP(BK_W256, BA_PRUNE, BC_PRUNE)
     prune_body(lb, d.flag, 3, d.maxcl, d.ncl, d.recf, d.jlist, d.jmask, d.jcount, d.jcap,
                (float)d.L, d.rin2, d.rfar2, d.bb, d.ilist, d.imask, d.icount, d.slot_orig, d.x,
                d.y, d.z, d.px, d.py, d.pz);
@@ -2397,7 +2395,7 @@ __global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune_b(BatchDev *__r
 }
 
 template <typename T, bool EN, bool VIR, bool SAME>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2)
+__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_BATCH_PAIR_MINB) : 2)
     k_pair_b(BatchDev *__restrict__ tab, PairConst k) {
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_QUEUE_LOOP(BK_W256, BC_PAIR)
@@ -2429,6 +2427,49 @@ __global__ void k_red_stage2_b(const BatchDev *__restrict__ tab) {
     red_stage2_body(lb, RED_BLOCKS, 5, d.part, d.red, 1.0);
     __syncthreads();
     SOFIA_BATCH_END
+}
+
+// One block: the replicas whose trigger word has a bit of mask 1 (rebuild) or 3
+// (rebuild or prune) this step, and the prefixes of their virtual blocks per
+// kind, so the conditional kernels walk only blocks with work.  Runs after the
+// step's first kernel has set the trigger words.
+__global__ void __launch_bounds__(MAXREP) k_batch_active_b(BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    __shared__ int s_scan[MAXREP];
+    const int t = threadIdx.x;
+    const int nrep = tab->nrep;
+    const int f = (t < nrep) ? tab->rep[t].flag[0] : 0;
+    for (int m = 0; m < BA_N; ++m) {
+        const int mask = (m == BA_BUILD) ? 1 : 3;
+        const int on = (t < nrep && (f & mask)) ? 1 : 0;
+        // rank of this replica among the active ones (inclusive scan)
+        s_scan[t] = on;
+        __syncthreads();
+        for (int off = 1; off < MAXREP; off <<= 1) {
+            const int v = (t >= off) ? s_scan[t - off] : 0;
+            __syncthreads();
+            s_scan[t] += v;
+            __syncthreads();
+        }
+        const int rank = s_scan[t] - on;
+        if (on) tab->act[m][rank] = t;
+        if (t == MAXREP - 1) tab->nact[m] = s_scan[t];
+        __syncthreads();
+        for (int k = 0; k < BK_N; ++k) {
+            const int cnt = on ? (tab->pre[k][t + 1] - tab->pre[k][t]) : 0;
+            s_scan[t] = cnt;
+            __syncthreads();
+            for (int off = 1; off < MAXREP; off <<= 1) {
+                const int v = (t >= off) ? s_scan[t - off] : 0;
+                __syncthreads();
+                s_scan[t] += v;
+                __syncthreads();
+            }
+            if (t == 0) tab->apre[m][k][0] = 0;
+            if (on) tab->apre[m][k][rank + 1] = s_scan[t];
+            __syncthreads();
+        }
+    }
 }
 
 #undef SOFIA_BATCH_LOOP
@@ -2514,6 +2555,7 @@ void repdev_fill_pair(const Sys *s, RepDev *d) {
 void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
                      cudaStream_t st, int nsm) {
     const int g256 = nsm * 8, g128 = nsm * 16;
+    launch_pdl(k_batch_active_b, 1, MAXREP, 0, st, tab);
     launch_pdl(k_wrap_bin_b, g256, 256, 0, st, tab);
     launch_pdl(k_scan_cols_b, nsm * 2, 1024, 0, st, tab);
     launch_pdl(k_col_scatter_b, g256, 256, 0, st, tab);
@@ -2521,7 +2563,7 @@ void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
     launch_pdl(k_pack_b, g256, 256, 0, st, tab);
     launch_pdl(k_bbox_b, g128, 128, 0, st, tab);
     launch_pdl(k_search_b, g256, 256, 0, st, tab);
-    launch_pdl(k_prune_b, nsm * SOFIA_PRUNE_MINB, 256, 0, st, tab);
+    launch_pdl(k_prune_b, nsm * SOFIA_BATCH_PRUNE_MINB, 256, 0, st, tab);
     const PairConst k = make_pair_const(s0, nullptr);
     const size_t smem = sizeof(float4) * (size_t)s0->ntypes * s0->ntypes;
     if (precision == SOFIA_PREC_FP64) {
@@ -2534,8 +2576,8 @@ void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
             launch_pdl(k_pair_b<float, true, false, true>, nsm * SOFIA_PAIR_MINB_EN, 256, smem, st,
                        tab, k);
         else
-            launch_pdl(k_pair_b<float, false, false, true>, nsm * SOFIA_PAIR_MINB, 256, smem, st,
-                       tab, k);
+            launch_pdl(k_pair_b<float, false, false, true>, nsm * SOFIA_BATCH_PAIR_MINB, 256, smem,
+                       st, tab, k);
     }
     launch_pdl(k_unpack_b, g256, 256, 0, st, tab);
     if (energy) {

@@ -206,9 +206,18 @@ struct RepDev {
 // launch of a step; the step's first kernel clears them).
 enum BatchCounter { BC_SEARCH = 1, BC_PRUNE, BC_PAIR, BC_BONDED, BC_SHAKE, BC_N = 8 };
 
+// Replicas whose list trigger fired this step, per trigger mask: BA_BUILD
+// (bit 0: rebuild) and BA_PRUNE (bits 0-1: rebuild or prune).  The conditional
+// kernels walk only the virtual blocks of these replicas: apre[m][K] is the
+// prefix of kind-K blocks over the active replicas act[m][0 .. nact[m]).
+enum BatchActive { BA_BUILD = 0, BA_PRUNE = 1, BA_N = 2 };
+
 struct BatchDev {
     int nrep;
     int ctr[BC_N];
+    int nact[BA_N];
+    int act[BA_N][MAXREP];
+    int apre[BA_N][BK_N][MAXREP + 1];
     int pre[BK_N][MAXREP + 1];
     RepDev rep[MAXREP];
 };
@@ -245,6 +254,32 @@ struct BatchDev {
         const RepDev &d = tab->rep[r_];                                          \
         const int lb = vb - pre_[r_];
 #endif
+
+// Loops over the virtual blocks of kind KIND of the replicas active for trigger
+// mask M (BatchActive), statically (ACTIVE_LOOP) or from work-queue counter CTR
+// (ACTIVE_QUEUE_LOOP).  Inside, d is the replica's entry and lb the block index
+// within that replica.
+#define SOFIA_BATCH_ACTIVE_LOOP(KIND, M)                                         \
+    for (int vb = blockIdx.x;; vb += gridDim.x) {                                \
+        const int na_ = *reinterpret_cast<const volatile int *>(&tab->nact[M]);  \
+        const int *ap_ = tab->apre[M][KIND];                                     \
+        if (vb >= ap_[na_]) break;                                               \
+        const int a_ = batch_rep(ap_, na_, vb);                                  \
+        const RepDev &d = tab->rep[tab->act[M][a_]];                             \
+        const int lb = vb - ap_[a_];
+#define SOFIA_BATCH_ACTIVE_QUEUE_LOOP(KIND, M, CTR)                              \
+    __shared__ int s_vb_;                                                        \
+    for (;;) {                                                                   \
+        if (threadIdx.x == 0) s_vb_ = atomicAdd(&tab->ctr[CTR], 1);              \
+        __syncthreads();                                                         \
+        const int vb = s_vb_;                                                    \
+        __syncthreads();                                                         \
+        const int na_ = *reinterpret_cast<const volatile int *>(&tab->nact[M]);  \
+        const int *ap_ = tab->apre[M][KIND];                                     \
+        if (vb >= ap_[na_]) break;                                               \
+        const int a_ = batch_rep(ap_, na_, vb);                                  \
+        const RepDev &d = tab->rep[tab->act[M][a_]];                             \
+        const int lb = vb - ap_[a_];
 
 // Replica of virtual block vb: the last r with pre[r] <= vb.
 __device__ __forceinline__ int batch_rep(const int *__restrict__ pre, int nrep, int vb) {
