@@ -1423,6 +1423,7 @@ extern "C" int sofia_batch_create(sofia_nb_ctx *ctx, sofia_system *const *system
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
     int rc = batch_check_members(ctx, systems, n);
     if (rc) return rc;
+    SOFIA_CUDA(ctx, sofia::batch_pair_smem_optin(systems[0]->s.ntypes));
     sofia_batch *b = new sofia_batch();
     b->ctx = ctx;
     b->sys.assign(systems, systems + n);

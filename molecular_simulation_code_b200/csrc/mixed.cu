@@ -50,6 +50,17 @@ constexpr int MAX_COL = 2048;
 #ifndef SOFIA_PRUNE_MINB
 #define SOFIA_PRUNE_MINB 4
 #endif
+// FP32 energy kernels of systems with at most this many atom types read their
+// LJ parameters from a three-index table (i type pair, j type): one 16-byte
+// load gives both packed operands of a lane's two pairs, where the two-index
+// tables take two 8-byte loads for the force and two for the energy (0 = never).
+// The force-only kernel keeps the two-index tables: there the 16-byte loads
+// from many distinct addresses cost more shared-memory wavefronts than they
+// save instructions (0.468 -> 0.478 ms per launch at 275k atoms; the energy
+// kernel 0.556 -> 0.549 ms).
+#ifndef SOFIA_PAIR_TRI_MAX
+#define SOFIA_PAIR_TRI_MAX 10
+#endif
 // resident blocks per SM of the batched pair and prune kernels (their replica
 // arguments come from the device table, not the constant bank)
 #ifndef SOFIA_BATCH_PAIR_MINB
@@ -709,8 +720,9 @@ struct PairMath<double> {
 // pair arithmetic takes half the issue slots; only the MUFU operations, the
 // range tests and the selects stay per component.  Each component goes
 // through the same operations, in the same order and rounding, as
-// PairMath<float>::eval.  The LJ operands arrive as a = {lj1, -lj2} and
-// b = {lj3, -lj4} (b read only for energies).
+// PairMath<float>::eval.  The LJ operands arrive packed over the two pairs:
+// l1 = {lj1, lj1'}, l2n = {-lj2, -lj2'}, l3 = {lj3, lj3'}, l4n = {-lj4, -lj4'}
+// (l3, l4n read only for energies).
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
@@ -720,7 +732,7 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
 struct PairMath2 {
     template <bool EN, bool SAME>
     __device__ __forceinline__ static float2 eval(float2 dx, float2 dy, float2 dz, float2 qq,
-                                                  float2 a0, float2 a1, float2 b0, float2 b1,
+                                                  float2 l1, float2 l2n, float2 l3, float2 l4n,
                                                   bool on0, bool on1,
                                                   const PairConst &k, float2 &elj, float2 &ec) {
         const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
@@ -731,8 +743,7 @@ struct PairMath2 {
         const bool lj0_on = on0 && r2.x <= k.rcut2, lj1_on = on1 && r2.y <= k.rcut2;
         const bool c0_on = SAME ? lj0_on : (on0 && r2.x <= k.cut_coulsq);
         const bool c1_on = SAME ? lj1_on : (on1 && r2.y <= k.cut_coulsq);
-        const float2 flj =
-            mul2(dr6i, fma2(make_float2(a0.x, a1.x), dr6i, make_float2(a0.y, a1.y)));
+        const float2 flj = mul2(dr6i, fma2(l1, dr6i, l2n));
         const float2 pref = mul2(qq, rinv);
         const float2 kr = mul2(k.kexp2, r2);
         const float2 ex = make_float2(ex2_a(kr.x), ex2_a(kr.y));
@@ -743,9 +754,8 @@ struct PairMath2 {
         const float2 erfcc = mul2(mul2(t, poly), ex);
         const float2 fc = mul2(pref, fma2(k.f_shift2, r2, fma2(mul2(k.c2a2, ex), r, erfcc)));
         if (EN) {
-            const float2 b3 = make_float2(b0.x, b1.x), b4 = make_float2(b0.y, b1.y);
-            const float2 esh = mul2(k.ljs6_2, fma2(k.ljs6_2, b3, b4));
-            const float2 e6 = fma2(esh, make_float2(-1.0f, -1.0f), mul2(dr6i, fma2(dr6i, b3, b4)));
+            const float2 esh = mul2(k.ljs6_2, fma2(k.ljs6_2, l3, l4n));
+            const float2 e6 = fma2(esh, make_float2(-1.0f, -1.0f), mul2(dr6i, fma2(dr6i, l3, l4n)));
             const float2 sh = fma2(r, k.e_shift2, mul2(r2, k.f_shift2));
             const float2 e1 = mul2(pref, fma2(sh, make_float2(-1.0f, -1.0f), erfcc));
             elj = make_float2(lj0_on ? e6.x : 0.0f, lj1_on ? e6.y : 0.0f);
@@ -821,7 +831,7 @@ __device__ __forceinline__ void flush_i(long long *__restrict__ fi, int lane, T 
 // Integer addition makes every sum independent of the order of the atomics, so
 // results stay bit-reproducible.  EN adds the LJ and Coulomb energies, VIR the
 // diagonal virial (each pair once).
-template <typename T, bool EN, bool VIR, bool SAME>
+template <typename T, bool EN, bool VIR, bool SAME, bool TRI>
 __device__ __forceinline__ void pair_body(
     int bx, int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
@@ -833,6 +843,10 @@ __device__ __forceinline__ void pair_body(
     // so a force-only lookup reads 8 bytes (fewer shared-memory wavefronts)
     float2 *s_lja = reinterpret_cast<float2 *>(s_lj);
     float2 *s_ljb = s_lja + k.ntypes * k.ntypes;
+    // TRI: entry (a nt + b) nt + c = {lj1(a,c), lj1(b,c), -lj2(a,c), -lj2(b,c)} and,
+    // for energies, the same of lj3 / lj4 nt^3 entries further on
+    float4 *s_lj3 = reinterpret_cast<float4 *>(s_ljb + k.ntypes * k.ntypes);
+    const int nt3 = k.ntypes * k.ntypes * k.ntypes;
 
     __shared__ double s_sh[27 * 3];
     __shared__ long long s_fi[8][6 * 32];  // per warp and lane: i-force sums (see flush_i)
@@ -845,6 +859,15 @@ __device__ __forceinline__ void pair_body(
             s_ljb[t] = make_float2(l.z, -l.w);
         } else {
             s_lj[t] = l;
+        }
+    }
+    if (TRI) {
+        const int nt = k.ntypes;
+        for (int t = threadIdx.x; t < nt3; t += blockDim.x) {
+            const int a = t / (nt * nt), b = (t / nt) % nt, c = t % nt;
+            const float4 la = ljtab[a * nt + c], lb = ljtab[b * nt + c];
+            s_lj3[t] = make_float4(la.x, lb.x, -la.y, -lb.y);
+            if (EN) s_lj3[nt3 + t] = make_float4(la.z, lb.z, -la.w, -lb.w);
         }
     }
     if (threadIdx.x < 27) {
@@ -867,6 +890,7 @@ __device__ __forceinline__ void pair_body(
     const AtomRec ri0 = rec[icl * CL + q], ri1 = rec[icl * CL + q + 4];
     const T qiq0 = (T)k.coulpre * (T)ri0.q, qiq1 = (T)k.coulpre * (T)ri1.q;
     const int ti0 = ri0.type * k.ntypes, ti1 = ri1.type * k.ntypes;
+    const int t3 = (ri0.type * k.ntypes + ri1.type) * k.ntypes;  // this lane's TRI row
     const int n = jcount[icl];
     const int *row = jlist + (size_t)icl * jcap;
     const unsigned long long *mrow = jmask + (size_t)icl * jcap;
@@ -945,11 +969,29 @@ __device__ __forceinline__ void pair_body(
                     const float2 qq = mul2(qiq2, make_float2(rj.q, rj.q));
                     const bool on0 = (m0 >> lane) & 1u;
                     const bool on1 = (m1 >> lane) & 1u;
+                    float2 l1, l2n, l3 = z2, l4n = z2;
+                    if constexpr (TRI) {
+                        const float4 u = s_lj3[t3 + rj.type];
+                        l1 = make_float2(u.x, u.y);
+                        l2n = make_float2(u.z, u.w);
+                        if (EN) {
+                            const float4 v = s_lj3[nt3 + t3 + rj.type];
+                            l3 = make_float2(v.x, v.y);
+                            l4n = make_float2(v.z, v.w);
+                        }
+                    } else {
+                        const float2 a0 = s_lja[ti0 + rj.type], a1 = s_lja[ti1 + rj.type];
+                        l1 = make_float2(a0.x, a1.x);
+                        l2n = make_float2(a0.y, a1.y);
+                        if (EN) {
+                            const float2 b0 = s_ljb[ti0 + rj.type], b1 = s_ljb[ti1 + rj.type];
+                            l3 = make_float2(b0.x, b1.x);
+                            l4n = make_float2(b0.y, b1.y);
+                        }
+                    }
                     float2 elj = z2, ec = z2;
                     const float2 fs = PairMath2::template eval<EN, SAME>(
-                        dx, dy, dz, qq, s_lja[ti0 + rj.type], s_lja[ti1 + rj.type],
-                        EN ? s_ljb[ti0 + rj.type] : z2, EN ? s_ljb[ti1 + rj.type] : z2, on0, on1, k,
-                        elj, ec);
+                        dx, dy, dz, qq, l1, l2n, l3, l4n, on0, on1, k, elj, ec);
                     const float2 px = mul2(dx, fs), py = mul2(dy, fs), pz = mul2(dz, fs);
                     ax2 = add2(ax2, px);
                     ay2 = add2(ay2, py);
@@ -1008,7 +1050,7 @@ __device__ __forceinline__ void pair_body(
                 }
                 const T fj = reduce_j4<T>(v0, v1, v2, lane);
                 if (q < 3 && fj != (T)0)
-                    atomicAdd(jdst + jc * CL + jj, (unsigned long long)(-to_fix<T>(fj)));
+                    atomicAdd(jdst + jc * CL + jj, (unsigned long long)to_fix<T>(-fj));
             }
             if constexpr (PACK) {
                 flush_i<float>(fi, lane, ax2.x, ay2.x, az2.x, ax2.y, ay2.y, az2.y);
@@ -1084,15 +1126,47 @@ __device__ __forceinline__ void pair_body(
         }
     }
 }
-template <typename T, bool EN, bool VIR, bool SAME>
+template <typename T, bool EN, bool VIR, bool SAME, bool TRI = false>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2) k_pair(
     int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
     const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
     unsigned long long *__restrict__ fslot, double *__restrict__ energy) {
     SOFIA_PDL_ENTRY();
-    pair_body<T, EN, VIR, SAME>(blockIdx.x, maxcl, ncl_dev, rec, jlist, jmask, jcount, jcap,
+    pair_body<T, EN, VIR, SAME, TRI>(blockIdx.x, maxcl, ncl_dev, rec, jlist, jmask, jcount, jcap,
                                 ljtab, k, k.L, fslot, energy);
+}
+
+// Dynamic shared memory of the pair kernels: the two-index LJ table (nt^2
+// float4) and, with the three-index table, nt^3 float4 (twice for energies).
+inline bool pair_tri(int nt) { return nt >= 1 && nt <= SOFIA_PAIR_TRI_MAX; }
+inline size_t pair_smem(int nt, bool tri, bool energy) {
+    const size_t n2 = (size_t)nt * nt, n3 = n2 * nt;
+    return sizeof(float4) * (n2 + (tri ? (energy ? 2 : 1) * n3 : 0));
+}
+
+// Types up to the documented maximum (48) need more than the default 48 KB of
+// shared memory per block for the two-index table plus the kernels' static
+// arrays: raise the pair kernels' dynamic limit to what nt needs (once, on the
+// host, outside any stream capture).
+inline cudaError_t pair_smem_optin(int nt) {
+    static size_t done = 0;
+    const size_t need = pair_smem(nt, false, true);
+    if (need <= done || need <= 32768) return cudaSuccess;
+    const int v = (int)need;
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void *f) {
+        const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        if (r != cudaSuccess) e = r;
+    };
+    set((const void *)k_pair<double, true, true, true>);
+    set((const void *)k_pair<double, true, false, true>);
+    set((const void *)k_pair<double, false, false, true>);
+    set((const void *)k_pair<float, true, true, true>);
+    set((const void *)k_pair<float, true, false, true>);
+    set((const void *)k_pair<float, false, false, true>);
+    if (e == cudaSuccess) done = need;
+    return e;
 }
 
 // Slot-ordered fixed-point pair forces -> the caller's atom order (sets the
@@ -1717,7 +1791,9 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
     cudaStream_t st = ctx->stream;
     PairConst k = make_pair_const(s, nullptr);
     const int blocks = grid_for((long)s->max_clusters * 32, 256);
-    const size_t smem = sizeof(float4) * (size_t)s->ntypes * s->ntypes;
+    const size_t smem = pair_smem(s->ntypes, false, energy || virial);
+    const bool tri = (energy || virial) && pair_tri(s->ntypes);
+    const size_t smem3 = pair_smem(s->ntypes, tri, energy || virial);
     long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
               *fz = s->f[2].as<long long>();
 #define SOFIA_PAIR_ARGS                                                                   \
@@ -1733,6 +1809,13 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
             sofia::launch_pdl(k_pair<double, true, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
         else
             sofia::launch_pdl(k_pair<double, false, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
+    } else if (tri) {
+        if (virial)
+            sofia::launch_pdl(k_pair<float, true, true, true, true>, blocks, 256, smem3, st,
+                              SOFIA_PAIR_ARGS);
+        else
+            sofia::launch_pdl(k_pair<float, true, false, true, true>, blocks, 256, smem3, st,
+                              SOFIA_PAIR_ARGS);
     } else {
         if (virial)
             sofia::launch_pdl(k_pair<float, true, true, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
@@ -1869,6 +1952,7 @@ extern "C" int sofia_system_create(sofia_nb_ctx *ctx, const sofia_system_desc *d
     if (d->rcut != d->cut_coul)
         return sofia::fail(ctx, SOFIA_EINVAL, "the cluster path needs rcut == cut_coul%s");
     SOFIA_CUDA(ctx, cudaSetDevice(ctx->device));
+    SOFIA_CUDA(ctx, sofia::pair_smem_optin(d->ntypes));
     sofia_system *ss = new sofia_system();
     Sys *s = &ss->s;
     s->ctx = ctx;
@@ -2394,12 +2478,12 @@ __global__ void __launch_bounds__(256, SOFIA_BATCH_PRUNE_MINB) k_prune_b(BatchDe
     SOFIA_BATCH_END
 }
 
-template <typename T, bool EN, bool VIR, bool SAME>
+template <typename T, bool EN, bool VIR, bool SAME, bool TRI = false>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_BATCH_PAIR_MINB) : 2)
     k_pair_b(BatchDev *__restrict__ tab, PairConst k) {
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_QUEUE_LOOP(BK_W256, BC_PAIR)
-    pair_body<T, EN, VIR, SAME>(lb, d.maxcl, d.ncl, d.rec, d.ilist, d.imask, d.icount, d.jcap,
+    pair_body<T, EN, VIR, SAME, TRI>(lb, d.maxcl, d.ncl, d.rec, d.ilist, d.imask, d.icount, d.jcap,
                                 d.ljtab, k, d.L, d.fslot, d.energy);
     __syncthreads();
     SOFIA_BATCH_END
@@ -2552,6 +2636,24 @@ void repdev_fill_pair(const Sys *s, RepDev *d) {
     d->red = s->red.as<double>();
 }
 
+cudaError_t batch_pair_smem_optin(int nt) {
+    static size_t done = 0;
+    const size_t need = pair_smem(nt, false, true);
+    if (need <= done || need <= 32768) return cudaSuccess;
+    const int v = (int)need;
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void *f) {
+        const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        if (r != cudaSuccess) e = r;
+    };
+    set((const void *)k_pair_b<double, true, false, true>);
+    set((const void *)k_pair_b<double, false, false, true>);
+    set((const void *)k_pair_b<float, true, false, true>);
+    set((const void *)k_pair_b<float, false, false, true>);
+    if (e == cudaSuccess) done = need;
+    return e;
+}
+
 void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
                      cudaStream_t st, int nsm) {
     const int g256 = nsm * 8, g128 = nsm * 16;
@@ -2565,12 +2667,17 @@ void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
     launch_pdl(k_search_b, g256, 256, 0, st, tab);
     launch_pdl(k_prune_b, nsm * SOFIA_BATCH_PRUNE_MINB, 256, 0, st, tab);
     const PairConst k = make_pair_const(s0, nullptr);
-    const size_t smem = sizeof(float4) * (size_t)s0->ntypes * s0->ntypes;
+    const size_t smem = pair_smem(s0->ntypes, false, energy);
+    const bool tri = energy && pair_tri(s0->ntypes);
+    const size_t smem3 = pair_smem(s0->ntypes, tri, energy);
     if (precision == SOFIA_PREC_FP64) {
         if (energy)
             launch_pdl(k_pair_b<double, true, false, true>, nsm * 2, 256, smem, st, tab, k);
         else
             launch_pdl(k_pair_b<double, false, false, true>, nsm * 2, 256, smem, st, tab, k);
+    } else if (tri) {
+        launch_pdl(k_pair_b<float, true, false, true, true>, nsm * SOFIA_PAIR_MINB_EN, 256, smem3,
+                   st, tab, k);
     } else {
         if (energy)
             launch_pdl(k_pair_b<float, true, false, true>, nsm * SOFIA_PAIR_MINB_EN, 256, smem, st,

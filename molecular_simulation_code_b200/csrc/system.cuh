@@ -301,6 +301,8 @@ void repdev_fill_pair(const Sys *s, RepDev *d);
 // Langevin force, and (energy) the pair-energy sums.  All replicas share the
 // pair constants k (all but the box) and the precision.
 // nsm: multiprocessors of the device (the grid-stride launches are sized from it).
+// raises the batched pair kernels' dynamic shared-memory limit for nt atom types
+cudaError_t batch_pair_smem_optin(int nt);
 void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
                      cudaStream_t st, int nsm);
 // The pair constants a captured batch graph holds (everything but the box).
