@@ -1405,7 +1405,7 @@ static int batch_upload(sofia_batch *b) {
         const int cnt[sofia::BK_N] = {
             sofia::grid_for(s->n, 256), 1, s->ncols, sofia::grid_for((long)s->max_clusters * 8, 256),
             sofia::grid_for(s->max_clusters, 128), sofia::grid_for((long)s->max_clusters * 32, 256),
-            sofia::grid_for(nterm, 128), sofia::grid_for(s->md.nshake, 128), sofia::RED_BLOCKS,
+            sofia::grid_for((long)s->max_clusters * 32, 256 * sofia::GRAIN), sofia::grid_for(nterm, 128), sofia::grid_for(s->md.nshake, 128), sofia::RED_BLOCKS,
             1, sofia::MD_NJOB * sofia::MRED, sofia::MD_NJOB};
         for (int k = 0; k < sofia::BK_N; ++k) h->pre[k][r + 1] = h->pre[k][r] + cnt[k];
     }

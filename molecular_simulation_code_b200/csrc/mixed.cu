@@ -2437,7 +2437,7 @@ __global__ void k_bbox_b(const BatchDev *__restrict__ tab) {
 
 __global__ void __launch_bounds__(256) k_search_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_ACTIVE_QUEUE_LOOP(BK_W256, BA_BUILD, BC_SEARCH)
+    SOFIA_BATCH_ACTIVE_QUEUE_LOOP(BK_W1024, BA_BUILD, BC_SEARCH)
     SearchArgs a;
     a.cond = d.flag;
     a.cmask = 1;
@@ -2463,18 +2463,24 @@ __global__ void __launch_bounds__(256) k_search_b(BatchDev *__restrict__ tab) {
     a.jcount = d.jcount;
     a.jmask = d.jmask;
     a.status = d.status;
-    search_body(lb, a);
-    __syncthreads();
+    const int nb = (d.maxcl * 32 + 255) / 256;
+    for (int g = lb * GRAIN; g < nb && g < (lb + 1) * GRAIN; ++g) {
+        search_body(g, a);
+        __syncthreads();
+    }
     SOFIA_BATCH_END
 }
 
 __global__ void __launch_bounds__(256, SOFIA_BATCH_PRUNE_MINB) k_prune_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_ACTIVE_QUEUE_LOOP(BK_W256, BA_PRUNE, BC_PRUNE)
-    prune_body(lb, d.flag, 3, d.maxcl, d.ncl, d.recf, d.jlist, d.jmask, d.jcount, d.jcap,
-               (float)d.L, d.rin2, d.rfar2, d.bb, d.ilist, d.imask, d.icount, d.slot_orig, d.x,
-               d.y, d.z, d.px, d.py, d.pz);
-    __syncthreads();
+    SOFIA_BATCH_ACTIVE_QUEUE_LOOP(BK_W1024, BA_PRUNE, BC_PRUNE)
+    const int nb = (d.maxcl * 32 + 255) / 256;
+    for (int g = lb * GRAIN; g < nb && g < (lb + 1) * GRAIN; ++g) {
+        prune_body(g, d.flag, 3, d.maxcl, d.ncl, d.recf, d.jlist, d.jmask, d.jcount, d.jcap,
+                   (float)d.L, d.rin2, d.rfar2, d.bb, d.ilist, d.imask, d.icount, d.slot_orig,
+                   d.x, d.y, d.z, d.px, d.py, d.pz);
+        __syncthreads();
+    }
     SOFIA_BATCH_END
 }
 
@@ -2516,43 +2522,62 @@ __global__ void k_red_stage2_b(const BatchDev *__restrict__ tab) {
 // One block: the replicas whose trigger word has a bit of mask 1 (rebuild) or 3
 // (rebuild or prune) this step, and the prefixes of their virtual blocks per
 // kind, so the conditional kernels walk only blocks with work.  Runs after the
-// step's first kernel has set the trigger words.
+// step's first kernel has set the trigger words.  Thread t is replica t; all
+// 2 x (1 + BK_N) prefix sums are taken at once (warp shuffles, then the warp
+// totals through shared memory).
 __global__ void __launch_bounds__(MAXREP) k_batch_active_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    __shared__ int s_scan[MAXREP];
-    const int t = threadIdx.x;
+    constexpr int NK = BK_N + 1;       // per mask: the active count, then one per kind
+    constexpr int NV = BA_N * NK;
+    constexpr int NW = MAXREP / 32;
+    __shared__ int s_w[NW][NV];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int nrep = tab->nrep;
     const int f = (t < nrep) ? tab->rep[t].flag[0] : 0;
+    int cnt[BK_N];
+#pragma unroll
+    for (int k = 0; k < BK_N; ++k)
+        cnt[k] = (t < nrep) ? tab->pre[k][t + 1] - tab->pre[k][t] : 0;
+    bool on[BA_N];
+    int v[NV];
+#pragma unroll
     for (int m = 0; m < BA_N; ++m) {
-        const int mask = (m == BA_BUILD) ? 1 : 3;
-        const int on = (t < nrep && (f & mask)) ? 1 : 0;
-        // rank of this replica among the active ones (inclusive scan)
-        s_scan[t] = on;
-        __syncthreads();
-        for (int off = 1; off < MAXREP; off <<= 1) {
-            const int v = (t >= off) ? s_scan[t - off] : 0;
-            __syncthreads();
-            s_scan[t] += v;
-            __syncthreads();
+        on[m] = (f & (m == BA_BUILD ? 1 : 3)) != 0;
+        v[m * NK] = on[m] ? 1 : 0;
+#pragma unroll
+        for (int k = 0; k < BK_N; ++k) v[m * NK + 1 + k] = on[m] ? cnt[k] : 0;
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const int x = __shfl_up_sync(FULL, v[i], off);
+            if (lane >= off) v[i] += x;
         }
-        const int rank = s_scan[t] - on;
-        if (on) tab->act[m][rank] = t;
-        if (t == MAXREP - 1) tab->nact[m] = s_scan[t];
-        __syncthreads();
-        for (int k = 0; k < BK_N; ++k) {
-            const int cnt = on ? (tab->pre[k][t + 1] - tab->pre[k][t]) : 0;
-            s_scan[t] = cnt;
-            __syncthreads();
-            for (int off = 1; off < MAXREP; off <<= 1) {
-                const int v = (t >= off) ? s_scan[t - off] : 0;
-                __syncthreads();
-                s_scan[t] += v;
-                __syncthreads();
-            }
-            if (t == 0) tab->apre[m][k][0] = 0;
-            if (on) tab->apre[m][k][rank + 1] = s_scan[t];
-            __syncthreads();
+    }
+    if (lane == 31) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) s_w[w][i] = v[i];
+    }
+    __syncthreads();
+    for (int ww = 0; ww < w; ++ww) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] += s_w[ww][i];
+    }
+    // v[] now holds inclusive prefixes over replicas 0..t
+#pragma unroll
+    for (int m = 0; m < BA_N; ++m) {
+        const int rank = v[m * NK] - (on[m] ? 1 : 0);
+        if (on[m]) {
+            tab->act[m][rank] = t;
+#pragma unroll
+            for (int k = 0; k < BK_N; ++k) tab->apre[m][k][rank + 1] = v[m * NK + 1 + k];
         }
+        if (t == 0) {
+#pragma unroll
+            for (int k = 0; k < BK_N; ++k) tab->apre[m][k][0] = 0;
+        }
+        if (t == MAXREP - 1) tab->nact[m] = v[m * NK];
     }
 }
 

@@ -154,6 +154,7 @@ enum BatchKind {
     BK_S256,      // ceil(max_clusters * 8 / 256): per-slot kernels
     BK_C128,      // ceil(max_clusters / 128): cluster boxes
     BK_W256,      // ceil(max_clusters * 32 / 256): warp-per-cluster kernels
+    BK_W1024,     // ceil(max_clusters * 32 / (256 GRAIN)): grains of BK_W256 blocks (search, prune)
     BK_B128,      // ceil(bonded terms / 128)
     BK_G128,      // ceil(SHAKE groups / 128)
     BK_RED,       // RED_BLOCKS: stage 1 of the pair-energy sums
@@ -163,6 +164,14 @@ enum BatchKind {
     BK_N
 };
 constexpr int MAXREP = 256;
+// The batched search and prune take grains of GRAIN consecutive 256-thread
+// blocks of one replica per work-queue pop: their blocks are short, and the
+// pop (an atomic, two barriers and the replica lookup) would otherwise take a
+// large share of each block's time.
+#ifndef SOFIA_BATCH_GRAIN
+#define SOFIA_BATCH_GRAIN 2
+#endif
+constexpr int GRAIN = SOFIA_BATCH_GRAIN;
 constexpr int RED_BLOCKS = 128;  // blocks of stage 1 of the pair-energy sums
 constexpr int MD_NJOB = 7;  // bonds, angles, torsion, coul14, lj14, impropers, kinetic
 

@@ -55,28 +55,40 @@ def bench_batch(args):
             m.set_state(r.xyz.astype(np.float64), r.velocity.astype(np.float64))
             m.md_setup(r, dt=1.0, gamma=0.02, seed=7)
             systems.append(m)
-        b = Batch(master, systems)
-        b.run(50)  # damped relaxation from the lattice start
-        for m, r in zip(systems, reps):
-            m.md_setup(r, dt=2.0, gamma=0.001, seed=8)
-        b.close()
-        b = Batch(master, systems)
-        b.run(args.segment)  # warm-up segment (also captures the graphs)
+        # the same preparation as the single-system benchmark: damped relaxation from
+        # the lattice start (100 x 1 fs), 300 K equilibration with strong coupling
+        # (400 x 2 fs), then the production coupling (gamma = 1/ps)
+        stages = ((1.0, 0.02, 100, 7), (2.0, 0.02, 400, 8), (2.0, 0.001, args.segment, 9))
+        for k, (dt, gamma, nsteps, seed) in enumerate(stages):
+            for m, r in zip(systems, reps):
+                m.md_setup(r, dt=dt, gamma=gamma, seed=seed)
+            b = Batch(master, systems)
+            b.run(nsteps)  # the last stage is the warm-up segment (captures the graphs)
+            if k < len(stages) - 1:
+                b.close()
         torch.cuda.synchronize()
+        st0 = [m.stats() for m in systems]
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.nvtx.range_push(f"batch_timed_{name}")  # lets ncu select the timed steps
         e0.record(stream)
         for _ in range(args.segments):
-            b.run(args.segment, energy_every=args.segment)
+            en = b.run(args.segment, energy_every=args.segment)
         e1.record(stream)
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         t = e0.elapsed_time(e1) / 1e3
         steps = args.segments * args.segment
+        st1 = [m.stats() for m in systems]
+        rsteps = len(reps) * steps
         out[name] = {"atom_steps_per_s": out["atoms_total"] * steps / t,
-                     "replica_steps_per_s": len(reps) * steps / t,
-                     "ms_per_batch_step": 1e3 * t / steps}
+                     "replica_steps_per_s": rsteps / t,
+                     "ms_per_batch_step": 1e3 * t / steps,
+                     "temperature_K_mean": float(np.mean([e["temperature"] for e in en])),
+                     "list_builds_per_replica_step":
+                         sum(b1["builds"] - b0["builds"] for b0, b1 in zip(st0, st1)) / rsteps,
+                     "prunes_per_replica_step":
+                         sum(b1["prunes"] - b0["prunes"] for b0, b1 in zip(st0, st1)) / rsteps}
         b.close()
         for m in systems:
             m.close()
