@@ -99,13 +99,17 @@ def apply_shape(system: M.System, shape):
 def autotune(ctx: Context, sysdata, aspects=ASPECTS, margins=(0.4, 0.6, 0.8), steps: int = 40,
              cut: float = 10.0, skin: float = 2.0, precision: int = M.MIXED):
     """Fastest (cluster aspect, prune margin) for this replica: short Langevin
-    segments timed with CUDA events, every candidate from the same state."""
+    segments timed with CUDA events, every candidate from the same 300 K state
+    (damped relaxation from the lattice start, then strong-coupling 2 fs steps,
+    as the benchmarks prepare their systems)."""
     import torch
     stream = torch.cuda.ExternalStream(ctx._lib.sofia_stream(ctx.handle))
     base = M.System(ctx, sysdata, cut=cut, skin=skin, precision=precision)
     base.set_state(sysdata.xyz.astype(np.float64), sysdata.velocity.astype(np.float64))
     base.md_setup(sysdata, dt=1.0, gamma=0.02, seed=1)
-    base.md_run(30)
+    base.md_run(100)
+    base.md_setup(sysdata, dt=2.0, gamma=0.02, seed=3)
+    base.md_run(200)
     x, v, _ = base.get_state()
     base.close()
     times = {}

@@ -922,12 +922,15 @@ __device__ __forceinline__ void pair_body(
                 const double zj = rj.z + s_sh[img * 3 + 2];
                 T v0 = 0, v1 = 0, v2 = 0;  // the entry's force on j atom jj (negated)
                 const unsigned m0 = (unsigned)mm, m1 = (unsigned)(mm >> 32);
+                // the lane's two i positions {q, q + 4} per component
+                const double2 pix = make_double2(ri0.x, ri1.x), piy = make_double2(ri0.y, ri1.y),
+                              piz = make_double2(ri0.z, ri1.z);
                 if (PACK && SOFIA_PAIR_HYBRID && (m0 == 0u || m1 == 0u)) {
                     // one i half without pairs in range: scalar evaluation of the other
                     // (a warp-uniform branch per half, so no selects of i data)
                     const bool h1 = m0 == 0u;
-                    const double xi = h1 ? ri1.x : ri0.x, yi = h1 ? ri1.y : ri0.y,
-                                 zi = h1 ? ri1.z : ri0.z;
+                    const double xi = h1 ? pix.y : pix.x, yi = h1 ? piy.y : piy.x,
+                                 zi = h1 ? piz.y : piz.x;
                     const float dx = (float)(xi - xj);
                     const float dy = (float)(yi - yj);
                     const float dz = (float)(zi - zj);
@@ -963,9 +966,9 @@ __device__ __forceinline__ void pair_body(
                 } else if constexpr (PACK) {
                     // both i halves at once; a half without pairs in range is computed
                     // and masked (the packed instructions cost the same for one or two)
-                    const float2 dx = make_float2((float)(ri0.x - xj), (float)(ri1.x - xj));
-                    const float2 dy = make_float2((float)(ri0.y - yj), (float)(ri1.y - yj));
-                    const float2 dz = make_float2((float)(ri0.z - zj), (float)(ri1.z - zj));
+                    const float2 dx = make_float2((float)(pix.x - xj), (float)(pix.y - xj));
+                    const float2 dy = make_float2((float)(piy.x - yj), (float)(piy.y - yj));
+                    const float2 dz = make_float2((float)(piz.x - zj), (float)(piz.y - zj));
                     const float2 qq = mul2(qiq2, make_float2(rj.q, rj.q));
                     const bool on0 = (m0 >> lane) & 1u;
                     const bool on1 = (m1 >> lane) & 1u;
