@@ -51,6 +51,23 @@ enum StatusSlot {
     ST_NSLOTS = 16
 };
 
+// Bit transpose of an 8 x 4 bit matrix held in one word: the bit at position
+// 4 j + i (j = 0..7, i = 0..3) moves to position 8 i + j.  The permutation of
+// the five index bits (j2 j1 j0 i1 i0) -> (i1 i0 j2 j1 j0) is done as four
+// exchanges of index-bit pairs, (1,0), (2,0), (3,1), (4,2), each one delta swap
+// (bits at positions p with index bit a clear and b set trade places with p + d,
+// d = 2^a - 2^b).
+__host__ __device__ inline uint32_t delta_swap(uint32_t x, uint32_t m, int d) {
+    const uint32_t t = ((x >> d) ^ x) & m;
+    return x ^ t ^ (t << d);
+}
+__host__ __device__ inline uint32_t transpose_8x4(uint32_t x) {
+    x = delta_swap(x, 0x22222222u, 1);
+    x = delta_swap(x, 0x0a0a0a0au, 3);
+    x = delta_swap(x, 0x00cc00ccu, 6);
+    return delta_swap(x, 0x0000f0f0u, 12);
+}
+
 }  // namespace sofia
 
 struct sofia_nb_ctx {

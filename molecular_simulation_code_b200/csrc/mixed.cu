@@ -1306,35 +1306,38 @@ __device__ __forceinline__ void prune_body(int bx,
                 // the j cluster's x[8], y[8], z[8]: three 16-byte loads per 4 atoms
                 // (one half at a time keeps the kernel within 64 registers)
                 const float4 *cj = reinterpret_cast<const float4 *>(recf + (size_t)jc * 3 * CL);
+                // r2 < rin2 exactly when the rounded r2 - rin2 is negative (a
+                // difference of two floats is zero only when they are equal), so
+                // its sign bit is the in-range bit, and one funnel shift appends it.
+                // Appended for j atoms 7 down to 0 and, within one, i atoms 3 down
+                // to 0 (7 down to 4 in hi), bit (jj, ii) ends at 4 jj + ii; the
+                // final transpose moves it to 8 ii + jj.
+                const float2 nrin2 = make_float2(-rin2, -rin2);
 #pragma unroll 1
-                for (int hh = 0; hh < 2; ++hh) {
+                for (int hh = 1; hh >= 0; --hh) {
                     const float4 jx = __ldg(&cj[hh]), jy = __ldg(&cj[2 + hh]),
                                  jz = __ldg(&cj[4 + hh]);
-                    // j atom jj = 4*hh + q: bit 8*(ii & 3) + jj of lo (i atoms 0-3)
-                    // or hi (4-7)
-                    const int sh = 4 * hh;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        // -(x_j + shift): adding it rounds exactly like x_i - (x_j + shift)
+                    for (int q = 3; q >= 0; --q) {
                         const float nx = -((&jx.x)[q] + sx), ny = -((&jy.x)[q] + sy),
                                     nz = -((&jz.x)[q] + sz);
                         const float2 nx2 = make_float2(nx, nx), ny2 = make_float2(ny, ny),
                                      nz2 = make_float2(nz, nz);
 #pragma unroll
-                        for (int pp = 0; pp < CL / 2; ++pp) {
+                        for (int pp = CL / 2 - 1; pp >= 0; --pp) {
                             // i atoms 2pp (component x) and 2pp + 1 (component y)
                             const float2 dx = add2(xi[pp], nx2), dy = add2(yi[pp], ny2),
                                          dz = add2(zi[pp], nz2);
                             const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
-                            const unsigned in = ((r2.x < rin2 ? 1u : 0u) |
-                                                 (r2.y < rin2 ? (1u << 8) : 0u)) << sh;
-                            if (pp < 2)
-                                lo |= in << (16 * pp + q);
-                            else
-                                hi |= in << (16 * (pp - 2) + q);
+                            const float2 dd = add2(r2, nrin2);
+                            unsigned &acc = (pp >= 2) ? hi : lo;
+                            acc = __funnelshift_l(__float_as_uint(dd.y), acc, 1);
+                            acc = __funnelshift_l(__float_as_uint(dd.x), acc, 1);
                         }
                     }
                 }
+                lo = transpose_8x4(lo);
+                hi = transpose_8x4(hi);
             }
         }
         const unsigned long long newm = (((unsigned long long)hi << 32) | lo) & m;
