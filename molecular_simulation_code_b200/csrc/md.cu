@@ -1168,11 +1168,39 @@ namespace {
         const int lb = vb - pre_[r_];
 #define SOFIA_BATCH_END }
 
+// Segment start for every replica in one launch: the snapshot a list regrow
+// restarts from (positions, velocities, step counter) and cleared status words.
+__global__ void k_snapshot_b(const BatchDev *__restrict__ tab) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_A256)
+    const int i = lb * blockDim.x + threadIdx.x;
+    if (i < d.n) {
+        d.snap[0][i] = d.x[i];
+        d.snap[1][i] = d.y[i];
+        d.snap[2][i] = d.z[i];
+        d.snap[3][i] = d.vx[i];
+        d.snap[4][i] = d.vy[i];
+        d.snap[5][i] = d.vz[i];
+    }
+    if (lb == 0 && threadIdx.x == 0) d.snap_step[0] = d.step[0];
+    if (lb == 0 && threadIdx.x < ST_NSLOTS) d.status[threadIdx.x] = 0;
+    SOFIA_BATCH_END
+}
+
+// The status words and the 16 energy sums of every replica into two arrays
+// (replica r at r * ST_NSLOTS and r * 16), each read back with one copy.
+__global__ void k_status_b(const BatchDev *__restrict__ tab, int *__restrict__ out,
+                           double *__restrict__ eout) {
+    SOFIA_PDL_ENTRY();
+    SOFIA_BATCH_LOOP(BK_REP)
+    const int r = (int)(&d - tab->rep);
+    if (threadIdx.x < ST_NSLOTS) out[r * ST_NSLOTS + threadIdx.x] = d.status[threadIdx.x];
+    if (threadIdx.x < 16) eout[r * 16 + threadIdx.x] = d.ered[threadIdx.x];
+    SOFIA_BATCH_END
+}
+
 __global__ void k_kick_drift_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    // the step's first kernel: clear the work-queue counters of the later ones
-    // (each of them starts after this grid has completed)
-    if (blockIdx.x == 0 && threadIdx.x < BC_N) tab->ctr[threadIdx.x] = 0;
     SOFIA_BATCH_LOOP(BK_A256)
     kick_drift_body(lb, d.n, d.h, d.invm, d.fx, d.fy, d.fz, d.vx, d.vy, d.vz, d.dt, d.x, d.y,
                     d.z, d.rx, d.ry, d.rz, d.px, d.py, d.pz, d.L, d.lim2, d.plim2, d.flag,
@@ -1270,6 +1298,8 @@ static void repdev_fill_md(Sys *s, RepDev *d) {
     d->shake = md.shake.as<int>();
     d->sbond = md.sbond.as<double>();
     d->step = md.step_dev.as<long long>();
+    for (int c = 0; c < 6; ++c) d->snap[c] = md.snap[c].as<double>();
+    d->snap_step = md.snap[6].as<long long>();
     LangevinArgs lg{};
     if (md.gamma > 0.0) {
         const double kT = KBOLTZ * md.temperature;
@@ -1325,10 +1355,10 @@ static void repdev_fill_md(Sys *s, RepDev *d) {
 
 // One batched MD step: the same kernels, in the same order, as md_step.
 static void batch_step(BatchDev *tab, Sys *s0, bool energy, bool rattle, cudaStream_t st,
-                       int nsm) {
+                       int nsm, int pair_blocks) {
     const int g256 = nsm * 8, g128 = nsm * 16;
     launch_pdl(k_kick_drift_b, g256, 256, 0, st, tab);
-    batch_pair_path(tab, s0, s0->precision, energy, st, nsm);
+    batch_pair_path(tab, s0, s0->precision, energy, st, nsm, pair_blocks);
     if (energy)
         launch_pdl(k_bonded_b<true>, g128, 128, 0, st, tab);
     else
@@ -1351,6 +1381,9 @@ struct sofia_batch {
     std::vector<sofia_system *> sys;
     sofia::DevBuf tab;                  // BatchDev on the device
     std::vector<unsigned char> htab;    // its host image
+    sofia::DevBuf stat, estat;          // every replica's status words and energy sums
+    std::vector<int> hstat;             // their host copies
+    std::vector<double> hestat;
     int seg = 100;                      // steps per captured segment graph
     int nsm = 148;
     // captured graphs: [0] one step, [1] one step with energies, [2] seg steps,
@@ -1409,7 +1442,7 @@ static int batch_upload(sofia_batch *b) {
         const int cnt[sofia::BK_N] = {
             sofia::grid_for(s->n, 256), 1, s->ncols, sofia::grid_for((long)s->max_clusters * 8, 256),
             sofia::grid_for(s->max_clusters, 128), sofia::grid_for((long)s->max_clusters * 32, 256),
-            sofia::grid_for((long)s->max_clusters * 32, 256 * sofia::GRAIN), sofia::grid_for(nterm, 128), sofia::grid_for(s->md.nshake, 128), sofia::RED_BLOCKS,
+            sofia::grid_for(nterm, 128), sofia::grid_for(s->md.nshake, 128), sofia::RED_BLOCKS,
             1, sofia::MD_NJOB * sofia::MRED, sofia::MD_NJOB};
         for (int k = 0; k < sofia::BK_N; ++k) h->pre[k][r + 1] = h->pre[k][r] + cnt[k];
     }
@@ -1441,6 +1474,8 @@ extern "C" int sofia_batch_destroy(sofia_batch *b) {
     if (b->ctx) cudaStreamSynchronize(b->ctx->stream);
     batch_drop_graphs(b);
     b->tab.release();
+    b->stat.release();
+    b->estat.release();
     delete b;
     return SOFIA_OK;
 }
@@ -1485,11 +1520,14 @@ static int batch_capture(sofia_batch *b) {
     bool rat = false;
     for (auto *s : b->sys) rat = rat || (s->s.md.rattle && s->s.md.nshake);
     const int nsteps[4] = {1, 1, b->seg, b->seg};
+    const auto *h = reinterpret_cast<const sofia::BatchDev *>(b->htab.data());
+    const int pair_blocks = h->pre[sofia::BK_W256][h->nrep];
     for (int g = 0; g < 4; ++g) {
         cudaGraph_t graph = nullptr;
         SOFIA_CUDA(ctx, cudaStreamBeginCapture(ms, cudaStreamCaptureModeThreadLocal));
         for (int k = 0; k < nsteps[g]; ++k)
-            sofia::batch_step(tab, s0, (g & 1) && k == nsteps[g] - 1, rat, ms, b->nsm);
+            sofia::batch_step(tab, s0, (g & 1) && k == nsteps[g] - 1, rat, ms, b->nsm,
+                              pair_blocks);
         cudaError_t ce = cudaStreamEndCapture(ms, &graph);
         if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaStreamEndCapture (batch)");
         ce = cudaGraphInstantiate(&b->graph[g], graph, 0);
@@ -1518,27 +1556,32 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
     cudaStream_t ms = ctx->stream;
     const int n = (int)b->sys.size();
     const bool want_e = energy_every > 0 && nsteps > 0;
+    SOFIA_CUDA(ctx, b->stat.ensure(sizeof(int) * sofia::ST_NSLOTS * sofia::MAXREP));
+    SOFIA_CUDA(ctx, b->estat.ensure(sizeof(double) * 16 * sofia::MAXREP));
+    b->hstat.resize((size_t)sofia::ST_NSLOTS * n);
+    b->hestat.resize((size_t)16 * n);
     for (int attempt = 0; attempt < 4; ++attempt) {
-        for (int i = 0; i < n; ++i) {
-            Sys *s = &b->sys[i]->s;
-            Md &md = s->md;
-            cudaStream_t st = s->ctx->stream;
-            const size_t nb = sizeof(double) * (size_t)s->n;
-            for (int d = 0; d < 3; ++d) {
-                SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[d].p, s->x[d].p, nb, cudaMemcpyDeviceToDevice, st));
-                SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[3 + d].p, s->v[d].p, nb, cudaMemcpyDeviceToDevice, st));
-            }
-            SOFIA_CUDA(ctx, cudaMemcpyAsync(md.snap[6].p, md.step_dev.p, sizeof(long long), cudaMemcpyDeviceToDevice, st));
-            SOFIA_CUDA(ctx, cudaMemsetAsync(s->status_local.p, 0, sizeof(int) * sofia::ST_NSLOTS, st));
-            if (!md.forces_valid) {
-                int rc = sofia::md_forces(s, false, true);
-                if (rc) return rc;
-                md.forces_valid = 1;
-            }
-        }
+        // work the caller queued on the members' own streams comes first
         for (int i = 0; i < n; ++i) SOFIA_CUDA(ctx, cudaStreamSynchronize(b->sys[i]->s.ctx->stream));
         int rc = batch_upload(b);
         if (rc) return rc;
+        auto *tab = b->tab.as<sofia::BatchDev>();
+        // snapshots and cleared status words for all members in one launch, before
+        // any initial force evaluation (whose list build reports into the status)
+        SOFIA_CUDA(ctx, sofia::launch_pdl(sofia::k_snapshot_b, b->nsm * 8, 256, 0, ms, tab));
+        bool stale = false;
+        for (int i = 0; i < n; ++i) stale = stale || !b->sys[i]->s.md.forces_valid;
+        if (stale) {
+            SOFIA_CUDA(ctx, cudaStreamSynchronize(ms));
+            for (int i = 0; i < n; ++i) {
+                Sys *s = &b->sys[i]->s;
+                if (s->md.forces_valid) continue;
+                rc = sofia::md_forces(s, false, true);
+                if (rc) return rc;
+                s->md.forces_valid = 1;
+                SOFIA_CUDA(ctx, cudaStreamSynchronize(s->ctx->stream));
+            }
+        }
         if (!b->graph_ok) {
             rc = batch_capture(b);
             if (rc) return rc;
@@ -1553,12 +1596,21 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
             launched += (long long)k * b->step_launches[0] + (en ? 6 : 0);
             left -= k;
         }
+        SOFIA_CUDA(ctx, sofia::launch_pdl(sofia::k_status_b, b->nsm, 32, 0, ms, tab,
+                                          b->stat.as<int>(), b->estat.as<double>()));
+        SOFIA_CUDA(ctx, cudaMemcpyAsync(b->hstat.data(), b->stat.p,
+                                        sizeof(int) * sofia::ST_NSLOTS * (size_t)n,
+                                        cudaMemcpyDeviceToHost, ms));
+        if (energies && want_e)
+            SOFIA_CUDA(ctx, cudaMemcpyAsync(b->hestat.data(), b->estat.p,
+                                            sizeof(double) * 16 * (size_t)n,
+                                            cudaMemcpyDeviceToHost, ms));
         SOFIA_CUDA(ctx, cudaStreamSynchronize(ms));
         bool regrow = false;
         for (int i = 0; i < n; ++i) {
             Sys *s = &b->sys[i]->s;
             s->launches += launched / (n > 0 ? n : 1);
-            const int r2 = sofia::sys_list_overflow(s);
+            const int r2 = sofia::sys_list_overflow(s, &b->hstat[(size_t)sofia::ST_NSLOTS * i]);
             if (r2 == SOFIA_ENEEDGROW) {
                 regrow = true;
                 continue;
@@ -1588,17 +1640,14 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
         for (int i = 0; i < n; ++i) {
             Sys *s = &b->sys[i]->s;
             Md &md = s->md;
-            int hs[sofia::ST_NSLOTS];
-            SOFIA_CUDA(ctx, cudaMemcpy(hs, s->status_local.p, sizeof(hs), cudaMemcpyDeviceToHost));
+            const int *hs = &b->hstat[(size_t)sofia::ST_NSLOTS * i];
             if (hs[sofia::ST_SHAKE])
                 return sofia::fail(ctx, SOFIA_ESTATE, "SHAKE determinant <= 0 in a batch replica%s");
             s->shake_nc += hs[sofia::ST_SHAKE_NC];
             md.step += nsteps;
             if (energies && want_e) {
-                double e[16];
-                SOFIA_CUDA(ctx, cudaMemcpy(e, md.ered.p, sizeof(double) * 16, cudaMemcpyDeviceToHost));
                 double *o = energies + (size_t)i * SOFIA_MD_NE;
-                sofia::md_fill_energies(md, e, o);
+                sofia::md_fill_energies(md, &b->hestat[(size_t)16 * i], o);
             }
         }
         return SOFIA_OK;

@@ -61,14 +61,6 @@ constexpr int MAX_COL = 2048;
 #ifndef SOFIA_PAIR_TRI_MAX
 #define SOFIA_PAIR_TRI_MAX 10
 #endif
-// resident blocks per SM of the batched pair and prune kernels (their replica
-// arguments come from the device table, not the constant bank)
-#ifndef SOFIA_BATCH_PAIR_MINB
-#define SOFIA_BATCH_PAIR_MINB SOFIA_PAIR_MINB
-#endif
-#ifndef SOFIA_BATCH_PRUNE_MINB
-#define SOFIA_BATCH_PRUNE_MINB SOFIA_PRUNE_MINB
-#endif
 #ifndef SOFIA_SEARCH_ZWIN
 #define SOFIA_SEARCH_ZWIN 1
 #endif
@@ -2443,7 +2435,7 @@ __global__ void k_bbox_b(const BatchDev *__restrict__ tab) {
 
 __global__ void __launch_bounds__(256) k_search_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_ACTIVE_QUEUE_LOOP(BK_W1024, BA_BUILD, BC_SEARCH)
+    SOFIA_BATCH_ACTIVE_LOOP(BK_W256, BA_BUILD)
     SearchArgs a;
     a.cond = d.flag;
     a.cmask = 1;
@@ -2469,32 +2461,25 @@ __global__ void __launch_bounds__(256) k_search_b(BatchDev *__restrict__ tab) {
     a.jcount = d.jcount;
     a.jmask = d.jmask;
     a.status = d.status;
-    const int nb = (d.maxcl * 32 + 255) / 256;
-    for (int g = lb * GRAIN; g < nb && g < (lb + 1) * GRAIN; ++g) {
-        search_body(g, a);
-        __syncthreads();
-    }
+    search_body(lb, a);
     SOFIA_BATCH_END
 }
 
-__global__ void __launch_bounds__(256, SOFIA_BATCH_PRUNE_MINB) k_prune_b(BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(256, SOFIA_PRUNE_MINB) k_prune_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_ACTIVE_QUEUE_LOOP(BK_W1024, BA_PRUNE, BC_PRUNE)
-    const int nb = (d.maxcl * 32 + 255) / 256;
-    for (int g = lb * GRAIN; g < nb && g < (lb + 1) * GRAIN; ++g) {
-        prune_body(g, d.flag, 3, d.maxcl, d.ncl, d.recf, d.jlist, d.jmask, d.jcount, d.jcap,
-                   (float)d.L, d.rin2, d.rfar2, d.bb, d.ilist, d.imask, d.icount, d.slot_orig,
-                   d.x, d.y, d.z, d.px, d.py, d.pz);
-        __syncthreads();
-    }
+    SOFIA_BATCH_ACTIVE_LOOP(BK_W256, BA_PRUNE)
+    prune_body(lb, d.flag, 3, d.maxcl, d.ncl, d.recf, d.jlist, d.jmask, d.jcount, d.jcap,
+               (float)d.L, d.rin2, d.rfar2, d.bb, d.ilist, d.imask, d.icount, d.slot_orig, d.x,
+               d.y, d.z, d.px, d.py, d.pz);
+    __syncthreads();
     SOFIA_BATCH_END
 }
 
 template <typename T, bool EN, bool VIR, bool SAME, bool TRI = false>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_BATCH_PAIR_MINB) : 2)
+__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2)
     k_pair_b(BatchDev *__restrict__ tab, PairConst k) {
     SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_QUEUE_LOOP(BK_W256, BC_PAIR)
+    SOFIA_BATCH_LOOP(BK_W256)
     pair_body<T, EN, VIR, SAME, TRI>(lb, d.maxcl, d.ncl, d.rec, d.ilist, d.imask, d.icount, d.jcap,
                                 d.ljtab, k, d.L, d.fslot, d.energy);
     __syncthreads();
@@ -2686,7 +2671,7 @@ cudaError_t batch_pair_smem_optin(int nt) {
 }
 
 void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
-                     cudaStream_t st, int nsm) {
+                     cudaStream_t st, int nsm, int pair_blocks) {
     const int g256 = nsm * 8, g128 = nsm * 16;
     launch_pdl(k_batch_active_b, 1, MAXREP, 0, st, tab);
     launch_pdl(k_wrap_bin_b, g256, 256, 0, st, tab);
@@ -2695,27 +2680,27 @@ void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
     launch_pdl(k_col_sort_assign_b, nsm * 4, 256, 0, st, tab);
     launch_pdl(k_pack_b, g256, 256, 0, st, tab);
     launch_pdl(k_bbox_b, g128, 128, 0, st, tab);
-    launch_pdl(k_search_b, g256, 256, 0, st, tab);
-    launch_pdl(k_prune_b, nsm * SOFIA_BATCH_PRUNE_MINB, 256, 0, st, tab);
+    // one block per warp-per-cluster virtual block of all members (blocks past the
+    // replicas whose trigger fired return at once)
+    const int gw = pair_blocks > 0 ? pair_blocks : 1;
+    launch_pdl(k_search_b, gw, 256, 0, st, tab);
+    launch_pdl(k_prune_b, gw, 256, 0, st, tab);
     const PairConst k = make_pair_const(s0, nullptr);
     const size_t smem = pair_smem(s0->ntypes, false, energy);
     const bool tri = energy && pair_tri(s0->ntypes);
     const size_t smem3 = pair_smem(s0->ntypes, tri, energy);
     if (precision == SOFIA_PREC_FP64) {
         if (energy)
-            launch_pdl(k_pair_b<double, true, false, true>, nsm * 2, 256, smem, st, tab, k);
+            launch_pdl(k_pair_b<double, true, false, true>, gw, 256, smem, st, tab, k);
         else
-            launch_pdl(k_pair_b<double, false, false, true>, nsm * 2, 256, smem, st, tab, k);
+            launch_pdl(k_pair_b<double, false, false, true>, gw, 256, smem, st, tab, k);
     } else if (tri) {
-        launch_pdl(k_pair_b<float, true, false, true, true>, nsm * SOFIA_PAIR_MINB_EN, 256, smem3,
-                   st, tab, k);
+        launch_pdl(k_pair_b<float, true, false, true, true>, gw, 256, smem3, st, tab, k);
     } else {
         if (energy)
-            launch_pdl(k_pair_b<float, true, false, true>, nsm * SOFIA_PAIR_MINB_EN, 256, smem, st,
-                       tab, k);
+            launch_pdl(k_pair_b<float, true, false, true>, gw, 256, smem, st, tab, k);
         else
-            launch_pdl(k_pair_b<float, false, false, true>, nsm * SOFIA_BATCH_PAIR_MINB, 256, smem,
-                       st, tab, k);
+            launch_pdl(k_pair_b<float, false, false, true>, gw, 256, smem, st, tab, k);
     }
     launch_pdl(k_unpack_b, g256, 256, 0, st, tab);
     if (energy) {

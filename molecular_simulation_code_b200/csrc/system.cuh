@@ -154,7 +154,6 @@ enum BatchKind {
     BK_S256,      // ceil(max_clusters * 8 / 256): per-slot kernels
     BK_C128,      // ceil(max_clusters / 128): cluster boxes
     BK_W256,      // ceil(max_clusters * 32 / 256): warp-per-cluster kernels
-    BK_W1024,     // ceil(max_clusters * 32 / (256 GRAIN)): grains of BK_W256 blocks (search, prune)
     BK_B128,      // ceil(bonded terms / 128)
     BK_G128,      // ceil(SHAKE groups / 128)
     BK_RED,       // RED_BLOCKS: stage 1 of the pair-energy sums
@@ -164,14 +163,6 @@ enum BatchKind {
     BK_N
 };
 constexpr int MAXREP = 256;
-// The batched search and prune take grains of GRAIN consecutive 256-thread
-// blocks of one replica per work-queue pop: their blocks are short, and the
-// pop (an atomic, two barriers and the replica lookup) would otherwise take a
-// large share of each block's time.
-#ifndef SOFIA_BATCH_GRAIN
-#define SOFIA_BATCH_GRAIN 2
-#endif
-constexpr int GRAIN = SOFIA_BATCH_GRAIN;
 constexpr int RED_BLOCKS = 128;  // blocks of stage 1 of the pair-energy sums
 constexpr int MD_NJOB = 7;  // bonds, angles, torsion, coul14, lj14, impropers, kinetic
 
@@ -206,14 +197,13 @@ struct RepDev {
     const int *shake;
     const double *sbond;
     double *ered, *ebpart, *ke;
+    // segment-start snapshot (x, y, z, vx, vy, vz; the step counter)
+    double *snap[6];
+    long long *snap_step;
     // energy-sum jobs: column count n (0 = off), width, column, input, output slot of ered
     int job_n[MD_NJOB], job_w[MD_NJOB], job_c[MD_NJOB], job_slot[MD_NJOB];
     const double *job_in[MD_NJOB];
 };
-
-// Work-queue counters of the dynamically scheduled batched kernels (one per
-// launch of a step; the step's first kernel clears them).
-enum BatchCounter { BC_SEARCH = 1, BC_PRUNE, BC_PAIR, BC_BONDED, BC_SHAKE, BC_N = 8 };
 
 // Replicas whose list trigger fired this step, per trigger mask: BA_BUILD
 // (bit 0: rebuild) and BA_PRUNE (bits 0-1: rebuild or prune).  The conditional
@@ -223,7 +213,6 @@ enum BatchActive { BA_BUILD = 0, BA_PRUNE = 1, BA_N = 2 };
 
 struct BatchDev {
     int nrep;
-    int ctr[BC_N];
     int nact[BA_N];
     int act[BA_N][MAXREP];
     int apre[BA_N][BK_N][MAXREP + 1];
@@ -231,43 +220,14 @@ struct BatchDev {
     RepDev rep[MAXREP];
 };
 
-// Dynamically scheduled loop over the virtual blocks of kind KIND: each block
-// takes the next virtual block from the work-queue counter CTR (an atomic add
-// by thread 0), so blocks that finish early take more work.  Inside, d is the
-// owning replica's entry and lb the block index within that replica.
-#ifndef SOFIA_BATCH_DYNAMIC
-#define SOFIA_BATCH_DYNAMIC 1
-#endif
-#if SOFIA_BATCH_DYNAMIC
-#define SOFIA_BATCH_QUEUE_LOOP(KIND, CTR)                                        \
-    __shared__ int s_vb_;                                                        \
-    for (;;) {                                                                   \
-        if (threadIdx.x == 0) s_vb_ = atomicAdd(&tab->ctr[CTR], 1);              \
-        __syncthreads();                                                         \
-        const int vb = s_vb_;                                                    \
-        __syncthreads();                                                         \
-        /* re-read each round: nothing of the loop stays live across the body */ \
-        const int nrep_ = *reinterpret_cast<const volatile int *>(&tab->nrep);   \
-        const int *pre_ = tab->pre[KIND];                                        \
-        if (vb >= pre_[nrep_]) break;                                            \
-        const int r_ = batch_rep(pre_, nrep_, vb);                               \
-        const RepDev &d = tab->rep[r_];                                          \
-        const int lb = vb - pre_[r_];
-#else
-#define SOFIA_BATCH_QUEUE_LOOP(KIND, CTR)                                        \
-    for (int vb = blockIdx.x;; vb += gridDim.x) {                                \
-        const int nrep_ = tab->nrep;                                             \
-        const int *pre_ = tab->pre[KIND];                                        \
-        if (vb >= pre_[nrep_]) break;                                            \
-        const int r_ = batch_rep(pre_, nrep_, vb);                               \
-        const RepDev &d = tab->rep[r_];                                          \
-        const int lb = vb - pre_[r_];
-#endif
-
-// Loops over the virtual blocks of kind KIND of the replicas active for trigger
-// mask M (BatchActive), statically (ACTIVE_LOOP) or from work-queue counter CTR
-// (ACTIVE_QUEUE_LOOP).  Inside, d is the replica's entry and lb the block index
-// within that replica.
+// Batched kernels walk virtual blocks in grid-stride order: block b takes
+// virtual blocks b, b + gridDim.x, ...  The pair, search and prune kernels are
+// launched with one block per virtual block of all members at capture time, so
+// each block takes at most one and the hardware block scheduler balances the
+// uneven rows; members added later without a recapture are covered by the
+// stride.  ACTIVE_LOOP walks the kind-KIND blocks of the replicas active for
+// trigger mask M (BatchActive).  Inside, d is the replica's entry and lb the
+// block index within that replica.
 #define SOFIA_BATCH_ACTIVE_LOOP(KIND, M)                                         \
     for (int vb = blockIdx.x;; vb += gridDim.x) {                                \
         const int na_ = *reinterpret_cast<const volatile int *>(&tab->nact[M]);  \
@@ -276,20 +236,6 @@ struct BatchDev {
         const int a_ = batch_rep(ap_, na_, vb);                                  \
         const RepDev &d = tab->rep[tab->act[M][a_]];                             \
         const int lb = vb - ap_[a_];
-#define SOFIA_BATCH_ACTIVE_QUEUE_LOOP(KIND, M, CTR)                              \
-    __shared__ int s_vb_;                                                        \
-    for (;;) {                                                                   \
-        if (threadIdx.x == 0) s_vb_ = atomicAdd(&tab->ctr[CTR], 1);              \
-        __syncthreads();                                                         \
-        const int vb = s_vb_;                                                    \
-        __syncthreads();                                                         \
-        const int na_ = *reinterpret_cast<const volatile int *>(&tab->nact[M]);  \
-        const int *ap_ = tab->apre[M][KIND];                                     \
-        if (vb >= ap_[na_]) break;                                               \
-        const int a_ = batch_rep(ap_, na_, vb);                                  \
-        const RepDev &d = tab->rep[tab->act[M][a_]];                             \
-        const int lb = vb - ap_[a_];
-
 // Replica of virtual block vb: the last r with pre[r] <= vb.
 __device__ __forceinline__ int batch_rep(const int *__restrict__ pre, int nrep, int vb) {
     int lo = 0, hi = nrep - 1;
@@ -310,10 +256,13 @@ void repdev_fill_pair(const Sys *s, RepDev *d);
 // Langevin force, and (energy) the pair-energy sums.  All replicas share the
 // pair constants k (all but the box) and the precision.
 // nsm: multiprocessors of the device (the grid-stride launches are sized from it).
+// pair_blocks: the warp-per-cluster virtual blocks over all members when the graph
+// is captured, the grid of the pair, search and prune kernels (later members that
+// need more are covered by the kernels' grid-stride loops).
+void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
+                     cudaStream_t st, int nsm, int pair_blocks);
 // raises the batched pair kernels' dynamic shared-memory limit for nt atom types
 cudaError_t batch_pair_smem_optin(int nt);
-void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
-                     cudaStream_t st, int nsm);
 // The pair constants a captured batch graph holds (everything but the box).
 struct PairKey {
     int precision, ntypes, lj_shift;
