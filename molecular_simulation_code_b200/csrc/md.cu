@@ -16,6 +16,7 @@
 // (Source/mod_force.f90:549-553); here every enabled term acts on the atoms.
 // State is FP64 (positions, velocities) with 64-bit fixed-point forces; all
 // force contributions are added in integers, so a step is bit-reproducible.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -61,7 +62,10 @@ __global__ void k_kick(int n, double h, const double *__restrict__ invm,
 // list triggers: v += h f / m (nve_v), x += dt v (nve_x), then bit 0 of the
 // trigger word if an atom moved more than skin/2 since the list build, bit 1
 // if more than margin/2 since the last prune (the word was cleared after the
-// previous step's list decisions).
+// previous step's list decisions).  TWICE: the previous step's closing
+// half-kick first, as its own rounded addition (v += h f / m twice with the same
+// forces), so a segment that skips the separate closing kick gives the same bits.
+template <bool TWICE = false>
 __device__ __forceinline__ void kick_drift_body(int bx, int n, double h, const double *__restrict__ invm,
                              const long long *__restrict__ fx, const long long *__restrict__ fy,
                              const long long *__restrict__ fz, double *__restrict__ vx,
@@ -77,9 +81,16 @@ __device__ __forceinline__ void kick_drift_body(int bx, int n, double h, const d
     bool far = false, pfar = false;
     if (i < n) {
         const double c = h * invm[i];
-        const double ux = vx[i] + c * unfix(fx[i]);
-        const double uy = vy[i] + c * unfix(fy[i]);
-        const double uz = vz[i] + c * unfix(fz[i]);
+        double ux = vx[i], uy = vy[i], uz = vz[i];
+        const double gx = c * unfix(fx[i]), gy = c * unfix(fy[i]), gz = c * unfix(fz[i]);
+        if (TWICE) {
+            ux = ux + gx;
+            uy = uy + gy;
+            uz = uz + gz;
+        }
+        ux = ux + gx;
+        uy = uy + gy;
+        uz = uz + gz;
         vx[i] = ux;
         vy[i] = uy;
         vz[i] = uz;
@@ -93,6 +104,7 @@ __device__ __forceinline__ void kick_drift_body(int bx, int n, double h, const d
     const bool a = __any_sync(0xffffffffu, far), b = __any_sync(0xffffffffu, pfar);
     if ((threadIdx.x & 31) == 0 && (a || b)) atomicOr(flag, (a ? 1 : 0) | (b ? 2 : 0));
 }
+template <bool TWICE>
 __global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
                              const long long *__restrict__ fx, const long long *__restrict__ fy,
                              const long long *__restrict__ fz, double *__restrict__ vx,
@@ -104,7 +116,7 @@ __global__ void k_kick_drift(int n, double h, const double *__restrict__ invm,
                              const double *__restrict__ pz, double L, double lim2, double plim2,
                              int *__restrict__ flag, long long *__restrict__ step) {
     SOFIA_PDL_ENTRY();
-    kick_drift_body(blockIdx.x, n, h, invm, fx, fy, fz, vx, vy, vz, dt, x, y, z, rx, ry, rz, px, py, pz, L, lim2, plim2, flag, step);
+    kick_drift_body<TWICE>(blockIdx.x, n, h, invm, fx, fy, fz, vx, vy, vz, dt, x, y, z, rx, ry, rz, px, py, pz, L, lim2, plim2, flag, step);
 }
 
 
@@ -829,7 +841,11 @@ static void md_fill_energies(const Md &md, const double *e, double *o) {
 }
 
 // One MD step (all device work; capturable).
-static int md_step(Sys *s, bool energy) {
+// One step.  twice: this step opens with the previous step's closing half-kick
+// (that step ran with close = false); close: launch this step's closing
+// half-kick (and RATTLE).  A segment of steps chains (close = false, twice =
+// true) pairs and gives the same bits as separate steps.
+static int md_step(Sys *s, bool energy, bool twice = false, bool close = true) {
     Md &md = s->md;
     cudaStream_t st = s->ctx->stream;
     const int n = s->n;
@@ -838,7 +854,7 @@ static int md_step(Sys *s, bool energy) {
     const long long *fx = s->f[0].as<long long>(), *fy = s->f[1].as<long long>(),
                     *fz = s->f[2].as<long long>();
     const double half = 0.5 * s->skin, phalf = 0.5 * s->margin;
-    sofia::launch_pdl(k_kick_drift, grid_for(n, 256), 256, 0, st,
+    sofia::launch_pdl(twice ? k_kick_drift<true> : k_kick_drift<false>, grid_for(n, 256), 256, 0, st,
         n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz, md.dt, s->x[0].as<double>(),
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->xprn[0].as<double>(),
@@ -846,6 +862,11 @@ static int md_step(Sys *s, bool energy) {
         s->flag.as<int>(), md.step_dev.as<long long>());
     int rc = md_forces(s, energy, false, true);
     if (rc) return rc;
+    if (!close) {
+        s->launches += 1;
+        SOFIA_CUDA(s->ctx, cudaGetLastError());
+        return SOFIA_OK;
+    }
     sofia::launch_pdl(k_kick, grid_for(n, 256), 256, 0, st, n, h, s->invm.as<double>(), fx, fy, fz, vx, vy, vz);
     if (md.rattle && md.nshake) {
         sofia::launch_pdl(k_rattle, grid_for(md.nshake, 128), 128, 0, st, md.nshake,
@@ -875,11 +896,19 @@ static int md_capture(Sys *s) {
     cudaStream_t st = s->ctx->stream;
     const int timing = s->timing;
     s->timing = 0;  // no event records inside the graph
-    for (int e = 0; e < 2; ++e) {
+    // RATTLE rewrites the full-step velocities after the closing kick, so its
+    // steps keep separate kicks
+    const bool fuse = !(s->md.rattle && s->md.nshake);
+    const int nsteps_g[4] = {1, 1, s->md.seg, s->md.seg};
+    for (int e = 0; e < 4; ++e) {
         cudaGraph_t g = nullptr;
         const long long l0 = s->launches;
         SOFIA_CUDA(s->ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        const int rc = md_step(s, e == 1);
+        int rc = SOFIA_OK;
+        for (int k = 0; k < nsteps_g[e] && !rc; ++k) {
+            const bool last = k == nsteps_g[e] - 1;
+            rc = md_step(s, (e & 1) && last, fuse && k > 0, !fuse || last);
+        }
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         s->md.graph_launches[e] = s->launches - l0;
         s->launches = l0;
@@ -1040,15 +1069,30 @@ extern "C" int sofia_system_md_run(sofia_system *ss, int nsteps, int energy_ever
             rc = sofia::md_capture(s);
             if (rc) return rc;
         }
-        for (int k = 0; k < nsteps; ++k) {
+        for (int k = 0; k < nsteps;) {
             const bool en = energy_every > 0 && ((k + 1) % energy_every == 0 || k + 1 == nsteps);
             if (use_graph) {
+                // a whole segment when steps k .. k + seg - 1 hold no energy step but
+                // possibly the last one
+                const int sg = md.seg;
+                int first_e = nsteps;  // first energy step at or after k
+                if (energy_every > 0)
+                    first_e = std::min(((k + energy_every) / energy_every) * energy_every - 1,
+                                       nsteps - 1);
+                if (sg > 1 && k + sg <= nsteps && first_e >= k + sg - 1) {
+                    const int g = (first_e == k + sg - 1) ? 3 : 2;
+                    SOFIA_CUDA(ctx, cudaGraphLaunch(md.graph[g], st));
+                    s->launches += md.graph_launches[g];
+                    k += sg;
+                    continue;
+                }
                 SOFIA_CUDA(ctx, cudaGraphLaunch(md.graph[en ? 1 : 0], st));
                 s->launches += md.graph_launches[en ? 1 : 0];
             } else {
                 rc = sofia::md_step(s, en);
                 if (rc) return rc;
             }
+            ++k;
         }
         rc = sofia::sys_list_overflow(s);
         if (rc == SOFIA_ENEEDGROW) {
@@ -1199,10 +1243,11 @@ __global__ void k_status_b(const BatchDev *__restrict__ tab, int *__restrict__ o
     SOFIA_BATCH_END
 }
 
+template <bool TWICE>
 __global__ void k_kick_drift_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_LOOP(BK_A256)
-    kick_drift_body(lb, d.n, d.h, d.invm, d.fx, d.fy, d.fz, d.vx, d.vy, d.vz, d.dt, d.x, d.y,
+    kick_drift_body<TWICE>(lb, d.n, d.h, d.invm, d.fx, d.fy, d.fz, d.vx, d.vy, d.vz, d.dt, d.x, d.y,
                     d.z, d.rx, d.ry, d.rz, d.px, d.py, d.pz, d.L, d.lim2, d.plim2, d.flag,
                     d.step);
     SOFIA_BATCH_END
@@ -1354,16 +1399,22 @@ static void repdev_fill_md(Sys *s, RepDev *d) {
 }
 
 // One batched MD step: the same kernels, in the same order, as md_step.
+// One batch step; twice and close as for md_step (a segment chains its steps'
+// closing half-kicks into the next steps' kick and drift).
 static void batch_step(BatchDev *tab, Sys *s0, bool energy, bool rattle, cudaStream_t st,
-                       int nsm, int pair_blocks) {
+                       int nsm, int pair_blocks, bool twice = false, bool close = true) {
     const int g256 = nsm * 8, g128 = nsm * 16;
-    launch_pdl(k_kick_drift_b, g256, 256, 0, st, tab);
+    if (twice)
+        launch_pdl(k_kick_drift_b<true>, g256, 256, 0, st, tab);
+    else
+        launch_pdl(k_kick_drift_b<false>, g256, 256, 0, st, tab);
     batch_pair_path(tab, s0, s0->precision, energy, st, nsm, pair_blocks);
     if (energy)
         launch_pdl(k_bonded_b<true>, g128, 128, 0, st, tab);
     else
         launch_pdl(k_bonded_b<false>, g128, 128, 0, st, tab);
     launch_pdl(k_shake_b, g128, 128, 0, st, tab);
+    if (!close) return;
     launch_pdl(k_kick_b, g256, 256, 0, st, tab);
     if (rattle) launch_pdl(k_rattle_b, g128, 128, 0, st, tab);
     if (energy) {
@@ -1392,7 +1443,7 @@ struct sofia_batch {
     int graph_ok = 0;
     int graph_rattle = 0;               // the graphs hold the RATTLE launch
     sofia::PairKey graph_key{};         // the pair constants the graphs hold
-    long long step_launches[2] = {0, 0};
+    long long graph_launches[4] = {0, 0, 0, 0};  // kernel launches each graph holds
 };
 
 static void batch_drop_graphs(sofia_batch *b) {
@@ -1525,19 +1576,28 @@ static int batch_capture(sofia_batch *b) {
     for (int g = 0; g < 4; ++g) {
         cudaGraph_t graph = nullptr;
         SOFIA_CUDA(ctx, cudaStreamBeginCapture(ms, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < nsteps[g]; ++k)
-            sofia::batch_step(tab, s0, (g & 1) && k == nsteps[g] - 1, rat, ms, b->nsm,
-                              pair_blocks);
+        // without RATTLE the steps of a segment chain their closing half-kicks
+        const bool fuse = !rat;
+        for (int k = 0; k < nsteps[g]; ++k) {
+            const bool last = k == nsteps[g] - 1;
+            sofia::batch_step(tab, s0, (g & 1) && last, rat, ms, b->nsm, pair_blocks,
+                              fuse && k > 0, !fuse || last);
+        }
         cudaError_t ce = cudaStreamEndCapture(ms, &graph);
         if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaStreamEndCapture (batch)");
         ce = cudaGraphInstantiate(&b->graph[g], graph, 0);
         cudaGraphDestroy(graph);
         if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaGraphInstantiate (batch)");
     }
-    // kick+drift, the pair path (active-replica compaction, bin, scan, scatter,
-    // sort, pack, bbox, search, prune, pair, unpack), bonded, SHAKE, kick
-    b->step_launches[0] = 1 + 11 + 3 + (rat ? 1 : 0);
-    b->step_launches[1] = b->step_launches[0] + 2 + 4;
+    // a step: kick+drift, the pair path (active-replica compaction, bin, scan,
+    // scatter, sort, pack, bbox, search, prune, pair, unpack), bonded, SHAKE; then
+    // the closing kick (+ RATTLE), once per segment when the kicks are chained;
+    // energies add the two pair-energy and four MD-energy reductions
+    const long long body = 1 + 11 + 2, closing = 1 + (rat ? 1 : 0);
+    b->graph_launches[0] = body + closing;
+    b->graph_launches[1] = body + closing + 6;
+    b->graph_launches[2] = rat ? b->seg * (body + closing) : b->seg * body + closing;
+    b->graph_launches[3] = b->graph_launches[2] + 6;
     b->graph_rattle = rat;
     b->graph_key = sofia::pair_key(s0);
     b->graph_ok = 1;
@@ -1593,11 +1653,12 @@ extern "C" int sofia_batch_md_run(sofia_batch *b, int nsteps, int energy_every,
             const int k = full ? b->seg : 1;
             const bool en = want_e && left == k;
             SOFIA_CUDA(ctx, cudaGraphLaunch(b->graph[(full ? 2 : 0) + (en ? 1 : 0)], ms));
-            launched += (long long)k * b->step_launches[0] + (en ? 6 : 0);
+            launched += b->graph_launches[(full ? 2 : 0) + (en ? 1 : 0)];
             left -= k;
         }
         SOFIA_CUDA(ctx, sofia::launch_pdl(sofia::k_status_b, b->nsm, 32, 0, ms, tab,
                                           b->stat.as<int>(), b->estat.as<double>()));
+        launched += 2;  // the snapshot and status kernels
         SOFIA_CUDA(ctx, cudaMemcpyAsync(b->hstat.data(), b->stat.p,
                                         sizeof(int) * sofia::ST_NSLOTS * (size_t)n,
                                         cudaMemcpyDeviceToHost, ms));

@@ -56,8 +56,12 @@ struct Md {
     int ndof = 0;
     long long step = 0;
     int forces_valid = 0;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    long long graph_launches[2] = {0, 0};
+    // captured graphs: [0] one step, [1] one step with energies, [2] seg steps,
+    // [3] seg steps with energies on the last; inside a segment each step's
+    // closing half-kick is fused into the next step's kick and drift
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long graph_launches[4] = {0, 0, 0, 0};
+    int seg = 10;
     int graph_ok = 0;
 };
 

@@ -68,6 +68,24 @@ def test_stats_before_first_build(ctx, small):
     a.close()
 
 
+def test_segment_graphs_with_energies_equal_eager(ctx, small):
+    """Segment graphs chain each step's closing half-kick into the next step's
+    kick and drift; with energies every 7th step (segments with and without an
+    energy step, single-step graphs between them) the state and the energies
+    equal the eager step-by-step path's bit for bit."""
+    s = small
+    a = _system(ctx, s, dt=2.0, gamma=0.01, seed=6)
+    ea = [a.md_run(37, energy_every=7, use_graph=True) for _ in range(2)]
+    b = _system(ctx, s, dt=2.0, gamma=0.01, seed=6)
+    eb = [b.md_run(37, energy_every=7, use_graph=False) for _ in range(2)]
+    xa, va, fa = a.get_state()
+    xb, vb, fb = b.get_state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb) and np.array_equal(fa, fb)
+    assert ea == eb
+    a.close()
+    b.close()
+
+
 def test_graph_conditional_build_and_prune_equal_eager(ctx, small):
     """Long enough for several list rebuilds and prunes: the captured step (build
     and prune as conditional graph nodes) takes exactly the eager path's steps."""
