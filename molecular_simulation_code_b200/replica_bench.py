@@ -63,6 +63,7 @@ def bench_batch(args):
             for m, r in zip(systems, reps):
                 m.md_setup(r, dt=dt, gamma=gamma, seed=seed)
             b = Batch(master, systems)
+            b.set_segment(args.segment)  # steps per captured segment graph
             b.run(nsteps)  # the last stage is the warm-up segment (captures the graphs)
             if k < len(stages) - 1:
                 b.close()
