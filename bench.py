@@ -676,6 +676,7 @@ def run_ours(args, rank, ws):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": args.workload, "atoms_per_gpu": n, "rc_A": CUT, "skin_A": SKIN,
+                   "prune_margin_A": 0.4,
                    "dt_fs": DT, "precision": "mixed FP32 pair / FP64 positions / int64 forces",
                    "parallelism": f"replicas x{ws} (no exchange)",
                    "l2": "inputs larger than L2 (cluster-pair list "

@@ -448,8 +448,9 @@ int sofia_batch_destroy(sofia_batch *batch);
 int sofia_batch_md_run(sofia_batch *batch, int nsteps, int energy_every, double *energies);
 int sofia_batch_set_systems(sofia_batch *batch, sofia_system *const *systems, int n);
 int sofia_batch_set_segment(sofia_batch *batch, int steps);
-/* Prune margin (A) of the pruned inner list (default 0.6): the tuning knob
- * the autotuner picks per size class. */
+/* Prune margin (A) of the pruned inner list (default 0.4): the tuning knob
+ * the autotuner picks per size class.  Any margin > 0 gives the same forces:
+ * the list is re-pruned as soon as an atom has moved more than margin/2. */
 int sofia_system_set_margin(sofia_system *sys, double margin);
 /* Cluster shape: the xy column width as a multiple (0.5..2) of the cube side of
  * 8 atoms (1 = default; < 1 taller, > 1 flatter clusters).  Reallocates the

@@ -96,7 +96,7 @@ def apply_shape(system: M.System, shape):
     set_margin(system, shape[1])
 
 
-def autotune(ctx: Context, sysdata, aspects=ASPECTS, margins=(0.4, 0.6, 0.8), steps: int = 40,
+def autotune(ctx: Context, sysdata, aspects=ASPECTS, margins=(0.35, 0.45, 0.6), steps: int = 40,
              cut: float = 10.0, skin: float = 2.0, precision: int = M.MIXED):
     """Fastest (cluster aspect, prune margin) for this replica: short Langevin
     segments timed with CUDA events, every candidate from the same 300 K state

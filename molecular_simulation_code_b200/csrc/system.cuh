@@ -97,7 +97,7 @@ struct Sys {
     int ptta_atoms = 0;                 // glycine atoms ptta holds (0 = not yet set)
     // pruned inner list (rc + margin) and the positions it was pruned at
     DevBuf ilist, imask, icount, xprn[3], part, dcount;
-    double margin = 0.6;
+    double margin = 0.4;
     // LJ energy of every pair inside the cut-off shifted by -E_LJ(rc) (SOFIA_MD_LJ_SHIFT);
     // forces are unchanged, so only the energy bookkeeping differs
     int lj_shift = 0;

@@ -215,8 +215,10 @@ def test_list_covers_every_pair_within_rlist(ctx):
     drifting trajectory with several prunes and rebuilds."""
     s = make_system(150, 2500, 1)
     n = s.np_atoms
-    cut, skin, margin = 10.0, 2.0, 0.6
+    from molecular_simulation_code_b200.batch import set_margin
+    cut, skin, margin = 10.0, 2.0, 0.4
     sysm = M.System(ctx, s, cut=cut, skin=skin, precision=M.MIXED)
+    set_margin(sysm, margin)
     sysm.set_state(s.xyz.astype(np.float64), s.velocity.astype(np.float64))
     sysm.md_setup(s, dt=2.0, temperature=300.0, gamma=0.01, seed=4)
     sysm.compute(M.MIXED, rebuild=True, energy=False, virial=False)
