@@ -325,7 +325,19 @@ __device__ __forceinline__ void dihedral_term(int n, const DihArgs &a) {
 
 // SHAKE (force form) per group; each atom belongs to at most one group, so the
 // owning thread adds its constraint forces without atomics.
-__device__ __forceinline__ void shake_body(int bx, int ns, const int *__restrict__ sa, const double *__restrict__ sb,
+// Constraint c of a SHAKE group of type NUM joins group atoms shake_cp and
+// shake_cq: NUM 1 = one bond (atoms 0-1), 3 = two bonds from atom 0, 4 = three
+// bonds from atom 0, -3 = a rigid triangle (0-1, 0-2, 1-2; mod_shake.f90).
+__host__ __device__ constexpr int shake_nc(int num) { return num == 1 ? 1 : (num == 3 ? 2 : 3); }
+__host__ __device__ constexpr int shake_na(int num) { return num == 1 ? 2 : (num == 4 ? 4 : 3); }
+__host__ __device__ constexpr int shake_cp(int num, int c) { return (num == -3 && c == 2) ? 1 : 0; }
+__host__ __device__ constexpr int shake_cq(int num, int c) { return (num == -3 && c == 2) ? 2 : c + 1; }
+
+// One SHAKE group of type NUM: the group's size and constraint pairs are
+// compile-time constants, so every loop unrolls and the small matrices live in
+// registers.  The operations and their order are those of the general solver.
+template <int NUM>
+__device__ __forceinline__ void shake_group(int g, const int (&at)[4], const double *__restrict__ sb,
                         const double *__restrict__ x, const double *__restrict__ y,
                         const double *__restrict__ z, const double *__restrict__ vx,
                         const double *__restrict__ vy, const double *__restrict__ vz,
@@ -333,26 +345,14 @@ __device__ __forceinline__ void shake_body(int bx, int ns, const int *__restrict
                         int maxiter, double tol, long long *__restrict__ fx,
                         long long *__restrict__ fy, long long *__restrict__ fz,
                         int *__restrict__ status) {
-    const int g = bx * blockDim.x + threadIdx.x;
-    if (g >= ns) return;
-    const int num = sa[5 * g];
-    int at[4] = {sa[5 * g + 1] - 1, sa[5 * g + 2] - 1, sa[5 * g + 3] - 1, sa[5 * g + 4] - 1};
-    int nc, cp[3], cq[3], na;
+    constexpr int nc = shake_nc(NUM), na = shake_na(NUM);
+    constexpr int cp[3] = {shake_cp(NUM, 0), shake_cp(NUM, 1), shake_cp(NUM, 2)};
+    constexpr int cq[3] = {shake_cq(NUM, 0), shake_cq(NUM, 1), shake_cq(NUM, 2)};
     double bl[3];
-    if (num == 1) {
-        nc = 1; na = 2; cp[0] = 0; cq[0] = 1; bl[0] = sb[3 * g];
-    } else if (num == 3) {
-        nc = 2; na = 3; cp[0] = 0; cq[0] = 1; cp[1] = 0; cq[1] = 2; bl[0] = sb[3 * g]; bl[1] = sb[3 * g + 1];
-    } else if (num == 4) {
-        nc = 3; na = 4;
-        for (int k = 0; k < 3; ++k) { cp[k] = 0; cq[k] = k + 1; bl[k] = sb[3 * g + k]; }
-    } else if (num == -3) {
-        nc = 3; na = 3; cp[0] = 0; cq[0] = 1; cp[1] = 0; cq[1] = 2; cp[2] = 1; cq[2] = 2;
-        for (int k = 0; k < 3; ++k) bl[k] = sb[3 * g + k];
-    } else {
-        return;
-    }
+#pragma unroll
+    for (int k = 0; k < nc; ++k) bl[k] = sb[3 * g + k];
     double im[4], xs[4][3], xc[4][3];
+#pragma unroll
     for (int a = 0; a < na; ++a) {
         const int i = at[a];
         im[a] = invm[i];
@@ -365,12 +365,16 @@ __device__ __forceinline__ void shake_body(int bx, int ns, const int *__restrict
         xs[a][2] = z[i] + dt * vz[i] + c * unfix(fz[i]);
     }
     double r[3][3], s[3][3], C[3][3];
+#pragma unroll
     for (int c = 0; c < nc; ++c)
+#pragma unroll
         for (int d = 0; d < 3; ++d) {
             r[c][d] = mimg(xc[cp[c]][d] - xc[cq[c]][d], L);
             s[c][d] = mimg(xs[cp[c]][d] - xs[cq[c]][d], L);
         }
+#pragma unroll
     for (int c = 0; c < nc; ++c)
+#pragma unroll
         for (int d = 0; d < nc; ++d) {
             double e = 0.0;
             if (cp[c] == cp[d]) e += im[cp[c]];
@@ -380,7 +384,7 @@ __device__ __forceinline__ void shake_body(int bx, int ns, const int *__restrict
             C[c][d] = e;
         }
     double lam[3] = {0.0, 0.0, 0.0};
-    if (nc == 1) {
+    if constexpr (nc == 1) {
         const double rr = r[0][0] * r[0][0] + r[0][1] * r[0][1] + r[0][2] * r[0][2];
         const double ss = s[0][0] * s[0][0] + s[0][1] * s[0][1] + s[0][2] * s[0][2];
         const double sr = s[0][0] * r[0][0] + s[0][1] * r[0][1] + s[0][2] * r[0][2];
@@ -394,14 +398,16 @@ __device__ __forceinline__ void shake_body(int bx, int ns, const int *__restrict
         lam[0] = (fabs(l1) <= fabs(l2)) ? l1 : l2;
     } else {
         double A[3][3], Ai[3][3], ss[3], rd[3][3];
+#pragma unroll
         for (int c = 0; c < nc; ++c) {
             ss[c] = s[c][0] * s[c][0] + s[c][1] * s[c][1] + s[c][2] * s[c][2];
+#pragma unroll
             for (int d = 0; d < nc; ++d) {
                 A[c][d] = 2.0 * C[c][d] * (s[c][0] * r[d][0] + s[c][1] * r[d][1] + s[c][2] * r[d][2]);
                 rd[c][d] = r[c][0] * r[d][0] + r[c][1] * r[d][1] + r[c][2] * r[d][2];
             }
         }
-        if (nc == 2) {
+        if constexpr (nc == 2) {
             const double det = A[0][0] * A[1][1] - A[0][1] * A[1][0];
             if (det == 0.0) {
                 atomicAdd(&status[ST_SHAKE], 1);
@@ -432,30 +438,61 @@ __device__ __forceinline__ void shake_body(int bx, int ns, const int *__restrict
         bool done = false;
         for (int it = 0; it < maxiter && !done; ++it) {
             double bvec[3], ln[3];
+#pragma unroll
             for (int c = 0; c < nc; ++c) {
                 double qd = 0.0;
+#pragma unroll
                 for (int d = 0; d < nc; ++d)
+#pragma unroll
                     for (int e = 0; e < nc; ++e) qd += C[c][d] * C[c][e] * rd[d][e] * lam[d] * lam[e];
                 bvec[c] = bl[c] * bl[c] - ss[c] - qd;
             }
             done = true;
+#pragma unroll
             for (int c = 0; c < nc; ++c) {
                 ln[c] = 0.0;
+#pragma unroll
                 for (int d = 0; d < nc; ++d) ln[c] += Ai[c][d] * bvec[d];
                 if (fabs(ln[c] - lam[c]) > tol) done = false;
             }
+#pragma unroll
             for (int c = 0; c < nc; ++c) lam[c] = ln[c];
         }
         if (!done) atomicAdd(&status[ST_SHAKE_NC], 1);  // warning only (mod_shake.f90:322-324)
     }
     long long *F[3] = {fx, fy, fz};
+#pragma unroll
     for (int c = 0; c < nc; ++c) {
         const double l = lam[c] / dtsq;
+#pragma unroll
         for (int d = 0; d < 3; ++d) {
             F[d][at[cp[c]]] += fixd(l * r[c][d]);
             F[d][at[cq[c]]] -= fixd(l * r[c][d]);
         }
     }
+}
+
+__device__ __forceinline__ void shake_body(int bx, int ns, const int *__restrict__ sa, const double *__restrict__ sb,
+                        const double *__restrict__ x, const double *__restrict__ y,
+                        const double *__restrict__ z, const double *__restrict__ vx,
+                        const double *__restrict__ vy, const double *__restrict__ vz,
+                        const double *__restrict__ invm, double L, double dt, double dtsq,
+                        int maxiter, double tol, long long *__restrict__ fx,
+                        long long *__restrict__ fy, long long *__restrict__ fz,
+                        int *__restrict__ status) {
+    const int g = bx * blockDim.x + threadIdx.x;
+    if (g >= ns) return;
+    const int num = sa[5 * g];
+    const int at[4] = {sa[5 * g + 1] - 1, sa[5 * g + 2] - 1, sa[5 * g + 3] - 1, sa[5 * g + 4] - 1};
+#define SOFIA_SHAKE_ARGS g, at, sb, x, y, z, vx, vy, vz, invm, L, dt, dtsq, maxiter, tol, fx, fy, fz, status
+    switch (num) {
+    case 1: shake_group<1>(SOFIA_SHAKE_ARGS); break;
+    case 3: shake_group<3>(SOFIA_SHAKE_ARGS); break;
+    case 4: shake_group<4>(SOFIA_SHAKE_ARGS); break;
+    case -3: shake_group<-3>(SOFIA_SHAKE_ARGS); break;
+    default: break;
+    }
+#undef SOFIA_SHAKE_ARGS
 }
 __global__ void k_shake(int ns, const int *__restrict__ sa, const double *__restrict__ sb,
                         const double *__restrict__ x, const double *__restrict__ y,
