@@ -695,28 +695,39 @@ static void md_reduce(cudaStream_t st, int n, int w, int c, const double *in, do
 // next na angles, then nd dihedrals (torsion and 1-4 pair), then ni impropers.
 // A count of 0 switches a term off.
 template <bool EN>
+// Threads take the torsions (the longest terms) first, then impropers, angles
+// and bonds, so the last wave of blocks holds the short terms.  Every term
+// adds fixed-point forces and writes its energy to its own slot, so the order
+// does not change any result.
 __device__ __forceinline__ void bonded_body(int bx, const BondedArgs &b) {
     int t = bx * blockDim.x + threadIdx.x;
     const DihArgs &d = b.dih;
-    if (t < b.nb) {
-        bond_term<EN>(t, b.nb, b.bl, b.bc, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.eb);
-        return;
-    }
-    t -= b.nb;
-    if (t < b.na) {
-        angle_term<EN>(t, b.na, b.al, b.ac, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.ea);
-        return;
-    }
-    t -= b.na;
     if (t < b.nd) {
         dihedral_term<EN>(t, d);
         return;
     }
     t -= b.nd;
-    if (t < b.ni) improper_term<EN>(t, b.ni, b.il, b.ic, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.ei);
+    if (t < b.ni) {
+        improper_term<EN>(t, b.ni, b.il, b.ic, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.ei);
+        return;
+    }
+    t -= b.ni;
+    if (t < b.na) {
+        angle_term<EN>(t, b.na, b.al, b.ac, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.ea);
+        return;
+    }
+    t -= b.na;
+    if (t < b.nb) bond_term<EN>(t, b.nb, b.bl, b.bc, d.x, d.y, d.z, d.L, d.fx, d.fy, d.fz, b.eb);
 }
+// 6 resident blocks of 128 per SM (at most 85 registers): the kernel's time is
+// a few waves of latency-bound torsion threads, and more resident blocks per SM
+// shorten it more than the few spills cost (MD 433 -> 436.5 M atom-steps/s at
+// 275k atoms; 8 blocks measured the same)
+#ifndef SOFIA_BONDED_MINB
+#define SOFIA_BONDED_MINB 6
+#endif
 template <bool EN>
-__global__ void __launch_bounds__(128) k_bonded(BondedArgs b) {
+__global__ void __launch_bounds__(128, SOFIA_BONDED_MINB) k_bonded(BondedArgs b) {
     SOFIA_PDL_ENTRY();
     bonded_body<EN>(blockIdx.x, b);
 }
