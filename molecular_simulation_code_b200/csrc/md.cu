@@ -1292,7 +1292,7 @@ __global__ void k_status_b(const BatchDev *__restrict__ tab, int *__restrict__ o
 }
 
 template <bool TWICE>
-__global__ void k_kick_drift_b(BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(256, SOFIA_BATCH_STREAM_MINB) k_kick_drift_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_LOOP(BK_A256)
     kick_drift_body<TWICE>(lb, d.n, d.h, d.invm, d.fx, d.fy, d.fz, d.vx, d.vy, d.vz, d.dt, d.x, d.y,
@@ -1306,7 +1306,7 @@ template <bool EN>
 // grid-stride order: one thread per term or group is short, uniform work, and
 // popping a work queue per block cost more than it balanced (64 replicas:
 // 363 -> 365 M atom-steps/s with the static order).
-__global__ void __launch_bounds__(128) k_bonded_b(BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(128, SOFIA_BONDED_MINB) k_bonded_b(BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_LOOP(BK_B128)
     bonded_body<EN>(lb, d.b);

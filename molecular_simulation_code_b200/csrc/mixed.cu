@@ -2418,7 +2418,7 @@ __global__ void k_col_sort_assign_b(const BatchDev *__restrict__ tab) {
     SOFIA_BATCH_END
 }
 
-__global__ void k_pack_b(const BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(256, SOFIA_BATCH_STREAM_MINB) k_pack_b(const BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_LOOP(BK_S256)
     pack_body(lb, d.nslots, d.ncl, d.slot_orig, d.x, d.y, d.z, d.rx, d.ry, d.rz, d.ix, d.iy, d.iz,
@@ -2486,7 +2486,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_
     SOFIA_BATCH_END
 }
 
-__global__ void k_unpack_b(const BatchDev *__restrict__ tab) {
+__global__ void __launch_bounds__(256, SOFIA_BATCH_STREAM_MINB) k_unpack_b(const BatchDev *__restrict__ tab) {
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_LOOP(BK_S256)
     unpack_body(lb, d.nslots, d.ncl, d.slot_orig, reinterpret_cast<const long long *>(d.fslot),

@@ -167,6 +167,14 @@ enum BatchKind {
     BK_N
 };
 constexpr int MAXREP = 256;
+// resident 256-thread blocks per SM of the batched per-atom streaming kernels
+// (kick and drift, pack, unpack): their replica arguments come from the device
+// table, and without a bound the compiler keeps them all in registers (70-87),
+// which halves the warps that hide memory latency (64 replicas: 380.5 -> 386.7 M
+// atom-steps/s with the bound)
+#ifndef SOFIA_BATCH_STREAM_MINB
+#define SOFIA_BATCH_STREAM_MINB 4
+#endif
 constexpr int RED_BLOCKS = 128;  // blocks of stage 1 of the pair-energy sums
 constexpr int MD_NJOB = 7;  // bonds, angles, torsion, coul14, lj14, impropers, kinetic
 
