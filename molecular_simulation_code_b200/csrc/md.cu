@@ -1540,7 +1540,7 @@ static int batch_upload(sofia_batch *b) {
         const long nterm = (long)d.b.nb + d.b.na + d.b.nd + d.b.ni;
         const int cnt[sofia::BK_N] = {
             sofia::grid_for(s->n, 256), 1, s->ncols, sofia::grid_for((long)s->max_clusters * 8, 256),
-            sofia::grid_for(s->max_clusters, 128), sofia::grid_for((long)s->max_clusters * 32, 256),
+            sofia::grid_for((long)s->max_clusters * 32, 256),
             sofia::grid_for(nterm, 128), sofia::grid_for(s->md.nshake, 128), sofia::RED_BLOCKS,
             1, sofia::MD_NJOB * sofia::MRED, sofia::MD_NJOB};
         for (int k = 0; k < sofia::BK_N; ++k) h->pre[k][r + 1] = h->pre[k][r] + cnt[k];
@@ -1638,10 +1638,11 @@ static int batch_capture(sofia_batch *b) {
         if (ce != cudaSuccess) return sofia::cuda_fail(ctx, ce, "cudaGraphInstantiate (batch)");
     }
     // a step: kick+drift, the pair path (active-replica compaction, bin, scan,
-    // scatter, sort, pack, bbox, search, prune, pair, unpack), bonded, SHAKE; then
-    // the closing kick (+ RATTLE), once per segment when the kicks are chained;
-    // energies add the two pair-energy and four MD-energy reductions
-    const long long body = 1 + 11 + 2, closing = 1 + (rat ? 1 : 0);
+    // scatter, sort, pack with the cluster boxes, search, prune, pair, unpack),
+    // bonded, SHAKE; then the closing kick (+ RATTLE), once per segment when the
+    // kicks are chained; energies add the two pair-energy and four MD-energy
+    // reductions
+    const long long body = 1 + 10 + 2, closing = 1 + (rat ? 1 : 0);
     b->graph_launches[0] = body + closing;
     b->graph_launches[1] = body + closing + 6;
     b->graph_launches[2] = rat ? b->seg * (body + closing) : b->seg * body + closing;

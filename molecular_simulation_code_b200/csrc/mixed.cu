@@ -262,15 +262,19 @@ __device__ __forceinline__ void pack_body(int bx, int nslots, const int *__restr
                        const double *__restrict__ iy, const double *__restrict__ iz,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
                        AtomRec *__restrict__ rec, float *__restrict__ recf,
-                       long long *__restrict__ fslot) {
+                       long long *__restrict__ fslot, float4 *__restrict__ bb) {
     const int s = bx * blockDim.x + threadIdx.x;
-    if (s >= nslots || s >= ncl_dev[0] * CL) return;
-    // the pair kernel adds into the slot-ordered accumulators: start them at zero
-    fslot[s] = 0;
-    fslot[nslots + s] = 0;
-    fslot[2 * nslots + s] = 0;
-    const int o = slot_orig[s];
+    // no early return: the 8 slots of a cluster (8 consecutive lanes) reduce the
+    // cluster's bounding box with shuffles below
+    const bool live = s < nslots && s < ncl_dev[0] * CL;
+    const int o = live ? slot_orig[s] : -1;
     AtomRec r;
+    if (live) {
+        // the pair kernel adds into the slot-ordered accumulators: start them at zero
+        fslot[s] = 0;
+        fslot[nslots + s] = 0;
+        fslot[2 * nslots + s] = 0;
+    }
     if (o >= 0) {
         double dx = x[o] - rx[o], dy = y[o] - ry[o], dz = z[o] - rz[o];
         dx -= L * rint(dx / L);
@@ -289,12 +293,38 @@ __device__ __forceinline__ void pack_body(int bx, int nslots, const int *__restr
         r.q = 0.0f;
         r.type = 0;
     }
-    rec[s] = r;
-    // FP32 copy for the prune, per cluster x[8], y[8], z[8]
-    float *rc = recf + (size_t)(s / CL) * (3 * CL) + (s % CL);
-    rc[0] = (float)r.x;
-    rc[CL] = (float)r.y;
-    rc[2 * CL] = (float)r.z;
+    if (live) {
+        rec[s] = r;
+        // FP32 copy for the prune, per cluster x[8], y[8], z[8]
+        float *rc = recf + (size_t)(s / CL) * (3 * CL) + (s % CL);
+        rc[0] = (float)r.x;
+        rc[CL] = (float)r.y;
+        rc[2 * CL] = (float)r.z;
+    }
+    // Cluster bounding box of the real atoms (FP64 bounds rounded outward to
+    // float), for the cluster-pair search and the prune; w of the low corner
+    // carries the cluster's real-atom bits (padding slots clear).  min and max
+    // are exact, so the shuffle order does not matter.
+    double lx = o >= 0 ? r.x : 1e300, ly = o >= 0 ? r.y : 1e300, lz = o >= 0 ? r.z : 1e300;
+    double hx = o >= 0 ? r.x : -1e300, hy = o >= 0 ? r.y : -1e300, hz = o >= 0 ? r.z : -1e300;
+#pragma unroll
+    for (int off = 1; off < CL; off <<= 1) {
+        lx = fmin(lx, __shfl_xor_sync(FULL, lx, off));
+        ly = fmin(ly, __shfl_xor_sync(FULL, ly, off));
+        lz = fmin(lz, __shfl_xor_sync(FULL, lz, off));
+        hx = fmax(hx, __shfl_xor_sync(FULL, hx, off));
+        hy = fmax(hy, __shfl_xor_sync(FULL, hy, off));
+        hz = fmax(hz, __shfl_xor_sync(FULL, hz, off));
+    }
+    const unsigned realw = __ballot_sync(FULL, o >= 0);
+    if (live && (s & (CL - 1)) == 0) {
+        const int c = s / CL;
+        const int real = (int)((realw >> (threadIdx.x & 31)) & 0xffu);
+        bb[2 * c] = make_float4(__double2float_rd(lx), __double2float_rd(ly),
+                                __double2float_rd(lz), __int_as_float(real));
+        bb[2 * c + 1] = make_float4(__double2float_ru(hx), __double2float_ru(hy),
+                                    __double2float_ru(hz), 0.0f);
+    }
 }
 __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
                        const int *__restrict__ slot_orig, const double *__restrict__ x,
@@ -304,45 +334,10 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
                        const double *__restrict__ iy, const double *__restrict__ iz,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
                        AtomRec *__restrict__ rec, float *__restrict__ recf,
-                       long long *__restrict__ fslot) {
+                       long long *__restrict__ fslot, float4 *__restrict__ bb) {
     SOFIA_PDL_ENTRY();
-    pack_body(blockIdx.x, nslots, ncl_dev, slot_orig, x, y, z, rx, ry, rz, ix, iy, iz, q, type, L, rec, recf, fslot);
-}
-
-// Cluster bounding boxes of the current records (FP64 bounds rounded outward
-// to float), for the cluster-pair search and the prune.
-__device__ __forceinline__ void bbox_body(int bx, const int *__restrict__ cond, int cmask, int maxcl,
-                       const int *__restrict__ ncl_dev,
-                       const AtomRec *__restrict__ rec, const int *__restrict__ slot_orig,
-                       float4 *__restrict__ bb) {
-    SOFIA_COND_RETURN;
-    const int c = bx * blockDim.x + threadIdx.x;
-    if (c >= maxcl || c >= ncl_dev[0]) return;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    int real = 0;
-    for (int k = 0; k < CL; ++k) {
-        if (slot_orig[c * CL + k] < 0) continue;
-        real |= 1 << k;
-        const AtomRec r = rec[c * CL + k];
-        lo[0] = fmin(lo[0], r.x);
-        lo[1] = fmin(lo[1], r.y);
-        lo[2] = fmin(lo[2], r.z);
-        hi[0] = fmax(hi[0], r.x);
-        hi[1] = fmax(hi[1], r.y);
-        hi[2] = fmax(hi[2], r.z);
-    }
-    // w of the low corner carries the cluster's real-atom bits (padding slots clear)
-    bb[2 * c] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
-                            __double2float_rd(lo[2]), __int_as_float(real));
-    bb[2 * c + 1] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
-                                __double2float_ru(hi[2]), 0.0f);
-}
-__global__ void k_bbox(const int *__restrict__ cond, int cmask, int maxcl,
-                       const int *__restrict__ ncl_dev,
-                       const AtomRec *__restrict__ rec, const int *__restrict__ slot_orig,
-                       float4 *__restrict__ bb) {
-    SOFIA_PDL_ENTRY();
-    bbox_body(blockIdx.x, cond, cmask, maxcl, ncl_dev, rec, slot_orig, bb);
+    pack_body(blockIdx.x, nslots, ncl_dev, slot_orig, x, y, z, rx, ry, rz, ix, iy, iz, q, type, L,
+              rec, recf, fslot, bb);
 }
 
 __device__ __forceinline__ float gap(float alo, float ahi, float blo, float bhi) {
@@ -1545,7 +1540,7 @@ static void sys_pack(Sys *s) {
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
         s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
-        s->rec.as<AtomRec>(), s->recf.as<float>(), s->fslot.as<long long>());
+        s->rec.as<AtomRec>(), s->recf.as<float>(), s->fslot.as<long long>(), s->bb.as<float4>());
     s->launches += 1;
 }
 
@@ -1587,10 +1582,7 @@ static int sys_build_search(Sys *s, const int *cond) {
     cudaStream_t st = ctx->stream;
     const int cm = 1;
     int *cl_col = s->slot_orig.as<int>() + (size_t)s->max_clusters * CL;
-    // the boxes serve the search (trigger bit 0) and the prune (bit 1)
-    sofia::launch_pdl(k_bbox, grid_for(s->max_clusters, 128), 128, 0, st,
-        cond, 3, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
-        s->slot_orig.as<int>(), s->bb.as<float4>());
+    // the cluster boxes come from the record pack that precedes the search
     SearchArgs a;
     a.cond = cond;
     a.cmask = cm;
@@ -1619,7 +1611,7 @@ static int sys_build_search(Sys *s, const int *cond) {
     a.status = s->status_local.as<int>();
     sofia::launch_pdl(k_search, grid_for((long)s->max_clusters * 32, 256), 256, 0, st, a);
     SOFIA_CUDA(ctx, cudaGetLastError());
-    s->launches += 2;
+    s->launches += 1;
     if (!cond) s->n_builds++;
     s->built = 1;
     return SOFIA_OK;
@@ -1700,19 +1692,12 @@ static PairConst make_pair_const(const Sys *s, const float *lj_dummy) {
 
 // Launches: displacement check, conditional rebuild, pack, pair kernel.
 // `force_build` rebuilds regardless of the trigger.
-// bb_current: the cluster boxes were computed from the current records (by
-// the build of this evaluation, or by its conditional box kernel).
-static void sys_prune(Sys *s, const int *cond, bool bb_current) {
+// The cluster boxes come from the record pack that precedes every prune.
+static void sys_prune(Sys *s, const int *cond) {
     cudaStream_t st = s->ctx->stream;
     const float rin = (float)(s->rc + s->margin);
     const float rin2 = rin * rin + 1e-3f;
     const float rfar = rin + 0.01f;
-    if (!bb_current) {
-        sofia::launch_pdl(k_bbox, grid_for(s->max_clusters, 128), 128, 0, st,
-            cond, 3, s->max_clusters, s->nclusters.as<int>(), s->rec.as<AtomRec>(),
-            s->slot_orig.as<int>(), s->bb.as<float4>());
-        s->launches += 1;
-    }
     sofia::launch_pdl(k_prune, grid_for((long)s->max_clusters * 32, 256), 256, 0, st,
         cond, 3, s->max_clusters, s->nclusters.as<int>(), s->recf.as<float>(),
         s->jlist.as<int>(), s->jmask.as<unsigned long long>(), s->jcount.as<int>(), s->jcap,
@@ -1778,7 +1763,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
         }
         break;
     }
-    if (prune) sys_prune(s, nullptr, build);
+    if (prune) sys_prune(s, nullptr);
     return sys_pair(s, precision, energy, virial);
 }
 
@@ -1871,7 +1856,7 @@ int sys_step_forces(Sys *s, int precision, bool energy, bool virial, bool force_
     }
     int rc = sys_build(s, flag);
     if (rc) return rc;
-    sys_prune(s, flag, true);
+    sys_prune(s, flag);
     s->launches += 1;
     // the force unpack counts the build/prune events and clears the trigger word
     return sys_pair(s, precision, energy, virial, flag, lg, ff_out);
@@ -2422,16 +2407,10 @@ __global__ void __launch_bounds__(256, SOFIA_BATCH_STREAM_MINB) k_pack_b(const B
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_LOOP(BK_S256)
     pack_body(lb, d.nslots, d.ncl, d.slot_orig, d.x, d.y, d.z, d.rx, d.ry, d.rz, d.ix, d.iy, d.iz,
-              d.q, d.type, d.L, d.rec, d.recf, reinterpret_cast<long long *>(d.fslot));
+              d.q, d.type, d.L, d.rec, d.recf, reinterpret_cast<long long *>(d.fslot), d.bb);
     SOFIA_BATCH_END
 }
 
-__global__ void k_bbox_b(const BatchDev *__restrict__ tab) {
-    SOFIA_PDL_ENTRY();
-    SOFIA_BATCH_ACTIVE_LOOP(BK_C128, BA_PRUNE)
-    bbox_body(lb, d.flag, 3, d.maxcl, d.ncl, d.rec, d.slot_orig, d.bb);
-    SOFIA_BATCH_END
-}
 
 // 4 resident blocks per SM (64 registers, a few spills) instead of the 80
 // registers the replica arguments would take (64 replicas: 383.5 -> 389 M
@@ -2685,7 +2664,6 @@ void batch_pair_path(BatchDev *tab, const Sys *s0, int precision, bool energy,
     launch_pdl(k_col_scatter_b, g256, 256, 0, st, tab);
     launch_pdl(k_col_sort_assign_b, nsm * 4, 256, 0, st, tab);
     launch_pdl(k_pack_b, g256, 256, 0, st, tab);
-    launch_pdl(k_bbox_b, g128, 128, 0, st, tab);
     // one block per warp-per-cluster virtual block of all members (blocks past the
     // replicas whose trigger fired return at once)
     const int gw = pair_blocks > 0 ? pair_blocks : 1;

@@ -156,7 +156,6 @@ enum BatchKind {
     BK_SCAN,      // 1: the column scans (1024 threads)
     BK_COLS,      // ncols: the column sort
     BK_S256,      // ceil(max_clusters * 8 / 256): per-slot kernels
-    BK_C128,      // ceil(max_clusters / 128): cluster boxes
     BK_W256,      // ceil(max_clusters * 32 / 256): warp-per-cluster kernels
     BK_B128,      // ceil(bonded terms / 128)
     BK_G128,      // ceil(SHAKE groups / 128)
