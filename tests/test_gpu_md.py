@@ -108,7 +108,11 @@ def test_graph_conditional_build_and_prune_equal_eager(ctx, small):
 
 def test_md_improper_term_matches_reference_entry(ctx, small):
     """The device MD's improper energy equals sofia_improper_harmonic on the same
-    (real*4-rounded) positions, and switching the term off removes it."""
+    positions, and switching the term off removes it.  The reference entry takes
+    real*4 positions, so the two evaluate at positions that differ by the float
+    rounding (hence rel 1e-4); the FP64 comparison of the improper forces and
+    energies with the oracle at the 1e-10 bar, on positions exact in real*4, is
+    in test_gpu_residency_parity.py."""
     s = small
     a = _system(ctx, s, dt=1.0, gamma=0.0, seed=1)
     e = a.md_run(1, energy_every=1)
