@@ -110,9 +110,9 @@ def test_md_improper_term_matches_reference_entry(ctx, small):
     """The device MD's improper energy equals sofia_improper_harmonic on the same
     positions, and switching the term off removes it.  The reference entry takes
     real*4 positions, so the two evaluate at positions that differ by the float
-    rounding (hence rel 1e-4); the FP64 comparison of the improper forces and
-    energies with the oracle at the 1e-10 bar, on positions exact in real*4, is
-    in test_gpu_residency_parity.py."""
+    rounding (hence rel 1e-4).  The comparison with the oracle on positions exact
+    in real*4 (energy at 1e-10, forces at the oracle's real*4 storage) is in
+    test_gpu_residency_parity.py."""
     s = small
     a = _system(ctx, s, dt=1.0, gamma=0.0, seed=1)
     e = a.md_run(1, energy_every=1)
