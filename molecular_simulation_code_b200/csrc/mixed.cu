@@ -44,6 +44,23 @@ constexpr int MAX_COL = 2048;
 #ifndef SOFIA_PAIR_MINB_EN
 #define SOFIA_PAIR_MINB_EN 4
 #endif
+// Threads per block of the single-system pair kernels (one warp per i-cluster):
+// the force-only kernel runs 8 blocks of 128 per SM (0.449 -> 0.447 ms at 275k,
+// MD +0.4 %); the energy kernels keep 4 blocks of 256, because every block
+// refills the 16 KB three-index LJ table (with 128 threads: 0.526 -> 0.556 ms).
+#ifndef SOFIA_PAIR_BLOCK
+#define SOFIA_PAIR_BLOCK 128
+#endif
+#ifndef SOFIA_PAIR_BLOCK_EN
+#define SOFIA_PAIR_BLOCK_EN 256
+#endif
+template <typename T, bool EN>
+constexpr int pair_block() { return (sizeof(T) == 4 && !EN) ? SOFIA_PAIR_BLOCK : SOFIA_PAIR_BLOCK_EN; }
+template <typename T, bool EN>
+constexpr int pair_minb() {
+    return sizeof(T) == 4 ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB * 256 / SOFIA_PAIR_BLOCK)
+                          : 2 * 256 / SOFIA_PAIR_BLOCK_EN;
+}
 #ifndef SOFIA_PAIR_HYBRID
 #define SOFIA_PAIR_HYBRID 1
 #endif
@@ -1117,7 +1134,7 @@ __device__ __forceinline__ void pair_body(
     }
 }
 template <typename T, bool EN, bool VIR, bool SAME, bool TRI = false>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4) ? (EN ? SOFIA_PAIR_MINB_EN : SOFIA_PAIR_MINB) : 2) k_pair(
+__global__ void __launch_bounds__((pair_block<T, EN>()), (pair_minb<T, EN>())) k_pair(
     int maxcl, const int *__restrict__ ncl_dev, const AtomRec *__restrict__ rec,
     const int *__restrict__ jlist, const unsigned long long *__restrict__ jmask,
     const int *__restrict__ jcount, int jcap, const float4 *__restrict__ ljtab, PairConst k,
@@ -1773,7 +1790,9 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
     sofia_nb_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     PairConst k = make_pair_const(s, nullptr);
-    const int blocks = grid_for((long)s->max_clusters * 32, 256);
+    // blocks of the force-only FP32 kernel and of the others (energies, FP64)
+    const int blocks = grid_for((long)s->max_clusters * 32, SOFIA_PAIR_BLOCK);
+    const int blocks_en = grid_for((long)s->max_clusters * 32, SOFIA_PAIR_BLOCK_EN);
     const size_t smem = pair_smem(s->ntypes, false, energy || virial);
     const bool tri = (energy || virial) && pair_tri(s->ntypes);
     const size_t smem3 = pair_smem(s->ntypes, tri, energy || virial);
@@ -1787,25 +1806,25 @@ int sys_pair(Sys *s, int precision, bool energy, bool virial, int *count_flag,
     // sofia_system_create requires rcut == cut_coul: one cut-off gates both terms
     if (precision == SOFIA_PREC_FP64) {
         if (virial)
-            sofia::launch_pdl(k_pair<double, true, true, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<double, true, true, true>, blocks_en, SOFIA_PAIR_BLOCK_EN, smem, st, SOFIA_PAIR_ARGS);
         else if (energy)
-            sofia::launch_pdl(k_pair<double, true, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<double, true, false, true>, blocks_en, SOFIA_PAIR_BLOCK_EN, smem, st, SOFIA_PAIR_ARGS);
         else
-            sofia::launch_pdl(k_pair<double, false, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<double, false, false, true>, blocks_en, SOFIA_PAIR_BLOCK_EN, smem, st, SOFIA_PAIR_ARGS);
     } else if (tri) {
         if (virial)
-            sofia::launch_pdl(k_pair<float, true, true, true, true>, blocks, 256, smem3, st,
+            sofia::launch_pdl(k_pair<float, true, true, true, true>, blocks_en, SOFIA_PAIR_BLOCK_EN, smem3, st,
                               SOFIA_PAIR_ARGS);
         else
-            sofia::launch_pdl(k_pair<float, true, false, true, true>, blocks, 256, smem3, st,
+            sofia::launch_pdl(k_pair<float, true, false, true, true>, blocks_en, SOFIA_PAIR_BLOCK_EN, smem3, st,
                               SOFIA_PAIR_ARGS);
     } else {
         if (virial)
-            sofia::launch_pdl(k_pair<float, true, true, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<float, true, true, true>, blocks_en, SOFIA_PAIR_BLOCK_EN, smem, st, SOFIA_PAIR_ARGS);
         else if (energy)
-            sofia::launch_pdl(k_pair<float, true, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<float, true, false, true>, blocks_en, SOFIA_PAIR_BLOCK_EN, smem, st, SOFIA_PAIR_ARGS);
         else
-            sofia::launch_pdl(k_pair<float, false, false, true>, blocks, 256, smem, st, SOFIA_PAIR_ARGS);
+            sofia::launch_pdl(k_pair<float, false, false, true>, blocks, SOFIA_PAIR_BLOCK, smem, st, SOFIA_PAIR_ARGS);
     }
 #undef SOFIA_PAIR_ARGS
     if (s->timing) {
