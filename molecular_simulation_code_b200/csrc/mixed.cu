@@ -28,15 +28,18 @@ namespace sofia {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int MAX_COL = 2048;
+constexpr int MAX_COL = 2048;  // atoms per xy column handled by the in-column sort
 
 // Build and prune kernels take an optional device flag: when `cond` is given
 // they return at once unless (cond[0] & cmask) != 0, so a whole step can be
 // launched (or captured into a CUDA graph) without a host round trip.
 #define SOFIA_COND_RETURN \
-    if (cond && !(cond[0] & cmask)) return  // atoms per xy column handled by the in-column sort
+    if (cond && !(cond[0] & cmask)) return
+// List entries between the pair kernel's FP32 -> fixed-point flushes of the i
+// forces: one flush per 32-entry batch of a list row (at 275k atoms, 16 ->
+// 32: force-only MD +0.9 %, the energy kernel 0.531 -> 0.517 ms).
 #ifndef SOFIA_PAIR_FLUSH
-#define SOFIA_PAIR_FLUSH 16
+#define SOFIA_PAIR_FLUSH 32
 #endif
 #ifndef SOFIA_PAIR_MINB
 #define SOFIA_PAIR_MINB 4
