@@ -200,14 +200,16 @@ int sofia_improper_harmonic(sofia_nb_ctx *ctx, int np, const sofia_ainfo *positi
  *     SOFIA_ETOOBIG.  The per-atom energy partials live in a fixed array of
  *     (5*SOFIA_NOALLOC_MAX_ATOMS + 1040) doubles (about 2.6 MB) compiled into
  *     the library, which every GPU that loads the library holds until exit.
- *   - The first call on a device looks up that array's device address and
- *     caches it for the process; after a cudaDeviceReset of that device the
- *     cached address is stale, so do not call it across a device reset.
+ *   - The first call on a device does a one-time set-up: it looks up that
+ *     array's device address (cudaGetSymbolAddress, with that device current)
+ *     and caches it for the process.  Make that first call before any stream
+ *     capture.  After a cudaDeviceReset of that device the cached address is
+ *     stale, so do not call it across a device reset.
  *   - All calls share the one array: calls that overlap on the GPU (on
  *     different streams, threads or processes sharing the context) race and
  *     corrupt each other's energies; order them on one stream or serialise.
  *   - The call copies the energies to host memory and synchronises the stream
- *     before it returns, so it cannot be recorded into a CUDA graph.
+ *     before it returns.
  */
 #define SOFIA_NOALLOC_MAX_ATOMS 65536
 int sofia_force_nonbond_dsf_noalloc(void *stream, int np, const sofia_ainfo *position,

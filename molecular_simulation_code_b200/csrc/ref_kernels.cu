@@ -1345,11 +1345,10 @@ extern "C" int sofia_correct_1x(sofia_nb_ctx *ctx, int np, const sofia_ainfo *po
 // Allocation-free variant of sofia_force_nonbond_dsf.
 //
 // Some callers cannot allocate device memory at the time they need forces:
-// code running while a CUDA stream is being captured into a graph (cudaMalloc
-// is not capturable), hosts that hand the library a fixed device arena or run
-// under a memory budget enforced outside the library, and Fortran drivers that
-// keep every device array in their own module and never expect a library to
-// allocate behind their back.  For them this entry point takes only caller-owned
+// hosts that hand the library a fixed device arena or run under a memory budget
+// enforced outside the library, and Fortran drivers that keep every device
+// array in their own module and never expect a library to allocate behind
+// their back.  For them this entry point takes only caller-owned
 // device buffers and keeps its per-atom energy partials in a fixed array that
 // lives in the library image.
 //
