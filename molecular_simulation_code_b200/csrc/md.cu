@@ -35,7 +35,12 @@ __device__ __forceinline__ void fadd(long long *f, double v) {
     atomicAdd(reinterpret_cast<unsigned long long *>(f), (unsigned long long)fixd(v));
 }
 
-__device__ __forceinline__ double mimg(double d, double L) { return d - L * rint(d / L); }
+// Minimum image.  d * (1/L) instead of d / L: the compiler hoists 1/L, so a
+// bonded term or SHAKE group takes one FP64 division instead of one per
+// component.  The two quotients differ by an ulp at most, which can change
+// rint only where d is within rounding of half a box, far beyond any bonded
+// distance.
+__device__ __forceinline__ double mimg(double d, double L) { return d - L * rint(d * (1.0 / L)); }
 
 
 // nve_v: v += (dt/2) * kcal2amu * f / m

@@ -297,9 +297,13 @@ __device__ __forceinline__ void pack_body(int bx, int nslots, const int *__restr
     }
     if (o >= 0) {
         double dx = x[o] - rx[o], dy = y[o] - ry[o], dz = z[o] - rz[o];
-        dx -= L * rint(dx / L);
-        dy -= L * rint(dy / L);
-        dz -= L * rint(dz / L);
+        // minimum image with one division per thread: d * (1/L) differs from d / L
+        // by an ulp at most, which could change rint only at a half box, far
+        // beyond any displacement between two list builds
+        const double Li = 1.0 / L;
+        dx -= L * rint(dx * Li);
+        dy -= L * rint(dy * Li);
+        dz -= L * rint(dz * Li);
         r.x = rx[o] + ix[o] + dx;
         r.y = ry[o] + iy[o] + dy;
         r.z = rz[o] + iz[o] + dz;
@@ -1313,9 +1317,10 @@ __device__ __forceinline__ void prune_body(int bx,
                 // the j cluster's x[8], y[8], z[8]: three 16-byte loads per 4 atoms
                 // (one half at a time keeps the kernel within 64 registers)
                 const float4 *cj = reinterpret_cast<const float4 *>(recf + (size_t)jc * 3 * CL);
-                // r2 < rin2 exactly when the rounded r2 - rin2 is negative (a
-                // difference of two floats is zero only when they are equal), so
-                // its sign bit is the in-range bit, and one funnel shift appends it.
+                // The sign bit of dz^2 - rin2 + dy^2 + dx^2 (rin2 folded into the
+                // first FMA of the chain) is the in-range bit, and one funnel shift
+                // appends it.  Its rounding differs from that of r2 by a few ulp of
+                // r2, far inside the 1e-3 A^2 that rin2 carries above (rc + margin)^2.
                 // Appended for j atoms 7 down to 0 and, within one, i atoms 3 down
                 // to 0 (7 down to 4 in hi), bit (jj, ii) ends at 4 jj + ii; the
                 // final transpose moves it to 8 ii + jj.
@@ -1335,8 +1340,7 @@ __device__ __forceinline__ void prune_body(int bx,
                             // i atoms 2pp (component x) and 2pp + 1 (component y)
                             const float2 dx = add2(xi[pp], nx2), dy = add2(yi[pp], ny2),
                                          dz = add2(zi[pp], nz2);
-                            const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
-                            const float2 dd = add2(r2, nrin2);
+                            const float2 dd = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, nrin2)));
                             unsigned &acc = (pp >= 2) ? hi : lo;
                             acc = __funnelshift_l(__float_as_uint(dd.y), acc, 1);
                             acc = __funnelshift_l(__float_as_uint(dd.x), acc, 1);
