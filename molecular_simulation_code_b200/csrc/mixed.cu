@@ -282,8 +282,20 @@ __device__ __forceinline__ void pack_body(int bx, int nslots, const int *__restr
                        const double *__restrict__ iy, const double *__restrict__ iz,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
                        AtomRec *__restrict__ rec, float *__restrict__ recf,
-                       long long *__restrict__ fslot, float4 *__restrict__ bb) {
+                       long long *__restrict__ fslot, float4 *__restrict__ bb,
+                       const int *__restrict__ cond, double *__restrict__ sref) {
     const int s = bx * blockDim.x + threadIdx.x;
+    // The build-time data of a slot (position and wrap shift at the last build,
+    // charge, type) change only at a list build.  On a build (cond null, or its
+    // build bit set) they are gathered through slot_orig and kept in slot order
+    // in sref: [3][nslots] positions, [3][nslots] position + shift, then
+    // [nslots] charges and [nslots] types; on the other steps they are read back
+    // from there, which leaves the three current coordinates as the only
+    // scattered reads.  sref holds exactly the gathered values, so both ways give
+    // the same bits.
+    const bool fresh = !cond || (cond[0] & 1);
+    float *sq = reinterpret_cast<float *>(sref + 6 * (size_t)nslots);
+    int *stype = reinterpret_cast<int *>(sq + nslots);
     // no early return: the 8 slots of a cluster (8 consecutive lanes) reduce the
     // cluster's bounding box with shuffles below
     const bool live = s < nslots && s < ncl_dev[0] * CL;
@@ -296,7 +308,35 @@ __device__ __forceinline__ void pack_body(int bx, int nslots, const int *__restr
         fslot[2 * nslots + s] = 0;
     }
     if (o >= 0) {
-        double dx = x[o] - rx[o], dy = y[o] - ry[o], dz = z[o] - rz[o];
+        double bx0, by0, bz0, ux, uy, uz;
+        if (fresh) {
+            bx0 = rx[o];
+            by0 = ry[o];
+            bz0 = rz[o];
+            ux = bx0 + ix[o];
+            uy = by0 + iy[o];
+            uz = bz0 + iz[o];
+            r.q = q[o];
+            r.type = type[o] - 1;
+            sref[s] = bx0;
+            sref[(size_t)nslots + s] = by0;
+            sref[2 * (size_t)nslots + s] = bz0;
+            sref[3 * (size_t)nslots + s] = ux;
+            sref[4 * (size_t)nslots + s] = uy;
+            sref[5 * (size_t)nslots + s] = uz;
+            sq[s] = r.q;
+            stype[s] = r.type;
+        } else {
+            bx0 = sref[s];
+            by0 = sref[(size_t)nslots + s];
+            bz0 = sref[2 * (size_t)nslots + s];
+            ux = sref[3 * (size_t)nslots + s];
+            uy = sref[4 * (size_t)nslots + s];
+            uz = sref[5 * (size_t)nslots + s];
+            r.q = sq[s];
+            r.type = stype[s];
+        }
+        double dx = x[o] - bx0, dy = y[o] - by0, dz = z[o] - bz0;
         // minimum image with one division per thread: d * (1/L) differs from d / L
         // by an ulp at most, which could change rint only at a half box, far
         // beyond any displacement between two list builds
@@ -304,11 +344,9 @@ __device__ __forceinline__ void pack_body(int bx, int nslots, const int *__restr
         dx -= L * rint(dx * Li);
         dy -= L * rint(dy * Li);
         dz -= L * rint(dz * Li);
-        r.x = rx[o] + ix[o] + dx;
-        r.y = ry[o] + iy[o] + dy;
-        r.z = rz[o] + iz[o] + dz;
-        r.q = q[o];
-        r.type = type[o] - 1;
+        r.x = ux + dx;
+        r.y = uy + dy;
+        r.z = uz + dz;
     } else {
         // padding: far away and distinct; every pair with it is masked out
         r.x = 1.0e6 + 16.0 * s;
@@ -358,10 +396,11 @@ __global__ void k_pack(int nslots, const int *__restrict__ ncl_dev,
                        const double *__restrict__ iy, const double *__restrict__ iz,
                        const float *__restrict__ q, const int *__restrict__ type, double L,
                        AtomRec *__restrict__ rec, float *__restrict__ recf,
-                       long long *__restrict__ fslot, float4 *__restrict__ bb) {
+                       long long *__restrict__ fslot, float4 *__restrict__ bb,
+                       const int *__restrict__ cond, double *__restrict__ sref) {
     SOFIA_PDL_ENTRY();
     pack_body(blockIdx.x, nslots, ncl_dev, slot_orig, x, y, z, rx, ry, rz, ix, iy, iz, q, type, L,
-              rec, recf, fslot, bb);
+              rec, recf, fslot, bb, cond, sref);
 }
 
 __device__ __forceinline__ float gap(float alo, float ahi, float blo, float bhi) {
@@ -1491,6 +1530,7 @@ static int sys_alloc(Sys *s) {
     const size_t maxcl = (size_t)s->max_clusters;
     SOFIA_CUDA(ctx, s->slot_orig.ensure(sizeof(int) * maxcl * CL + sizeof(int) * maxcl));
     SOFIA_CUDA(ctx, s->rec.ensure(sizeof(AtomRec) * maxcl * CL));
+    SOFIA_CUDA(ctx, s->sref.ensure((6 * sizeof(double) + sizeof(float) + sizeof(int)) * maxcl * CL));
     SOFIA_CUDA(ctx, s->recf.ensure(sizeof(float) * 3 * maxcl * CL));
     SOFIA_CUDA(ctx, s->fslot.ensure(sizeof(long long) * 3 * maxcl * CL));
     SOFIA_CUDA(ctx, s->atom_slot.ensure(sizeof(int) * n));
@@ -1556,7 +1596,7 @@ static int sys_alloc_list(Sys *s) {
     return SOFIA_OK;
 }
 
-static void sys_pack(Sys *s) {
+static void sys_pack(Sys *s, const int *cond) {
     cudaStream_t st = s->ctx->stream;
     const int nslots = s->max_clusters * CL;
     sofia::launch_pdl(k_pack, grid_for(nslots, 256), 256, 0, st,
@@ -1564,7 +1604,8 @@ static void sys_pack(Sys *s) {
         s->x[1].as<double>(), s->x[2].as<double>(), s->xref[0].as<double>(),
         s->xref[1].as<double>(), s->xref[2].as<double>(), s->img[0].as<double>(),
         s->img[1].as<double>(), s->img[2].as<double>(), s->q.as<float>(), s->type.as<int>(), s->L,
-        s->rec.as<AtomRec>(), s->recf.as<float>(), s->fslot.as<long long>(), s->bb.as<float4>());
+        s->rec.as<AtomRec>(), s->recf.as<float>(), s->fslot.as<long long>(), s->bb.as<float4>(),
+        cond, s->sref.as<double>());
     s->launches += 1;
 }
 
@@ -1645,7 +1686,7 @@ static int sys_build_search(Sys *s, const int *cond) {
 // list was rebuilt.
 static int sys_build(Sys *s, const int *cond) {
     sys_build_bin(s, cond);
-    sys_pack(s);
+    sys_pack(s, cond);
     return sys_build_search(s, cond);
 }
 
@@ -1783,7 +1824,7 @@ int sys_eval(Sys *s, int precision, bool energy, bool virial, bool force_build) 
                 continue;
             }
         } else {
-            sys_pack(s);
+            sys_pack(s, nullptr);
         }
         break;
     }
@@ -2060,6 +2101,7 @@ extern "C" int sofia_system_destroy(sofia_system *ss) {
     s->imask.release();
     s->recf.release();
     s->fslot.release();
+    s->sref.release();
     s->atom_slot.release();
     s->dcount.release();
     s->icount.release();
@@ -2433,7 +2475,8 @@ __global__ void __launch_bounds__(256, SOFIA_BATCH_STREAM_MINB) k_pack_b(const B
     SOFIA_PDL_ENTRY();
     SOFIA_BATCH_LOOP(BK_S256)
     pack_body(lb, d.nslots, d.ncl, d.slot_orig, d.x, d.y, d.z, d.rx, d.ry, d.rz, d.ix, d.iy, d.iz,
-              d.q, d.type, d.L, d.rec, d.recf, reinterpret_cast<long long *>(d.fslot), d.bb);
+              d.q, d.type, d.L, d.rec, d.recf, reinterpret_cast<long long *>(d.fslot), d.bb,
+              d.flag, d.sref);
     SOFIA_BATCH_END
 }
 
@@ -2643,6 +2686,7 @@ void repdev_fill_pair(const Sys *s, RepDev *d) {
     d->atom_slot = s->atom_slot.as<int>();
     d->col_key = s->col_key.as<float>();
     d->rec = s->rec.as<AtomRec>();
+    d->sref = s->sref.as<double>();
     d->recf = s->recf.as<float>();
     d->bb = s->bb.as<float4>();
     d->jlist = s->jlist.as<int>();

@@ -86,6 +86,7 @@ struct Sys {
     DevBuf slot_orig, rec, bb, jlist, jmask, jcount, nclusters;
     DevBuf recf;                        // FP32 positions per cluster: x[8], y[8], z[8]
     DevBuf fslot;                       // pair forces in cluster-slot order, 64-bit fixed point [3][slots]
+    DevBuf sref;                        // build-time data in slot order (see pack_body)
     DevBuf atom_slot;                   // cluster slot of every atom (inverse of slot_orig)
     DevBuf status_local;
     DevBuf energy;                      // per-i-cluster energy partials (pot, ecoul, vir x,y,z)
@@ -193,6 +194,7 @@ struct RepDev {
         *atom_slot;
     float *col_key;
     AtomRec *rec;
+    double *sref;
     float *recf;
     float4 *bb;
     int *jlist, *jcount, *ilist, *icount;
