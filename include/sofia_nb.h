@@ -186,9 +186,11 @@ int sofia_improper_harmonic(sofia_nb_ctx *ctx, int np, const sofia_ainfo *positi
  * Allocation-free form of sofia_force_nonbond_dsf.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot allocate device
  * memory when they need forces: hosts that give the library a fixed device
- * arena or enforce a memory budget from outside, and drivers that keep every
- * device array themselves.  It needs no context and allocates nothing: no
- * cudaMalloc, no cudaFree, no allocating library routine.
+ * arena or enforce a memory budget from outside (an allocation inside the call
+ * would bypass the arena or break the budget), and drivers that keep every
+ * device array themselves and must know the library's footprint up front.  It
+ * needs no context and allocates nothing: no cudaMalloc, no cudaFree, no
+ * allocating library routine.
  *   - stream: the caller's cudaStream_t (NULL = the legacy default stream).
  *   - position, q, lj1..lj4, nlist, numneigh and ff must be device memory of
  *     the current device (or managed memory); host pointers and buffers on
